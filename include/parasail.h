@@ -1,0 +1,2410 @@
+/**
+ * @file parasail.h
+ *
+ * parasail-b200: drop-in C API for the score-only and statistics paths of
+ * parasail (jeffdaily/parasail v2.6.2), computed on an NVIDIA B200 (sm_100a).
+ *
+ * Types, flag bits and signatures match the reference header (parasail.h:
+ * flags 44-74, result/matrix/profile types 88-180, core API 182-296,
+ * accessors 476-521) so that code written against parasail compiles and links
+ * unchanged for the declared entry points. GENERATED by gen_parasail_h.py.
+ */
+#ifndef _PARASAIL_H_
+#define _PARASAIL_H_
+
+#include <stdio.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PARASAIL_VERSION_MAJOR 2
+#define PARASAIL_VERSION_MINOR 6
+#define PARASAIL_VERSION_PATCH 2
+#define PARASAIL_MAKE_VERSION(major, minor, patch) \
+    ((major) * 10000 + (minor) * 100 + (patch))
+#define PARASAIL_VERSION \
+    PARASAIL_MAKE_VERSION(PARASAIL_VERSION_MAJOR, \
+                          PARASAIL_VERSION_MINOR, \
+                          PARASAIL_VERSION_PATCH)
+
+/* result flag bits (reference parasail.h:44-74) */
+#define PARASAIL_FLAG_NW          (1 << 0)
+#define PARASAIL_FLAG_SG          (1 << 1)
+#define PARASAIL_FLAG_SW          (1 << 2)
+#define PARASAIL_FLAG_SG_S1_BEG   (1 << 3)
+#define PARASAIL_FLAG_SG_S1_END   (1 << 4)
+#define PARASAIL_FLAG_SATURATED   (1 << 6)
+#define PARASAIL_FLAG_BANDED      (1 << 7)
+#define PARASAIL_FLAG_NOVEC       (1 << 8)
+#define PARASAIL_FLAG_NOVEC_SCAN  (1 << 9)
+#define PARASAIL_FLAG_SCAN        (1 <<10)
+#define PARASAIL_FLAG_STRIPED     (1 <<11)
+#define PARASAIL_FLAG_DIAG        (1 <<12)
+#define PARASAIL_FLAG_BLOCKED     (1 <<13)
+#define PARASAIL_FLAG_SG_S2_BEG   (1 <<14)
+#define PARASAIL_FLAG_SG_S2_END   (1 <<15)
+#define PARASAIL_FLAG_STATS       (1 <<16)
+#define PARASAIL_FLAG_TABLE       (1 <<17)
+#define PARASAIL_FLAG_ROWCOL      (1 <<18)
+#define PARASAIL_FLAG_TRACE       (1 <<19)
+#define PARASAIL_FLAG_BITS_8      (1 <<20)
+#define PARASAIL_FLAG_BITS_16     (1 <<21)
+#define PARASAIL_FLAG_BITS_32     (1 <<22)
+#define PARASAIL_FLAG_BITS_64     (1 <<23)
+#define PARASAIL_FLAG_LANES_1     (1 <<24)
+#define PARASAIL_FLAG_LANES_2     (1 <<25)
+#define PARASAIL_FLAG_LANES_4     (1 <<26)
+#define PARASAIL_FLAG_LANES_8     (1 <<27)
+#define PARASAIL_FLAG_LANES_16    (1 <<28)
+#define PARASAIL_FLAG_LANES_32    (1 <<29)
+#define PARASAIL_FLAG_LANES_64    (1 <<30)
+#define PARASAIL_FLAG_INVALID  0x80000020
+
+#if !defined(restrict) && (defined(__cplusplus) || __STDC_VERSION__ < 199901L)
+#define restrict
+#define PARASAIL_RESTRICT_REMOVED
+#endif
+
+typedef struct parasail_result_extra_stats {
+    int matches;    /* number of exactly matching characters in the alignment */
+    int similar;    /* number of similar characters (positive substitutions) */
+    int length;     /* length of the alignment */
+    union {
+        void *extra;
+    };
+} parasail_result_extra_stats_t;
+
+typedef struct parasail_result {
+    int score;      /* alignment score */
+    int end_query;  /* end position of query sequence */
+    int end_ref;    /* end position of reference sequence */
+    int flag;       /* bit field of PARASAIL_FLAG_* */
+    union {
+        void *extra;
+        parasail_result_extra_stats_t *stats;
+    };
+} parasail_result_t;
+
+#define PARASAIL_MATRIX_TYPE_SQUARE 0
+#define PARASAIL_MATRIX_TYPE_PSSM 1
+
+typedef struct parasail_matrix {
+    const char * name;
+    const int * matrix;
+    const int * mapper;
+    int size;
+    int max;
+    int min;
+    int * user_matrix;
+    int type;
+    int length;
+    const char * alphabet;
+    const char * query;
+} parasail_matrix_t;
+
+typedef struct parasail_profile_data {
+    void * score;
+    void * matches;
+    void * similar;
+} parasail_profile_data_t;
+
+/* Same layout as the reference. In parasail-b200 the profileN.score members
+ * hold an opaque handle to the device-resident query profile; `free` releases
+ * it. s1 is borrowed from the caller, as in the reference (src/memory.c:673). */
+typedef struct parasail_profile {
+    const char *s1;
+    int s1Len;
+    const parasail_matrix_t *matrix;
+    struct parasail_profile_data profile8;
+    struct parasail_profile_data profile16;
+    struct parasail_profile_data profile32;
+    struct parasail_profile_data profile64;
+    void (*free)(void * profile);
+    int stop;
+} parasail_profile_t;
+
+extern void parasail_profile_free(parasail_profile_t *profile);
+
+typedef parasail_result_t* parasail_function_t(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t *matrix);
+
+typedef struct parasail_function_info {
+    parasail_function_t * pointer;
+    const char * name;
+    const char * alg;
+    const char * type;
+    const char * isa;
+    const char * bits;
+    const char * width;
+    int lanes;
+    char is_table;
+    char is_rowcol;
+    char is_trace;
+    char is_stats;
+    char is_ref;
+} parasail_function_info_t;
+
+typedef parasail_result_t* parasail_pfunction_t(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+
+typedef parasail_profile_t* parasail_pcreator_t(
+        const char * const restrict s1, const int s1Len,
+        const parasail_matrix_t *matrix);
+
+typedef struct parasail_pfunction_info {
+    parasail_pfunction_t * pointer;
+    parasail_pcreator_t * creator;
+    const char * name;
+    const char * alg;
+    const char * type;
+    const char * isa;
+    const char * bits;
+    const char * width;
+    int lanes;
+    char is_table;
+    char is_rowcol;
+    char is_trace;
+    char is_stats;
+    char is_ref;
+} parasail_pfunction_info_t;
+
+/* reference parasail.h:224 */
+extern void parasail_version(int *major, int *minor, int *patch);
+/* reference parasail.h:227; src/memory.c:277-327 */
+extern void parasail_result_free(parasail_result_t *result);
+/* reference parasail.h:230-245; src/function_lookup.c:16-65 */
+extern parasail_function_t * parasail_lookup_function(const char *funcname);
+extern parasail_pfunction_t * parasail_lookup_pfunction(const char *funcname);
+extern parasail_pcreator_t * parasail_lookup_pcreator(const char *funcname);
+extern const parasail_function_info_t * parasail_lookup_function_info(const char *funcname);
+extern const parasail_pfunction_info_t * parasail_lookup_pfunction_info(const char *funcname);
+/* reference parasail.h:248; src/time.c:19-70 */
+extern double parasail_time(void);
+
+/* matrices: reference parasail.h:251-286; src/memory.c:336-660, src/matrix_lookup.c */
+extern const parasail_matrix_t* parasail_matrix_lookup(const char *matrixname);
+extern parasail_matrix_t* parasail_matrix_create(
+        const char *alphabet, const int match, const int mismatch);
+extern parasail_matrix_t* parasail_matrix_create_case_sensitive(
+        const char *alphabet, const int match, const int mismatch);
+extern parasail_matrix_t* parasail_matrix_pssm_create(
+        const char *alphabet, const int *values, const int length);
+extern parasail_matrix_t* parasail_matrix_pssm_create_case_sensitive(
+        const char *alphabet, const int *values, const int length);
+extern void parasail_matrix_free(parasail_matrix_t *matrix);
+extern parasail_matrix_t* parasail_matrix_copy(const parasail_matrix_t *original);
+extern parasail_matrix_t* parasail_matrix_convert_square_to_pssm(
+        const parasail_matrix_t *original, const char *seq, int len);
+extern void parasail_matrix_set_value(parasail_matrix_t *matrix, int row, int col, int value);
+
+/* banded global alignment: reference parasail.h:293-296; src/nw_banded.c:29-189 */
+extern parasail_result_t* parasail_nw_banded(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap, const int k,
+        const parasail_matrix_t* matrix);
+
+/* result accessors: reference parasail.h:476-521; src/memory.c:777-1028 */
+extern int parasail_result_is_nw(const parasail_result_t * const restrict result);
+extern int parasail_result_is_sg(const parasail_result_t * const restrict result);
+extern int parasail_result_is_sw(const parasail_result_t * const restrict result);
+extern int parasail_result_is_saturated(const parasail_result_t * const restrict result);
+extern int parasail_result_is_banded(const parasail_result_t * const restrict result);
+extern int parasail_result_is_scan(const parasail_result_t * const restrict result);
+extern int parasail_result_is_striped(const parasail_result_t * const restrict result);
+extern int parasail_result_is_diag(const parasail_result_t * const restrict result);
+extern int parasail_result_is_blocked(const parasail_result_t * const restrict result);
+extern int parasail_result_is_stats(const parasail_result_t * const restrict result);
+extern int parasail_result_is_stats_table(const parasail_result_t * const restrict result);
+extern int parasail_result_is_stats_rowcol(const parasail_result_t * const restrict result);
+extern int parasail_result_is_table(const parasail_result_t * const restrict result);
+extern int parasail_result_is_rowcol(const parasail_result_t * const restrict result);
+extern int parasail_result_is_trace(const parasail_result_t * const restrict result);
+extern int parasail_result_get_score(const parasail_result_t * const restrict result);
+extern int parasail_result_get_end_query(const parasail_result_t * const restrict result);
+extern int parasail_result_get_end_ref(const parasail_result_t * const restrict result);
+extern int parasail_result_get_matches(const parasail_result_t * const restrict result);
+extern int parasail_result_get_similar(const parasail_result_t * const restrict result);
+extern int parasail_result_get_length(const parasail_result_t * const restrict result);
+
+/* query profiles: reference parasail.h:85201-85317; src/memory_avx2.c:28-528,
+ * src/dispatch_profile.c. The 8/16/32 creators build one device profile; the
+ * _sat creators build the bundle used by the 8->16->32 chains. */
+extern parasail_profile_t* parasail_profile_create_8(
+        const char * const restrict s1, const int s1Len,
+        const parasail_matrix_t* matrix);
+extern parasail_profile_t* parasail_profile_create_16(
+        const char * const restrict s1, const int s1Len,
+        const parasail_matrix_t* matrix);
+extern parasail_profile_t* parasail_profile_create_32(
+        const char * const restrict s1, const int s1Len,
+        const parasail_matrix_t* matrix);
+extern parasail_profile_t* parasail_profile_create_sat(
+        const char * const restrict s1, const int s1Len,
+        const parasail_matrix_t* matrix);
+extern parasail_profile_t* parasail_profile_create_stats_8(
+        const char * const restrict s1, const int s1Len,
+        const parasail_matrix_t* matrix);
+extern parasail_profile_t* parasail_profile_create_stats_16(
+        const char * const restrict s1, const int s1Len,
+        const parasail_matrix_t* matrix);
+extern parasail_profile_t* parasail_profile_create_stats_32(
+        const char * const restrict s1, const int s1Len,
+        const parasail_matrix_t* matrix);
+extern parasail_profile_t* parasail_profile_create_stats_sat(
+        const char * const restrict s1, const int s1Len,
+        const parasail_matrix_t* matrix);
+
+/* alignment entry points. Serial forms: reference src/{sw,nw,sg}{,_stats}.c;
+ * striped/scan forms: reference src/{sw,nw,sg}{,_stats}_{striped,scan}_*.c and
+ * the _sat chains of src/satcheck.c. All run on the GPU. */
+extern parasail_result_t* parasail_sw(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_stats(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_stats_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_stats_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_stats_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_stats_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_stats_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_stats_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_stats_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_stats_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_stats_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_stats_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_stats_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_stats_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_stats_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_stats_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_stats_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_stats_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_stats_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_stats(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_stats_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_stats_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_stats_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_stats_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_stats_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_stats_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_stats_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_stats_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_stats_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_stats_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_stats_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_stats_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_stats_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_stats_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_stats_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_stats_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_stats_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_stats(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_stats_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_stats_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_stats_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_stats_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_stats_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_stats_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_stats_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_stats_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_stats_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_stats_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_stats_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_stats_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_stats_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_stats_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_stats_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_stats_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_stats_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_stats(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_stats_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_stats_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_stats_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_stats_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_stats_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_stats_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_stats_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_stats_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_stats_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_stats_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_stats_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_stats_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_stats_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_stats_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_stats_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_stats_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_stats_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_stats(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_stats_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_stats_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_stats_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_stats_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_stats_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_stats_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_stats_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_stats_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_stats_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_stats_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_stats_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_stats_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_stats_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_stats_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_stats_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_stats_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_stats_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_stats(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_stats_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_stats_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_stats_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_stats_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_stats_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_stats_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_stats_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_stats_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_stats_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_stats_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_stats_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_stats_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_stats_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_stats_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_stats_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_stats_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_stats_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_stats(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_stats_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_stats_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_stats_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_stats_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_stats_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_stats_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_stats_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_stats_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_stats_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_stats_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_stats_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_stats_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_stats_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_stats_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_stats_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_stats_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_stats_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_stats(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_stats_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_stats_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_stats_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_stats_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_stats_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_stats_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_stats_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_stats_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_stats_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_stats_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_stats_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_stats_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_stats_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_stats_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_stats_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_stats_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_stats_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_stats(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_stats_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_stats_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_stats_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_stats_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_stats_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_stats_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_stats_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_stats_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_stats_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_stats_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_stats_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_stats_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_stats_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_stats_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_stats_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_stats_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_stats_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_stats(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_stats_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_stats_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_stats_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_stats_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_stats_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_stats_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_stats_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_stats_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_stats_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_stats_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_stats_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_stats_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_stats_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_stats_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_stats_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_stats_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_stats_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_stats(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_stats_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_stats_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_stats_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_stats_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_stats_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_stats_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_stats_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_stats_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_stats_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_stats_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_stats_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_stats_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_stats_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_stats_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_stats_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_stats_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_stats_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_stats(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_stats_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_stats_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_stats_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_stats_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_stats_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_stats_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_stats_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_stats_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_stats_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_stats_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_stats_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_stats_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_stats_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_stats_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_stats_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_stats_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_stats_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_stats(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_stats_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_stats_striped_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_stats_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_stats_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_stats_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_stats_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_stats_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_stats_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_stats_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_stats_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_stats_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_stats_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_stats_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_stats_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_stats_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_stats_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_stats_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+
+#ifdef PARASAIL_RESTRICT_REMOVED
+#undef restrict
+#undef PARASAIL_RESTRICT_REMOVED
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* _PARASAIL_H_ */

@@ -1,0 +1,325 @@
+"""CPU oracle for parasail-b200 -- TEST INFRASTRUCTURE ONLY.
+
+Two checkers, both CPU-only:
+
+* `liboracle.so` (built from oracle/oracle.c): the project's plain-C
+  restatement of the reference's serial dynamic programs (jeffdaily/parasail
+  v2.6.2 src/sw.c, src/nw.c, src/sg.c, their _stats twins and src/nw_banded.c)
+  plus the padded-layout statistics the vector kernels' saturation checks read.
+* `libparasail_ref.so` (built by oracle/Makefile from the reference's own
+  sources, when they were available at build time): the reference itself --
+  its serial functions and its AVX2 striped/scan kernels -- used to pin the
+  restatement and as the flag-exact checker.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline/reference
+legs import this package, and only as the checker / CPU baseline. The product
+(parasail_b200/libparasail_b200.so) never loads it.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+ORACLE_SO = os.path.join(REF_DIR, "liboracle.so")
+REF_SO = os.path.join(REF_DIR, "libparasail_ref.so")
+
+SW, NW, SG = 0, 1, 2
+S1_BEG, S1_END, S2_BEG, S2_END = 1, 2, 4, 8
+SG_CASES = {  # reference src/sg_helper.h:53-63
+    "sg": S1_BEG | S1_END | S2_BEG | S2_END, "sg_qb": S1_BEG, "sg_qe": S1_END,
+    "sg_qx": S1_BEG | S1_END, "sg_db": S2_BEG, "sg_de": S2_END, "sg_dx": S2_BEG | S2_END,
+    "sg_qb_de": S1_BEG | S2_END, "sg_qe_db": S1_END | S2_BEG, "sg_qb_db": S1_BEG | S2_BEG,
+    "sg_qe_de": S1_END | S2_END,
+}
+
+
+def alg_of(name):
+    """('sw'|'nw'|'sg_qx'|...) -> (alg, sgflags)."""
+    if name == "sw":
+        return SW, 0
+    if name == "nw":
+        return NW, 0
+    return SG, SG_CASES[name]
+
+
+class OMatrix(ctypes.Structure):
+    _fields_ = [("size", ctypes.c_int), ("matrix", ctypes.POINTER(ctypes.c_int)),
+                ("is_pssm", ctypes.c_int), ("max", ctypes.c_int), ("min", ctypes.c_int)]
+
+
+class OResult(ctypes.Structure):
+    _fields_ = [("score", ctypes.c_int), ("end_query", ctypes.c_int), ("end_ref", ctypes.c_int),
+                ("matches", ctypes.c_int), ("similar", ctypes.c_int), ("length", ctypes.c_int)]
+
+
+class OPadStats(ctypes.Structure):
+    _fields_ = [("max_h", ctypes.c_int64), ("min_h_real", ctypes.c_int64),
+                ("min_h_pad", ctypes.c_int64), ("min_f", ctypes.c_int64),
+                ("max_stat", ctypes.c_int64), ("max_stat_real", ctypes.c_int64)]
+
+
+# parasail.h-compatible structs for the reference library
+class PMatrix(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char_p), ("matrix", ctypes.POINTER(ctypes.c_int)),
+                ("mapper", ctypes.POINTER(ctypes.c_int)), ("size", ctypes.c_int),
+                ("max", ctypes.c_int), ("min", ctypes.c_int),
+                ("user_matrix", ctypes.POINTER(ctypes.c_int)), ("type", ctypes.c_int),
+                ("length", ctypes.c_int), ("alphabet", ctypes.c_char_p),
+                ("query", ctypes.c_char_p)]
+
+
+class PResult(ctypes.Structure):
+    _fields_ = [("score", ctypes.c_int), ("end_query", ctypes.c_int),
+                ("end_ref", ctypes.c_int), ("flag", ctypes.c_int),
+                ("extra", ctypes.c_void_p)]
+
+
+class PStats(ctypes.Structure):
+    _fields_ = [("matches", ctypes.c_int), ("similar", ctypes.c_int),
+                ("length", ctypes.c_int), ("extra", ctypes.c_void_p)]
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            raise RuntimeError("oracle not built: make -C oracle oracle")
+        _lib = ctypes.CDLL(ORACLE_SO)
+        _lib.oracle_align.argtypes = [ctypes.c_int] * 3 + [
+            ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+            ctypes.c_int, ctypes.c_int, ctypes.POINTER(OMatrix), ctypes.POINTER(OResult)]
+        _lib.oracle_padstats.argtypes = [ctypes.c_int] * 3 + [
+            ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
+            ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+            ctypes.POINTER(OMatrix), ctypes.POINTER(OPadStats)]
+        _lib.oracle_nw_banded.argtypes = [
+            ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+            ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(OMatrix), ctypes.POINTER(OResult)]
+        _lib.oracle_align_batch.argtypes = [ctypes.c_int] * 4 + [
+            ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int),
+            ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int),
+            ctypes.c_int, ctypes.c_int, ctypes.POINTER(OMatrix), ctypes.POINTER(OResult), ctypes.c_int]
+        _lib.oracle_nw_diag_range.argtypes = [
+            ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+            ctypes.c_int, ctypes.c_int, ctypes.POINTER(OMatrix), ctypes.POINTER(ctypes.c_int),
+            ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    return _lib
+
+
+def ref():
+    """The reference library compiled from source, or None when absent."""
+    global _ref
+    if _ref is None and os.path.exists(REF_SO):
+        _ref = ctypes.CDLL(REF_SO)
+        _ref.parasail_matrix_lookup.restype = ctypes.POINTER(PMatrix)
+        _ref.parasail_matrix_lookup.argtypes = [ctypes.c_char_p]
+        _ref.parasail_matrix_create.restype = ctypes.POINTER(PMatrix)
+        _ref.parasail_matrix_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+        _ref.parasail_result_free.argtypes = [ctypes.POINTER(PResult)]
+        _ref.parasail_profile_free.argtypes = [ctypes.c_void_p]
+    return _ref
+
+
+class Matrix:
+    """Plain-Python copy of a substitution matrix (values, mapper, max, min)."""
+
+    def __init__(self, values, mapper, alphabet, mx, mn, name=""):
+        self.values = np.ascontiguousarray(values, dtype=np.int32)
+        self.size = self.values.shape[0]
+        self.mapper = np.asarray(mapper, dtype=np.int32)
+        self.alphabet = alphabet
+        self.max, self.min, self.name = mx, mn, name
+        self._om = OMatrix(self.size, self.values.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), 0,
+                           mx, mn)
+
+    @staticmethod
+    def from_struct(pm, name=""):
+        m = pm.contents
+        n = m.size
+        vals = np.ctypeslib.as_array(m.matrix, shape=(n * n,)).reshape(n, n).copy()
+        mapper = np.ctypeslib.as_array(m.mapper, shape=(256,)).copy()
+        return Matrix(vals, mapper, m.alphabet.decode(), m.max, m.min, name)
+
+    @staticmethod
+    def simple(alphabet, match, mismatch):
+        """parasail_matrix_create semantics (reference src/memory.c:336-407)."""
+        n = len(alphabet) + 1
+        v = np.zeros((n, n), dtype=np.int32)
+        v[: n - 1, : n - 1] = mismatch
+        np.fill_diagonal(v[: n - 1, : n - 1], match)
+        mapper = np.full(256, n - 1, dtype=np.int32)
+        for i, c in enumerate(alphabet):
+            mapper[ord(c.upper())] = i
+            mapper[ord(c.lower())] = i
+        return Matrix(v, mapper, alphabet + "*", max(match, mismatch), min(match, mismatch))
+
+    def codes(self, s):
+        b = np.frombuffer(s.encode() if isinstance(s, str) else s, dtype=np.uint8)
+        return np.ascontiguousarray(self.mapper[b], dtype=np.int32)
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def align(alg, sgflags, stats, q, t, open_, gap, m):
+    """Serial restatement. q, t: strings. Returns a dict."""
+    qc, tc = m.codes(q), m.codes(t)
+    r = OResult()
+    rc = lib().oracle_align(alg, sgflags, int(stats), _ip(qc), len(qc), _ip(tc), len(tc),
+                            open_, gap, ctypes.byref(m._om), ctypes.byref(r))
+    if rc != 0:
+        raise ValueError("oracle_align rejected its input")
+    out = {"score": r.score, "end_query": r.end_query, "end_ref": r.end_ref}
+    if stats:
+        out.update(matches=r.matches, similar=r.similar, length=r.length)
+    return out
+
+
+def padstats(alg, sgflags, stats, q, t, open_, gap, m, padlen):
+    qc, tc = m.codes(q), m.codes(t)
+    ps = OPadStats()
+    lib().oracle_padstats(alg, sgflags, int(stats), _ip(qc), len(qc), padlen, _ip(tc), len(tc),
+                          open_, gap, ctypes.byref(m._om), ctypes.byref(ps))
+    return {f: getattr(ps, f) for f, _ in OPadStats._fields_}
+
+
+def nw_banded(q, t, open_, gap, k, m):
+    qc, tc = m.codes(q), m.codes(t)
+    r = OResult()
+    lib().oracle_nw_banded(_ip(qc), len(qc), _ip(tc), len(tc), open_, gap, k,
+                           ctypes.byref(m._om), ctypes.byref(r))
+    return {"score": r.score, "end_query": r.end_query, "end_ref": r.end_ref}
+
+
+def align_batch(alg, sgflags, stats, queries, targets, open_, gap, m, nthreads=0):
+    """Many pairs (OpenMP). queries/targets: lists of strings of equal count."""
+    n = len(targets)
+    qcat = [m.codes(q) for q in queries]
+    tcat = [m.codes(t) for t in targets]
+    qlen = np.array([len(x) for x in qcat], dtype=np.int32)
+    tlen = np.array([len(x) for x in tcat], dtype=np.int32)
+    qoff = np.zeros(n, dtype=np.int64)
+    toff = np.zeros(n, dtype=np.int64)
+    qoff[1:] = np.cumsum(qlen)[:-1]
+    toff[1:] = np.cumsum(tlen)[:-1]
+    qc = np.concatenate(qcat).astype(np.int32)
+    tc = np.concatenate(tcat).astype(np.int32)
+    res = (OResult * n)()
+    nthreads = nthreads or os.cpu_count() or 1
+    rc = lib().oracle_align_batch(alg, sgflags, int(stats), n, _ip(qc),
+                                  qoff.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _ip(qlen),
+                                  _ip(tc), toff.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                  _ip(tlen), open_, gap, ctypes.byref(m._om), res, nthreads)
+    if rc != 0:
+        raise ValueError("oracle_align_batch rejected an input")
+    return res
+
+
+def nw_diag_range(q, t, open_, gap, m):
+    qc, tc = m.codes(q), m.codes(t)
+    lo, hi, sc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    lib().oracle_nw_diag_range(_ip(qc), len(qc), _ip(tc), len(tc), open_, gap, ctypes.byref(m._om),
+                               ctypes.byref(lo), ctypes.byref(hi), ctypes.byref(sc))
+    return lo.value, hi.value, sc.value
+
+
+# ----------------------------------------------------------------------------
+# The reference library itself (when built)
+
+def ref_matrix(name):
+    r = ref()
+    if r is None:
+        return None
+    pm = r.parasail_matrix_lookup(name.encode())
+    return Matrix.from_struct(pm, name) if pm else None
+
+
+def _ref_result(r, rp):
+    if not rp:
+        return None
+    c = rp.contents
+    out = {"score": c.score, "end_query": c.end_query, "end_ref": c.end_ref, "flag": c.flag}
+    if c.flag & (1 << 16) and c.extra:
+        st = ctypes.cast(c.extra, ctypes.POINTER(PStats)).contents
+        out.update(matches=st.matches, similar=st.similar, length=st.length)
+    r.parasail_result_free(rp)
+    return out
+
+
+_ref_matrix_cache = {}
+
+
+def ref_matrix_ptr(name_or_simple):
+    """Reference-library matrix pointer for a built-in name or ('ACGT', match, mismatch)."""
+    r = ref()
+    key = name_or_simple if isinstance(name_or_simple, str) else tuple(name_or_simple)
+    if key not in _ref_matrix_cache:
+        if isinstance(name_or_simple, str):
+            _ref_matrix_cache[key] = r.parasail_matrix_lookup(name_or_simple.encode())
+        else:
+            a, mt, mm = name_or_simple
+            _ref_matrix_cache[key] = r.parasail_matrix_create(a.encode(), mt, mm)
+    return _ref_matrix_cache[key]
+
+
+def ref_vector(alg_name, stats, scheme, width, q, t, open_, gap, matrix_key):
+    """Runs the reference's AVX2 profile kernel (or its 8->16->32 chain for
+    width 'sat', src/satcheck.c) on one pair. Returns a dict or None."""
+    r = ref()
+    if r is None:
+        return None
+    mp = ref_matrix_ptr(matrix_key)
+    qb = q.encode()
+    tb = t.encode()
+    widths = [8, 16, 32] if width == "sat" else [int(width)]
+    st = "_stats" if stats else ""
+    out = None
+    for w in widths:
+        cname = "parasail_profile_create%s_avx_256_%d" % (st, w)
+        fname = "parasail_%s%s_%s_profile_avx2_256_%d" % (alg_name, st, scheme, w)
+        creator = getattr(r, cname)
+        creator.restype = ctypes.c_void_p
+        creator.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(PMatrix)]
+        fn = getattr(r, fname)
+        fn.restype = ctypes.POINTER(PResult)
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        prof = creator(qb, len(qb), mp)
+        out = _ref_result(r, fn(prof, tb, len(tb), open_, gap))
+        r.parasail_profile_free(prof)
+        if not (out["flag"] & (1 << 6)):
+            break
+    return out
+
+
+def ref_serial(alg_name, stats, q, t, open_, gap, matrix_key, scan=False):
+    r = ref()
+    if r is None:
+        return None
+    mp = ref_matrix_ptr(matrix_key)
+    fname = "parasail_%s%s%s" % (alg_name, "_stats" if stats else "", "_scan" if scan else "")
+    fn = getattr(r, fname)
+    fn.restype = ctypes.POINTER(PResult)
+    fn.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                   ctypes.c_int, ctypes.POINTER(PMatrix)]
+    qb, tb = q.encode(), t.encode()
+    return _ref_result(r, fn(qb, len(qb), tb, len(tb), open_, gap, mp))
+
+
+def ref_nw_banded(q, t, open_, gap, k, matrix_key):
+    r = ref()
+    if r is None:
+        return None
+    mp = ref_matrix_ptr(matrix_key)
+    fn = r.parasail_nw_banded
+    fn.restype = ctypes.POINTER(PResult)
+    fn.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                   ctypes.c_int, ctypes.c_int, ctypes.POINTER(PMatrix)]
+    qb, tb = q.encode(), t.encode()
+    return _ref_result(r, fn(qb, len(qb), tb, len(tb), open_, gap, k, mp))

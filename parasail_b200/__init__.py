@@ -1,0 +1,161 @@
+"""parasail-b200: Python access to the drop-in parasail.h library.
+
+The product is the C library `libparasail_b200.so` (C host code + sm_100a
+CUDA kernels) built in this directory; this module is a thin ctypes mirror of
+its C API, used by the tests and the benchmark. Every call goes through the
+C ABI. There is no Python or CPU implementation of any alignment here: if the
+library is missing the import fails, and on a machine without a usable GPU
+the alignment calls return NULL, which this module raises as RuntimeError.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libparasail_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError("parasail_b200: %s is not built (run __graft_entry__.build())" % LIB_PATH)
+
+lib = ctypes.CDLL(LIB_PATH)
+
+FLAG_NW = 1 << 0
+FLAG_SG = 1 << 1
+FLAG_SW = 1 << 2
+FLAG_SG_S1_BEG = 1 << 3
+FLAG_SG_S1_END = 1 << 4
+FLAG_SATURATED = 1 << 6
+FLAG_BANDED = 1 << 7
+FLAG_NOVEC = 1 << 8
+FLAG_NOVEC_SCAN = 1 << 9
+FLAG_SCAN = 1 << 10
+FLAG_STRIPED = 1 << 11
+FLAG_SG_S2_BEG = 1 << 14
+FLAG_SG_S2_END = 1 << 15
+FLAG_STATS = 1 << 16
+FLAG_BITS_8 = 1 << 20
+FLAG_BITS_16 = 1 << 21
+FLAG_BITS_32 = 1 << 22
+
+
+class ResultStats(ctypes.Structure):
+    _fields_ = [("matches", ctypes.c_int), ("similar", ctypes.c_int),
+                ("length", ctypes.c_int), ("extra", ctypes.c_void_p)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("score", ctypes.c_int), ("end_query", ctypes.c_int),
+                ("end_ref", ctypes.c_int), ("flag", ctypes.c_int),
+                ("extra", ctypes.c_void_p)]
+
+
+class Matrix(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char_p), ("matrix", ctypes.POINTER(ctypes.c_int)),
+                ("mapper", ctypes.POINTER(ctypes.c_int)), ("size", ctypes.c_int),
+                ("max", ctypes.c_int), ("min", ctypes.c_int),
+                ("user_matrix", ctypes.POINTER(ctypes.c_int)), ("type", ctypes.c_int),
+                ("length", ctypes.c_int), ("alphabet", ctypes.c_char_p),
+                ("query", ctypes.c_char_p)]
+
+
+class ProfileData(ctypes.Structure):
+    _fields_ = [("score", ctypes.c_void_p), ("matches", ctypes.c_void_p),
+                ("similar", ctypes.c_void_p)]
+
+
+class Profile(ctypes.Structure):
+    _fields_ = [("s1", ctypes.c_char_p), ("s1Len", ctypes.c_int),
+                ("matrix", ctypes.POINTER(Matrix)),
+                ("profile8", ProfileData), ("profile16", ProfileData),
+                ("profile32", ProfileData), ("profile64", ProfileData),
+                ("free", ctypes.c_void_p), ("stop", ctypes.c_int)]
+
+
+_RP = ctypes.POINTER(Result)
+_MP = ctypes.POINTER(Matrix)
+_PP = ctypes.POINTER(Profile)
+
+lib.parasail_matrix_lookup.restype = _MP
+lib.parasail_matrix_lookup.argtypes = [ctypes.c_char_p]
+lib.parasail_matrix_create.restype = _MP
+lib.parasail_matrix_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+lib.parasail_matrix_free.argtypes = [_MP]
+lib.parasail_result_free.argtypes = [_RP]
+lib.parasail_profile_free.argtypes = [_PP]
+lib.parasail_nw_banded.restype = _RP
+lib.parasail_nw_banded.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, _MP]
+for _n in ("get_matches", "get_similar", "get_length"):
+    getattr(lib, "parasail_result_" + _n).argtypes = [_RP]
+
+
+def matrix_lookup(name):
+    m = lib.parasail_matrix_lookup(name.encode())
+    if not m:
+        raise KeyError(name)
+    return m
+
+
+def matrix_create(alphabet, match, mismatch):
+    return lib.parasail_matrix_create(alphabet.encode(), match, mismatch)
+
+
+def _fn(name, profile_form):
+    f = getattr(lib, name)
+    f.restype = _RP
+    if profile_form:
+        f.argtypes = [_PP, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    else:
+        f.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                      ctypes.c_int, ctypes.c_int, _MP]
+    return f
+
+
+def _unpack(r, name):
+    if not r:
+        raise RuntimeError("%s returned NULL" % name)
+    c = r.contents
+    out = {"score": c.score, "end_query": c.end_query, "end_ref": c.end_ref, "flag": c.flag}
+    if c.flag & FLAG_STATS:
+        st = ctypes.cast(c.extra, ctypes.POINTER(ResultStats)).contents
+        out.update(matches=st.matches, similar=st.similar, length=st.length)
+    lib.parasail_result_free(r)
+    return out
+
+
+def align(name, s1, s2, open_, gap, matrix):
+    """Calls a direct-form entry point, e.g. align('parasail_sw_striped_16', ...)."""
+    b1, b2 = s1.encode() if isinstance(s1, str) else s1, s2.encode() if isinstance(s2, str) else s2
+    return _unpack(_fn(name, False)(b1, len(b1), b2, len(b2), open_, gap, matrix), name)
+
+
+class ProfileHandle:
+    """Owns a parasail_profile_t and the query bytes it borrows."""
+
+    def __init__(self, creator, s1, matrix):
+        self.s1 = s1.encode() if isinstance(s1, str) else s1
+        self.matrix = matrix
+        f = getattr(lib, creator)
+        f.restype = _PP
+        f.argtypes = [ctypes.c_char_p, ctypes.c_int, _MP]
+        self.ptr = f(self.s1, len(self.s1), matrix)
+        if not self.ptr:
+            raise RuntimeError("%s returned NULL" % creator)
+
+    def close(self):
+        if self.ptr:
+            lib.parasail_profile_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        self.close()
+
+
+def align_profile(name, profile, s2, open_, gap):
+    b2 = s2.encode() if isinstance(s2, str) else s2
+    return _unpack(_fn(name, True)(profile.ptr, b2, len(b2), open_, gap), name)
+
+
+def nw_banded(s1, s2, open_, gap, k, matrix):
+    b1, b2 = s1.encode(), s2.encode()
+    return _unpack(lib.parasail_nw_banded(b1, len(b1), b2, len(b2), open_, gap, k, matrix),
+                   "parasail_nw_banded")

@@ -1,0 +1,126 @@
+/*
+ * pb_cuda.h -- the thin C ABI between the parasail-b200 host library (C) and
+ * its CUDA kernels. Plain pointers, sizes and PODs only.
+ *
+ * Terminology follows parasail: s1 is the query (DP rows, i), s2 the
+ * database/reference sequence (DP columns, j); a profile is the query scored
+ * against every alphabet letter; a pair is one query/target alignment.
+ */
+#ifndef PARASAIL_B200_PB_CUDA_H
+#define PARASAIL_B200_PB_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { PB_SW = 0, PB_NW = 1, PB_SG = 2 };
+/* semi-global free ends; same order as the reference's SG_CASE tuples
+ * (src/sg_helper.h:53-63: s1_beg, s1_end, s2_beg, s2_end) */
+enum { PB_S1_BEG = 1, PB_S1_END = 2, PB_S2_BEG = 4, PB_S2_END = 8 };
+
+/* Device-resident query profile. prof32[k * lp + i] = score of query
+ * position i against alphabet letter k (0 for i >= qlen), the value layout of
+ * the reference's striped profile (src/memory_avx2.c:111-127) before
+ * striping. prof8 is the same table in int8 when every value fits. */
+typedef struct pb_device_profile {
+    int qlen;            /* query length (rows) */
+    int lp;              /* padded row count, multiple of 64, >= qlen + 32 */
+    int size;            /* alphabet size */
+    int fits8;           /* 1 when prof8 is valid */
+    int mmax, mmin;      /* matrix max / min (parasail_matrix_t.max/min) */
+    int32_t *d_prof32;   /* [size][lp] */
+    int8_t  *d_prof8;    /* [size][lp] or NULL */
+    uint8_t *d_qcodes;   /* [lp], query codes, 255 past qlen */
+    int device;          /* CUDA device ordinal the profile lives on */
+} pb_device_profile;
+
+/* Per-pair output of the exact kernels. All DP values are exact 32-bit.
+ * Predicate statistics: "real" = query rows [0, qlim), pad[k] = padded rows
+ * of region k: [qlim, ceil8), [ceil8, ceil16), [ceil16, ceil32) where ceilN
+ * rounds qlim up to a multiple of N (the row padding of the reference's
+ * 32-, 16- and 8-bit AVX2 layouts). Fields that were not tracked hold
+ * INT32_MAX (for minima) or INT32_MIN (for maxima). */
+typedef struct pb_pair_out {
+    int score, end_query, end_ref;
+    int matches, similar, length;
+    int max_h;                 /* max H over real and padded rows */
+    int min_h_real;
+    int max_stat_real;         /* max of matches/similar/length */
+    int min_f_real;            /* min vertical-gap value */
+    int min_h_pad[3];
+    int max_stat_pad[3];
+    int min_f_pad[3];
+    int status;                /* 0 ok; PB_ST_* bits */
+} pb_pair_out;
+
+enum {
+    PB_ST_OVERFLOW16 = 1,   /* a 16-bit lane left its exact range: rerun in 32 bits */
+    PB_ST_BADCODE = 2       /* a residue code outside the profile alphabet */
+};
+
+/* A batch of pairs sharing one alignment mode. Every pointer is DEVICE
+ * memory except `prof` (host struct describing device memory). */
+typedef struct pb_batch {
+    int alg, sgflags, stats;
+    int open, gap;
+    int pad_rows;              /* 0: real rows only; 8/16/32: also compute the
+                                  padded rows up to a multiple of this */
+    int npairs;
+    const pb_device_profile *const *profs;  /* host array, nprofs entries */
+    int nprofs;
+    const int *d_prof_index;   /* per pair profile index, or NULL (all use 0) */
+    const uint8_t *d_targets;  /* concatenated target codes */
+    const int64_t *d_toff;     /* per pair offset into d_targets */
+    const int *d_tlen;         /* per pair target length */
+    const int *d_qlim;         /* per pair row limit (prefix pass) or NULL */
+    const int *d_tlim;         /* per pair column limit or NULL */
+    pb_pair_out *d_out;        /* per pair output */
+} pb_batch;
+
+/* --- device management ------------------------------------------------- */
+int pb_cuda_init(void);                     /* 0 ok, <0 no usable GPU */
+const char *pb_cuda_last_error(void);
+int pb_cuda_device_count(void);
+
+/* --- profiles ------------------------------------------------------------ */
+/* table: square (size*size, row = target letter, col = query letter as in
+ * the reference profile builder) or pssm (length*size, row = query pos). */
+int pb_cuda_profile_create(const int *table, int is_pssm, int size,
+                           const uint8_t *qcodes, int qlen, int mmax, int mmin,
+                           pb_device_profile *out);
+void pb_cuda_profile_destroy(pb_device_profile *p);
+
+/* --- memory helpers (device, stream-ordered on the library stream) -------- */
+void *pb_cuda_malloc(size_t bytes);
+void pb_cuda_free(void *p);
+int pb_cuda_h2d(void *dst, const void *src, size_t bytes);
+int pb_cuda_d2h(void *dst, const void *src, size_t bytes);
+int pb_cuda_sync(void);
+
+/* --- alignment ------------------------------------------------------------- */
+/* Exact int32 kernel: any mode, stats, padded-row predicate statistics. */
+int pb_cuda_align_exact(const pb_batch *b);
+/* Fast Smith-Waterman score-only kernel: two pairs per thread in packed
+ * int16x2 lanes. Pairs whose values leave the 16-bit range come back with
+ * PB_ST_OVERFLOW16 and must be rerun with pb_cuda_align_exact. Only
+ * score/end_query/end_ref/max_h/status are written. */
+int pb_cuda_align_sw16(const pb_batch *b);
+
+/* parasail_nw_banded for one pair: the reference's band recurrence
+ * (src/nw_banded.c) on the GPU; h_s2 holds mapped target codes. */
+int pb_cuda_nw_banded(const pb_device_profile *dp, const uint8_t *h_s2, int s2Len,
+                      int open, int gap, int k, int *score);
+
+/* Host convenience: copy targets to the device, run, copy results back. */
+int pb_cuda_align_host(int kernel /* 0 exact, 1 sw16 */, const pb_batch *tmpl,
+                       const uint8_t *h_targets, const int64_t *h_toff,
+                       const int *h_tlen, const int *h_qlim, const int *h_tlim,
+                       const int *h_prof_index, int npairs, pb_pair_out *h_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,314 @@
+/*
+ * pb_device.cu -- device management, profile construction, memory helpers
+ * and the launch entry points of the C ABI in pb_cuda.h.
+ *
+ * Every host thread gets its own non-blocking stream; device memory comes
+ * from the stream-ordered pool allocator, whose release threshold is raised
+ * so that repeated calls reuse memory instead of returning it to the driver.
+ */
+#include <cstdio>
+#include <cstring>
+#include <cstdint>
+#include <vector>
+#include <mutex>
+
+#include <cuda_runtime.h>
+#include <cub/device/device_scan.cuh>
+
+#include "pb_cuda.h"
+#include "pb_kernels.cuh"
+
+namespace {
+
+thread_local char g_err[256] = "";
+thread_local cudaStream_t g_stream = nullptr;
+std::once_flag g_init_once;
+int g_init_rc = -1;
+
+void set_err(const char *what, cudaError_t e)
+{
+    snprintf(g_err, sizeof g_err, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call)                                   \
+    do {                                           \
+        cudaError_t e_ = (call);                   \
+        if (e_ != cudaSuccess) {                   \
+            set_err(#call, e_);                    \
+            return -1;                             \
+        }                                          \
+    } while (0)
+
+cudaStream_t stream()
+{
+    if (!g_stream) cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking);
+    return g_stream;
+}
+
+void do_init()
+{
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n <= 0) {
+        snprintf(g_err, sizeof g_err, "no CUDA device available (%s)",
+                 e != cudaSuccess ? cudaGetErrorString(e) : "count 0");
+        g_init_rc = -1;
+        return;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    g_init_rc = 0;
+}
+
+__global__ void k_build_profile(const int *__restrict__ table, int is_pssm, int size,
+                                const uint8_t *__restrict__ qcodes, int qlen, int lp,
+                                int32_t *__restrict__ prof32, int8_t *__restrict__ prof8)
+{
+    const int64_t n = (int64_t)size * lp;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(idx / lp), i = (int)(idx % lp);
+        int v = 0;
+        if (i < qlen) v = is_pssm ? table[(int64_t)i * size + k] : table[(int64_t)k * size + qcodes[i]];
+        prof32[idx] = v;
+        if (prof8) prof8[idx] = (int8_t)v;
+    }
+}
+
+__global__ void k_scratch_sizes(const int *__restrict__ tlen, const int *__restrict__ tlim,
+                                int n, int nv, int64_t *__restrict__ sizes)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) sizes[p] = (int64_t)(tlim ? tlim[p] : tlen[p]) * nv;
+}
+
+/* Copies the host descriptors of the batch's profiles to the device. */
+pb::ProfDesc *upload_profs(const pb_batch *b, cudaStream_t st)
+{
+    std::vector<pb::ProfDesc> h(b->nprofs);
+    for (int k = 0; k < b->nprofs; ++k) {
+        const pb_device_profile *p = b->profs[k];
+        h[k].prof = p->d_prof32;
+        h[k].prof8 = p->d_prof8;
+        h[k].qcodes = p->d_qcodes;
+        h[k].qlen = p->qlen;
+        h[k].lp = p->lp;
+        h[k].size = p->size;
+        h[k].pad_ = 0;
+    }
+    pb::ProfDesc *d = nullptr;
+    if (cudaMallocAsync((void **)&d, sizeof(pb::ProfDesc) * h.size(), st) != cudaSuccess) return nullptr;
+    cudaMemcpyAsync(d, h.data(), sizeof(pb::ProfDesc) * h.size(), cudaMemcpyHostToDevice, st);
+    /* the host vector dies at return: make the copy complete first */
+    cudaStreamSynchronize(st);
+    return d;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pb_cuda_init(void)
+{
+    std::call_once(g_init_once, do_init);
+    return g_init_rc;
+}
+
+const char *pb_cuda_last_error(void) { return g_err; }
+
+int pb_cuda_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+void *pb_cuda_malloc(size_t bytes)
+{
+    void *p = nullptr;
+    if (pb_cuda_init() != 0) return nullptr;
+    if (cudaMallocAsync(&p, bytes ? bytes : 1, stream()) != cudaSuccess) {
+        snprintf(g_err, sizeof g_err, "device allocation of %zu bytes failed", bytes);
+        return nullptr;
+    }
+    return p;
+}
+
+void pb_cuda_free(void *p)
+{
+    if (p) cudaFreeAsync(p, stream());
+}
+
+int pb_cuda_h2d(void *dst, const void *src, size_t bytes)
+{
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream()));
+    return 0;
+}
+
+int pb_cuda_d2h(void *dst, const void *src, size_t bytes)
+{
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream()));
+    CK(cudaStreamSynchronize(stream()));
+    return 0;
+}
+
+int pb_cuda_sync(void)
+{
+    CK(cudaStreamSynchronize(stream()));
+    return 0;
+}
+
+int pb_cuda_profile_create(const int *table, int is_pssm, int size,
+                           const uint8_t *qcodes, int qlen, int mmax, int mmin,
+                           pb_device_profile *out)
+{
+    if (pb_cuda_init() != 0) return -1;
+    memset(out, 0, sizeof *out);
+    const int lp = ((qlen + 32 + 63) / 64) * 64;
+    const size_t tsz = (size_t)(is_pssm ? qlen : size) * size;
+    cudaStream_t st = stream();
+    int vmin = 0, vmax = 0;
+    for (size_t k = 0; k < tsz; ++k) {
+        vmin = table[k] < vmin ? table[k] : vmin;
+        vmax = table[k] > vmax ? table[k] : vmax;
+    }
+    const int fits8 = vmin >= -128 && vmax <= 127;
+    int *d_table = nullptr;
+    std::vector<uint8_t> hq(lp, 255);
+    memcpy(hq.data(), qcodes, qlen);
+    CK(cudaMallocAsync((void **)&d_table, tsz * sizeof(int), st));
+    CK(cudaMallocAsync((void **)&out->d_qcodes, lp, st));
+    CK(cudaMallocAsync((void **)&out->d_prof32, (size_t)size * lp * sizeof(int32_t), st));
+    if (fits8) CK(cudaMallocAsync((void **)&out->d_prof8, (size_t)size * lp, st));
+    CK(cudaMemcpyAsync(d_table, table, tsz * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(out->d_qcodes, hq.data(), lp, cudaMemcpyHostToDevice, st));
+    k_build_profile<<<148, 256, 0, st>>>(d_table, is_pssm, size, out->d_qcodes, qlen, lp,
+                                         out->d_prof32, fits8 ? out->d_prof8 : nullptr);
+    CK(cudaGetLastError());
+    CK(cudaFreeAsync(d_table, st));
+    CK(cudaStreamSynchronize(st));
+    out->qlen = qlen;
+    out->lp = lp;
+    out->size = size;
+    out->fits8 = fits8;
+    out->mmax = mmax;
+    out->mmin = mmin;
+    cudaGetDevice(&out->device);
+    return 0;
+}
+
+void pb_cuda_profile_destroy(pb_device_profile *p)
+{
+    if (!p) return;
+    cudaStream_t st = stream();
+    if (p->d_prof32) cudaFreeAsync(p->d_prof32, st);
+    if (p->d_prof8) cudaFreeAsync(p->d_prof8, st);
+    if (p->d_qcodes) cudaFreeAsync(p->d_qcodes, st);
+    cudaStreamSynchronize(st);
+    memset(p, 0, sizeof *p);
+}
+
+int pb_cuda_align_exact(const pb_batch *b)
+{
+    if (pb_cuda_init() != 0) return -1;
+    if (b->npairs <= 0) return 0;
+    cudaStream_t st = stream();
+    const int nv = b->stats ? 8 : 2;
+    int64_t *sizes = nullptr, *soff = nullptr;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0;
+    CK(cudaMallocAsync((void **)&sizes, sizeof(int64_t) * b->npairs, st));
+    CK(cudaMallocAsync((void **)&soff, sizeof(int64_t) * b->npairs, st));
+    k_scratch_sizes<<<(b->npairs + 255) / 256, 256, 0, st>>>(b->d_tlen, b->d_tlim, b->npairs, nv, sizes);
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, sizes, soff, b->npairs, st);
+    CK(cudaMallocAsync(&tmp, tmp_bytes, st));
+    cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, sizes, soff, b->npairs, st);
+    int64_t last_off = 0, last_size = 0;
+    CK(cudaMemcpyAsync(&last_off, soff + b->npairs - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last_size, sizes + b->npairs - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    int *scratch = nullptr;
+    CK(cudaMallocAsync((void **)&scratch, sizeof(int) * (size_t)(last_off + last_size + 1), st));
+    pb::ProfDesc *d_profs = upload_profs(b, st);
+    if (!d_profs) { snprintf(g_err, sizeof g_err, "profile descriptor upload failed"); return -1; }
+
+    pb::ExactParams p;
+    p.alg = b->alg; p.sgflags = b->sgflags; p.open = b->open; p.gap = b->gap;
+    p.pad_rows = b->pad_rows; p.npairs = b->npairs;
+    p.profs = d_profs; p.prof_index = b->d_prof_index;
+    p.targets = b->d_targets; p.toff = b->d_toff; p.tlen = b->d_tlen;
+    p.qlim = b->d_qlim; p.tlim = b->d_tlim;
+    p.scratch = scratch; p.soff = soff; p.out = b->d_out;
+    pb::launch_exact(p, b->alg, b->stats != 0, st);
+    CK(cudaGetLastError());
+    cudaFreeAsync(scratch, st);
+    cudaFreeAsync(tmp, st);
+    cudaFreeAsync(sizes, st);
+    cudaFreeAsync(soff, st);
+    cudaFreeAsync(d_profs, st);
+    CK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+int pb_cuda_align_host(int kernel, const pb_batch *tmpl,
+                       const uint8_t *h_targets, const int64_t *h_toff,
+                       const int *h_tlen, const int *h_qlim, const int *h_tlim,
+                       const int *h_prof_index, int npairs, pb_pair_out *h_out)
+{
+    if (pb_cuda_init() != 0) return -1;
+    if (npairs <= 0) return 0;
+    cudaStream_t st = stream();
+    int64_t total = 0;
+    for (int p = 0; p < npairs; ++p) {
+        const int64_t e = h_toff[p] + h_tlen[p];
+        total = e > total ? e : total;
+    }
+    pb_batch b = *tmpl;
+    uint8_t *d_t = nullptr;
+    int64_t *d_off = nullptr;
+    int *d_len = nullptr, *d_ql = nullptr, *d_tl = nullptr, *d_pi = nullptr;
+    pb_pair_out *d_out = nullptr;
+    CK(cudaMallocAsync((void **)&d_t, total + 16, st));
+    CK(cudaMallocAsync((void **)&d_off, sizeof(int64_t) * npairs, st));
+    CK(cudaMallocAsync((void **)&d_len, sizeof(int) * npairs, st));
+    CK(cudaMallocAsync((void **)&d_out, sizeof(pb_pair_out) * npairs, st));
+    CK(cudaMemcpyAsync(d_t, h_targets, total, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_off, h_toff, sizeof(int64_t) * npairs, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_len, h_tlen, sizeof(int) * npairs, cudaMemcpyHostToDevice, st));
+    if (h_qlim) {
+        CK(cudaMallocAsync((void **)&d_ql, sizeof(int) * npairs, st));
+        CK(cudaMemcpyAsync(d_ql, h_qlim, sizeof(int) * npairs, cudaMemcpyHostToDevice, st));
+    }
+    if (h_tlim) {
+        CK(cudaMallocAsync((void **)&d_tl, sizeof(int) * npairs, st));
+        CK(cudaMemcpyAsync(d_tl, h_tlim, sizeof(int) * npairs, cudaMemcpyHostToDevice, st));
+    }
+    if (h_prof_index) {
+        CK(cudaMallocAsync((void **)&d_pi, sizeof(int) * npairs, st));
+        CK(cudaMemcpyAsync(d_pi, h_prof_index, sizeof(int) * npairs, cudaMemcpyHostToDevice, st));
+    }
+    b.npairs = npairs;
+    b.d_targets = d_t; b.d_toff = d_off; b.d_tlen = d_len;
+    b.d_qlim = d_ql; b.d_tlim = d_tl; b.d_prof_index = d_pi;
+    b.d_out = d_out;
+    int rc = kernel == 1 ? pb_cuda_align_sw16(&b) : pb_cuda_align_exact(&b);
+    if (rc == 0) {
+        CK(cudaMemcpyAsync(h_out, d_out, sizeof(pb_pair_out) * npairs, cudaMemcpyDeviceToHost, st));
+    }
+    cudaFreeAsync(d_t, st);
+    cudaFreeAsync(d_off, st);
+    cudaFreeAsync(d_len, st);
+    cudaFreeAsync(d_out, st);
+    if (d_ql) cudaFreeAsync(d_ql, st);
+    if (d_tl) cudaFreeAsync(d_tl, st);
+    if (d_pi) cudaFreeAsync(d_pi, st);
+    CK(cudaStreamSynchronize(st));
+    return rc;
+}
+
+}  // extern "C"

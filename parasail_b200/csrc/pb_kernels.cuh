@@ -1,0 +1,53 @@
+/*
+ * pb_kernels.cuh -- device-side parameter blocks shared by the CUDA files.
+ */
+#ifndef PARASAIL_B200_PB_KERNELS_CUH
+#define PARASAIL_B200_PB_KERNELS_CUH
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pb_cuda.h"
+
+namespace pb {
+
+/* Device copy of one profile's descriptor. */
+struct ProfDesc {
+    const int32_t *prof;    /* [size][lp] */
+    const int8_t *prof8;    /* [size][lp] or nullptr */
+    const uint8_t *qcodes;  /* [lp] */
+    int qlen, lp, size, pad_;
+};
+
+struct ExactParams {
+    int alg, sgflags, open, gap, pad_rows, npairs;
+    const ProfDesc *profs;
+    const int *prof_index;
+    const uint8_t *targets;
+    const int64_t *toff;
+    const int *tlen;
+    const int *qlim;
+    const int *tlim;
+    int *scratch;
+    const int64_t *soff;     /* per pair scratch offset in ints */
+    pb_pair_out *out;
+};
+
+struct Sw16Params {
+    int open, gap, npairs;
+    const ProfDesc *profs;
+    const int *order;        /* pair ids sorted by target length (desc) */
+    const uint8_t *targets;
+    const int64_t *toff;
+    const int *tlen;
+    uint32_t *scratch;       /* per warp: [maxlen][32] x 2 words */
+    const int64_t *woff;     /* per warp scratch offset (words) */
+    pb_pair_out *out;
+};
+
+void launch_exact(const ExactParams &p, int alg, bool stats, cudaStream_t st);
+void launch_sw16(const Sw16Params &p, cudaStream_t st);
+
+}  // namespace pb
+
+#endif

@@ -1,0 +1,155 @@
+"""GPU parity: every parasail.h entry point of parasail-b200, called through
+the C ABI, against the oracle and the reference's own outputs.
+
+* serial forms (parasail_sw, parasail_nw_stats_scan, ...) vs the oracle's
+  restatement of the reference's serial DP: score, ends and stats, bit-exact;
+* striped/scan profile forms at 8/16/32 bits and the _sat chains vs the
+  golden outputs of the reference's AVX2 kernels (tests/golden/vector_golden.json),
+  flags included, and vs the live reference library when it was built;
+* parasail_nw_banded vs the oracle's banded restatement.
+"""
+import json
+import os
+import random
+
+import pytest
+
+import oracle as O
+from conftest import AA, DNA, rand_seq, mutate
+
+pb = pytest.importorskip("parasail_b200")
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+ALGS = ["sw", "nw", "sg", "sg_qb", "sg_qe", "sg_qx", "sg_db", "sg_de", "sg_dx",
+        "sg_qb_de", "sg_qe_db", "sg_qb_db", "sg_qe_de"]
+
+pytestmark = pytest.mark.gpu
+
+
+def _pb_matrix(key):
+    if isinstance(key, str):
+        return pb.matrix_lookup(key)
+    return pb.matrix_create(key[0], key[1], key[2])
+
+
+def _o_matrix(key, cache={}):
+    k = key if isinstance(key, str) else tuple(key)
+    if k not in cache:
+        if isinstance(key, str):
+            g = json.load(open(os.path.join(GOLDEN, "matrices.json")))[key]
+            cache[k] = O.Matrix(g["values"], g["mapper"], g["alphabet"], g["max"], g["min"], key)
+        else:
+            cache[k] = O.Matrix.simple(key[0], key[1], key[2])
+    return cache[k]
+
+
+def test_kat_test_basic():
+    # reference tests/test_basic.c:22-80
+    b62 = pb.matrix_lookup("blosum62")
+    assert pb.align("parasail_sw", "asdf", "asdf", 10, 1, b62)["score"] == 20
+    assert pb.align("parasail_sw", "asdf", "asdf", 10, 1, pb.matrix_lookup("pam50"))["score"] == 27
+    acgt = pb.matrix_create("acgt", 1, -1)
+    assert pb.align("parasail_sw", "acgt", "acgt", 10, 1, acgt)["score"] == 4
+    prof = pb.ProfileHandle("parasail_profile_create_8", "asdf", b62)
+    assert pb.align_profile("parasail_sw_striped_profile_8", prof, "asdf", 10, 1)["score"] == 20
+    prof.close()
+
+
+@pytest.mark.parametrize("alg_name", ALGS)
+def test_serial_forms_vs_oracle(alg_name):
+    rng = random.Random(len(alg_name) * 7919)
+    alg, sgf = O.alg_of(alg_name)
+    for stats in (0, 1):
+        for scan in (0, 1):
+            for it in range(6):
+                if it % 2:
+                    key, a, op, gp = "blosum62", AA, 11, 1
+                else:
+                    key, a, op, gp = ("ACGT", 2, -3), DNA, 5, 2
+                q = rand_seq(rng, rng.randint(1, 200), a)
+                t = mutate(rng, q, a) if it % 3 == 0 else rand_seq(rng, rng.randint(1, 200), a)
+                name = "parasail_%s%s%s" % (alg_name, "_stats" if stats else "", "_scan" if scan else "")
+                got = pb.align(name, q, t, op, gp, _pb_matrix(key))
+                exp = O.align(alg, sgf, stats, q, t, op, gp, _o_matrix(key))
+                for k in exp:
+                    assert got[k] == exp[k], (name, q, t, got, exp)
+                assert got["flag"] & (pb.FLAG_NOVEC_SCAN if scan else pb.FLAG_NOVEC)
+
+
+def _vector_cases():
+    return json.load(open(os.path.join(GOLDEN, "vector_golden.json")))["cases"]
+
+
+def test_vector_forms_vs_reference_golden():
+    """All 1040 golden cases: 13 algorithms x stats x striped/scan x 8/16/32/sat."""
+    bad = []
+    for c in _vector_cases():
+        st = "_stats" if c["stats"] else ""
+        w = c["width"]
+        creator = "parasail_profile_create%s_%s" % (st, w)
+        name = "parasail_%s%s_%s_profile_%s" % (c["alg"], st, c["scheme"], w)
+        m = _pb_matrix(c["matrix"])
+        prof = pb.ProfileHandle(creator, c["q"], m)
+        got = pb.align_profile(name, prof, c["t"], c["open"], c["gap"])
+        prof.close()
+        exp = c["expect"]
+        if any(got.get(k) != v for k, v in exp.items()):
+            bad.append((name, c["q"], c["t"], got, exp))
+    assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:3])
+
+
+def test_direct_forms_match_profile_forms():
+    rng = random.Random(5)
+    b62 = pb.matrix_lookup("blosum62")
+    for alg_name in ("sw", "nw", "sg_qx", "sg_de"):
+        for st in ("", "_stats"):
+            for scheme in ("striped", "scan"):
+                q = rand_seq(rng, rng.randint(20, 150), AA)
+                t = mutate(rng, q, AA, 0.3, 0.05)
+                a = pb.align("parasail_%s%s_%s_sat" % (alg_name, st, scheme), q, t, 11, 1, b62)
+                prof = pb.ProfileHandle("parasail_profile_create%s_sat" % st, q, b62)
+                b = pb.align_profile("parasail_%s%s_%s_profile_sat" % (alg_name, st, scheme), prof, t, 11, 1)
+                prof.close()
+                assert a == b
+
+
+@pytest.mark.skipif(O.ref() is None, reason="reference library not built")
+@pytest.mark.parametrize("width", ["8", "16", "32", "sat"])
+def test_vector_forms_vs_live_reference(width):
+    rng = random.Random(int(width) if width != "sat" else 99)
+    b62 = pb.matrix_lookup("blosum62")
+    dna = pb.matrix_create("ACGT", 2, -3)
+    bad = []
+    for it in range(30):
+        for alg_name in ("sw", "nw", "sg_qx", "sg_qe_db"):
+            for stats in (0, 1):
+                for scheme in ("striped", "scan"):
+                    if it % 2:
+                        key, m, a, op, gp = "blosum62", b62, AA, 11, 1
+                    else:
+                        key, m, a, op, gp = ("ACGT", 2, -3), dna, DNA, 5, 2
+                    q = rand_seq(rng, rng.randint(5, 260), a)
+                    t = mutate(rng, q, a, 0.2, 0.04) if it % 3 == 0 else rand_seq(rng, rng.randint(5, 260), a)
+                    st = "_stats" if stats else ""
+                    prof = pb.ProfileHandle("parasail_profile_create%s_%s" % (st, width), q, m)
+                    got = pb.align_profile("parasail_%s%s_%s_profile_%s" % (alg_name, st, scheme, width),
+                                           prof, t, op, gp)
+                    prof.close()
+                    exp = O.ref_vector(alg_name, stats, scheme, width, q, t, op, gp, key)
+                    if any(got.get(k) != v for k, v in exp.items()):
+                        bad.append((alg_name, stats, scheme, width, q, t, got, exp))
+    assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])
+
+
+def test_nw_banded_vs_oracle():
+    rng = random.Random(11)
+    dna = pb.matrix_create("ACGT", 2, -3)
+    om = O.Matrix.simple("ACGT", 2, -3)
+    for _ in range(40):
+        q = rand_seq(rng, rng.randint(1, 120), DNA)
+        t = mutate(rng, q, DNA) if rng.random() < 0.6 else rand_seq(rng, rng.randint(1, 120), DNA)
+        k = rng.randint(1, 30)
+        got = pb.nw_banded(q, t, 5, 2, k, dna)
+        exp = O.nw_banded(q, t, 5, 2, k, om)
+        assert (got["score"], got["end_query"], got["end_ref"]) == (exp["score"], exp["end_query"], exp["end_ref"])
+        assert got["flag"] & pb.FLAG_BANDED
