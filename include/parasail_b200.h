@@ -1,0 +1,85 @@
+/**
+ * @file parasail_b200.h
+ *
+ * Batch extensions of parasail-b200 (additive; the reference has no batch
+ * API). Each call aligns many targets against one query profile in a few
+ * GPU launches and returns the same values and flags that the per-pair
+ * parasail.h function of the same name returns for each pair.
+ *
+ * They replace the reference's per-pair driver loops, e.g.
+ * apps/parasail_aligner.cpp:1694-1740 (a pfunction called per database
+ * sequence under OpenMP) and tests/test_openmp.c:353-378.
+ *
+ * `funcname` names any in-scope profile function of parasail.h, with or
+ * without the "parasail_" prefix: "sw_striped_profile_sat",
+ * "parasail_nw_stats_scan_profile_16", "sg_qx_stats_striped_profile_sat", ...
+ */
+#ifndef PARASAIL_B200_H
+#define PARASAIL_B200_H
+
+#include <stdint.h>
+
+#include "parasail.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/** One pair's result, the fields of parasail_result_t and its stats. */
+typedef struct parasail_b200_record {
+    int score;
+    int end_query;
+    int end_ref;
+    int flag;       /**< PARASAIL_FLAG_* exactly as the per-pair function sets them */
+    int matches;    /**< 0 unless flag has PARASAIL_FLAG_STATS */
+    int similar;
+    int length;
+    int reserved;
+} parasail_b200_record_t;
+
+/** Aligns n targets (host memory; target i is targets[offsets[i] ..
+ * offsets[i] + lengths[i])) against the profile's query with the profile
+ * function `funcname`. Results go to records[0..n). Returns 0 on success,
+ * -1 on invalid arguments or a device error (message on stderr).
+ * Replaces n calls of the reference pfunction (parasail.h:206-209). */
+extern int parasail_b200_batch_profile(
+        const char *funcname, const parasail_profile_t *profile,
+        const char *targets, const int64_t *offsets, const int *lengths, int n,
+        int open, int gap, parasail_b200_record_t *records);
+
+/** As parasail_b200_batch_profile, but with inputs and outputs already in
+ * device memory on the current CUDA device: d_codes holds the targets
+ * already mapped through profile->matrix->mapper (one byte per residue),
+ * d_records receives the results. Asynchronous with respect to the host
+ * until it returns; it synchronizes its own stream before returning. */
+extern int parasail_b200_batch_profile_device(
+        const char *funcname, const parasail_profile_t *profile,
+        const uint8_t *d_codes, const int64_t *d_offsets, const int *d_lengths, int n,
+        int open, int gap, parasail_b200_record_t *d_records);
+
+/** Independent pairs: query i against target i, both from host memory,
+ * scored with `matrix` by the direct-form function `funcname`
+ * ("nw_stats_scan_16", "sg_qx_stats_striped_16", ...). Replaces n calls of
+ * the reference's direct function (parasail.h:184-188). */
+extern int parasail_b200_batch_pairs(
+        const char *funcname, const parasail_matrix_t *matrix,
+        const char *queries, const int64_t *qoffsets, const int *qlengths,
+        const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+        int open, int gap, parasail_b200_record_t *records);
+
+/** Diagnostics: number of this library's kernel launches so far. */
+extern long parasail_b200_kernel_launches(void);
+/** Diagnostics: summed device time (ms) of the int16x2 Smith-Waterman score
+ * kernel, measured with CUDA events on its stream; *launches its count. */
+extern double parasail_b200_sw16_kernel_ms(long *launches);
+/** Diagnostics: zero the two counters above. */
+extern void parasail_b200_reset_counters(void);
+/** Measured lane-operations per second of the DPX int16x2 add-max pipe on
+ * the current device (the integer roofline of the DP kernels). */
+extern double parasail_b200_dpx_peak(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PARASAIL_B200_H */

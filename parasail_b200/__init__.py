@@ -159,3 +159,96 @@ def nw_banded(s1, s2, open_, gap, k, matrix):
     b1, b2 = s1.encode(), s2.encode()
     return _unpack(lib.parasail_nw_banded(b1, len(b1), b2, len(b2), open_, gap, k, matrix),
                    "parasail_nw_banded")
+
+
+# ---------------------------------------------------------------------------
+# Batch API (include/parasail_b200.h)
+
+class Record(ctypes.Structure):
+    _fields_ = [("score", ctypes.c_int), ("end_query", ctypes.c_int), ("end_ref", ctypes.c_int),
+                ("flag", ctypes.c_int), ("matches", ctypes.c_int), ("similar", ctypes.c_int),
+                ("length", ctypes.c_int), ("reserved", ctypes.c_int)]
+
+
+lib.parasail_b200_batch_profile.restype = ctypes.c_int
+lib.parasail_b200_batch_profile.argtypes = [ctypes.c_char_p, _PP, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_void_p]
+lib.parasail_b200_batch_profile_device.restype = ctypes.c_int
+lib.parasail_b200_batch_profile_device.argtypes = [ctypes.c_char_p, _PP, ctypes.c_void_p, ctypes.c_void_p,
+                                                   ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                                   ctypes.c_int, ctypes.c_void_p]
+lib.parasail_b200_batch_pairs.restype = ctypes.c_int
+lib.parasail_b200_batch_pairs.argtypes = [ctypes.c_char_p, _MP] + [ctypes.c_void_p] * 6 + \
+    [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+lib.parasail_b200_kernel_launches.restype = ctypes.c_long
+lib.parasail_b200_sw16_kernel_ms.restype = ctypes.c_double
+lib.parasail_b200_sw16_kernel_ms.argtypes = [ctypes.POINTER(ctypes.c_long)]
+lib.parasail_b200_dpx_peak.restype = ctypes.c_double
+
+
+def _np():
+    import numpy
+    return numpy
+
+
+def pack(seqs):
+    """list of str/bytes -> (uint8 buffer, int64 offsets, int32 lengths)."""
+    np = _np()
+    bs = [s.encode() if isinstance(s, str) else s for s in seqs]
+    lens = np.array([len(b) for b in bs], dtype=np.int32)
+    offs = np.zeros(len(bs), dtype=np.int64)
+    if len(bs):
+        offs[1:] = np.cumsum(lens, dtype=np.int64)[:-1]
+    buf = np.frombuffer(b"".join(bs), dtype=np.uint8).copy() if bs else np.zeros(0, np.uint8)
+    return buf, offs, lens
+
+
+def records_to_dicts(recs, stats):
+    out = []
+    for r in recs:
+        d = {"score": int(r["score"]), "end_query": int(r["end_query"]), "end_ref": int(r["end_ref"]),
+             "flag": int(r["flag"])}
+        if stats and (d["flag"] & FLAG_STATS):
+            d.update(matches=int(r["matches"]), similar=int(r["similar"]), length=int(r["length"]))
+        out.append(d)
+    return out
+
+
+RECORD_DTYPE = None
+
+
+def record_dtype():
+    global RECORD_DTYPE
+    if RECORD_DTYPE is None:
+        np = _np()
+        RECORD_DTYPE = np.dtype([(n, np.int32) for n, _ in Record._fields_])
+    return RECORD_DTYPE
+
+
+def batch_profile(name, profile, targets, open_, gap, packed=None):
+    """Aligns many targets against profile with one batch call. Returns a
+    numpy structured array of records."""
+    np = _np()
+    buf, offs, lens = packed if packed is not None else pack(targets)
+    n = len(lens)
+    recs = np.zeros(n, dtype=record_dtype())
+    rc = lib.parasail_b200_batch_profile(name.encode(), profile.ptr, buf.ctypes.data, offs.ctypes.data,
+                                         lens.ctypes.data, n, open_, gap, recs.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("parasail_b200_batch_profile failed")
+    return recs
+
+
+def batch_pairs(name, matrix, queries, targets, open_, gap):
+    np = _np()
+    qb, qo, ql = pack(queries)
+    tb, to, tl = pack(targets)
+    n = len(tl)
+    recs = np.zeros(n, dtype=record_dtype())
+    rc = lib.parasail_b200_batch_pairs(name.encode(), matrix, qb.ctypes.data, qo.ctypes.data, ql.ctypes.data,
+                                       tb.ctypes.data, to.ctypes.data, tl.ctypes.data, n, open_, gap,
+                                       recs.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("parasail_b200_batch_pairs failed")
+    return recs

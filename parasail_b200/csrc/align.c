@@ -46,46 +46,65 @@ static int sg_bits(int alg, int sgflags)
     return f;
 }
 
-/* Runs one pair through the exact kernel. */
-static int run_pair(const pb_device_profile *dp, const pb_mode *m, int pad_rows,
-                    const uint8_t *codes, int tlen, int qlim, int tlim, pb_pair_out *out)
+/* Runs one pair. kernel 1 = the int16x2 Smith-Waterman score kernel, which
+ * reruns out-of-range pairs on the exact kernel itself; 0 = exact kernel. */
+static int run_pair(int kernel, const pb_device_profile *dp, const pb_mode *m, int stats,
+                    int pad_rows, const uint8_t *codes, int tlen, int qlim, int tlim,
+                    pb_pair_out *out)
 {
     pb_batch b;
     const pb_device_profile *profs[1];
     int64_t off = 0;
     memset(&b, 0, sizeof b);
     profs[0] = dp;
-    b.alg = m->alg; b.sgflags = m->sgflags; b.stats = m->stats;
+    b.alg = m->alg; b.sgflags = m->sgflags; b.stats = stats;
     b.open = m->open; b.gap = m->gap; b.pad_rows = pad_rows;
     b.profs = profs; b.nprofs = 1;
-    return pb_cuda_align_host(0, &b, codes, &off, &tlen, qlim > 0 ? &qlim : NULL,
+    return pb_cuda_align_host(kernel, &b, codes, &off, &tlen, qlim > 0 ? &qlim : NULL,
                               tlim > 0 ? &tlim : NULL, NULL, 1, out);
 }
 
-static parasail_result_t *make_result(int flags, int stats, int score, int eq, int er,
-                                      int matches, int similar, int length)
+parasail_result_t *pb_record_to_result(const pb_record *rec)
 {
+    const int stats = (rec->flag & PARASAIL_FLAG_STATS) != 0;
     parasail_result_t *r = pb_result_new(stats);
     if (!r) return NULL;
-    r->score = score;
-    r->end_query = eq;
-    r->end_ref = er;
-    r->flag = flags | (stats ? PARASAIL_FLAG_STATS : 0);
+    r->score = rec->score;
+    r->end_query = rec->end_query;
+    r->end_ref = rec->end_ref;
+    r->flag = rec->flag;
     if (stats) {
-        r->stats->matches = matches;
-        r->stats->similar = similar;
-        r->stats->length = length;
+        r->stats->matches = rec->matches;
+        r->stats->similar = rec->similar;
+        r->stats->length = rec->length;
     }
+    if (rec->ambig) pb_ambiguous_count += rec->ambig;
     return r;
 }
 
-/* Saturated values of the reference's kernels: biased SW striped kernels
- * report INT_MAX_w - INT_MIN_w (src/sw_striped_avx2_256_16.c:379-382, :412),
- * the 32-bit one INT32_MAX (src/sw_striped_avx2_256_32.c:356), all others 0
- * (src/nw_scan_avx2_256_16.c:386-392). */
-static int sat_score_sw_striped(int bits)
+/* One pair through the job's passes and the reference's width chain
+ * (pb_chain_resolve). */
+int pb_run_job_pair(const pb_device_profile *dp, const pb_job *job, const uint8_t *codes,
+                    int tlen, pb_record *rec)
 {
-    return bits == 8 ? 255 : bits == 16 ? 65535 : INT32_MAX;
+    const pb_mode *m = &job->mode;
+    pb_pair_out o1, o2;
+    const int score_only_sw = m->alg == PB_SW && (!m->stats || pb_job_is_faststats(job));
+    const int pad = (job->bits < 0 || (m->alg == PB_SW && !m->stats)) ? 0
+                  : (job->bits == 0 || job->bits == 8) ? 32 : job->bits == 16 ? 16 : 8;
+    int rc;
+    memset(&o2, 0, sizeof o2);
+    if (score_only_sw && job->bits >= 0)
+        rc = run_pair(1, dp, m, 0, 0, codes, tlen, 0, 0, &o1);
+    else
+        rc = run_pair(0, dp, m, m->stats, pad, codes, tlen, 0, 0, &o1);
+    if (rc != 0) return rc;
+    if (pb_needs_pass2(job, &o1)) {
+        rc = run_pair(0, dp, m, 1, 32, codes, tlen, o1.end_query + 1, o1.end_ref + 1, &o2);
+        if (rc != 0) return rc;
+    }
+    *rec = pb_chain_resolve(job, &o1, &o2, dp->qlen, tlen);
+    return 0;
 }
 
 /* bits: 8/16/32, or 0 for the 8->16->32 chain. scheme_flag: STRIPED/SCAN. */
@@ -93,62 +112,16 @@ static parasail_result_t *align_vector(const pb_device_profile *dp, const pb_mod
                                        const uint8_t *codes, int tlen, int bits,
                                        int scheme_flag)
 {
-    static const int chain[3] = {8, 16, 32};
-    const int first = bits == 0 ? 0 : (bits == 8 ? 0 : bits == 16 ? 1 : 2);
-    const int last = bits == 0 ? 2 : first;
-    const int qlen = dp->qlen;
-    const int base = alg_flag(m->alg) | sg_bits(m->alg, m->sgflags) | scheme_flag;
-    pb_pair_out o, o2;
-    int t, have2 = 0;
-    int v = PB_CLEAN;
-
-    if (m->alg == PB_SW && m->stats && m->striped) {
-        /* FASTSTATS: score pass, then a stats pass on the prefix */
-        pb_mode m1 = *m;
-        m1.stats = 0;
-        if (run_pair(dp, &m1, 0, codes, tlen, 0, 0, &o) != 0) goto gpu_error;
-        for (t = first; t <= last; ++t) {
-            const int w = chain[t];
-            const int fl = base | pb_flag_bits(w) | pb_flag_lanes(w);
-            if (pb_resolve_faststats_pass1(m, w, &o) == PB_SAT) {
-                if (t < last) continue;
-                return make_result(fl | PARASAIL_FLAG_SATURATED, 0, sat_score_sw_striped(w), 0, 0, 0, 0, 0);
-            }
-            if (!have2) {
-                if (run_pair(dp, m, 32, codes, tlen, o.end_query + 1, o.end_ref + 1, &o2) != 0) goto gpu_error;
-                have2 = 1;
-            }
-            v = pb_resolve_tier(m, w, &o2, o.end_query + 1, o.end_ref + 1);
-            if (v == PB_SAT) {
-                if (t < last) continue;
-                return make_result(fl | PARASAIL_FLAG_SATURATED, 1, 0, o.end_query, o.end_ref, 0, 0, 0);
-            }
-            return make_result(fl, 1, o.score, o.end_query, o.end_ref, o2.matches, o2.similar, o2.length);
-        }
+    pb_job job;
+    pb_record rec;
+    job.mode = *m;
+    job.bits = bits;
+    job.base_flags = alg_flag(m->alg) | sg_bits(m->alg, m->sgflags) | scheme_flag;
+    if (pb_run_job_pair(dp, &job, codes, tlen, &rec) != 0) {
+        fprintf(stderr, "parasail-b200: GPU alignment failed: %s\n", pb_cuda_last_error());
         return NULL;
     }
-
-    {
-        const int need_pad = !(m->alg == PB_SW && !m->stats);
-        const int pad = need_pad ? (bits == 0 || bits == 8 ? 32 : bits == 16 ? 16 : 8) : 0;
-        if (run_pair(dp, m, pad, codes, tlen, 0, 0, &o) != 0) goto gpu_error;
-        for (t = first; t <= last; ++t) {
-            const int w = chain[t];
-            const int fl = base | pb_flag_bits(w) | pb_flag_lanes(w);
-            v = pb_resolve_tier(m, w, &o, qlen, tlen);
-            if (v == PB_SAT) {
-                if (t < last) continue;
-                if (m->alg == PB_SW && m->striped && !m->stats)
-                    return make_result(fl | PARASAIL_FLAG_SATURATED, 0, sat_score_sw_striped(w), 0, 0, 0, 0, 0);
-                return make_result(fl | PARASAIL_FLAG_SATURATED, m->stats, 0, 0, 0, 0, 0, 0);
-            }
-            return make_result(fl, m->stats, o.score, o.end_query, o.end_ref, o.matches, o.similar, o.length);
-        }
-    }
-    return NULL;
-gpu_error:
-    fprintf(stderr, "parasail-b200: GPU alignment failed: %s\n", pb_cuda_last_error());
-    return NULL;
+    return pb_record_to_result(&rec);
 }
 
 static uint8_t *map_target(const parasail_matrix_t *matrix, const char *s2, int s2Len)
@@ -239,9 +212,10 @@ static parasail_result_t *serial_entry(const char *func, const char *s1, int s1L
     parasail_profile_t *profile;
     const pb_device_profile *dp;
     uint8_t *codes;
-    pb_pair_out o;
     pb_mode m;
-    int flags;
+    pb_job job;
+    pb_record rec;
+    int rc;
     if (!s2) { fprintf(stderr, "%s: missing %s\n", func, "_s2"); return NULL; }
     if (s2Len <= 0) { fprintf(stderr, "%s: %s must be > 0\n", func, "s2Len"); return NULL; }
     if (open < 0) { fprintf(stderr, "%s: %s must be >= 0\n", func, "open"); return NULL; }
@@ -261,17 +235,19 @@ static parasail_result_t *serial_entry(const char *func, const char *s1, int s1L
     if (!codes) { parasail_profile_free(profile); return NULL; }
     m.alg = alg; m.sgflags = sgflags; m.stats = stats; m.striped = 0;
     m.open = open; m.gap = gap; m.mmax = matrix->max; m.mmin = matrix->min;
-    if (run_pair(dp, &m, 0, codes, s2Len, 0, 0, &o) != 0) {
-        fprintf(stderr, "%s: GPU alignment failed: %s\n", func, pb_cuda_last_error());
-        free(codes);
-        parasail_profile_free(profile);
-        return NULL;
-    }
+    job.mode = m;
+    job.bits = -1;
+    job.base_flags = alg_flag(alg) | sg_bits(alg, sgflags)
+                   | (scan ? PARASAIL_FLAG_NOVEC_SCAN : PARASAIL_FLAG_NOVEC)
+                   | PARASAIL_FLAG_BITS_32 | PARASAIL_FLAG_LANES_1;
+    rc = pb_run_job_pair(dp, &job, codes, s2Len, &rec);
     free(codes);
     parasail_profile_free(profile);
-    flags = alg_flag(alg) | sg_bits(alg, sgflags) | (scan ? PARASAIL_FLAG_NOVEC_SCAN : PARASAIL_FLAG_NOVEC)
-          | PARASAIL_FLAG_BITS_32 | PARASAIL_FLAG_LANES_1;
-    return make_result(flags, stats, o.score, o.end_query, o.end_ref, o.matches, o.similar, o.length);
+    if (rc != 0) {
+        fprintf(stderr, "%s: GPU alignment failed: %s\n", func, pb_cuda_last_error());
+        return NULL;
+    }
+    return pb_record_to_result(&rec);
 }
 
 /* ---- generated entry points -------------------------------------------- */

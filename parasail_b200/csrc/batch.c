@@ -1,4 +1,207 @@
 /*
  * batch.c -- parasail-b200 batch API (include/parasail_b200.h).
+ *
+ * Parses the parasail function name into a job (algorithm, semi-global ends,
+ * stats, striped/scan, width or the _sat chain), validates the arguments with
+ * the reference's checks, and runs the device pipeline of pb_batch.cu.
  */
+#include <stdlib.h>
+#include <string.h>
+
 #include "pb_internal.h"
+#include "parasail_b200.h"
+
+static const struct { const char *name; int alg, sgflags; } g_algs[] = {
+    {"sw", PB_SW, 0}, {"nw", PB_NW, 0},
+    {"sg_qb_de", PB_SG, PB_S1_BEG | PB_S2_END}, {"sg_qe_db", PB_SG, PB_S1_END | PB_S2_BEG},
+    {"sg_qb_db", PB_SG, PB_S1_BEG | PB_S2_BEG}, {"sg_qe_de", PB_SG, PB_S1_END | PB_S2_END},
+    {"sg_qb", PB_SG, PB_S1_BEG}, {"sg_qe", PB_SG, PB_S1_END},
+    {"sg_qx", PB_SG, PB_S1_BEG | PB_S1_END}, {"sg_db", PB_SG, PB_S2_BEG},
+    {"sg_de", PB_SG, PB_S2_END}, {"sg_dx", PB_SG, PB_S2_BEG | PB_S2_END},
+    {"sg", PB_SG, PB_S1_BEG | PB_S1_END | PB_S2_BEG | PB_S2_END},
+};
+
+/* "[parasail_]ALG[_stats]_{striped,scan}[_profile]_{8,16,32,sat}" -> job.
+ * want_profile: 1 profile form required, 0 direct form required. */
+static int parse_job(const char *funcname, int want_profile, int open, int gap,
+                     const parasail_matrix_t *matrix, pb_job *job)
+{
+    const char *s = funcname;
+    size_t k, n;
+    int alg = -1, sgf = 0, stats = 0, striped = -1, bits = -1, prof = 0;
+    if (!s) return -1;
+    if (0 == strncmp(s, "parasail_", 9)) s += 9;
+    for (k = 0; k < sizeof g_algs / sizeof g_algs[0]; ++k) {
+        n = strlen(g_algs[k].name);
+        if (0 == strncmp(s, g_algs[k].name, n) && s[n] == '_') {
+            alg = g_algs[k].alg; sgf = g_algs[k].sgflags; s += n; break;
+        }
+    }
+    if (alg < 0) return -1;
+    if (0 == strncmp(s, "_stats", 6)) { stats = 1; s += 6; }
+    if (0 == strncmp(s, "_striped", 8)) { striped = 1; s += 8; }
+    else if (0 == strncmp(s, "_scan", 5)) { striped = 0; s += 5; }
+    else return -1;
+    if (0 == strncmp(s, "_profile", 8)) { prof = 1; s += 8; }
+    if (0 == strcmp(s, "_8")) bits = 8;
+    else if (0 == strcmp(s, "_16")) bits = 16;
+    else if (0 == strcmp(s, "_32")) bits = 32;
+    else if (0 == strcmp(s, "_sat")) bits = 0;
+    else return -1;
+    if (prof != want_profile) return -1;
+    memset(job, 0, sizeof *job);
+    job->mode.alg = alg; job->mode.sgflags = sgf; job->mode.stats = stats;
+    job->mode.striped = striped; job->mode.open = open; job->mode.gap = gap;
+    job->mode.mmax = matrix->max; job->mode.mmin = matrix->min;
+    job->bits = bits;
+    job->base_flags = (alg == PB_SW ? PARASAIL_FLAG_SW : alg == PB_NW ? PARASAIL_FLAG_NW : PARASAIL_FLAG_SG)
+                    | (striped ? PARASAIL_FLAG_STRIPED : PARASAIL_FLAG_SCAN);
+    if (alg == PB_SG) {
+        if (sgf & PB_S1_BEG) job->base_flags |= PARASAIL_FLAG_SG_S1_BEG;
+        if (sgf & PB_S1_END) job->base_flags |= PARASAIL_FLAG_SG_S1_END;
+        if (sgf & PB_S2_BEG) job->base_flags |= PARASAIL_FLAG_SG_S2_BEG;
+        if (sgf & PB_S2_END) job->base_flags |= PARASAIL_FLAG_SG_S2_END;
+    }
+    return 0;
+}
+
+static void mapper_bytes(const parasail_matrix_t *m, uint8_t *out)
+{
+    int c;
+    for (c = 0; c < 256; ++c) out[c] = (uint8_t)m->mapper[c];
+}
+
+static void copy_records(const pb_record *in, parasail_b200_record_t *out, int n)
+{
+    int i;
+    for (i = 0; i < n; ++i) {
+        out[i].score = in[i].score; out[i].end_query = in[i].end_query;
+        out[i].end_ref = in[i].end_ref; out[i].flag = in[i].flag;
+        out[i].matches = in[i].matches; out[i].similar = in[i].similar;
+        out[i].length = in[i].length; out[i].reserved = 0;
+        if (in[i].ambig) pb_ambiguous_count += in[i].ambig;
+    }
+}
+
+static int check_common(const char *func, const parasail_profile_t *profile, int n, int open, int gap)
+{
+    if (!profile) { fprintf(stderr, "%s: missing %s\n", func, "profile"); return -1; }
+    if (!profile->matrix) { fprintf(stderr, "%s: missing %s\n", func, "profile->matrix"); return -1; }
+    if (!pb_profile_device(profile)) { fprintf(stderr, "%s: missing %s\n", func, "profile->profile.score"); return -1; }
+    if (n < 0) { fprintf(stderr, "%s: %s must be >= 0\n", func, "n"); return -1; }
+    if (open < 0) { fprintf(stderr, "%s: %s must be >= 0\n", func, "open"); return -1; }
+    if (gap < 0) { fprintf(stderr, "%s: %s must be >= 0\n", func, "gap"); return -1; }
+    return 0;
+}
+
+int parasail_b200_batch_profile(const char *funcname, const parasail_profile_t *profile,
+                                const char *targets, const int64_t *offsets, const int *lengths,
+                                int n, int open, int gap, parasail_b200_record_t *records)
+{
+    pb_job job;
+    pb_batch b;
+    const pb_device_profile *profs[1];
+    uint8_t map[256];
+    pb_record *tmp;
+    int i, rc;
+    if (check_common(__func__, profile, n, open, gap) != 0) return -1;
+    if (n == 0) return 0;
+    if (!targets || !offsets || !lengths || !records) { fprintf(stderr, "%s: missing arrays\n", __func__); return -1; }
+    for (i = 0; i < n; ++i)
+        if (lengths[i] <= 0) { fprintf(stderr, "%s: lengths[%d] must be > 0\n", __func__, i); return -1; }
+    if (parse_job(funcname, 1, open, gap, profile->matrix, &job) != 0) {
+        fprintf(stderr, "%s: unknown profile function '%s'\n", __func__, funcname ? funcname : "(null)");
+        return -1;
+    }
+    if (!pb_gpu_ready(__func__)) return -1;
+    memset(&b, 0, sizeof b);
+    profs[0] = pb_profile_device(profile);
+    b.alg = job.mode.alg; b.sgflags = job.mode.sgflags; b.stats = job.mode.stats;
+    b.open = open; b.gap = gap; b.profs = profs; b.nprofs = 1; b.npairs = n;
+    mapper_bytes(profile->matrix, map);
+    tmp = (pb_record *)malloc(sizeof(pb_record) * (size_t)n);
+    if (!tmp) return -1;
+    rc = pb_cuda_batch_host(&job, &b, map, targets, offsets, lengths, NULL, NULL, NULL, n, tmp);
+    if (rc == 0) copy_records(tmp, records, n);
+    else fprintf(stderr, "%s: GPU alignment failed: %s\n", __func__, pb_cuda_last_error());
+    free(tmp);
+    return rc;
+}
+
+int parasail_b200_batch_profile_device(const char *funcname, const parasail_profile_t *profile,
+                                       const uint8_t *d_codes, const int64_t *d_offsets,
+                                       const int *d_lengths, int n, int open, int gap,
+                                       parasail_b200_record_t *d_records)
+{
+    pb_job job;
+    pb_batch b;
+    const pb_device_profile *profs[1];
+    if (check_common(__func__, profile, n, open, gap) != 0) return -1;
+    if (n == 0) return 0;
+    if (!d_codes || !d_offsets || !d_lengths || !d_records) { fprintf(stderr, "%s: missing arrays\n", __func__); return -1; }
+    if (parse_job(funcname, 1, open, gap, profile->matrix, &job) != 0) {
+        fprintf(stderr, "%s: unknown profile function '%s'\n", __func__, funcname ? funcname : "(null)");
+        return -1;
+    }
+    if (!pb_gpu_ready(__func__)) return -1;
+    memset(&b, 0, sizeof b);
+    profs[0] = pb_profile_device(profile);
+    b.alg = job.mode.alg; b.sgflags = job.mode.sgflags; b.stats = job.mode.stats;
+    b.open = open; b.gap = gap; b.profs = profs; b.nprofs = 1; b.npairs = n;
+    b.d_targets = d_codes; b.d_toff = d_offsets; b.d_tlen = d_lengths;
+    /* parasail_b200_record_t and pb_record share one layout of 8 ints */
+    return pb_cuda_batch_run(&job, &b, (pb_record *)d_records);
+}
+
+int parasail_b200_batch_pairs(const char *funcname, const parasail_matrix_t *matrix,
+                              const char *queries, const int64_t *qoffsets, const int *qlengths,
+                              const char *targets, const int64_t *toffsets, const int *tlengths,
+                              int n, int open, int gap, parasail_b200_record_t *records)
+{
+    pb_job job;
+    pb_batch b;
+    uint8_t map[256];
+    pb_record *tmp;
+    int32_t *d_mat = NULL;
+    int i, rc;
+    if (!matrix) { fprintf(stderr, "%s: missing %s\n", __func__, "matrix"); return -1; }
+    if (matrix->type != PARASAIL_MATRIX_TYPE_SQUARE) {
+        fprintf(stderr, "%s: pairs batches need a square matrix\n", __func__);
+        return -1;
+    }
+    if (n < 0 || open < 0 || gap < 0) { fprintf(stderr, "%s: invalid n/open/gap\n", __func__); return -1; }
+    if (n == 0) return 0;
+    if (!queries || !qoffsets || !qlengths || !targets || !toffsets || !tlengths || !records) {
+        fprintf(stderr, "%s: missing arrays\n", __func__);
+        return -1;
+    }
+    for (i = 0; i < n; ++i)
+        if (qlengths[i] <= 0 || tlengths[i] <= 0) { fprintf(stderr, "%s: pair %d has an empty sequence\n", __func__, i); return -1; }
+    if (parse_job(funcname, 0, open, gap, matrix, &job) != 0) {
+        fprintf(stderr, "%s: unknown function '%s'\n", __func__, funcname ? funcname : "(null)");
+        return -1;
+    }
+    if (!pb_gpu_ready(__func__)) return -1;
+    d_mat = (int32_t *)pb_cuda_malloc(sizeof(int32_t) * (size_t)matrix->size * matrix->size);
+    if (!d_mat) return -1;
+    /* vector-kernel orientation: row = target letter (src/memory_avx2.c:113-116) */
+    if (pb_cuda_h2d(d_mat, matrix->matrix, sizeof(int32_t) * (size_t)matrix->size * matrix->size) != 0) {
+        pb_cuda_free(d_mat);
+        return -1;
+    }
+    pb_cuda_sync();
+    memset(&b, 0, sizeof b);
+    b.alg = job.mode.alg; b.sgflags = job.mode.sgflags; b.stats = job.mode.stats;
+    b.open = open; b.gap = gap; b.nprofs = 0; b.npairs = n;
+    b.d_mat = d_mat; b.msize = matrix->size; b.mmax = matrix->max; b.mmin = matrix->min;
+    mapper_bytes(matrix, map);
+    tmp = (pb_record *)malloc(sizeof(pb_record) * (size_t)n);
+    if (!tmp) { pb_cuda_free(d_mat); return -1; }
+    rc = pb_cuda_batch_host(&job, &b, map, targets, toffsets, tlengths, queries, qoffsets, qlengths, n, tmp);
+    if (rc == 0) copy_records(tmp, records, n);
+    else fprintf(stderr, "%s: GPU alignment failed: %s\n", __func__, pb_cuda_last_error());
+    free(tmp);
+    pb_cuda_free(d_mat);
+    pb_cuda_sync();
+    return rc;
+}

@@ -1,0 +1,186 @@
+/*
+ * pb_batch.cu -- the batch pipeline: score pass, optional prefix stats pass
+ * (SW stats striped, the reference's FASTSTATS wrapper), and the width
+ * resolution of every pair on the device, producing compact records.
+ */
+#include <cstdio>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pb_cuda.h"
+#include "pb_kernels.cuh"
+#include "pb_resolve.h"
+
+namespace pb {
+
+__global__ void k_resolve(pb_job job, const pb_pair_out *__restrict__ o1,
+                          const pb_pair_out *__restrict__ o2, const int *__restrict__ qlen,
+                          int qlen_all, const int *__restrict__ tlen, int n,
+                          pb_record *__restrict__ rec)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const pb_pair_out a = o1[i];
+    pb_pair_out b;
+    if (o2) b = o2[i];
+    rec[i] = pb_chain_resolve(&job, &a, o2 ? &b : nullptr, qlen ? qlen[i] : qlen_all, tlen[i]);
+}
+
+/* prefix limits of the FASTSTATS stats pass; pairs that need none get a
+ * 1x1 problem */
+__global__ void k_prefix_limits(pb_job job, const pb_pair_out *__restrict__ o1, int n,
+                                int *__restrict__ qlim, int *__restrict__ tlim)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const pb_pair_out a = o1[i];
+    const bool need = pb_needs_pass2(&job, &a);
+    qlim[i] = need ? a.end_query + 1 : 1;
+    tlim[i] = need ? a.end_ref + 1 : 1;
+}
+
+void launch_resolve(const pb_job &job, const pb_pair_out *o1, const pb_pair_out *o2, const int *qlen,
+                    int qlen_all, const int *tlen, int n, pb_record *rec, cudaStream_t st)
+{
+    k_resolve<<<(n + 255) / 256, 256, 0, st>>>(job, o1, o2, qlen, qlen_all, tlen, n, rec);
+}
+
+}  // namespace pb
+
+extern "C" int pb_cuda_batch_run(const pb_job *job, const pb_batch *tmpl, pb_record *d_rec)
+{
+    if (pb_cuda_init() != 0) return -1;
+    const int n = tmpl->npairs;
+    if (n <= 0) return 0;
+    const pb_mode *m = &job->mode;
+    cudaStream_t st = nullptr;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    pb_pair_out *o1 = nullptr, *o2 = nullptr;
+    int *qlim = nullptr, *tlim = nullptr;
+    int rc = 0;
+    cudaMallocAsync((void **)&o1, sizeof(pb_pair_out) * n, st);
+    cudaStreamSynchronize(st);
+    pb_batch b = *tmpl;
+    b.d_out = o1;
+    b.d_qlim = nullptr;
+    b.d_tlim = nullptr;
+    const bool sw_score = m->alg == PB_SW && (!m->stats || pb_job_is_faststats(job)) && job->bits >= 0;
+    if (sw_score && b.nprofs == 1) {
+        b.stats = 0;
+        b.pad_rows = 0;
+        rc = pb_cuda_align_sw16(&b);
+    } else {
+        b.stats = sw_score ? 0 : m->stats;
+        b.pad_rows = (job->bits < 0 || (m->alg == PB_SW && !m->stats)) ? 0
+                   : (job->bits == 0 || job->bits == 8) ? 32 : job->bits == 16 ? 16 : 8;
+        rc = pb_cuda_align_exact(&b);
+    }
+    if (rc == 0 && pb_job_is_faststats(job)) {
+        cudaMallocAsync((void **)&o2, sizeof(pb_pair_out) * n, st);
+        cudaMallocAsync((void **)&qlim, sizeof(int) * n, st);
+        cudaMallocAsync((void **)&tlim, sizeof(int) * n, st);
+        pb::k_prefix_limits<<<(n + 255) / 256, 256, 0, st>>>(*job, o1, n, qlim, tlim);
+        pb_diag_count_launch(1);
+        cudaStreamSynchronize(st);
+        pb_batch b2 = *tmpl;
+        b2.stats = 1;
+        b2.pad_rows = 32;
+        b2.d_qlim = qlim;
+        b2.d_tlim = tlim;
+        b2.d_out = o2;
+        rc = pb_cuda_align_exact(&b2);
+    }
+    if (rc == 0) {
+        const int qall = tmpl->nprofs > 0 ? tmpl->profs[0]->qlen : 0;
+        pb::launch_resolve(*job, o1, o2, tmpl->nprofs > 0 ? nullptr : tmpl->d_qlen, qall,
+                           tmpl->d_tlen, n, d_rec, st);
+        pb_diag_count_launch(1);
+        if (cudaGetLastError() != cudaSuccess) rc = -1;
+    }
+    cudaFreeAsync(o1, st);
+    if (o2) cudaFreeAsync(o2, st);
+    if (qlim) cudaFreeAsync(qlim, st);
+    if (tlim) cudaFreeAsync(tlim, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
+    cudaStreamDestroy(st);
+    return rc;
+}
+
+namespace {
+
+__global__ void k_map_codes(uint8_t *__restrict__ buf, int64_t n, const uint8_t *__restrict__ map)
+{
+    __shared__ uint8_t smap[256];
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) smap[k] = map[k];
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        buf[i] = smap[buf[i]];
+}
+
+}  // namespace
+
+/* Host-memory batch: copies the characters of targets (and, in pairs mode,
+ * queries) to the device, maps them to codes there, runs the pipeline and
+ * copies the records back. */
+extern "C" int pb_cuda_batch_host(const pb_job *job, const pb_batch *tmpl, const uint8_t *mapper256,
+                                  const char *h_targets, const int64_t *h_toff, const int *h_tlen,
+                                  const char *h_queries, const int64_t *h_qoff, const int *h_qlen,
+                                  int n, pb_record *h_rec)
+{
+    if (pb_cuda_init() != 0) return -1;
+    if (n <= 0) return 0;
+    cudaStream_t st = nullptr;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    int64_t tbytes = 0, qbytes = 0;
+    for (int i = 0; i < n; ++i) {
+        const int64_t e = h_toff[i] + h_tlen[i];
+        tbytes = e > tbytes ? e : tbytes;
+        if (h_queries) {
+            const int64_t q = h_qoff[i] + h_qlen[i];
+            qbytes = q > qbytes ? q : qbytes;
+        }
+    }
+    uint8_t *d_t = nullptr, *d_q = nullptr, *d_map = nullptr;
+    int64_t *d_toff = nullptr, *d_qoff = nullptr;
+    int *d_tlen = nullptr, *d_qlen = nullptr;
+    pb_record *d_rec = nullptr;
+    int rc = 0;
+    cudaMallocAsync((void **)&d_t, tbytes + 16, st);
+    cudaMallocAsync((void **)&d_toff, sizeof(int64_t) * n, st);
+    cudaMallocAsync((void **)&d_tlen, sizeof(int) * n, st);
+    cudaMallocAsync((void **)&d_map, 256, st);
+    cudaMallocAsync((void **)&d_rec, sizeof(pb_record) * n, st);
+    cudaMemcpyAsync(d_t, h_targets, tbytes, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_toff, h_toff, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_tlen, h_tlen, sizeof(int) * n, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_map, mapper256, 256, cudaMemcpyHostToDevice, st);
+    k_map_codes<<<296, 256, 0, st>>>(d_t, tbytes, d_map);
+    pb_diag_count_launch(1);
+    if (h_queries) {
+        cudaMallocAsync((void **)&d_q, qbytes + 16, st);
+        cudaMallocAsync((void **)&d_qoff, sizeof(int64_t) * n, st);
+        cudaMallocAsync((void **)&d_qlen, sizeof(int) * n, st);
+        cudaMemcpyAsync(d_q, h_queries, qbytes, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_qoff, h_qoff, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_qlen, h_qlen, sizeof(int) * n, cudaMemcpyHostToDevice, st);
+        k_map_codes<<<296, 256, 0, st>>>(d_q, qbytes, d_map);
+        pb_diag_count_launch(1);
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
+    if (rc == 0) {
+        pb_batch b = *tmpl;
+        b.npairs = n;
+        b.d_targets = d_t; b.d_toff = d_toff; b.d_tlen = d_tlen;
+        if (h_queries) { b.d_qall = d_q; b.d_qoff = d_qoff; b.d_qlen = d_qlen; }
+        rc = pb_cuda_batch_run(job, &b, d_rec);
+    }
+    if (rc == 0 && cudaMemcpyAsync(h_rec, d_rec, sizeof(pb_record) * n, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        rc = -1;
+    cudaFreeAsync(d_t, st); cudaFreeAsync(d_toff, st); cudaFreeAsync(d_tlen, st);
+    cudaFreeAsync(d_map, st); cudaFreeAsync(d_rec, st);
+    if (d_q) { cudaFreeAsync(d_q, st); cudaFreeAsync(d_qoff, st); cudaFreeAsync(d_qlen, st); }
+    if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
+    cudaStreamDestroy(st);
+    return rc;
+}

@@ -78,6 +78,13 @@ typedef struct pb_batch {
     const int *d_qlim;         /* per pair row limit (prefix pass) or NULL */
     const int *d_tlim;         /* per pair column limit or NULL */
     pb_pair_out *d_out;        /* per pair output */
+    /* pairs mode (nprofs == 0): per-pair queries scored through a square
+     * matrix table on the device, mat[target letter * msize + query letter] */
+    const int32_t *d_mat;
+    int msize, mmax, mmin;
+    const uint8_t *d_qall;
+    const int64_t *d_qoff;
+    const int *d_qlen;
 } pb_batch;
 
 /* --- device management ------------------------------------------------- */
@@ -113,6 +120,25 @@ int pb_cuda_align_sw16(const pb_batch *b);
  * (src/nw_banded.c) on the GPU; h_s2 holds mapped target codes. */
 int pb_cuda_nw_banded(const pb_device_profile *dp, const uint8_t *h_s2, int s2Len,
                       int open, int gap, int k, int *score);
+
+/* The batch pipeline: score pass, FASTSTATS prefix pass when the job is SW
+ * stats striped, and the reference's width resolution of every pair, all on
+ * the device. tmpl carries the device inputs; d_rec receives npairs records.
+ * (pb_job and pb_record are defined in pb_resolve.h.) */
+struct pb_job;
+struct pb_record;
+int pb_cuda_batch_run(const struct pb_job *job, const pb_batch *tmpl, struct pb_record *d_rec);
+/* The same from host memory: characters are copied and mapped to codes on
+ * the device through mapper256 (the matrix mapper as bytes); queries are
+ * given in pairs mode only (tmpl->nprofs == 0). */
+int pb_cuda_batch_host(const struct pb_job *job, const pb_batch *tmpl, const uint8_t *mapper256,
+                       const char *h_targets, const int64_t *h_toff, const int *h_tlen,
+                       const char *h_queries, const int64_t *h_qoff, const int *h_qlen,
+                       int n, struct pb_record *h_rec);
+
+/* diagnostics (pb_diag.cu) */
+void pb_diag_count_launch(long n);
+void pb_diag_sw16_time(double ms);
 
 /* Host convenience: copy targets to the device, run, copy results back. */
 int pb_cuda_align_host(int kernel /* 0 exact, 1 sw16 */, const pb_batch *tmpl,

@@ -234,8 +234,11 @@ int pb_cuda_align_exact(const pb_batch *b)
     CK(cudaStreamSynchronize(st));
     int *scratch = nullptr;
     CK(cudaMallocAsync((void **)&scratch, sizeof(int) * (size_t)(last_off + last_size + 1), st));
-    pb::ProfDesc *d_profs = upload_profs(b, st);
-    if (!d_profs) { snprintf(g_err, sizeof g_err, "profile descriptor upload failed"); return -1; }
+    pb::ProfDesc *d_profs = nullptr;
+    if (b->nprofs > 0) {
+        d_profs = upload_profs(b, st);
+        if (!d_profs) { snprintf(g_err, sizeof g_err, "profile descriptor upload failed"); return -1; }
+    }
 
     pb::ExactParams p;
     p.alg = b->alg; p.sgflags = b->sgflags; p.open = b->open; p.gap = b->gap;
@@ -244,13 +247,15 @@ int pb_cuda_align_exact(const pb_batch *b)
     p.targets = b->d_targets; p.toff = b->d_toff; p.tlen = b->d_tlen;
     p.qlim = b->d_qlim; p.tlim = b->d_tlim;
     p.scratch = scratch; p.soff = soff; p.out = b->d_out;
+    p.mat = b->d_mat; p.msize = b->msize; p.qall = b->d_qall; p.qoff = b->d_qoff; p.qlen = b->d_qlen;
     pb::launch_exact(p, b->alg, b->stats != 0, st);
+    pb_diag_count_launch(2);   /* k_scratch_sizes, k_exact */
     CK(cudaGetLastError());
     cudaFreeAsync(scratch, st);
     cudaFreeAsync(tmp, st);
     cudaFreeAsync(sizes, st);
     cudaFreeAsync(soff, st);
-    cudaFreeAsync(d_profs, st);
+    if (d_profs) cudaFreeAsync(d_profs, st);
     CK(cudaStreamSynchronize(st));
     return 0;
 }

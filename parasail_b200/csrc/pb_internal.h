@@ -9,6 +9,7 @@
 
 #include "parasail.h"
 #include "pb_cuda.h"
+#include "pb_resolve.h"
 
 /* Validation macros with the reference's messages and return contract
  * (parasail/memory.h:46-80): print "<func>: ..." to stderr, return 0/NULL. */
@@ -52,15 +53,11 @@ const pb_device_profile *pb_profile_device(const parasail_profile_t *profile);
 
 /* align.c */
 int pb_gpu_ready(const char *func);
+int pb_run_job_pair(const pb_device_profile *dp, const pb_job *job, const uint8_t *codes,
+                    int tlen, pb_record *rec);
+parasail_result_t *pb_record_to_result(const pb_record *rec);
 
-/* tier resolution (resolve.c) */
-enum { PB_CLEAN = 0, PB_SAT = 1, PB_AMBIG = 2 };
-typedef struct pb_mode {
-    int alg, sgflags, stats, striped;
-    int open, gap, mmax, mmin;
-} pb_mode;
-int pb_resolve_tier(const pb_mode *m, int bits, const pb_pair_out *o, int qlim, int tlim);
-int pb_resolve_faststats_pass1(const pb_mode *m, int bits, const pb_pair_out *o);
+/* tier resolution helpers (resolve.c) */
 int pb_flag_lanes(int bits);
 int pb_flag_bits(int bits);
 extern volatile long pb_ambiguous_count;

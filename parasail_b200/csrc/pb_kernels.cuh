@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include "pb_cuda.h"
+#include "pb_resolve.h"
 
 namespace pb {
 
@@ -31,10 +32,17 @@ struct ExactParams {
     int *scratch;
     const int64_t *soff;     /* per pair scratch offset in ints */
     pb_pair_out *out;
+    /* pairs mode: per-pair query codes scored through a square matrix
+     * mat[target letter * msize + query letter] instead of a profile */
+    const int32_t *mat;
+    int msize;
+    const uint8_t *qall;
+    const int64_t *qoff;
+    const int *qlen;
 };
 
 struct Sw16Params {
-    int open, gap, npairs;
+    int open, gap, npairs, posmax;
     const ProfDesc *profs;
     const int *order;        /* pair ids sorted by target length (desc) */
     const uint8_t *targets;
@@ -46,6 +54,8 @@ struct Sw16Params {
 };
 
 void launch_exact(const ExactParams &p, int alg, bool stats, cudaStream_t st);
+void launch_resolve(const pb_job &job, const pb_pair_out *o1, const pb_pair_out *o2, const int *qlen,
+                    int qlen_all, const int *tlen, int n, pb_record *rec, cudaStream_t st);
 void launch_sw16(const Sw16Params &p, cudaStream_t st);
 
 }  // namespace pb

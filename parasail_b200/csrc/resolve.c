@@ -1,38 +1,6 @@
 /*
- * resolve.c -- which of parasail's 8/16/32-bit results a pair gets.
- *
- * The reference runs a pair in 8-bit lanes and, when that kernel reports
- * saturation, reruns it in 16 and then 32 bits (src/satcheck.c, e.g.
- * :41520-41538). A non-saturated result at any width equals the exact DP
- * result, so the GPU computes exact values once and this file decides, per
- * width, whether the reference's kernel of that width would have flagged the
- * pair. The reference's checks (constants from the kernels' preambles, e.g.
- * src/nw_scan_avx2_256_16.c:205-206, src/sw_striped_avx2_256_16.c:205-210):
- *
- *   NEG_LIMIT = (-open < min ? INT_MIN_w + open : INT_MIN_w - min) + 1
- *   POS_LIMIT = INT_MAX_w - max - 1
- *   SW striped 8/16 (biased lanes): max H > INT_MAX_w - max - 1 - INT_MIN_w
- *   SW striped 32:                  max H > INT32_MAX - max - 1
- *   scan, all:   any H outside [NEG_LIMIT, POS_LIMIT]; sg also any F below
- *                NEG_LIMIT and the gap ramp -open - segLen*gap
- *                (src/sg_scan_avx2_256_16.c:293-301, :355-360)
- *   stats:       additionally matches/similar/length above POS_LIMIT
- *   striped nw/sg: min also over E and the first-pass F and H
- *                (src/nw_striped_avx2_256_16.c:278-283)
- *   SW stats striped (src/sw_stats_striped_avx2_256_16.c:694-730): a score
- *                pass with the SW striped check, then a stats pass on the
- *                prefix [0,end_query]x[0,end_ref] that saturates when a count
- *                reaches INT_MAX_w - INT_MIN_w.
- *
- * Every check reads all rows of the AVX2 layout, including the padded query
- * rows up to ceil(qlen/lanes)*lanes (lanes = 32, 16, 8 for 8, 16, 32 bits);
- * the exact kernel reports those rows' extremes separately. Checks that read
- * the striped first pass (values before the lazy-F correction) are decided
- * here from sound bounds; a pair whose verdict the bounds cannot settle is
- * PB_AMBIG and goes to the lane-exact striped kernel.
+ * resolve.c -- host helpers around pb_resolve.h (flag bits of each width).
  */
-#include <limits.h>
-
 #include "pb_internal.h"
 
 volatile long pb_ambiguous_count = 0;
@@ -46,90 +14,4 @@ int pb_flag_bits(int bits)
 int pb_flag_lanes(int bits)
 {
     return bits == 8 ? PARASAIL_FLAG_LANES_32 : bits == 16 ? PARASAIL_FLAG_LANES_16 : PARASAIL_FLAG_LANES_8;
-}
-
-static int64_t int_min_w(int bits) { return bits == 8 ? INT8_MIN : bits == 16 ? INT16_MIN : INT32_MIN; }
-static int64_t int_max_w(int bits) { return bits == 8 ? INT8_MAX : bits == 16 ? INT16_MAX : INT32_MAX; }
-
-/* number of padded-row regions that belong to the layout of `bits` */
-static int pad_regions(int bits) { return bits == 32 ? 1 : bits == 16 ? 2 : 3; }
-static int lanes_of(int bits) { return 256 / bits; }
-
-static int64_t boundary_h(const pb_mode *m, int idx, int is_row)
-{
-    if (idx < 0) return 0;
-    if (m->alg == PB_SW) return 0;
-    if (m->alg == PB_SG && (m->sgflags & (is_row ? PB_S2_BEG : PB_S1_BEG))) return 0;
-    return -(int64_t)m->open - (int64_t)idx * m->gap;
-}
-
-int pb_resolve_faststats_pass1(const pb_mode *m, int bits, const pb_pair_out *o)
-{
-    if (bits == 32) return (int64_t)o->max_h > (int64_t)INT32_MAX - m->mmax - 1 ? PB_SAT : PB_CLEAN;
-    return (int64_t)o->max_h > int_max_w(bits) - m->mmax - 1 - int_min_w(bits) ? PB_SAT : PB_CLEAN;
-}
-
-int pb_resolve_tier(const pb_mode *m, int bits, const pb_pair_out *o, int qlim, int tlim)
-{
-    const int64_t imin = int_min_w(bits), imax = int_max_w(bits);
-    const int64_t neg = ((-(int64_t)m->open < m->mmin) ? imin + m->open : imin - m->mmin) + 1;
-    const int64_t pos = imax - m->mmax - 1;
-    const int L = lanes_of(bits);
-    const int64_t seglen = (qlim + L - 1) / L;
-    const int64_t padlen = seglen * L;
-    int64_t min_h = o->min_h_real, max_st = o->max_stat_real, min_f = o->min_f_real;
-    const int64_t max_h = o->max_h;
-    int k;
-    for (k = 0; k < pad_regions(bits); ++k) {
-        if (o->min_h_pad[k] < min_h) min_h = o->min_h_pad[k];
-        if (o->max_stat_pad[k] > max_st) max_st = o->max_stat_pad[k];
-        if (o->min_f_pad[k] < min_f) min_f = o->min_f_pad[k];
-    }
-
-    if (m->alg == PB_SW && !m->stats) {
-        if (m->striped) return pb_resolve_faststats_pass1(m, bits, o);
-        return max_h > pos ? PB_SAT : PB_CLEAN;
-    }
-    if (m->alg == PB_SW && m->stats && !m->striped) {
-        return (max_h > pos || max_st > pos) ? PB_SAT : PB_CLEAN;
-    }
-    if (m->alg == PB_SW && m->stats && m->striped) {
-        /* prefix stats pass of the FASTSTATS wrapper; o describes the prefix */
-        const int64_t lim = bits == 32 ? INT32_MAX : imax - imin;
-        if (bits == 32) return PB_CLEAN;
-        if (max_st >= lim) return PB_SAT;
-        if (padlen + tlim < lim) return PB_CLEAN;
-        pb_ambiguous_count++;
-        return PB_AMBIG;
-    }
-    /* NW and SG */
-    if (!m->striped) {
-        if (max_h > pos || min_h < neg) return PB_SAT;
-        if (m->stats && max_st > pos) return PB_SAT;
-        if (!m->stats && m->alg == PB_SG) {
-            int64_t ramp = -(int64_t)m->open - seglen * m->gap;
-            if (ramp < imin) ramp = imin;
-            if (min_f < neg || ramp < neg) return PB_SAT;
-        }
-        return PB_CLEAN;
-    }
-    /* striped NW/SG. Without stats the first-pass E and F are range-checked
-     * too, so an unflagged result is always exact and a true value outside
-     * the limits is always flagged. With stats only H is checked while the
-     * first-pass F of every stripe starts at NEG_LIMIT, which can lift an
-     * underflowing H back into range unflagged (the reference then returns a
-     * wrong score): such pairs are left to the lane-exact kernel. */
-    if (!m->stats && (max_h > pos || min_h < neg)) return PB_SAT;
-    {
-        int64_t minb = 0, lb;
-        const int64_t top = boundary_h(m, tlim - 1, 1), left = boundary_h(m, (int)padlen - 1, 0);
-        if (top < minb) minb = top;
-        if (left < minb) minb = left;
-        lb = (min_h < minb ? min_h : minb) + (m->mmin < 0 ? m->mmin : 0);
-        if (!m->stats) lb -= m->open;   /* E and the first-pass F are also checked */
-        else lb -= 1;                   /* strict: H == NEG_LIMIT ties the F floor */
-        if (lb >= neg && (!m->stats || padlen + tlim <= pos)) return PB_CLEAN;
-    }
-    pb_ambiguous_count++;
-    return PB_AMBIG;
 }

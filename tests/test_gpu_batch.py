@@ -1,0 +1,121 @@
+"""GPU parity of the batch API (include/parasail_b200.h) through the C ABI.
+
+Covers the int16x2 Smith-Waterman kernel (length-sorted, two targets per
+thread, strips of query rows) including its rerun of out-of-16-bit-range
+pairs on the exact 32-bit kernel, the pairs mode used for read/window
+batches, and the two-pass SW stats striped path.
+"""
+import random
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import AA, DNA, rand_seq, mutate
+
+pb = pytest.importorskip("parasail_b200")
+pytestmark = pytest.mark.gpu
+
+
+def _b62():
+    return O.Matrix.from_struct(pb.matrix_lookup("blosum62"))
+
+
+def _oracle_batch(alg, sgf, stats, q, targets, op, gp, m):
+    res = O.align_batch(alg, sgf, stats, [q] * len(targets), targets, op, gp, m)
+    return [(r.score, r.end_query, r.end_ref, r.matches, r.similar, r.length) for r in res]
+
+
+@pytest.mark.parametrize("qlen", [1, 15, 16, 17, 100, 333, 1200])
+def test_sw16_batch_vs_oracle(qlen):
+    rng = random.Random(qlen)
+    q = rand_seq(rng, qlen, AA)
+    targets = []
+    for k in range(700):
+        r = rng.random()
+        if r < 0.1:
+            targets.append(mutate(rng, q, AA, 0.2, 0.03))
+        elif r < 0.15:
+            targets.append(q)
+        else:
+            targets.append(rand_seq(rng, rng.randint(1, 600), AA))
+    b62 = pb.matrix_lookup("blosum62")
+    prof = pb.ProfileHandle("parasail_profile_create_sat", q, b62)
+    recs = pb.batch_profile("sw_striped_profile_sat", prof, targets, 11, 1)
+    prof.close()
+    exp = _oracle_batch(O.SW, 0, 0, q, targets, 11, 1, _b62())
+    for k, (r, e) in enumerate(zip(recs, exp)):
+        assert (r["score"], r["end_query"], r["end_ref"]) == e[:3], (k, targets[k], r, e)
+        # width the reference's chain reports: 8 bits while the score fits
+        # the biased 8-bit limit (255 - 12 for BLOSUM62), else 16
+        want = pb.FLAG_BITS_8 if e[0] <= 127 - 11 - 1 + 128 else pb.FLAG_BITS_16
+        assert r["flag"] & (pb.FLAG_BITS_8 | pb.FLAG_BITS_16 | pb.FLAG_BITS_32) == want
+
+
+def test_sw16_overflow_rerun_exact():
+    """Scores beyond the 16-bit lanes' range go to the exact kernel."""
+    rng = random.Random(3)
+    m = pb.matrix_create("ACGT", 100, -100)
+    q = rand_seq(rng, 800, DNA)
+    targets = [q[:500], q, mutate(rng, q, DNA, 0.01, 0.0), rand_seq(rng, 300, DNA), q[:200]]
+    prof = pb.ProfileHandle("parasail_profile_create_sat", q, m)
+    recs = pb.batch_profile("sw_striped_profile_sat", prof, targets, 10, 1)
+    prof.close()
+    om = O.Matrix.simple("ACGT", 100, -100)
+    exp = _oracle_batch(O.SW, 0, 0, q, targets, 10, 1, om)
+    for r, e in zip(recs, exp):
+        assert (r["score"], r["end_query"], r["end_ref"]) == e[:3]
+    # 16-bit biased lanes hold scores up to 65535 - 101 (src/sw_striped_avx2_256_16.c:205)
+    assert recs[0]["score"] == 50000 and recs[0]["flag"] & pb.FLAG_BITS_16
+    assert recs[1]["score"] == 80000 and recs[1]["flag"] & pb.FLAG_BITS_32
+
+
+def test_batch_matches_per_pair_api():
+    rng = random.Random(9)
+    b62 = pb.matrix_lookup("blosum62")
+    q = rand_seq(rng, 230, AA)
+    targets = [mutate(rng, q, AA, 0.5, 0.05) if k % 3 == 0 else rand_seq(rng, rng.randint(20, 400), AA)
+               for k in range(60)]
+    for name, creator in [("sw_striped_profile_16", "parasail_profile_create_16"),
+                          ("nw_scan_profile_sat", "parasail_profile_create_sat"),
+                          ("sg_qx_stats_striped_profile_16", "parasail_profile_create_stats_16"),
+                          ("sw_stats_striped_profile_sat", "parasail_profile_create_stats_sat"),
+                          ("sw_stats_scan_profile_32", "parasail_profile_create_stats_32")]:
+        prof = pb.ProfileHandle(creator, q, b62)
+        recs = pb.records_to_dicts(pb.batch_profile(name, prof, targets, 11, 1), "stats" in name)
+        for t, r in zip(targets, recs):
+            assert r == pb.align_profile("parasail_" + name, prof, t, 11, 1), (name, t)
+        prof.close()
+
+
+def test_pairs_mode_reads_vs_windows():
+    rng = random.Random(4)
+    reads, wins = [], []
+    for _ in range(400):
+        w = rand_seq(rng, rng.randint(132, 332), DNA)
+        reads.append(mutate(rng, w[: len(w) - 32], DNA, 0.05, 0.01))
+        wins.append(w)
+    dna = pb.matrix_create("ACGT", 2, -3)
+    om = O.Matrix.simple("ACGT", 2, -3)
+    for name, alg, sgf in [("nw_stats_scan_16", O.NW, 0), ("sg_qx_stats_striped_16", O.SG, O.S1_BEG | O.S1_END),
+                           ("nw_stats_striped_16", O.NW, 0), ("sg_qx_stats_scan_16", O.SG, O.S1_BEG | O.S1_END)]:
+        recs = pb.batch_pairs(name, dna, reads, wins, 5, 2)
+        res = O.align_batch(alg, sgf, 1, reads, wins, 5, 2, om)
+        for r, e in zip(recs, res):
+            assert (r["score"], r["end_query"], r["end_ref"], r["matches"], r["similar"], r["length"]) == \
+                (e.score, e.end_query, e.end_ref, e.matches, e.similar, e.length)
+            assert r["flag"] & pb.FLAG_BITS_16 and not (r["flag"] & pb.FLAG_SATURATED)
+
+
+def test_faststats_batch_vs_oracle():
+    rng = random.Random(21)
+    b62 = pb.matrix_lookup("blosum62")
+    q = rand_seq(rng, 700, AA)
+    targets = [mutate(rng, q[rng.randint(0, 300):], AA, 0.6, 0.03) if k % 4 == 0
+               else rand_seq(rng, rng.randint(50, 1500), AA) for k in range(200)]
+    prof = pb.ProfileHandle("parasail_profile_create_stats_32", q, b62)
+    recs = pb.batch_profile("sw_stats_striped_profile_32", prof, targets, 11, 1)
+    prof.close()
+    exp = _oracle_batch(O.SW, 0, 1, q, targets, 11, 1, _b62())
+    for r, e in zip(recs, exp):
+        assert (r["score"], r["end_query"], r["end_ref"], r["matches"], r["similar"], r["length"]) == e
