@@ -57,6 +57,23 @@ extern int parasail_b200_batch_profile_device(
         const uint8_t *d_codes, const int64_t *d_offsets, const int *d_lengths, int n,
         int open, int gap, parasail_b200_record_t *d_records);
 
+/** Database search: every one of nq query profiles (sharing one matrix)
+ * against every target, in one pipeline; a Smith-Waterman score batch runs
+ * all queries in a single kernel launch. records[q * n + i] is query q
+ * against target i. Replaces the reference aligner's per-query loop
+ * (apps/parasail_aligner.cpp:1694-1740). */
+extern int parasail_b200_batch_db(
+        const char *funcname, const parasail_profile_t *const *profiles, int nq,
+        const char *targets, const int64_t *offsets, const int *lengths, int n,
+        int open, int gap, parasail_b200_record_t *records);
+
+/** parasail_b200_batch_db with device-resident, already mapped targets and
+ * device-resident records (see parasail_b200_batch_profile_device). */
+extern int parasail_b200_batch_db_device(
+        const char *funcname, const parasail_profile_t *const *profiles, int nq,
+        const uint8_t *d_codes, const int64_t *d_offsets, const int *d_lengths, int n,
+        int open, int gap, parasail_b200_record_t *d_records);
+
 /** Independent pairs: query i against target i, both from host memory,
  * scored with `matrix` by the direct-form function `funcname`
  * ("nw_stats_scan_16", "sg_qx_stats_striped_16", ...). Replaces n calls of

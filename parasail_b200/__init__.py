@@ -252,3 +252,31 @@ def batch_pairs(name, matrix, queries, targets, open_, gap):
     if rc != 0:
         raise RuntimeError("parasail_b200_batch_pairs failed")
     return recs
+
+lib.parasail_b200_batch_db.restype = ctypes.c_int
+lib.parasail_b200_batch_db.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_void_p]
+lib.parasail_b200_batch_db_device.restype = ctypes.c_int
+lib.parasail_b200_batch_db_device.argtypes = lib.parasail_b200_batch_db.argtypes
+
+
+def profile_array(profiles):
+    arr = (_PP * len(profiles))(*[p.ptr for p in profiles])
+    return arr
+
+
+def batch_db(name, profiles, targets, open_, gap, packed=None):
+    """Every profile against every target in one call; returns records
+    shaped [len(profiles), n]."""
+    np = _np()
+    buf, offs, lens = packed if packed is not None else pack(targets)
+    n = len(lens)
+    recs = np.zeros(len(profiles) * n, dtype=record_dtype())
+    arr = profile_array(profiles)
+    rc = lib.parasail_b200_batch_db(name.encode(), ctypes.cast(arr, ctypes.c_void_p), len(profiles),
+                                    buf.ctypes.data, offs.ctypes.data, lens.ctypes.data, n, open_, gap,
+                                    recs.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("parasail_b200_batch_db failed")
+    return recs.reshape(len(profiles), n)

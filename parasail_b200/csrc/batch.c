@@ -205,3 +205,78 @@ int parasail_b200_batch_pairs(const char *funcname, const parasail_matrix_t *mat
     pb_cuda_sync();
     return rc;
 }
+
+/* Database search: nq profiles x n targets in one pipeline (all queries of
+ * a Smith-Waterman score batch share one kernel launch). records[q * n + i]. */
+static int db_common(const char *func, const char *funcname, const parasail_profile_t *const *profiles,
+                     int nq, int n, int open, int gap, pb_job *job, const pb_device_profile **profs)
+{
+    int q;
+    if (!profiles || nq <= 0) { fprintf(stderr, "%s: missing %s\n", func, "profiles"); return -1; }
+    for (q = 0; q < nq; ++q) {
+        if (check_common(func, profiles[q], n, open, gap) != 0) return -1;
+        if (profiles[q]->matrix != profiles[0]->matrix) {
+            fprintf(stderr, "%s: all profiles must share one matrix\n", func);
+            return -1;
+        }
+        profs[q] = pb_profile_device(profiles[q]);
+    }
+    if (parse_job(funcname, 1, open, gap, profiles[0]->matrix, job) != 0) {
+        fprintf(stderr, "%s: unknown profile function '%s'\n", func, funcname ? funcname : "(null)");
+        return -1;
+    }
+    return pb_gpu_ready(func) ? 0 : -1;
+}
+
+int parasail_b200_batch_db(const char *funcname, const parasail_profile_t *const *profiles, int nq,
+                           const char *targets, const int64_t *offsets, const int *lengths, int n,
+                           int open, int gap, parasail_b200_record_t *records)
+{
+    pb_job job;
+    pb_batch b;
+    const pb_device_profile **profs;
+    uint8_t map[256];
+    pb_record *tmp;
+    int i, rc;
+    if (n == 0) return 0;
+    if (!targets || !offsets || !lengths || !records) { fprintf(stderr, "%s: missing arrays\n", __func__); return -1; }
+    for (i = 0; i < n; ++i)
+        if (lengths[i] <= 0) { fprintf(stderr, "%s: lengths[%d] must be > 0\n", __func__, i); return -1; }
+    profs = (const pb_device_profile **)malloc(sizeof(*profs) * (size_t)(nq > 0 ? nq : 1));
+    if (!profs) return -1;
+    if (db_common(__func__, funcname, profiles, nq, n, open, gap, &job, profs) != 0) { free(profs); return -1; }
+    memset(&b, 0, sizeof b);
+    b.alg = job.mode.alg; b.sgflags = job.mode.sgflags; b.stats = job.mode.stats;
+    b.open = open; b.gap = gap; b.profs = profs; b.nprofs = nq; b.npairs = n;
+    mapper_bytes(profiles[0]->matrix, map);
+    tmp = (pb_record *)malloc(sizeof(pb_record) * (size_t)n * nq);
+    if (!tmp) { free(profs); return -1; }
+    rc = pb_cuda_batch_host(&job, &b, map, targets, offsets, lengths, NULL, NULL, NULL, n, tmp);
+    if (rc == 0) copy_records(tmp, records, n * nq);
+    else fprintf(stderr, "%s: GPU alignment failed: %s\n", __func__, pb_cuda_last_error());
+    free(tmp);
+    free(profs);
+    return rc;
+}
+
+int parasail_b200_batch_db_device(const char *funcname, const parasail_profile_t *const *profiles, int nq,
+                                  const uint8_t *d_codes, const int64_t *d_offsets, const int *d_lengths,
+                                  int n, int open, int gap, parasail_b200_record_t *d_records)
+{
+    pb_job job;
+    pb_batch b;
+    const pb_device_profile **profs;
+    int rc;
+    if (n == 0) return 0;
+    if (!d_codes || !d_offsets || !d_lengths || !d_records) { fprintf(stderr, "%s: missing arrays\n", __func__); return -1; }
+    profs = (const pb_device_profile **)malloc(sizeof(*profs) * (size_t)(nq > 0 ? nq : 1));
+    if (!profs) return -1;
+    if (db_common(__func__, funcname, profiles, nq, n, open, gap, &job, profs) != 0) { free(profs); return -1; }
+    memset(&b, 0, sizeof b);
+    b.alg = job.mode.alg; b.sgflags = job.mode.sgflags; b.stats = job.mode.stats;
+    b.open = open; b.gap = gap; b.profs = profs; b.nprofs = nq; b.npairs = n;
+    b.d_targets = d_codes; b.d_toff = d_offsets; b.d_tlen = d_lengths;
+    rc = pb_cuda_batch_run(&job, &b, (pb_record *)d_records);
+    free(profs);
+    return rc;
+}

@@ -53,47 +53,58 @@ extern "C" int pb_cuda_batch_run(const pb_job *job, const pb_batch *tmpl, pb_rec
     const int n = tmpl->npairs;
     if (n <= 0) return 0;
     const pb_mode *m = &job->mode;
+    const int nq = tmpl->nprofs > 0 ? tmpl->nprofs : 1;   /* pairs mode: one "query set" */
     cudaStream_t st = nullptr;
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     pb_pair_out *o1 = nullptr, *o2 = nullptr;
     int *qlim = nullptr, *tlim = nullptr;
     int rc = 0;
-    cudaMallocAsync((void **)&o1, sizeof(pb_pair_out) * n, st);
+    cudaMallocAsync((void **)&o1, sizeof(pb_pair_out) * n * (size_t)nq, st);
     cudaStreamSynchronize(st);
-    pb_batch b = *tmpl;
-    b.d_out = o1;
-    b.d_qlim = nullptr;
-    b.d_tlim = nullptr;
     const bool sw_score = m->alg == PB_SW && (!m->stats || pb_job_is_faststats(job)) && job->bits >= 0;
-    if (sw_score && b.nprofs == 1) {
+    if (sw_score && tmpl->nprofs >= 1) {
+        pb_batch b = *tmpl;
         b.stats = 0;
         b.pad_rows = 0;
-        rc = pb_cuda_align_sw16(&b);
+        b.d_qlim = nullptr;
+        b.d_tlim = nullptr;
+        rc = pb_cuda_align_sw16_multi(&b, o1);
     } else {
-        b.stats = sw_score ? 0 : m->stats;
-        b.pad_rows = (job->bits < 0 || (m->alg == PB_SW && !m->stats)) ? 0
-                   : (job->bits == 0 || job->bits == 8) ? 32 : job->bits == 16 ? 16 : 8;
-        rc = pb_cuda_align_exact(&b);
+        for (int q = 0; q < nq && rc == 0; ++q) {
+            pb_batch b = *tmpl;
+            if (tmpl->nprofs > 0) { b.profs = &tmpl->profs[q]; b.nprofs = 1; }
+            b.d_out = o1 + (size_t)q * n;
+            b.d_qlim = nullptr;
+            b.d_tlim = nullptr;
+            b.stats = sw_score ? 0 : m->stats;
+            b.pad_rows = (job->bits < 0 || (m->alg == PB_SW && !m->stats)) ? 0
+                       : (job->bits == 0 || job->bits == 8) ? 32 : job->bits == 16 ? 16 : 8;
+            rc = pb_cuda_align_exact(&b);
+        }
     }
     if (rc == 0 && pb_job_is_faststats(job)) {
-        cudaMallocAsync((void **)&o2, sizeof(pb_pair_out) * n, st);
+        cudaMallocAsync((void **)&o2, sizeof(pb_pair_out) * n * (size_t)nq, st);
         cudaMallocAsync((void **)&qlim, sizeof(int) * n, st);
         cudaMallocAsync((void **)&tlim, sizeof(int) * n, st);
-        pb::k_prefix_limits<<<(n + 255) / 256, 256, 0, st>>>(*job, o1, n, qlim, tlim);
-        pb_diag_count_launch(1);
-        cudaStreamSynchronize(st);
-        pb_batch b2 = *tmpl;
-        b2.stats = 1;
-        b2.pad_rows = 32;
-        b2.d_qlim = qlim;
-        b2.d_tlim = tlim;
-        b2.d_out = o2;
-        rc = pb_cuda_align_exact(&b2);
+        for (int q = 0; q < nq && rc == 0; ++q) {
+            pb::k_prefix_limits<<<(n + 255) / 256, 256, 0, st>>>(*job, o1 + (size_t)q * n, n, qlim, tlim);
+            pb_diag_count_launch(1);
+            cudaStreamSynchronize(st);
+            pb_batch b2 = *tmpl;
+            if (tmpl->nprofs > 0) { b2.profs = &tmpl->profs[q]; b2.nprofs = 1; }
+            b2.stats = 1;
+            b2.pad_rows = 32;
+            b2.d_qlim = qlim;
+            b2.d_tlim = tlim;
+            b2.d_out = o2 + (size_t)q * n;
+            rc = pb_cuda_align_exact(&b2);
+        }
     }
-    if (rc == 0) {
-        const int qall = tmpl->nprofs > 0 ? tmpl->profs[0]->qlen : 0;
-        pb::launch_resolve(*job, o1, o2, tmpl->nprofs > 0 ? nullptr : tmpl->d_qlen, qall,
-                           tmpl->d_tlen, n, d_rec, st);
+    for (int q = 0; q < nq && rc == 0; ++q) {
+        const int qall = tmpl->nprofs > 0 ? tmpl->profs[q]->qlen : 0;
+        pb::launch_resolve(*job, o1 + (size_t)q * n, o2 ? o2 + (size_t)q * n : nullptr,
+                           tmpl->nprofs > 0 ? nullptr : tmpl->d_qlen, qall, tmpl->d_tlen, n,
+                           d_rec + (size_t)q * n, st);
         pb_diag_count_launch(1);
         if (cudaGetLastError() != cudaSuccess) rc = -1;
     }
@@ -146,11 +157,12 @@ extern "C" int pb_cuda_batch_host(const pb_job *job, const pb_batch *tmpl, const
     int *d_tlen = nullptr, *d_qlen = nullptr;
     pb_record *d_rec = nullptr;
     int rc = 0;
+    const int nq = tmpl->nprofs > 0 ? tmpl->nprofs : 1;
     cudaMallocAsync((void **)&d_t, tbytes + 16, st);
     cudaMallocAsync((void **)&d_toff, sizeof(int64_t) * n, st);
     cudaMallocAsync((void **)&d_tlen, sizeof(int) * n, st);
     cudaMallocAsync((void **)&d_map, 256, st);
-    cudaMallocAsync((void **)&d_rec, sizeof(pb_record) * n, st);
+    cudaMallocAsync((void **)&d_rec, sizeof(pb_record) * n * (size_t)nq, st);
     cudaMemcpyAsync(d_t, h_targets, tbytes, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(d_toff, h_toff, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(d_tlen, h_tlen, sizeof(int) * n, cudaMemcpyHostToDevice, st);
@@ -175,7 +187,7 @@ extern "C" int pb_cuda_batch_host(const pb_job *job, const pb_batch *tmpl, const
         if (h_queries) { b.d_qall = d_q; b.d_qoff = d_qoff; b.d_qlen = d_qlen; }
         rc = pb_cuda_batch_run(job, &b, d_rec);
     }
-    if (rc == 0 && cudaMemcpyAsync(h_rec, d_rec, sizeof(pb_record) * n, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    if (rc == 0 && cudaMemcpyAsync(h_rec, d_rec, sizeof(pb_record) * n * (size_t)nq, cudaMemcpyDeviceToHost, st) != cudaSuccess)
         rc = -1;
     cudaFreeAsync(d_t, st); cudaFreeAsync(d_toff, st); cudaFreeAsync(d_tlen, st);
     cudaFreeAsync(d_map, st); cudaFreeAsync(d_rec, st);

@@ -115,6 +115,9 @@ int pb_cuda_align_exact(const pb_batch *b);
  * PB_ST_OVERFLOW16 and must be rerun with pb_cuda_align_exact. Only
  * score/end_query/end_ref/max_h/status are written. */
 int pb_cuda_align_sw16(const pb_batch *b);
+/* The same for nprofs queries against the same targets in one launch;
+ * d_out_all[q * npairs + i]. */
+int pb_cuda_align_sw16_multi(const pb_batch *b, pb_pair_out *d_out_all);
 
 /* parasail_nw_banded for one pair: the reference's band recurrence
  * (src/nw_banded.c) on the GPU; h_s2 holds mapped target codes. */

@@ -41,16 +41,28 @@ struct ExactParams {
     const int *qlen;
 };
 
+struct Sw16Query {
+    int prof_off;            /* byte offset of the query's int8 profile in shared memory */
+    int qlen, lp, posmax;
+};
+
+struct Sw16Task {
+    int q;                   /* query index */
+    int first;               /* first position in the length-sorted target order */
+};
+
 struct Sw16Params {
-    int open, gap, npairs, posmax;
-    const ProfDesc *profs;
-    const int *order;        /* pair ids sorted by target length (desc) */
+    int open, gap, npairs, nq, ntasks, maxlen;
+    const Sw16Query *queries;
+    const int8_t *prof_all;  /* concatenated [size][lp] int8 profiles */
+    int prof_bytes;
+    const int *order;        /* target ids sorted by length (desc) */
+    const Sw16Task *tasks;   /* most cells first */
     const uint8_t *targets;
     const int64_t *toff;
     const int *tlen;
-    uint32_t *scratch;       /* per warp: [maxlen][32] x 2 words */
-    const int64_t *woff;     /* per warp scratch offset (words) */
-    pb_pair_out *out;
+    uint32_t *scratch;       /* per resident warp: [maxlen][32] uint2 */
+    pb_pair_out *out;        /* [nq][npairs] */
 };
 
 void launch_exact(const ExactParams &p, int alg, bool stats, cudaStream_t st);

@@ -116,13 +116,15 @@ PB_HD static inline int pb_resolve_tier(const pb_mode *m, int bits, const pb_pai
         }
         return PB_CLEAN;
     }
-    /* striped NW/SG. Without stats the first-pass E and F are range-checked
-     * too, so an unflagged result is always exact and a true value outside
-     * the limits is always flagged. With stats only H is checked while the
-     * first-pass F of every stripe starts at NEG_LIMIT, which can lift an
-     * underflowing H back into range unflagged (the reference then returns a
-     * wrong score): such pairs are left to the lane-exact kernel. */
-    if (!m->stats && (max_h > pos || min_h < neg)) return PB_SAT;
+    /* striped NW/SG. The first pass starts every stripe's F at NEG_LIMIT,
+     * which lifts an underflowing H back into range; the E and F checks of
+     * the non-stats kernels usually catch it one step later, but not when a
+     * stripe has a single segment and the low cell sits in the last column,
+     * and the stats kernels do not check E and F at all (the reference then
+     * returns a wrong, unflagged score). Only an overflowing maximum is a
+     * certain flag; pairs with values near NEG_LIMIT go to the lane-exact
+     * kernel. */
+    if (max_h > pos) return PB_SAT;
     if (!m->stats && boundary_h(m, (int)padlen - 1, 0) - m->open < neg) {
         /* column 0 loads E = H(i,-1) - open for every row of the layout
          * (src/nw_striped_avx2_256_16.c:243-258), and E is range-checked */
@@ -193,12 +195,22 @@ PB_HD static inline int pb_needs_pass2(const pb_job *j, const pb_pair_out *o1)
     return 0;
 }
 
-/* Interim rule for PB_AMBIG: the scan-style check on the exact values. */
-PB_HD static inline int pb_ambig_fallback(const pb_mode *m, int bits, const pb_pair_out *o)
+/* Rule for PB_AMBIG pairs when the lane-exact kernel is not run: the
+ * width's check evaluated on the exact final values. */
+PB_HD static inline int pb_ambig_fallback(const pb_mode *m, int bits, const pb_pair_out *o,
+                                          int qlim, int tlim)
 {
-    pb_mode s = *m;
-    s.striped = 0;
-    return pb_resolve_tier(&s, bits, o, 0x7fffffff, 0x7fffffff) == PB_SAT ? PB_SAT : PB_CLEAN;
+    if (m->alg == PB_SW && m->stats && m->striped) {
+        int64_t st = o->max_stat_real;
+        int k;
+        for (k = 0; k < pad_regions(bits); ++k) if (o->max_stat_pad[k] > st) st = o->max_stat_pad[k];
+        return st >= int_max_w(bits) - int_min_w(bits) ? PB_SAT : PB_CLEAN;
+    }
+    {
+        pb_mode s = *m;
+        s.striped = 0;
+        return pb_resolve_tier(&s, bits, o, qlim, tlim) == PB_SAT ? PB_SAT : PB_CLEAN;
+    }
 }
 
 /* The result the reference returns for one pair (src/satcheck.c chains,
@@ -233,7 +245,7 @@ PB_HD static inline pb_record pb_chain_resolve(const pb_job *j, const pb_pair_ou
                 return r;
             }
             v = pb_resolve_tier(m, w, o2, o1->end_query + 1, o1->end_ref + 1);
-            if (v == PB_AMBIG) { r.ambig++; v = pb_ambig_fallback(m, w, o2); }
+            if (v == PB_AMBIG) { r.ambig++; v = pb_ambig_fallback(m, w, o2, o1->end_query + 1, o1->end_ref + 1); }
             if (v == PB_SAT) {
                 if (t < l) continue;
                 r.end_query = o1->end_query; r.end_ref = o1->end_ref;
@@ -246,7 +258,7 @@ PB_HD static inline pb_record pb_chain_resolve(const pb_job *j, const pb_pair_ou
             return r;
         }
         v = pb_resolve_tier(m, w, o1, qlen, tlen);
-        if (v == PB_AMBIG) { r.ambig++; v = pb_ambig_fallback(m, w, o1); }
+        if (v == PB_AMBIG) { r.ambig++; v = pb_ambig_fallback(m, w, o1, qlen, tlen); }
         if (v == PB_SAT) {
             if (t < l) continue;
             if (m->alg == PB_SW && m->striped && !m->stats)

@@ -1,17 +1,22 @@
 /*
  * pb_sw16.cu -- Smith-Waterman score-only kernel in packed int16x2 lanes.
  *
- * Inter-task schedule: every thread aligns TWO targets against the same query
- * at once, one per 16-bit half of each register (targets are sorted by
- * length so the two halves, and the 32 threads of a warp, run similar
- * lengths). The query is processed in strips of R rows held in registers;
- * each strip sweeps the targets' columns and hands its bottom row (H and the
- * vertical-gap value F) to the next strip through a per-warp buffer laid out
- * [column][lane] so that every access of a warp is one contiguous 256-byte
- * transaction. The int8 query profile lives in shared memory; a column's R
- * scores for both targets are two 16-byte loads expanded to R int16x2 words
- * by sign-extending byte permutes. The recurrence uses the Hopper/Blackwell
- * DPX instructions (viaddmax, vimax3, vibmax).
+ * Inter-task schedule: every thread aligns one query/target pair; a warp
+ * takes 32 targets of similar length (targets are sorted by length) against
+ * one query, and a persistent grid pulls such tasks for all queries of the
+ * batch, longest first. The query is processed in passes of 2 x 16 rows:
+ * the low 16-bit half of every register holds strip A (rows r0..r0+15) at
+ * target column j, the high half strip B (rows r0+16..r0+31) at column j-1,
+ * so strip B reads strip A's bottom row from the previous iteration and both
+ * halves of one DPX instruction always do useful, independent work. A pass
+ * hands its bottom row (H and the vertical-gap value F) to the next pass
+ * through a per-warp buffer laid out [column][lane]: one contiguous
+ * 256-byte transaction per warp access. The int8 query profiles of all the
+ * batch's queries live in shared memory; a column's 16 + 16 scores are two
+ * 16-byte loads expanded to int16x2 words by sign-extending byte permutes.
+ * The recurrence is written so that only two DPX operations per row sit on
+ * the column's dependency chain (F = viaddmax(H_up, -open, F_up - gap) and
+ * H = max(A, F), with A = max(H_diag + s, E, 0) computed off the chain).
  *
  * Semantics: the Smith-Waterman recurrence of the reference's striped/scan
  * kernels and of src/sw.c:131-158, with its end-position rule (first column
@@ -33,9 +38,12 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
+#include <algorithm>
+#include <vector>
+
 namespace pb {
 
-static constexpr int SW16_R = 16;          /* query rows per strip */
+static constexpr int SW16_R = 16;          /* query rows per strip (two strips per pass) */
 static constexpr int SW16_WARPS = 8;       /* warps per block */
 
 /* Packs two signed bytes (byte k of a and of b) into one int16x2 word:
@@ -49,7 +57,13 @@ __device__ __forceinline__ uint32_t pack_pair(uint32_t a, uint32_t b)
     return d;
 }
 
-__device__ __forceinline__ uint32_t lo16(uint32_t x) { return x & 0xffffu; }
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel)
+{
+    uint32_t d;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
+    return d;
+}
+
 __device__ __forceinline__ int s16lo(uint32_t x) { return (int)(int16_t)(x & 0xffffu); }
 __device__ __forceinline__ int s16hi(uint32_t x) { return (int)(int16_t)(x >> 16); }
 __device__ __forceinline__ uint32_t splat16(int v) { return ((uint32_t)(uint16_t)v) | ((uint32_t)(uint16_t)v << 16); }
@@ -58,69 +72,81 @@ struct Sw16Best {
     int score, i, j;
 };
 
-/*
- * One warp task = 64 consecutive pairs of the length-sorted order; lane l
- * takes sorted positions 2l (low half) and 2l+1 (high half).
- */
-__global__ void __launch_bounds__(SW16_WARPS * 32)
-k_sw16(Sw16Params p, int ntasks, int *task_counter)
+__device__ __forceinline__ void fold_best(Sw16Best &best, bool &have, const Sw16Best &s)
+{
+    /* higher score, then smaller column; an equal column keeps the earlier
+     * (smaller) row, which was folded first */
+    if (s.j >= 0 && (!have || s.score > best.score || (s.score == best.score && s.j < best.j))) {
+        best = s;
+        have = true;
+    }
+}
+
+__global__ void __launch_bounds__(SW16_WARPS * 32, 2)
+k_sw16(Sw16Params p, int *task_counter)
 {
     extern __shared__ __align__(16) int8_t s_prof[];
-    const ProfDesc pd = p.profs[0];
-    const int lp = pd.lp;
-    const int size = pd.size;
-    const int ql = pd.qlen;
-    /* whole int8 profile into shared memory, 16 bytes per thread-step */
     {
-        const int4 *src = reinterpret_cast<const int4 *>(pd.prof8);
+        const int4 *src = reinterpret_cast<const int4 *>(p.prof_all);
         int4 *dst = reinterpret_cast<int4 *>(s_prof);
-        const int n16 = size * lp / 16;
+        const int n16 = p.prof_bytes / 16;
         for (int k = threadIdx.x; k < n16; k += blockDim.x) dst[k] = src[k];
     }
     __syncthreads();
 
     const int lane = threadIdx.x & 31;
+    const int slot = blockIdx.x * SW16_WARPS + (threadIdx.x >> 5);
+    uint2 *buf = reinterpret_cast<uint2 *>(p.scratch) + (size_t)slot * p.maxlen * 32;
     const uint32_t gapO = splat16(-p.open);
     const uint32_t gapE = splat16(-p.gap);
-    const int posmax = p.posmax;       /* H + max(matrix) must stay <= 32767 */
 
     for (;;) {
         int task = 0;
         if (lane == 0) task = atomicAdd(task_counter, 1);
         task = __shfl_sync(0xffffffffu, task, 0);
-        if (task >= ntasks) break;
-
-        const int s0 = task * 64 + 2 * lane, s1 = s0 + 1;
-        const bool v0 = s0 < p.npairs, v1 = s1 < p.npairs;
-        const int pa = v0 ? p.order[s0] : -1, pbid = v1 ? p.order[s1] : -1;
-        const int la = v0 ? p.tlen[pa] : 0, lb = v1 ? p.tlen[pbid] : 0;
-        const uint8_t *ta = v0 ? p.targets + p.toff[pa] : nullptr;
-        const uint8_t *tb = v1 ? p.targets + p.toff[pbid] : nullptr;
-        int wmax = max(la, lb);
+        if (task >= p.ntasks) break;
+        const Sw16Task T = p.tasks[task];
+        const Sw16Query Q = p.queries[T.q];
+        const int s = T.first + lane;
+        const bool valid = s < p.npairs;
+        const int pid = valid ? p.order[s] : 0;
+        const int len = valid ? p.tlen[pid] : 0;
+        const uint8_t *tseq = p.targets + (valid ? p.toff[pid] : 0);
+        int wmax = len;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) wmax = max(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
-        uint2 *buf = reinterpret_cast<uint2 *>(p.scratch + p.woff[task]);
+        const int8_t *prof = s_prof + Q.prof_off;
+        const int lp = Q.lp, ql = Q.qlen;
 
-        Sw16Best ba = {0, ql, la}, bb = {0, ql, lb};
-        bool have_a = false, have_b = false;
-        int status_a = 0, status_b = 0;
+        Sw16Best best = {0, 0, 0};
+        bool have = false;
+        int status = 0;
 
-        for (int r0 = 0; r0 < ql; r0 += SW16_R) {
+        for (int r0 = 0; r0 < ql; r0 += 2 * SW16_R) {
             uint32_t H[SW16_R], E[SW16_R];
 #pragma unroll
             for (int r = 0; r < SW16_R; ++r) { H[r] = 0u; E[r] = gapO; }
-            uint32_t dg = 0u;                 /* H(r0-1, j-1) */
-            Sw16Best sa = {0, -1, -1}, sb = {0, -1, -1};   /* strip-local first max */
+            uint32_t dg = 0u;               /* lo: H(r0-1, j-1); hi: H(r0+15, j-2) */
+            uint32_t prev_h = 0u, prev_f = gapO;   /* lo halves: strip A bottom at j-1 */
+            Sw16Best sa = {0, -1, -1}, sb = {0, -1, -1};
             uint32_t sbest = 0u;
-            const int8_t *prow_base = s_prof + r0;
-            for (int j = 0; j < wmax; ++j) {
-                const int ca = j < la ? ta[j] : 0;
-                const int cb = j < lb ? tb[j] : 0;
+            int cb = 0;                     /* residue of column j-1 (strip B) */
+            const int8_t *pa_base = prof + r0;
+            const int8_t *pb_base = prof + r0 + SW16_R;
+            const bool more = r0 + 2 * SW16_R < ql;
+            for (int j = 0; j <= wmax; ++j) {
+                const int ca = j < len ? tseq[j] : 0;
                 uint32_t hu, fu;
-                if (r0 == 0) { hu = 0u; fu = gapO; }
-                else { const uint2 v = buf[(size_t)j * 32 + lane]; hu = v.x; fu = v.y; }
-                const uint4 pa4 = *reinterpret_cast<const uint4 *>(prow_base + (size_t)ca * lp);
-                const uint4 pb4 = *reinterpret_cast<const uint4 *>(prow_base + (size_t)cb * lp);
+                if (r0 == 0) {
+                    hu = prev_h << 16;                      /* top row H = 0 */
+                    fu = prmt(gapO, prev_f, 0x5410u);       /* top row F = -inf */
+                } else {
+                    const uint2 v = j < wmax ? buf[(size_t)j * 32 + lane] : make_uint2(0u, gapO);
+                    hu = prmt(v.x, prev_h, 0x5432u);        /* lo <- previous pass's strip B bottom */
+                    fu = prmt(v.y, prev_f, 0x5432u);
+                }
+                const uint4 pa4 = *reinterpret_cast<const uint4 *>(pa_base + (size_t)ca * lp);
+                const uint4 pb4 = *reinterpret_cast<const uint4 *>(pb_base + (size_t)cb * lp);
                 uint32_t hd = dg;
                 dg = hu;
                 uint32_t cmax = 0u;
@@ -135,71 +161,68 @@ k_sw16(Sw16Params p, int ntasks, int *task_counter)
                         case 2: sc = pack_pair<2>(wa, wb); break;
                         default: sc = pack_pair<3>(wa, wb); break;
                     }
-                    /* F: vertical gap from the row above, E: horizontal gap */
-                    const uint32_t ho_up = __vadd2(hu, gapO);
-                    const uint32_t f = __viaddmax_s16x2(fu, gapE, ho_up);
-                    const uint32_t ho_left = __vadd2(H[r], gapO);
-                    const uint32_t e = __viaddmax_s16x2(E[r], gapE, ho_left);
-                    const uint32_t h = __viaddmax_s16x2_relu(hd, sc, __vmaxs2(e, f));
+                    /* E(i,j) = max(E(i,j-1) - gap, H(i,j-1) - open): off the chain */
+                    const uint32_t e = __viaddmax_s16x2(E[r], gapE, __vadd2(H[r], gapO));
+                    const uint32_t a = __viaddmax_s16x2_relu(hd, sc, e);
+                    /* F(i,j) = max(H(i-1,j) - open, F(i-1,j) - gap): on the chain */
+                    const uint32_t f = __viaddmax_s16x2(hu, gapO, __vadd2(fu, gapE));
+                    const uint32_t h = __vmaxs2(a, f);
                     E[r] = e;
                     hd = H[r];
                     H[r] = h;
                     hu = h;
                     fu = f;
-                    cmax = __vmaxs2(cmax, h);
+                    if (r & 1) cmax = __vimax3_s16x2(cmax, H[r - 1], h);
                 }
-                if (r0 + SW16_R < ql) buf[(size_t)j * 32 + lane] = make_uint2(hu, fu);
-                /* strip-local first column reaching a new maximum */
+                if (j >= 1 && more) buf[(size_t)(j - 1) * 32 + lane] = make_uint2(hu, fu);
+                prev_h = hu;
+                prev_f = fu;
+                cb = ca;
+                if (j == 0) {
+                    /* the high half computed column -1: restore strip B's
+                     * left boundary (H = 0, E = -inf) */
+#pragma unroll
+                    for (int r = 0; r < SW16_R; ++r) {
+                        H[r] &= 0xffffu;
+                        E[r] = (E[r] & 0xffffu) | (gapO & 0xffff0000u);
+                    }
+                }
                 bool ge_lo, ge_hi;
                 (void)__vibmax_s16x2(sbest, cmax, &ge_hi, &ge_lo);
-                const bool up_a = !ge_lo && j < la, up_b = !ge_hi && j < lb;
+                const bool up_a = !ge_lo && j < len;
+                const bool up_b = !ge_hi && j >= 1 && j <= len;
                 if (up_a || up_b) {
                     if (up_a) {
                         const int c = s16lo(cmax);
-                        int rr = -1;
+                        int rr = 0;
 #pragma unroll
                         for (int r = SW16_R - 1; r >= 0; --r) if (s16lo(H[r]) == c) rr = r;
                         sa.score = c; sa.j = j; sa.i = r0 + rr;
-                        if (c >= posmax) status_a |= PB_ST_OVERFLOW16;
+                        if (c >= Q.posmax) status |= PB_ST_OVERFLOW16;
                     }
                     if (up_b) {
                         const int c = s16hi(cmax);
-                        int rr = -1;
+                        int rr = 0;
 #pragma unroll
                         for (int r = SW16_R - 1; r >= 0; --r) if (s16hi(H[r]) == c) rr = r;
-                        sb.score = c; sb.j = j; sb.i = r0 + rr;
-                        if (c >= posmax) status_b |= PB_ST_OVERFLOW16;
+                        sb.score = c; sb.j = j - 1; sb.i = r0 + SW16_R + rr;
+                        if (c >= Q.posmax) status |= PB_ST_OVERFLOW16;
                     }
                     sbest = (uint32_t)(uint16_t)sa.score | ((uint32_t)(uint16_t)sb.score << 16);
                 }
             }
-            /* fold the strip into the pair's best: higher score, then smaller
-             * column; an equal column keeps the earlier strip (smaller row) */
-            if (sa.j >= 0 && (!have_a || sa.score > ba.score || (sa.score == ba.score && sa.j < ba.j))) {
-                ba = sa; have_a = true;
-            }
-            if (sb.j >= 0 && (!have_b || sb.score > bb.score || (sb.score == bb.score && sb.j < bb.j))) {
-                bb = sb; have_b = true;
-            }
+            fold_best(best, have, sa);
+            fold_best(best, have, sb);
         }
         /* no positive cell: score 0 at (0, 0), the first cell (src/sw.c:150-158) */
-        if (v0) {
+        if (valid) {
             pb_pair_out o = {};
-            o.score = have_a ? ba.score : 0;
-            o.end_query = have_a ? ba.i : 0;
-            o.end_ref = have_a ? ba.j : 0;
+            o.score = have ? best.score : 0;
+            o.end_query = have ? best.i : 0;
+            o.end_ref = have ? best.j : 0;
             o.max_h = o.score;
-            o.status = status_a;
-            p.out[pa] = o;
-        }
-        if (v1) {
-            pb_pair_out o = {};
-            o.score = have_b ? bb.score : 0;
-            o.end_query = have_b ? bb.i : 0;
-            o.end_ref = have_b ? bb.j : 0;
-            o.max_h = o.score;
-            o.status = status_b;
-            p.out[pbid] = o;
+            o.status = status;
+            p.out[(size_t)T.q * p.npairs + pid] = o;
         }
     }
 }
@@ -212,13 +235,6 @@ __global__ void k_iota(int *v, int n)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) v[i] = i;
-}
-
-/* words of per-warp strip buffer: longest target of the task x 32 lanes x 2 */
-__global__ void k_task_sizes(const int *sorted_len, int npairs, int ntasks, int64_t *sz)
-{
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < ntasks) sz[t] = (int64_t)sorted_len[t * 64] * 64;
 }
 
 __global__ void k_collect_overflow(const pb_pair_out *out, int n, int *list, int *count,
@@ -242,90 +258,121 @@ __global__ void k_scatter(const pb_pair_out *src, const int *list, int n, pb_pai
 
 }  // namespace
 
-extern "C" int pb_cuda_align_sw16(const pb_batch *b)
+/* nq profiles against the same targets; out[q * npairs + i]. */
+extern "C" int pb_cuda_align_sw16_multi(const pb_batch *b, pb_pair_out *d_out_all)
 {
-    static thread_local char err[160];
-    (void)err;
     if (pb_cuda_init() != 0) return -1;
-    if (b->npairs <= 0) return 0;
-    const pb_device_profile *dp = b->profs[0];
-    if (b->alg != PB_SW || b->stats || b->nprofs != 1 || !dp->fits8 || b->d_qlim || b->d_tlim ||
-        b->open + b->gap > 30000) {
-        return pb_cuda_align_exact(b);   /* outside this kernel's domain: the exact kernel */
+    const int n = b->npairs, nq = b->nprofs;
+    if (n <= 0 || nq <= 0) return 0;
+    bool ok = b->alg == PB_SW && !b->stats && !b->d_qlim && !b->d_tlim && b->open + b->gap <= 30000;
+    size_t prof_bytes = 0;
+    for (int q = 0; q < nq && ok; ++q) {
+        const pb_device_profile *dp = b->profs[q];
+        ok = dp->fits8 && dp->size == b->profs[0]->size;
+        prof_bytes += (size_t)dp->size * dp->lp;
     }
-    const size_t smem = (size_t)dp->size * dp->lp;
-    if (smem > 200 * 1024) return pb_cuda_align_exact(b);
+    if (!ok || prof_bytes > 200 * 1024) {
+        /* outside this kernel's domain: the exact kernel, one profile at a time */
+        for (int q = 0; q < nq; ++q) {
+            pb_batch one = *b;
+            one.profs = &b->profs[q];
+            one.nprofs = 1;
+            one.d_out = d_out_all + (size_t)q * n;
+            if (pb_cuda_align_exact(&one) != 0) return -1;
+        }
+        return 0;
+    }
     cudaStream_t st = 0;
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-    const int n = b->npairs;
-    const int ntasks = (n + 63) / 64;
+    int rc = 0;
+    /* targets sorted by length, descending */
     int *keys_sorted = nullptr, *idx = nullptr, *order = nullptr, *counter = nullptr;
-    int64_t *tsz = nullptr, *woff = nullptr;
     void *tmp = nullptr;
-    size_t tmp_sort = 0, tmp_scan = 0;
+    size_t tmp_sort = 0;
     cudaMallocAsync((void **)&keys_sorted, sizeof(int) * n, st);
     cudaMallocAsync((void **)&idx, sizeof(int) * n, st);
     cudaMallocAsync((void **)&order, sizeof(int) * n, st);
-    cudaMallocAsync((void **)&tsz, sizeof(int64_t) * ntasks, st);
-    cudaMallocAsync((void **)&woff, sizeof(int64_t) * ntasks, st);
     cudaMallocAsync((void **)&counter, sizeof(int) * 2, st);
     k_iota<<<(n + 255) / 256, 256, 0, st>>>(idx, n);
     cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_sort, b->d_tlen, keys_sorted, idx, order, n, 0, 32, st);
-    cub::DeviceScan::ExclusiveSum(nullptr, tmp_scan, tsz, woff, ntasks, st);
-    cudaMallocAsync(&tmp, tmp_sort > tmp_scan ? tmp_sort : tmp_scan, st);
+    cudaMallocAsync(&tmp, tmp_sort, st);
     cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_sort, b->d_tlen, keys_sorted, idx, order, n, 0, 32, st);
-    k_task_sizes<<<(ntasks + 255) / 256, 256, 0, st>>>(keys_sorted, n, ntasks, tsz);
-    cub::DeviceScan::ExclusiveSum(tmp, tmp_scan, tsz, woff, ntasks, st);
-    int64_t last_off = 0, last_sz = 0;
-    cudaMemcpyAsync(&last_off, woff + ntasks - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(&last_sz, tsz + ntasks - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+    std::vector<int> hlen(n);
+    cudaMemcpyAsync(hlen.data(), keys_sorted, sizeof(int) * n, cudaMemcpyDeviceToHost, st);
     cudaMemsetAsync(counter, 0, sizeof(int) * 2, st);
-    cudaStreamSynchronize(st);
-    uint32_t *scratch = nullptr;
-    if (cudaMallocAsync((void **)&scratch, sizeof(uint32_t) * (size_t)(last_off + last_sz + 64), st) != cudaSuccess) {
-        cudaStreamDestroy(st);
-        return -1;
+    /* concatenated int8 profiles */
+    std::vector<pb::Sw16Query> hq(nq);
+    int8_t *prof_all = nullptr;
+    cudaMallocAsync((void **)&prof_all, prof_bytes, st);
+    {
+        size_t off = 0;
+        for (int q = 0; q < nq; ++q) {
+            const pb_device_profile *dp = b->profs[q];
+            const size_t bytes = (size_t)dp->size * dp->lp;
+            cudaMemcpyAsync(prof_all + off, dp->d_prof8, bytes, cudaMemcpyDeviceToDevice, st);
+            hq[q].prof_off = (int)off;
+            hq[q].qlen = dp->qlen;
+            hq[q].lp = dp->lp;
+            hq[q].posmax = 32767 - dp->mmax - 1;
+            off += bytes;
+        }
     }
-    pb::ProfDesc hd;
-    hd.prof = dp->d_prof32; hd.prof8 = dp->d_prof8; hd.qcodes = dp->d_qcodes;
-    hd.qlen = dp->qlen; hd.lp = dp->lp; hd.size = dp->size; hd.pad_ = 0;
-    pb::ProfDesc *d_pd = nullptr;
-    cudaMallocAsync((void **)&d_pd, sizeof hd, st);
-    cudaMemcpyAsync(d_pd, &hd, sizeof hd, cudaMemcpyHostToDevice, st);
+    cudaStreamSynchronize(st);
+    /* tasks: (query, block of 32 sorted targets), most cells first */
+    const int nblk = (n + 31) / 32;
+    std::vector<pb::Sw16Task> tasks((size_t)nq * nblk);
+    std::vector<int64_t> cost((size_t)nq * nblk);
+    for (int q = 0; q < nq; ++q)
+        for (int k = 0; k < nblk; ++k) {
+            tasks[(size_t)q * nblk + k].q = q;
+            tasks[(size_t)q * nblk + k].first = 32 * k;
+        }
+    std::vector<int> perm(tasks.size());
+    for (size_t k = 0; k < perm.size(); ++k) perm[k] = (int)k;
+    std::sort(perm.begin(), perm.end(), [&](int x, int y) {
+        const int64_t cx = (int64_t)hq[tasks[x].q].qlen * hlen[tasks[x].first];
+        const int64_t cy = (int64_t)hq[tasks[y].q].qlen * hlen[tasks[y].first];
+        return cx > cy;
+    });
+    std::vector<pb::Sw16Task> sorted_tasks(tasks.size());
+    for (size_t k = 0; k < perm.size(); ++k) sorted_tasks[k] = tasks[perm[k]];
+    pb::Sw16Task *d_tasks = nullptr;
+    pb::Sw16Query *d_q = nullptr;
+    cudaMallocAsync((void **)&d_tasks, sizeof(pb::Sw16Task) * sorted_tasks.size(), st);
+    cudaMallocAsync((void **)&d_q, sizeof(pb::Sw16Query) * nq, st);
+    cudaMemcpyAsync(d_tasks, sorted_tasks.data(), sizeof(pb::Sw16Task) * sorted_tasks.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_q, hq.data(), sizeof(pb::Sw16Query) * nq, cudaMemcpyHostToDevice, st);
 
-    pb::Sw16Params p;
-    p.open = b->open; p.gap = b->gap; p.npairs = n;
-    p.posmax = 32767 - dp->mmax - 1;
-    p.profs = d_pd; p.order = order;
-    p.targets = b->d_targets; p.toff = b->d_toff; p.tlen = b->d_tlen;
-    p.scratch = scratch; p.woff = woff; p.out = b->d_out;
-    cudaFuncSetAttribute(pb::k_sw16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0, nsm = 0, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pb::k_sw16, pb::SW16_WARPS * 32, smem);
+    cudaFuncSetAttribute(pb::k_sw16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prof_bytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pb::k_sw16, pb::SW16_WARPS * 32, prof_bytes);
     if (per_sm < 1) per_sm = 1;
     int blocks = per_sm * nsm;
-    const int need = (ntasks + pb::SW16_WARPS - 1) / pb::SW16_WARPS;
+    const int need = (int)((sorted_tasks.size() + pb::SW16_WARPS - 1) / pb::SW16_WARPS);
     if (blocks > need) blocks = need;
+    const int maxlen = hlen[0] + 1;
+    uint32_t *scratch = nullptr;
+    if (cudaMallocAsync((void **)&scratch, sizeof(uint2) * (size_t)maxlen * 32 * blocks * pb::SW16_WARPS, st) != cudaSuccess) {
+        cudaStreamDestroy(st);
+        return -1;
+    }
+    pb::Sw16Params p;
+    p.open = b->open; p.gap = b->gap; p.npairs = n; p.nq = nq;
+    p.ntasks = (int)sorted_tasks.size(); p.maxlen = maxlen;
+    p.queries = d_q; p.prof_all = prof_all; p.prof_bytes = (int)prof_bytes;
+    p.order = order; p.tasks = d_tasks;
+    p.targets = b->d_targets; p.toff = b->d_toff; p.tlen = b->d_tlen;
+    p.scratch = scratch; p.out = d_out_all;
     cudaEvent_t ev0, ev1;
     cudaEventCreate(&ev0);
     cudaEventCreate(&ev1);
     cudaEventRecord(ev0, st);
-    pb::k_sw16<<<blocks, pb::SW16_WARPS * 32, smem, st>>>(p, ntasks, counter);
+    pb::k_sw16<<<blocks, pb::SW16_WARPS * 32, prof_bytes, st>>>(p, counter);
     cudaEventRecord(ev1, st);
-    cudaError_t e = cudaGetLastError();
-    pb_diag_count_launch(4);   /* k_iota, k_task_sizes, k_sw16, k_collect_overflow */
-
-    /* pairs that left the 16-bit range: the exact kernel */
-    int *list = nullptr, *otlen = nullptr, nover = 0;
-    int64_t *otoff = nullptr;
-    cudaMallocAsync((void **)&list, sizeof(int) * n, st);
-    cudaMallocAsync((void **)&otlen, sizeof(int) * n, st);
-    cudaMallocAsync((void **)&otoff, sizeof(int64_t) * n, st);
-    k_collect_overflow<<<(n + 255) / 256, 256, 0, st>>>(b->d_out, n, list, counter + 1, b->d_toff,
-                                                        b->d_tlen, otoff, otlen);
-    cudaMemcpyAsync(&nover, counter + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaGetLastError() != cudaSuccess) rc = -1;
+    pb_diag_count_launch(2);   /* k_iota, k_sw16 */
     cudaStreamSynchronize(st);
     {
         float ms = 0.f;
@@ -334,27 +381,50 @@ extern "C" int pb_cuda_align_sw16(const pb_batch *b)
         cudaEventDestroy(ev0);
         cudaEventDestroy(ev1);
     }
-    int rc = (e == cudaSuccess) ? 0 : -1;
-    if (rc == 0 && nover > 0) {
-        pb_pair_out *tmpo = nullptr;
-        cudaMallocAsync((void **)&tmpo, sizeof(pb_pair_out) * nover, st);
-        cudaStreamSynchronize(st);
-        pb_batch sub = *b;
-        sub.npairs = nover;
-        sub.d_toff = otoff;
-        sub.d_tlen = otlen;
-        sub.d_out = tmpo;
-        sub.d_prof_index = nullptr;
-        rc = pb_cuda_align_exact(&sub);
-        k_scatter<<<(nover + 255) / 256, 256, 0, st>>>(tmpo, list, nover, b->d_out);
+    /* pairs that left the 16-bit range: the exact kernel, per query */
+    int *list = nullptr, *otlen = nullptr;
+    int64_t *otoff = nullptr;
+    cudaMallocAsync((void **)&list, sizeof(int) * n, st);
+    cudaMallocAsync((void **)&otlen, sizeof(int) * n, st);
+    cudaMallocAsync((void **)&otoff, sizeof(int64_t) * n, st);
+    for (int q = 0; q < nq && rc == 0; ++q) {
+        int nover = 0;
+        pb_pair_out *oq = d_out_all + (size_t)q * n;
+        cudaMemsetAsync(counter + 1, 0, sizeof(int), st);
+        k_collect_overflow<<<(n + 255) / 256, 256, 0, st>>>(oq, n, list, counter + 1, b->d_toff,
+                                                            b->d_tlen, otoff, otlen);
         pb_diag_count_launch(1);
-        cudaFreeAsync(tmpo, st);
+        cudaMemcpyAsync(&nover, counter + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        if (nover > 0) {
+            pb_pair_out *tmpo = nullptr;
+            cudaMallocAsync((void **)&tmpo, sizeof(pb_pair_out) * nover, st);
+            cudaStreamSynchronize(st);
+            pb_batch sub = *b;
+            sub.profs = &b->profs[q];
+            sub.nprofs = 1;
+            sub.npairs = nover;
+            sub.d_toff = otoff;
+            sub.d_tlen = otlen;
+            sub.d_out = tmpo;
+            sub.d_prof_index = nullptr;
+            rc = pb_cuda_align_exact(&sub);
+            k_scatter<<<(nover + 255) / 256, 256, 0, st>>>(tmpo, list, nover, oq);
+            pb_diag_count_launch(1);
+            cudaFreeAsync(tmpo, st);
+        }
     }
     cudaFreeAsync(list, st); cudaFreeAsync(otlen, st); cudaFreeAsync(otoff, st);
-    cudaFreeAsync(scratch, st); cudaFreeAsync(d_pd, st); cudaFreeAsync(tmp, st);
+    cudaFreeAsync(scratch, st); cudaFreeAsync(prof_all, st); cudaFreeAsync(tmp, st);
     cudaFreeAsync(keys_sorted, st); cudaFreeAsync(idx, st); cudaFreeAsync(order, st);
-    cudaFreeAsync(tsz, st); cudaFreeAsync(woff, st); cudaFreeAsync(counter, st);
+    cudaFreeAsync(counter, st); cudaFreeAsync(d_tasks, st); cudaFreeAsync(d_q, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
     cudaStreamDestroy(st);
     return rc;
+}
+
+extern "C" int pb_cuda_align_sw16(const pb_batch *b)
+{
+    if (b->nprofs != 1 || b->d_prof_index) return pb_cuda_align_exact(b);
+    return pb_cuda_align_sw16_multi(b, b->d_out);
 }

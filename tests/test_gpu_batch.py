@@ -119,3 +119,20 @@ def test_faststats_batch_vs_oracle():
     exp = _oracle_batch(O.SW, 0, 1, q, targets, 11, 1, _b62())
     for r, e in zip(recs, exp):
         assert (r["score"], r["end_query"], r["end_ref"], r["matches"], r["similar"], r["length"]) == e
+
+
+def test_db_batch_matches_single_query_batches():
+    rng = random.Random(17)
+    b62 = pb.matrix_lookup("blosum62")
+    queries = [rand_seq(rng, L, AA) for L in (5, 40, 100, 250, 777)]
+    targets = [rand_seq(rng, rng.randint(1, 900), AA) for _ in range(500)]
+    targets += [mutate(rng, q, AA, 0.3, 0.02) for q in queries]
+    profs = [pb.ProfileHandle("parasail_profile_create_sat", q, b62) for q in queries]
+    db = pb.batch_db("sw_striped_profile_sat", profs, targets, 11, 1)
+    for k, p in enumerate(profs):
+        one = pb.batch_profile("sw_striped_profile_sat", p, targets, 11, 1)
+        assert (db[k] == one).all()
+        exp = _oracle_batch(O.SW, 0, 0, queries[k], targets, 11, 1, _b62())
+        assert [(int(r["score"]), int(r["end_query"]), int(r["end_ref"])) for r in one] == [e[:3] for e in exp]
+    for p in profs:
+        p.close()
