@@ -132,6 +132,49 @@ def cpu_baseline(queries, buf, offs, lens, target_seconds):
             "ntargets": nt, "checksum": chk, "saturated_32": nsat}, None
 
 
+def learned_band_leg(pb, n_train=2000, n_test=300, epochs=40):
+    """Config-5 leg: long DNA pairs (5-50 kbp, 1-15% divergence, a large
+    indel in 30%), +1/-2, open 4, extend 1. Plain full-DP global alignment
+    vs the learned band (features + MLP + banded DP + certificate + full-DP
+    fallback), both through the host API, scores compared pair by pair."""
+    import numpy as np
+    import torch
+    from parasail_b200 import synth
+    dna = pb.matrix_create("ACGT", 1, -2)
+    tr = synth.dna_long_pairs(seed=101, n_pairs=n_train)
+    te = synth.dna_long_pairs(seed=102, n_pairs=n_test)
+    model = pb.BandModel(seed=7)
+    t0 = time.time()
+    loss = model.train(dna, *tr[:6], 4, 1, epochs=epochs, batch=256, lr=2e-3)
+    train_s = time.time() - t0
+    cells = float((te[2].astype(np.int64) * te[5]).sum())
+    pb.nw_long(dna, *te[:6], 4, 1)                      # warm-up
+    model.align(dna, *te[:6], 4, 1, widen=1.1, slack=32)
+    torch.cuda.synchronize()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1) / 1e3
+
+    full, t_full = timed(lambda: pb.nw_long(dna, *te[:6], 4, 1))
+    (sc, lo, hi, st), t_band = timed(lambda: model.align(dna, *te[:6], 4, 1, widen=1.1, slack=32))
+    fb = (lo == -te[5] - 1) & (hi == te[2] + 1)
+    model.close()
+    return {"workload": "%d DNA pairs 5-50 kbp (1-15%% divergence, 30%% with a 50-500 bp indel), +1/-2, "
+                        "open 4, extend 1; model trained on %d separate pairs" % (n_test, n_train),
+            "full_dp": {"pairs_per_s": n_test / t_full, "GCUPS": cells / t_full / 1e9, "seconds": t_full},
+            "learned_band": {"pairs_per_s": n_test / t_band, "seconds": t_band,
+                             "certified": int(st.certified), "fallback": int(st.fallback),
+                             "band_cells_frac": (st.band_cells + float((te[2][fb].astype(np.int64) * te[5][fb]).sum())) / cells},
+            "speedup_pairs_per_s": t_full / t_band,
+            "scores_identical_to_full_dp": bool((sc == full).all()),
+            "train": {"pairs": n_train, "epochs": epochs, "final_loss": loss, "seconds": train_s}}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -262,6 +305,7 @@ def main():
         ours = int(sum(int(dev_rec[q][:nt, 0].astype(np.int64).sum()) for q in range(len(queries))))
         parity = {"pairs_checked": len(queries) * nt, "score_checksum_equal": ours == base["checksum"],
                   "device_and_host_api_equal": bool(same)}
+    lb = learned_band_leg(pb) if os.environ.get("PB_BENCH_SKIP_BAND") is None else None
     peak = pb.lib.parasail_b200_dpx_peak()
     kernel_ms_per_launch = sw16_ms / max(1, nk.value)
     cells_per_launch = cells
@@ -288,6 +332,7 @@ def main():
                          "peak": 6543.4, "unit": "GB/s", "note": "target bytes streamed per launch; of measured"},
         "cpu_baseline": base if base is not None else {"unavailable": why},
         "parity": parity,
+        "config5_learned_band": lb,
         "clocks": summarize_clocks(samples),
     }
     print(json.dumps(line))

@@ -84,6 +84,75 @@ extern int parasail_b200_batch_pairs(
         const char *targets, const int64_t *toffsets, const int *tlengths, int n,
         int open, int gap, parasail_b200_record_t *records);
 
+/* ---- long global alignments and the learned band ---------------------- */
+
+/** Global alignment score of each long pair (query i against target i),
+ * the value of the reference's parasail_nw_scan_profile_32 for the pair
+ * (src/nw_scan_avx2_256_32.c); one warp per pair on the GPU. Square matrix
+ * of at most 32 letters with |scores| <= 127. */
+extern int parasail_b200_nw_long(
+        const parasail_matrix_t *matrix,
+        const char *queries, const int64_t *qoffsets, const int *qlengths,
+        const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+        int open, int gap, int *scores);
+
+/** The learned-band model: a 258 -> 128 -> 128 -> 2 MLP (ReLU, BF16 weights,
+ * FP32 accumulation) mapping a pair's k = 8 diagonal-offset histogram (256
+ * bins) and both lengths to a band centre and half-width. */
+typedef struct parasail_b200_band_model parasail_b200_band_model_t;
+
+typedef struct parasail_b200_band_stats {
+    long long pairs;        /**< pairs aligned */
+    long long certified;    /**< pairs whose banded score passed the certificate */
+    long long fallback;     /**< pairs rerun on the full DP */
+    double band_cells;      /**< DP cells inside the predicted bands */
+} parasail_b200_band_stats_t;
+
+extern parasail_b200_band_model_t *parasail_b200_band_model_new(unsigned seed);
+extern void parasail_b200_band_model_free(parasail_b200_band_model_t *model);
+/** Sizes of the model: inputs, hidden units, outputs, weight and bias counts. */
+extern int parasail_b200_band_model_sizes(int *n_in, int *n_hidden, int *n_out, int *n_weights, int *n_biases);
+/** FP32 master weights (w1 [128][258] | w2 [128][128] | w3 [2][128]) and
+ * biases (b1 | b2 | b3), to or from host memory. */
+extern int parasail_b200_band_model_get(const parasail_b200_band_model_t *model, float *weights, float *biases);
+extern int parasail_b200_band_model_set(parasail_b200_band_model_t *model, const float *weights, const float *biases);
+/** Input features ([n][258]) of DNA pairs. */
+extern int parasail_b200_band_features(
+        const parasail_matrix_t *matrix,
+        const char *queries, const int64_t *qoffsets, const int *qlengths,
+        const char *targets, const int64_t *toffsets, const int *tlengths, int n, float *features);
+/** Gradients of the training loss over a batch of features/targets
+ * (squared error on the centre, pinball loss with quantile tau on the
+ * half-width), computed by the GPU backward kernels; for gradient checks. */
+extern int parasail_b200_band_model_gradients(
+        const parasail_b200_band_model_t *model, const float *x, const float *target, int n, float tau,
+        float *grad_weights, float *grad_biases, float *loss);
+/** Trains on the GPU with Adam: labels are the smallest certifiable band of
+ * each pair's optimal score from the full-DP kernel. */
+extern int parasail_b200_band_model_train(
+        parasail_b200_band_model_t *model, const parasail_matrix_t *matrix,
+        const char *queries, const int64_t *qoffsets, const int *qlengths,
+        const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+        int open, int gap, int epochs, int batch, float lr, float *final_loss);
+/** Global alignment scores through the learned band: predicted band
+ * (half-width scaled by `widen`, plus `slack` diagonals), banded DP,
+ * exactness certificate, full-DP fallback. scores[] always equals
+ * parasail_b200_nw_long's; band_lo/band_hi receive the bands used (the
+ * whole matrix for fallback pairs), either may be NULL. */
+extern int parasail_b200_nw_learned_band(
+        const parasail_b200_band_model_t *model, const parasail_matrix_t *matrix,
+        const char *queries, const int64_t *qoffsets, const int *qlengths,
+        const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+        int open, int gap, float widen, int slack,
+        int *scores, int *band_lo, int *band_hi, parasail_b200_band_stats_t *stats);
+/** Banded DP with caller-given bands and the certificate, no fallback:
+ * certified[i] = 1 when scores[i] is provably the full optimum. */
+extern int parasail_b200_nw_banded_certified(
+        const parasail_matrix_t *matrix,
+        const char *queries, const int64_t *qoffsets, const int *qlengths,
+        const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+        int open, int gap, const int *band_lo, const int *band_hi, int *scores, int *certified);
+
 /** Diagnostics: number of this library's kernel launches so far. */
 extern long parasail_b200_kernel_launches(void);
 /** Diagnostics: summed device time (ms) of the int16x2 Smith-Waterman score

@@ -105,6 +105,10 @@ def lib():
             ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int),
             ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int),
             ctypes.c_int, ctypes.c_int, ctypes.POINTER(OMatrix), ctypes.POINTER(OResult), ctypes.c_int]
+        _lib.oracle_nw_band.argtypes = [
+            ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+            ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(OMatrix),
+            ctypes.POINTER(ctypes.c_int64)]
         _lib.oracle_nw_diag_range.argtypes = [
             ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
             ctypes.c_int, ctypes.c_int, ctypes.POINTER(OMatrix), ctypes.POINTER(ctypes.c_int),
@@ -220,6 +224,15 @@ def align_batch(alg, sgflags, stats, queries, targets, open_, gap, m, nthreads=0
     if rc != 0:
         raise ValueError("oracle_align_batch rejected an input")
     return res
+
+
+def nw_band(q, t, open_, gap, lo, hi, m):
+    """Global score restricted to diagonals lo <= i - j <= hi."""
+    qc, tc = m.codes(q), m.codes(t)
+    out = ctypes.c_int64()
+    lib().oracle_nw_band(_ip(qc), len(qc), _ip(tc), len(tc), open_, gap, lo, hi, ctypes.byref(m._om),
+                         ctypes.byref(out))
+    return out.value
 
 
 def nw_diag_range(q, t, open_, gap, m):

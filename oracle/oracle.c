@@ -357,3 +357,48 @@ int oracle_nw_diag_range(const int *s1, int s1Len, const int *s2, int s2Len,
     free(fH); free(fE); free(fF); free(bH); free(bE); free(bF);
     return 0;
 }
+
+/* Global alignment restricted to the band of diagonals lo <= i - j <= hi
+ * (i, j: 1-based grid points, (0,0) the start): grid points outside the
+ * band, boundary points included, are unreachable. The full-matrix case
+ * (lo <= -s2Len, hi >= s1Len) equals oracle_align(ORACLE_NW). Used to check
+ * the learned-band kernels; the reference has no such function (its
+ * parasail_nw_banded, restated above, uses its own band layout). */
+int oracle_nw_band(const int *s1, int s1Len, const int *s2, int s2Len,
+                   int open, int gap, int lo, int hi, const oracle_matrix_t *m, int64_t *score)
+{
+    int64_t *H = malloc(sizeof(int64_t) * (s2Len + 1));
+    int64_t *F = malloc(sizeof(int64_t) * (s2Len + 1));
+    int i, j;
+    if (!H || !F) { free(H); free(F); return -1; }
+#define INB(a, b) ((a) - (b) >= lo && (a) - (b) <= hi)
+    H[0] = 0;
+    F[0] = NEG_INF;
+    for (j = 1; j <= s2Len; ++j) {
+        H[j] = INB(0, j) ? -(int64_t)open - (int64_t)(j - 1) * gap : NEG_INF;
+        F[j] = NEG_INF;
+    }
+    for (i = 1; i <= s1Len; ++i) {
+        int64_t NH = H[0];
+        int64_t WH = INB(i, 0) ? -(int64_t)open - (int64_t)(i - 1) * gap : NEG_INF;
+        int64_t E = NEG_INF;
+        H[0] = WH;
+        for (j = 1; j <= s2Len; ++j) {
+            int64_t NWH = NH, f, e, h;
+            NH = H[j];
+            f = MAX2(NH - open, F[j] - gap);
+            e = MAX2(WH - open, E - gap);
+            h = MAX2(NWH + subst(m, s1, i - 1, s2[j - 1]), MAX2(e, f));
+            if (!INB(i, j)) { h = NEG_INF; e = NEG_INF; f = NEG_INF; }
+            F[j] = f;
+            E = e;
+            WH = h;
+            H[j] = h;
+        }
+    }
+#undef INB
+    *score = H[s2Len];
+    free(H);
+    free(F);
+    return 0;
+}

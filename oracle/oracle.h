@@ -85,6 +85,10 @@ int oracle_nw_diag_range(const int *s1, int s1Len, const int *s2, int s2Len,
                          int open, int gap, const oracle_matrix_t *m,
                          int *dmin, int *dmax, int *score);
 
+/* Global alignment restricted to diagonals lo <= i - j <= hi. */
+int oracle_nw_band(const int *s1, int s1Len, const int *s2, int s2Len,
+                   int open, int gap, int lo, int hi, const oracle_matrix_t *m, int64_t *score);
+
 #ifdef __cplusplus
 }
 #endif

@@ -280,3 +280,139 @@ def batch_db(name, profiles, targets, open_, gap, packed=None):
     if rc != 0:
         raise RuntimeError("parasail_b200_batch_db failed")
     return recs.reshape(len(profiles), n)
+
+
+# ---------------------------------------------------------------------------
+# Long global alignments and the learned band
+
+class BandStats(ctypes.Structure):
+    _fields_ = [("pairs", ctypes.c_longlong), ("certified", ctypes.c_longlong),
+                ("fallback", ctypes.c_longlong), ("band_cells", ctypes.c_double)]
+
+
+_V = ctypes.c_void_p
+lib.parasail_b200_nw_long.restype = ctypes.c_int
+lib.parasail_b200_nw_long.argtypes = [_MP, _V, _V, _V, _V, _V, _V, ctypes.c_int, ctypes.c_int, ctypes.c_int, _V]
+lib.parasail_b200_band_model_new.restype = _V
+lib.parasail_b200_band_model_new.argtypes = [ctypes.c_uint]
+lib.parasail_b200_band_model_free.argtypes = [_V]
+lib.parasail_b200_band_model_sizes.argtypes = [ctypes.POINTER(ctypes.c_int)] * 5
+lib.parasail_b200_band_model_get.argtypes = [_V, _V, _V]
+lib.parasail_b200_band_model_set.argtypes = [_V, _V, _V]
+lib.parasail_b200_band_features.argtypes = [_MP, _V, _V, _V, _V, _V, _V, ctypes.c_int, _V]
+lib.parasail_b200_band_model_gradients.argtypes = [_V, _V, _V, ctypes.c_int, ctypes.c_float, _V, _V,
+                                                   ctypes.POINTER(ctypes.c_float)]
+lib.parasail_b200_band_model_train.argtypes = [_V, _MP, _V, _V, _V, _V, _V, _V, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                               ctypes.POINTER(ctypes.c_float)]
+lib.parasail_b200_nw_learned_band.argtypes = [_V, _MP, _V, _V, _V, _V, _V, _V, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_float, ctypes.c_int, _V, _V, _V,
+                                              ctypes.POINTER(BandStats)]
+lib.parasail_b200_nw_banded_certified.argtypes = [_MP, _V, _V, _V, _V, _V, _V, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_int, _V, _V, _V, _V]
+
+
+def _pairs_args(qbuf, qoff, qlen, tbuf, toff, tlen):
+    return (qbuf.ctypes.data, qoff.ctypes.data, qlen.ctypes.data, tbuf.ctypes.data, toff.ctypes.data,
+            tlen.ctypes.data)
+
+
+def nw_long(matrix, qbuf, qoff, qlen, tbuf, toff, tlen, open_, gap):
+    np = _np()
+    n = len(qlen)
+    out = np.zeros(n, dtype=np.int32)
+    rc = lib.parasail_b200_nw_long(matrix, *_pairs_args(qbuf, qoff, qlen, tbuf, toff, tlen), n, open_, gap,
+                                   out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("parasail_b200_nw_long failed")
+    return out
+
+
+class BandModel:
+    def __init__(self, seed=1):
+        self.ptr = lib.parasail_b200_band_model_new(seed)
+        if not self.ptr:
+            raise RuntimeError("parasail_b200_band_model_new failed")
+        v = [ctypes.c_int() for _ in range(5)]
+        lib.parasail_b200_band_model_sizes(*[ctypes.byref(x) for x in v])
+        self.n_in, self.n_hidden, self.n_out, self.n_weights, self.n_biases = [x.value for x in v]
+
+    def close(self):
+        if self.ptr:
+            lib.parasail_b200_band_model_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        self.close()
+
+    def get(self):
+        np = _np()
+        w = np.zeros(self.n_weights, np.float32)
+        b = np.zeros(self.n_biases, np.float32)
+        if lib.parasail_b200_band_model_get(self.ptr, w.ctypes.data, b.ctypes.data) != 0:
+            raise RuntimeError("get failed")
+        return w, b
+
+    def set(self, w, b):
+        np = _np()
+        w = np.ascontiguousarray(w, np.float32)
+        b = np.ascontiguousarray(b, np.float32)
+        if lib.parasail_b200_band_model_set(self.ptr, w.ctypes.data, b.ctypes.data) != 0:
+            raise RuntimeError("set failed")
+
+    def gradients(self, x, target, tau):
+        np = _np()
+        x = np.ascontiguousarray(x, np.float32)
+        target = np.ascontiguousarray(target, np.float32)
+        gw = np.zeros(self.n_weights, np.float32)
+        gb = np.zeros(self.n_biases, np.float32)
+        loss = ctypes.c_float()
+        rc = lib.parasail_b200_band_model_gradients(self.ptr, x.ctypes.data, target.ctypes.data, len(x), tau,
+                                                    gw.ctypes.data, gb.ctypes.data, ctypes.byref(loss))
+        if rc != 0:
+            raise RuntimeError("gradients failed")
+        return gw, gb, loss.value
+
+    def train(self, matrix, qbuf, qoff, qlen, tbuf, toff, tlen, open_, gap, epochs=30, batch=256, lr=1e-3):
+        loss = ctypes.c_float()
+        rc = lib.parasail_b200_band_model_train(self.ptr, matrix, *_pairs_args(qbuf, qoff, qlen, tbuf, toff, tlen),
+                                                len(qlen), open_, gap, epochs, batch, lr, ctypes.byref(loss))
+        if rc != 0:
+            raise RuntimeError("train failed")
+        return loss.value
+
+    def align(self, matrix, qbuf, qoff, qlen, tbuf, toff, tlen, open_, gap, widen=1.0, slack=32):
+        np = _np()
+        n = len(qlen)
+        sc, lo, hi = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.int32)
+        st = BandStats()
+        rc = lib.parasail_b200_nw_learned_band(self.ptr, matrix, *_pairs_args(qbuf, qoff, qlen, tbuf, toff, tlen),
+                                               n, open_, gap, widen, slack, sc.ctypes.data, lo.ctypes.data,
+                                               hi.ctypes.data, ctypes.byref(st))
+        if rc != 0:
+            raise RuntimeError("learned band failed")
+        return sc, lo, hi, st
+
+
+def band_features(matrix, qbuf, qoff, qlen, tbuf, toff, tlen, n_in=258):
+    np = _np()
+    n = len(qlen)
+    f = np.zeros((n, n_in), np.float32)
+    if lib.parasail_b200_band_features(matrix, *_pairs_args(qbuf, qoff, qlen, tbuf, toff, tlen), n,
+                                       f.ctypes.data) != 0:
+        raise RuntimeError("features failed")
+    return f
+
+
+def nw_banded_certified(matrix, qbuf, qoff, qlen, tbuf, toff, tlen, open_, gap, lo, hi):
+    np = _np()
+    n = len(qlen)
+    lo = np.ascontiguousarray(lo, np.int32)
+    hi = np.ascontiguousarray(hi, np.int32)
+    sc, cert = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    rc = lib.parasail_b200_nw_banded_certified(matrix, *_pairs_args(qbuf, qoff, qlen, tbuf, toff, tlen), n,
+                                               open_, gap, lo.ctypes.data, hi.ctypes.data, sc.ctypes.data,
+                                               cert.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("banded certified failed")
+    return sc, cert

@@ -1,0 +1,401 @@
+/*
+ * band.c -- long global alignments, full and with a learned band
+ * (include/parasail_b200.h), host side.
+ *
+ * The plain path (parasail_b200_nw_long) returns the global score of every
+ * pair, the value the reference's parasail_nw_scan_profile_32 returns. The
+ * learned path predicts a band per pair from k-mer diagonal histograms with
+ * a small MLP, aligns inside the band, keeps the banded score only when the
+ * exactness certificate holds and reruns every other pair on the full DP;
+ * its scores therefore always equal the plain path's.
+ */
+#include <stdlib.h>
+#include <string.h>
+
+#include "pb_internal.h"
+#include "parasail_b200.h"
+
+struct pb_band_model;
+struct pb_band_model *pb_cuda_band_model_new(unsigned seed);
+void pb_cuda_band_model_free(struct pb_band_model *m);
+int pb_cuda_band_model_get(const struct pb_band_model *m, float *w, float *b);
+int pb_cuda_band_model_set(struct pb_band_model *m, const float *w, const float *b);
+int pb_cuda_band_sizes(int *n_in, int *n_hidden, int *n_out, int *nw, int *nb);
+int pb_cuda_band_features(int npairs, const uint8_t *d_q, const int64_t *d_qoff, const int *d_qlen,
+                          const uint8_t *d_t, const int64_t *d_toff, const int *d_tlen, float *d_feat);
+int pb_cuda_band_forward(const struct pb_band_model *m, int n, const float *d_x, float *d_h1, float *d_h2,
+                         float *d_y);
+int pb_cuda_band_gradients(const struct pb_band_model *m, int n, const float *d_x, const float *d_target,
+                           float tau, float *d_gw, float *d_gb, float *loss_out);
+int pb_cuda_band_adam(struct pb_band_model *m, const float *d_gw, const float *d_gb, float lr);
+int pb_cuda_band_labels(int npairs, int a, int open, int ext, const int *d_qlen, const int *d_tlen,
+                        const int *d_score, float *d_target, int *d_lo, int *d_hi);
+int pb_cuda_band_from_pred(int npairs, const int *d_qlen, const int *d_tlen, const float *d_y,
+                           float widen, int slack, int *d_lo, int *d_hi);
+int pb_cuda_band_certify(int npairs, int a, int open, int ext, const int *d_qlen, const int *d_tlen,
+                         const int *d_lo, const int *d_hi, const int *d_score, int *d_cert, int *h_failures);
+int pb_cuda_band_cells(int npairs, const int *d_qlen, const int *d_tlen, const int *d_lo, const int *d_hi,
+                       unsigned long long *h_cells);
+
+#define BAND_TAU 0.9f
+
+typedef struct dev_pairs {
+    uint8_t *q, *t;
+    int64_t *qoff, *toff;
+    int *qlen, *tlen;
+    int n, maxlen;
+} dev_pairs;
+
+static void dev_pairs_free(dev_pairs *d)
+{
+    pb_cuda_free(d->q); pb_cuda_free(d->t); pb_cuda_free(d->qoff); pb_cuda_free(d->toff);
+    pb_cuda_free(d->qlen); pb_cuda_free(d->tlen);
+    pb_cuda_sync();
+    memset(d, 0, sizeof *d);
+}
+
+/* host sequences -> device codes through the matrix mapper */
+static int dev_pairs_upload(const parasail_matrix_t *matrix, const char *queries, const int64_t *qoff,
+                            const int *qlen, const char *targets, const int64_t *toff, const int *tlen,
+                            int n, dev_pairs *d)
+{
+    int64_t qb = 0, tb = 0, k;
+    int i;
+    uint8_t *hq, *ht;
+    memset(d, 0, sizeof *d);
+    d->n = n;
+    for (i = 0; i < n; ++i) {
+        if (qlen[i] <= 0 || tlen[i] <= 0) return -1;
+        if (qoff[i] + qlen[i] > qb) qb = qoff[i] + qlen[i];
+        if (toff[i] + tlen[i] > tb) tb = toff[i] + tlen[i];
+        if (tlen[i] > d->maxlen) d->maxlen = tlen[i];
+    }
+    hq = (uint8_t *)malloc((size_t)qb + 1);
+    ht = (uint8_t *)malloc((size_t)tb + 1);
+    if (!hq || !ht) { free(hq); free(ht); return -1; }
+    for (k = 0; k < qb; ++k) hq[k] = (uint8_t)matrix->mapper[(unsigned char)queries[k]];
+    for (k = 0; k < tb; ++k) ht[k] = (uint8_t)matrix->mapper[(unsigned char)targets[k]];
+    d->q = (uint8_t *)pb_cuda_malloc((size_t)qb + 16);
+    d->t = (uint8_t *)pb_cuda_malloc((size_t)tb + 16);
+    d->qoff = (int64_t *)pb_cuda_malloc(sizeof(int64_t) * n);
+    d->toff = (int64_t *)pb_cuda_malloc(sizeof(int64_t) * n);
+    d->qlen = (int *)pb_cuda_malloc(sizeof(int) * n);
+    d->tlen = (int *)pb_cuda_malloc(sizeof(int) * n);
+    if (!d->q || !d->t || !d->qoff || !d->toff || !d->qlen || !d->tlen) {
+        free(hq); free(ht); dev_pairs_free(d); return -1;
+    }
+    pb_cuda_h2d(d->q, hq, (size_t)qb);
+    pb_cuda_h2d(d->t, ht, (size_t)tb);
+    pb_cuda_h2d(d->qoff, qoff, sizeof(int64_t) * n);
+    pb_cuda_h2d(d->toff, toff, sizeof(int64_t) * n);
+    pb_cuda_h2d(d->qlen, qlen, sizeof(int) * n);
+    pb_cuda_h2d(d->tlen, tlen, sizeof(int) * n);
+    pb_cuda_sync();
+    free(hq);
+    free(ht);
+    return 0;
+}
+
+static int long_ok(const char *func, const parasail_matrix_t *matrix, int open, int gap)
+{
+    if (!matrix) { fprintf(stderr, "%s: missing %s\n", func, "matrix"); return 0; }
+    if (matrix->type != PARASAIL_MATRIX_TYPE_SQUARE || matrix->size > 32) {
+        fprintf(stderr, "%s: needs a square matrix of at most 32 letters\n", func);
+        return 0;
+    }
+    if (open < 0 || gap < 0) { fprintf(stderr, "%s: open and gap must be >= 0\n", func); return 0; }
+    return pb_gpu_ready(func);
+}
+
+static int run_full(const parasail_matrix_t *matrix, const dev_pairs *d, int open, int gap, int *d_score)
+{
+    return pb_cuda_nw_long(d->n, open, gap, matrix->matrix, matrix->size, d->q, d->qoff, d->qlen,
+                           d->t, d->toff, d->tlen, NULL, NULL, d->maxlen, d_score);
+}
+
+int parasail_b200_nw_long(const parasail_matrix_t *matrix,
+                          const char *queries, const int64_t *qoffsets, const int *qlengths,
+                          const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+                          int open, int gap, int *scores)
+{
+    dev_pairs d;
+    int *d_score;
+    int rc;
+    if (!long_ok(__func__, matrix, open, gap)) return -1;
+    if (n <= 0) return n == 0 ? 0 : -1;
+    if (dev_pairs_upload(matrix, queries, qoffsets, qlengths, targets, toffsets, tlengths, n, &d) != 0) {
+        fprintf(stderr, "%s: invalid pairs\n", __func__);
+        return -1;
+    }
+    d_score = (int *)pb_cuda_malloc(sizeof(int) * n);
+    pb_cuda_sync();
+    rc = run_full(matrix, &d, open, gap, d_score);
+    if (rc == 0) rc = pb_cuda_d2h(scores, d_score, sizeof(int) * n);
+    pb_cuda_free(d_score);
+    dev_pairs_free(&d);
+    return rc;
+}
+
+parasail_b200_band_model_t *parasail_b200_band_model_new(unsigned seed)
+{
+    if (!pb_gpu_ready(__func__)) return NULL;
+    return (parasail_b200_band_model_t *)pb_cuda_band_model_new(seed);
+}
+
+void parasail_b200_band_model_free(parasail_b200_band_model_t *model)
+{
+    pb_cuda_band_model_free((struct pb_band_model *)model);
+}
+
+int parasail_b200_band_model_sizes(int *n_in, int *n_hidden, int *n_out, int *n_weights, int *n_biases)
+{
+    return pb_cuda_band_sizes(n_in, n_hidden, n_out, n_weights, n_biases);
+}
+
+int parasail_b200_band_model_get(const parasail_b200_band_model_t *model, float *weights, float *biases)
+{
+    return model ? pb_cuda_band_model_get((const struct pb_band_model *)model, weights, biases) : -1;
+}
+
+int parasail_b200_band_model_set(parasail_b200_band_model_t *model, const float *weights, const float *biases)
+{
+    return (model && weights && biases) ? pb_cuda_band_model_set((struct pb_band_model *)model, weights, biases) : -1;
+}
+
+int parasail_b200_band_features(const parasail_matrix_t *matrix,
+                                const char *queries, const int64_t *qoffsets, const int *qlengths,
+                                const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+                                float *features)
+{
+    dev_pairs d;
+    float *d_feat;
+    int rc, nin, nh, no, nw, nb;
+    if (!long_ok(__func__, matrix, 0, 0)) return -1;
+    pb_cuda_band_sizes(&nin, &nh, &no, &nw, &nb);
+    if (dev_pairs_upload(matrix, queries, qoffsets, qlengths, targets, toffsets, tlengths, n, &d) != 0) return -1;
+    d_feat = (float *)pb_cuda_malloc(sizeof(float) * (size_t)n * nin);
+    pb_cuda_sync();
+    rc = pb_cuda_band_features(n, d.q, d.qoff, d.qlen, d.t, d.toff, d.tlen, d_feat);
+    if (rc == 0) rc = pb_cuda_d2h(features, d_feat, sizeof(float) * (size_t)n * nin);
+    pb_cuda_free(d_feat);
+    dev_pairs_free(&d);
+    return rc;
+}
+
+int parasail_b200_band_model_gradients(const parasail_b200_band_model_t *model, const float *x,
+                                       const float *target, int n, float tau,
+                                       float *grad_weights, float *grad_biases, float *loss)
+{
+    int nin, nh, no, nw, nb, rc;
+    float *d_x, *d_t, *d_gw, *d_gb;
+    if (!model || n <= 0) return -1;
+    pb_cuda_band_sizes(&nin, &nh, &no, &nw, &nb);
+    d_x = (float *)pb_cuda_malloc(sizeof(float) * (size_t)n * nin);
+    d_t = (float *)pb_cuda_malloc(sizeof(float) * (size_t)n * no);
+    d_gw = (float *)pb_cuda_malloc(sizeof(float) * (size_t)nw);
+    d_gb = (float *)pb_cuda_malloc(sizeof(float) * (size_t)nb);
+    pb_cuda_h2d(d_x, x, sizeof(float) * (size_t)n * nin);
+    pb_cuda_h2d(d_t, target, sizeof(float) * (size_t)n * no);
+    pb_cuda_sync();
+    rc = pb_cuda_band_gradients((const struct pb_band_model *)model, n, d_x, d_t, tau, d_gw, d_gb, loss);
+    if (rc == 0) rc = pb_cuda_d2h(grad_weights, d_gw, sizeof(float) * (size_t)nw);
+    if (rc == 0) rc = pb_cuda_d2h(grad_biases, d_gb, sizeof(float) * (size_t)nb);
+    pb_cuda_free(d_x); pb_cuda_free(d_t); pb_cuda_free(d_gw); pb_cuda_free(d_gb);
+    pb_cuda_sync();
+    return rc;
+}
+
+int parasail_b200_band_model_train(parasail_b200_band_model_t *model, const parasail_matrix_t *matrix,
+                                   const char *queries, const int64_t *qoffsets, const int *qlengths,
+                                   const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+                                   int open, int gap, int epochs, int batch, float lr, float *final_loss)
+{
+    dev_pairs d;
+    int nin, nh, no, nw, nb, rc, e, s;
+    float *d_feat, *d_tgt, *d_gw, *d_gb, loss = 0.0f;
+    int *d_score;
+    if (!model || !long_ok(__func__, matrix, open, gap)) return -1;
+    if (n <= 0 || epochs <= 0 || batch <= 0) return -1;
+    pb_cuda_band_sizes(&nin, &nh, &no, &nw, &nb);
+    if (dev_pairs_upload(matrix, queries, qoffsets, qlengths, targets, toffsets, tlengths, n, &d) != 0) return -1;
+    d_feat = (float *)pb_cuda_malloc(sizeof(float) * (size_t)n * nin);
+    d_tgt = (float *)pb_cuda_malloc(sizeof(float) * (size_t)n * no);
+    d_score = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    d_gw = (float *)pb_cuda_malloc(sizeof(float) * (size_t)nw);
+    d_gb = (float *)pb_cuda_malloc(sizeof(float) * (size_t)nb);
+    pb_cuda_sync();
+    /* labels: the smallest certifiable band of the full-DP optimum */
+    rc = pb_cuda_band_features(n, d.q, d.qoff, d.qlen, d.t, d.toff, d.tlen, d_feat);
+    if (rc == 0) rc = run_full(matrix, &d, open, gap, d_score);
+    if (rc == 0) rc = pb_cuda_band_labels(n, matrix->max, open, gap, d.qlen, d.tlen, d_score, d_tgt, NULL, NULL);
+    for (e = 0; rc == 0 && e < epochs; ++e) {
+        double tot = 0.0;
+        int nbat = 0;
+        for (s = 0; rc == 0 && s < n; s += batch) {
+            const int bn = (n - s) < batch ? (n - s) : batch;
+            float l = 0.0f;
+            rc = pb_cuda_band_gradients((const struct pb_band_model *)model, bn, d_feat + (size_t)s * nin,
+                                        d_tgt + (size_t)s * no, BAND_TAU, d_gw, d_gb, &l);
+            if (rc == 0) rc = pb_cuda_band_adam((struct pb_band_model *)model, d_gw, d_gb, lr);
+            tot += l;
+            ++nbat;
+        }
+        loss = (float)(tot / (nbat ? nbat : 1));
+    }
+    if (final_loss) *final_loss = loss;
+    pb_cuda_free(d_feat); pb_cuda_free(d_tgt); pb_cuda_free(d_score); pb_cuda_free(d_gw); pb_cuda_free(d_gb);
+    dev_pairs_free(&d);
+    return rc;
+}
+
+/* shared by the host and device entry points */
+static int learned_run(const struct pb_band_model *model, const parasail_matrix_t *matrix, const dev_pairs *d,
+                       int open, int gap, float widen, int slack, int *d_score, int *d_lo, int *d_hi,
+                       parasail_b200_band_stats_t *stats)
+{
+    int nin, nh, no, nw, nb, rc, nfail = 0;
+    float *d_feat, *d_y;
+    int *d_cert;
+    const int n = d->n;
+    pb_cuda_band_sizes(&nin, &nh, &no, &nw, &nb);
+    d_feat = (float *)pb_cuda_malloc(sizeof(float) * (size_t)n * nin);
+    d_y = (float *)pb_cuda_malloc(sizeof(float) * (size_t)n * no);
+    d_cert = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    pb_cuda_sync();
+    rc = pb_cuda_band_features(n, d->q, d->qoff, d->qlen, d->t, d->toff, d->tlen, d_feat);
+    if (rc == 0) rc = pb_cuda_band_forward(model, n, d_feat, NULL, NULL, d_y);
+    if (rc == 0) rc = pb_cuda_band_from_pred(n, d->qlen, d->tlen, d_y, widen, slack, d_lo, d_hi);
+    if (rc == 0) rc = pb_cuda_nw_long(n, open, gap, matrix->matrix, matrix->size, d->q, d->qoff, d->qlen,
+                                      d->t, d->toff, d->tlen, d_lo, d_hi, d->maxlen, d_score);
+    if (rc == 0) rc = pb_cuda_band_certify(n, matrix->max, open, gap, d->qlen, d->tlen, d_lo, d_hi, d_score,
+                                           d_cert, &nfail);
+    if (rc == 0 && stats) {
+        unsigned long long cells = 0;
+        pb_cuda_band_cells(n, d->qlen, d->tlen, d_lo, d_hi, &cells);
+        stats->band_cells = (double)cells;
+    }
+    if (rc == 0 && nfail > 0) {
+        /* the fallback: full DP for every pair that failed the certificate */
+        int *hc = (int *)malloc(sizeof(int) * (size_t)n);
+        int *hq = (int *)malloc(sizeof(int) * (size_t)n), *ht = (int *)malloc(sizeof(int) * (size_t)n);
+        int64_t *hqo = (int64_t *)malloc(sizeof(int64_t) * (size_t)n), *hto = (int64_t *)malloc(sizeof(int64_t) * (size_t)n);
+        int *hs = (int *)malloc(sizeof(int) * (size_t)n);
+        int *idx = (int *)malloc(sizeof(int) * (size_t)n);
+        int k, f = 0;
+        pb_cuda_d2h(hc, d_cert, sizeof(int) * n);
+        pb_cuda_d2h(hq, d->qlen, sizeof(int) * n);
+        pb_cuda_d2h(ht, d->tlen, sizeof(int) * n);
+        pb_cuda_d2h(hqo, d->qoff, sizeof(int64_t) * n);
+        pb_cuda_d2h(hto, d->toff, sizeof(int64_t) * n);
+        for (k = 0; k < n; ++k) {
+            if (!hc[k]) {
+                idx[f] = k; hq[f] = hq[k]; ht[f] = ht[k]; hqo[f] = hqo[k]; hto[f] = hto[k];
+                ++f;
+            }
+        }
+        {
+            dev_pairs sub = *d;
+            int *fs = (int *)pb_cuda_malloc(sizeof(int) * f);
+            sub.n = f;
+            sub.qlen = (int *)pb_cuda_malloc(sizeof(int) * f);
+            sub.tlen = (int *)pb_cuda_malloc(sizeof(int) * f);
+            sub.qoff = (int64_t *)pb_cuda_malloc(sizeof(int64_t) * f);
+            sub.toff = (int64_t *)pb_cuda_malloc(sizeof(int64_t) * f);
+            pb_cuda_h2d(sub.qlen, hq, sizeof(int) * f);
+            pb_cuda_h2d(sub.tlen, ht, sizeof(int) * f);
+            pb_cuda_h2d(sub.qoff, hqo, sizeof(int64_t) * f);
+            pb_cuda_h2d(sub.toff, hto, sizeof(int64_t) * f);
+            pb_cuda_sync();
+            rc = run_full(matrix, &sub, open, gap, fs);
+            if (rc == 0) {
+                pb_cuda_d2h(hs, fs, sizeof(int) * f);
+                /* scatter the fallback scores, widen the reported band */
+                {
+                    int *all = (int *)malloc(sizeof(int) * (size_t)n);
+                    int *alo = (int *)malloc(sizeof(int) * (size_t)n), *ahi = (int *)malloc(sizeof(int) * (size_t)n);
+                    pb_cuda_d2h(all, d_score, sizeof(int) * n);
+                    pb_cuda_d2h(alo, d_lo, sizeof(int) * n);
+                    pb_cuda_d2h(ahi, d_hi, sizeof(int) * n);
+                    for (k = 0; k < f; ++k) {
+                        all[idx[k]] = hs[k];
+                        alo[idx[k]] = -ht[k] - 1;
+                        ahi[idx[k]] = hq[k] + 1;
+                    }
+                    pb_cuda_h2d(d_score, all, sizeof(int) * n);
+                    pb_cuda_h2d(d_lo, alo, sizeof(int) * n);
+                    pb_cuda_h2d(d_hi, ahi, sizeof(int) * n);
+                    pb_cuda_sync();
+                    free(all); free(alo); free(ahi);
+                }
+            }
+            pb_cuda_free(fs); pb_cuda_free(sub.qlen); pb_cuda_free(sub.tlen);
+            pb_cuda_free(sub.qoff); pb_cuda_free(sub.toff);
+            pb_cuda_sync();
+        }
+        free(hc); free(hq); free(ht); free(hqo); free(hto); free(hs); free(idx);
+    }
+    if (stats) {
+        stats->pairs = n;
+        stats->certified = n - nfail;
+        stats->fallback = nfail;
+    }
+    pb_cuda_free(d_feat); pb_cuda_free(d_y); pb_cuda_free(d_cert);
+    pb_cuda_sync();
+    return rc;
+}
+
+int parasail_b200_nw_learned_band(const parasail_b200_band_model_t *model, const parasail_matrix_t *matrix,
+                                  const char *queries, const int64_t *qoffsets, const int *qlengths,
+                                  const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+                                  int open, int gap, float widen, int slack,
+                                  int *scores, int *band_lo, int *band_hi, parasail_b200_band_stats_t *stats)
+{
+    dev_pairs d;
+    int *d_score, *d_lo, *d_hi, rc;
+    if (!model || !long_ok(__func__, matrix, open, gap)) return -1;
+    if (n <= 0) return n == 0 ? 0 : -1;
+    if (dev_pairs_upload(matrix, queries, qoffsets, qlengths, targets, toffsets, tlengths, n, &d) != 0) return -1;
+    d_score = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    d_lo = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    d_hi = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    pb_cuda_sync();
+    rc = learned_run((const struct pb_band_model *)model, matrix, &d, open, gap, widen, slack, d_score, d_lo, d_hi,
+                     stats);
+    if (rc == 0) rc = pb_cuda_d2h(scores, d_score, sizeof(int) * n);
+    if (rc == 0 && band_lo) rc = pb_cuda_d2h(band_lo, d_lo, sizeof(int) * n);
+    if (rc == 0 && band_hi) rc = pb_cuda_d2h(band_hi, d_hi, sizeof(int) * n);
+    pb_cuda_free(d_score); pb_cuda_free(d_lo); pb_cuda_free(d_hi);
+    dev_pairs_free(&d);
+    return rc;
+}
+
+/* band given by the caller (e.g. fixed-width baselines): banded score,
+ * certificate, full-DP fallback; the same contract as the learned path */
+int parasail_b200_nw_banded_certified(const parasail_matrix_t *matrix,
+                                      const char *queries, const int64_t *qoffsets, const int *qlengths,
+                                      const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+                                      int open, int gap, const int *band_lo, const int *band_hi,
+                                      int *scores, int *certified)
+{
+    dev_pairs d;
+    int *d_score, *d_lo, *d_hi, *d_cert, rc, nfail = 0;
+    if (!long_ok(__func__, matrix, open, gap)) return -1;
+    if (n <= 0) return n == 0 ? 0 : -1;
+    if (dev_pairs_upload(matrix, queries, qoffsets, qlengths, targets, toffsets, tlengths, n, &d) != 0) return -1;
+    d_score = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    d_lo = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    d_hi = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    d_cert = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    pb_cuda_h2d(d_lo, band_lo, sizeof(int) * n);
+    pb_cuda_h2d(d_hi, band_hi, sizeof(int) * n);
+    pb_cuda_sync();
+    rc = pb_cuda_nw_long(n, open, gap, matrix->matrix, matrix->size, d.q, d.qoff, d.qlen, d.t, d.toff, d.tlen,
+                         d_lo, d_hi, d.maxlen, d_score);
+    if (rc == 0) rc = pb_cuda_band_certify(n, matrix->max, open, gap, d.qlen, d.tlen, d_lo, d_hi, d_score, d_cert,
+                                           &nfail);
+    if (rc == 0) rc = pb_cuda_d2h(scores, d_score, sizeof(int) * n);
+    if (rc == 0 && certified) rc = pb_cuda_d2h(certified, d_cert, sizeof(int) * n);
+    pb_cuda_free(d_score); pb_cuda_free(d_lo); pb_cuda_free(d_hi); pb_cuda_free(d_cert);
+    dev_pairs_free(&d);
+    return rc;
+}

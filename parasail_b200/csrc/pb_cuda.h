@@ -139,6 +139,15 @@ int pb_cuda_batch_host(const struct pb_job *job, const pb_batch *tmpl, const uin
                        const char *h_queries, const int64_t *h_qoff, const int *h_qlen,
                        int n, struct pb_record *h_rec);
 
+/* Global alignment scores of long pairs (pb_nwlong.cu): one warp per pair,
+ * device-resident codes, square matrix h_mat (msize x msize, row = target
+ * letter, |values| <= 127, msize <= 32); optional per-pair band of
+ * diagonals [d_lo, d_hi] (i - j), cells outside it unreachable. */
+int pb_cuda_nw_long(int npairs, int open, int gap, const int32_t *h_mat, int msize,
+                    const uint8_t *d_q, const int64_t *d_qoff, const int *d_qlen,
+                    const uint8_t *d_t, const int64_t *d_toff, const int *d_tlen,
+                    const int *d_lo, const int *d_hi, int maxlen, int *d_score);
+
 /* diagnostics (pb_diag.cu) */
 void pb_diag_count_launch(long n);
 void pb_diag_sw16_time(double ms);

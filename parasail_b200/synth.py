@@ -112,3 +112,38 @@ def dna_read_windows(seed=3, n_pairs=1_000_000, lo=100, hi=300, flank=32, sub=0.
     roff = np.zeros(n_pairs, dtype=np.int64)
     roff[1:] = np.cumsum(rlen, dtype=np.int64)[:-1]
     return np.concatenate(reads), roff, rlen, wbuf, woff, wl.astype(np.int32)
+
+
+def dna_long_pairs(seed=5, n_pairs=20_000, lo=5_000, hi=50_000, div_lo=0.01, div_hi=0.15,
+                   indel_share=0.30, indel_mean=3.0, big_frac=0.30, big_lo=50, big_hi=500):
+    """Long DNA pairs: A uniform ACGT of length U[lo, hi]; B = A with a
+    per-pair divergence d ~ U[div_lo, div_hi] split 70/30 between
+    substitutions and indels (indel lengths geometric with the given mean),
+    plus one large insertion or deletion of U[big_lo, big_hi] bp in big_frac
+    of the pairs. Returns (A buf, offs, lens, B buf, offs, lens, divergences)."""
+    rng = np.random.default_rng(seed)
+    la = rng.integers(lo, hi + 1, n_pairs)
+    div = rng.uniform(div_lo, div_hi, n_pairs)
+    a_all = DNA_BYTES[rng.integers(0, 4, int(la.sum()))]
+    aoff = np.zeros(n_pairs, dtype=np.int64)
+    aoff[1:] = np.cumsum(la)[:-1]
+    bs = []
+    gp = 1.0 / indel_mean
+    for k in range(n_pairs):
+        a = a_all[aoff[k]:aoff[k] + la[k]]
+        sub = div[k] * (1.0 - indel_share)
+        # indel events: each costs on average indel_mean bases of divergence
+        ind = div[k] * indel_share / indel_mean
+        b = mutate(rng, a, 1.0 - sub * 4.0 / 3.0, 2.0 * ind, protein=False, geom_p=gp)
+        if rng.random() < big_frac:
+            L = int(rng.integers(big_lo, big_hi + 1))
+            p = int(rng.integers(0, max(1, len(b) - L)))
+            if rng.random() < 0.5:
+                b = np.concatenate([b[:p], DNA_BYTES[rng.integers(0, 4, L)], b[p:]])
+            else:
+                b = np.concatenate([b[:p], b[p + L:]]) if len(b) > L + 1 else b
+        bs.append(b)
+    lb = np.array([len(b) for b in bs], dtype=np.int32)
+    boff = np.zeros(n_pairs, dtype=np.int64)
+    boff[1:] = np.cumsum(lb, dtype=np.int64)[:-1]
+    return a_all, aoff, la.astype(np.int32), np.concatenate(bs), boff, lb, div
