@@ -305,7 +305,7 @@ def main():
         ours = int(sum(int(dev_rec[q][:nt, 0].astype(np.int64).sum()) for q in range(len(queries))))
         parity = {"pairs_checked": len(queries) * nt, "score_checksum_equal": ours == base["checksum"],
                   "device_and_host_api_equal": bool(same)}
-    lb = learned_band_leg(pb) if os.environ.get("PB_BENCH_SKIP_BAND") is None else None
+    lb = learned_band_leg(pb)
     peak = pb.lib.parasail_b200_dpx_peak()
     kernel_ms_per_launch = sw16_ms / max(1, nk.value)
     cells_per_launch = cells

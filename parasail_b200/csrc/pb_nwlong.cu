@@ -1,14 +1,15 @@
 /*
- * pb_nwlong.cu -- global alignment of long pairs: one warp per pair,
- * anti-diagonal wavefront across the warp's lanes, exact 32-bit values,
+ * pb_nwlong.cu -- global alignment of long pairs: one CTA per pair,
+ * anti-diagonal wavefront across each warp's lanes, exact 32-bit values,
  * optionally restricted to a band of diagonals.
  *
  * Intra-task schedule: a pass covers 32 x NWL_RL query rows; lane k owns
  * rows r0 + k*NWL_RL .. + NWL_RL - 1 and, at iteration t, computes target
  * column t - k. Lane k therefore receives the bottom row of lane k-1 (H and
  * the vertical-gap value F at the same column) through one warp shuffle of
- * the previous iteration's outputs, and lane 0 reads the previous pass's
- * bottom row from a per-warp buffer that lane 31 writes. Scores come from a
+ * the previous iteration's outputs. The passes of one pair are spread over
+ * the warps of a CTA and pipelined: lane 0 of pass p reads the bottom row
+ * that lane 31 of pass p-1 (the previous warp) publishes. Scores come from a
  * square substitution table in shared memory indexed by (target letter,
  * query letter); for alphabets of at most 8 letters one byte-permute selects
  * the score from the target letter's table row held in two registers.
@@ -26,13 +27,14 @@
 #include <algorithm>
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
+#include <cstdio>
 
 #include "pb_cuda.h"
 
 namespace pb {
 
 static constexpr int NWL_RL = 8;          /* query rows per lane */
-static constexpr int NWL_WARPS = 4;       /* warps per block */
+static constexpr int NWL_WARPS = 8;       /* warps per CTA, one CTA per pair */
 static constexpr int NWL_NEG = INT32_MIN / 4;
 
 struct NwWaveParams {
@@ -42,7 +44,7 @@ struct NwWaveParams {
     const uint8_t *t; const int64_t *toff; const int *tlen;
     const int *lo; const int *hi; /* per pair band (diagonal i - j), or nullptr */
     const int *order;             /* pairs, most cells first */
-    int2 *scratch;                /* per resident warp: [maxlen] (H, F) */
+    int2 *scratch;                /* per CTA: NWL_WARPS ring buffers of [maxlen] (H, F) */
     int maxlen;
     int *score;                   /* per pair */
 };
@@ -56,25 +58,42 @@ __device__ __forceinline__ int sext_byte(uint32_t lo, uint32_t hi, int k)
     return (int)d;
 }
 
+/*
+ * One CTA of NWL_WARPS warps per pair. Pass p (rows p*256 .. p*256+255) is
+ * run by warp p % NWL_WARPS; its lane 0 reads pass p-1's bottom row from
+ * ring buffer (p-1) % NWL_WARPS, which pass p-1's lane 31 fills column by
+ * column and publishes through a progress counter in shared memory every 32
+ * columns. Waits are bounded: a spin that exceeds NWL_SPIN polls sets the
+ * error flag and abandons the pair (the host reports the failure).
+ */
+static constexpr long long NWL_SPIN = 1ll << 26;
+
 template <bool BANDED>
 __global__ void __launch_bounds__(NWL_WARPS * 32)
-k_nw_wave(NwWaveParams p, int *counter)
+k_nw_wave(NwWaveParams p, int *counter, int *error)
 {
     __shared__ __align__(16) int8_t s_mat[32 * 32];
+    /* progress of ring buffer k: g * (m + 1) + j + 1 once generation g (the
+     * pass g * NWL_WARPS + k) has published column j; monotone, so a reader
+     * never mistakes an older pass's progress for its predecessor's */
+    __shared__ volatile long long s_prog[NWL_WARPS];
+    __shared__ int s_pair;
+    __shared__ volatile int s_abort;
     for (int k = threadIdx.x; k < p.msize * p.msize; k += blockDim.x) {
         const int r = k / p.msize, c = k % p.msize;
         s_mat[r * 32 + c] = p.mat[k];
     }
-    __syncthreads();
     const int lane = threadIdx.x & 31;
-    const int slot = blockIdx.x * NWL_WARPS + (threadIdx.x >> 5);
-    int2 *buf = p.scratch + (size_t)slot * p.maxlen;
+    const int warp = threadIdx.x >> 5;
     const int open = p.open, gap = p.gap;
+    int2 *ring = p.scratch + (size_t)blockIdx.x * NWL_WARPS * p.maxlen;
 
     for (;;) {
-        int w = 0;
-        if (lane == 0) w = atomicAdd(counter, 1);
-        w = __shfl_sync(0xffffffffu, w, 0);
+        __syncthreads();
+        if (threadIdx.x == 0) { s_pair = atomicAdd(counter, 1); s_abort = 0; }
+        if (threadIdx.x < NWL_WARPS) s_prog[threadIdx.x] = 0;
+        __syncthreads();
+        const int w = s_pair;
         if (w >= p.npairs) break;
         const int pid = p.order[w];
         const int n = p.qlen[pid], m = p.tlen[pid];
@@ -82,21 +101,44 @@ k_nw_wave(NwWaveParams p, int *counter)
         const uint8_t *ts = p.t + p.toff[pid];
         const int lo = BANDED ? p.lo[pid] : -(m + 1);
         const int hi = BANDED ? p.hi[pid] : n + 1;
+        const int npass = (n + 32 * NWL_RL - 1) / (32 * NWL_RL);
         int result = NWL_NEG;
-        int prev_jhi = -1;
+        bool have_result = false;
 
-        for (int r0 = 0; r0 < n; r0 += 32 * NWL_RL) {
+        for (int pass = warp; pass < npass; pass += NWL_WARPS) {
+            const int r0 = pass * 32 * NWL_RL;
             const int R0 = r0 + lane * NWL_RL;
+            int2 *in_buf = ring + (size_t)((pass + NWL_WARPS - 1) % NWL_WARPS) * p.maxlen;
+            int2 *out_buf = ring + (size_t)(pass % NWL_WARPS) * p.maxlen;
+            const long long stride = (long long)m + 1;
+            volatile long long *in_prog = &s_prog[(pass + NWL_WARPS - 1) % NWL_WARPS];
+            volatile long long *out_prog = &s_prog[pass % NWL_WARPS];
+            const long long in_base = pass > 0 ? (long long)((pass - 1) / NWL_WARPS) * stride + 1 : 0;
+            const long long out_base = (long long)(pass / NWL_WARPS) * stride + 1;
             int qc[NWL_RL];
 #pragma unroll
             for (int r = 0; r < NWL_RL; ++r) qc[r] = (R0 + r < n) ? qs[R0 + r] : 0;
-            /* columns this pass touches */
-            int jlo = 0, jhi = m - 1;
+            int jlo = 0, jhi = m - 1, prev_jlo = 0, prev_jhi = m - 1;
             if (BANDED) {
                 jlo = max(0, r0 - hi);
                 jhi = min(m - 1, r0 + 32 * NWL_RL - 1 - lo);
+                prev_jlo = max(0, r0 - 32 * NWL_RL - hi);
+                prev_jhi = min(m - 1, r0 - 1 - lo);
             }
-            /* left state: column jlo - 1 */
+            if (pass == 0) prev_jhi = -1;
+            /* the previous pass must have published column c before it is read */
+            auto wait_for = [&](int c) -> bool {
+                if (pass == 0) return true;
+                const int need = min(c, prev_jhi);
+                if (need < 0) return true;
+                long long spins = 0;
+                while (*in_prog < in_base + need) {
+                    if (s_abort) return false;
+                    if (++spins > NWL_SPIN) { s_abort = 1; atomicExch(error, 1); return false; }
+                }
+                __threadfence_block();
+                return true;
+            };
             int Hl[NWL_RL], E[NWL_RL];
 #pragma unroll
             for (int r = 0; r < NWL_RL; ++r) {
@@ -106,30 +148,45 @@ k_nw_wave(NwWaveParams p, int *counter)
                 Hl[r] = v;
                 E[r] = NWL_NEG;
             }
-            /* diagonal of each lane's first row at column jlo: H(R0 - 1, jlo - 1) */
             int dg;
             if (jlo == 0) {
                 dg = (R0 == 0) ? 0 : ((!BANDED || (R0 >= lo && R0 <= hi)) ? -open - (R0 - 1) * gap : NWL_NEG);
-            } else if (lane == 0 && jlo - 1 <= prev_jhi) {
-                dg = buf[jlo - 1].x;    /* H(r0 - 1, jlo - 1), on the band's edge */
             } else {
-                dg = NWL_NEG;           /* outside the band */
+                dg = NWL_NEG;
+                bool ok = true;
+                if (lane == 0) ok = wait_for(jlo - 1);
+                ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0);
+                if (!ok) break;
+                if (lane == 0 && jlo - 1 <= prev_jhi && jlo - 1 >= prev_jlo) dg = __ldcg(&in_buf[jlo - 1]).x;
             }
-            int sh_h = NWL_NEG, sh_f = NWL_NEG;   /* outputs of the previous iteration (this lane's bottom) */
+            int sh_h = NWL_NEG, sh_f = NWL_NEG;
             const int tend = jhi + 31;
+            /* residue and score row of this lane's next column, loaded one
+             * iteration ahead */
+            int jn = jlo - lane;
+            int tc_next = (jn >= jlo && jn <= jhi) ? ts[jn] : 0;
+            bool aborted = false;
             for (int it = jlo; it <= tend; ++it) {
                 const int j = it - lane;
-                /* bottom row of lane-1 at column j (computed last iteration) */
+                if (((it - jlo) & 31) == 0) {
+                    bool ok = true;
+                    if (lane == 0) ok = wait_for(min(it + 31, jhi));
+                    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0);
+                    if (!ok) { aborted = true; break; }
+                }
                 int up_h = __shfl_up_sync(0xffffffffu, sh_h, 1);
                 int up_f = __shfl_up_sync(0xffffffffu, sh_f, 1);
                 const bool active = j >= jlo && j <= jhi;
+                const int tc = tc_next;
+                jn = j + 1;
+                tc_next = (jn >= jlo && jn <= jhi) ? ts[jn] : 0;
                 if (lane == 0 && active) {
                     if (r0 == 0) {
                         const bool inb = !BANDED || (-1 - j >= lo && -1 - j <= hi);
                         up_h = inb ? -open - j * gap : NWL_NEG;
                         up_f = NWL_NEG;
-                    } else if (j <= prev_jhi) {
-                        const int2 v = buf[j];
+                    } else if (j <= prev_jhi && j >= prev_jlo) {
+                        const int2 v = __ldcg(&in_buf[j]);
                         up_h = v.x;
                         up_f = v.y;
                     } else {
@@ -138,7 +195,6 @@ k_nw_wave(NwWaveParams p, int *counter)
                     }
                 }
                 if (active) {
-                    const int tc = ts[j];
                     int hd = dg;
                     int hu = up_h, fu = up_f;
                     uint32_t row_lo = 0, row_hi = 0;
@@ -158,7 +214,7 @@ k_nw_wave(NwWaveParams p, int *counter)
                             const int d = i - j;
                             if (d < lo || d > hi) { h = NWL_NEG; ee = NWL_NEG; ff = NWL_NEG; }
                         }
-                        if (i == n - 1 && j == m - 1) result = h;
+                        if (i == n - 1 && j == m - 1) { result = h; have_result = true; }
                         E[r] = ee;
                         hd = Hl[r];
                         Hl[r] = h;
@@ -168,16 +224,23 @@ k_nw_wave(NwWaveParams p, int *counter)
                     dg = up_h;
                     sh_h = hu;
                     sh_f = fu;
-                    if (lane == 31 && r0 + 32 * NWL_RL < n) buf[j] = make_int2(hu, fu);
+                    if (lane == 31 && pass + 1 < npass) {
+                        out_buf[j] = make_int2(hu, fu);
+                        if (((j - jlo) & 31) == 31 || j == jhi) {
+                            __threadfence_block();
+                            *out_prog = out_base + j;
+                        }
+                    }
                 }
             }
-            prev_jhi = jhi;
+            if (aborted) break;
             __syncwarp();
         }
-        /* the corner's owner holds the result */
-        const int owner = ((n - 1) % (32 * NWL_RL)) / NWL_RL;
-        result = __shfl_sync(0xffffffffu, result, owner);
-        if (lane == 0) p.score[pid] = result;
+        /* the corner's owner publishes the result */
+        __shared__ int s_result;
+        if (have_result) s_result = result;
+        __syncthreads();
+        if (threadIdx.x == 0) p.score[pid] = s_abort ? NWL_NEG : s_result;
     }
 }
 
@@ -240,10 +303,12 @@ extern "C" int pb_cuda_nw_long(int npairs, int open, int gap, const int32_t *h_m
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pb::k_nw_wave<false>, pb::NWL_WARPS * 32, 0);
     if (per_sm < 1) per_sm = 1;
     int blocks = per_sm * nsm;
-    const int need = (npairs + pb::NWL_WARPS - 1) / pb::NWL_WARPS;
-    if (blocks > need) blocks = need;
+    if (blocks > npairs) blocks = npairs;
     int2 *scratch = nullptr;
-    int rc = 0;
+    int *d_err = nullptr;
+    int rc = 0, herr = 0;
+    cudaMallocAsync((void **)&d_err, sizeof(int), st);
+    cudaMemsetAsync(d_err, 0, sizeof(int), st);
     if (cudaMallocAsync((void **)&scratch, sizeof(int2) * (size_t)(maxlen + 1) * blocks * pb::NWL_WARPS, st) != cudaSuccess)
         rc = -1;
     if (rc == 0) {
@@ -252,16 +317,22 @@ extern "C" int pb_cuda_nw_long(int npairs, int open, int gap, const int32_t *h_m
         p.mat = d_mat; p.q = d_q; p.qoff = d_qoff; p.qlen = d_qlen;
         p.t = d_t; p.toff = d_toff; p.tlen = d_tlen; p.lo = d_lo; p.hi = d_hi;
         p.order = order; p.scratch = scratch; p.maxlen = maxlen + 1; p.score = d_score;
-        if (d_lo) pb::k_nw_wave<true><<<blocks, pb::NWL_WARPS * 32, 0, st>>>(p, counter);
-        else pb::k_nw_wave<false><<<blocks, pb::NWL_WARPS * 32, 0, st>>>(p, counter);
+        if (d_lo) pb::k_nw_wave<true><<<blocks, pb::NWL_WARPS * 32, 0, st>>>(p, counter, d_err);
+        else pb::k_nw_wave<false><<<blocks, pb::NWL_WARPS * 32, 0, st>>>(p, counter, d_err);
         if (cudaGetLastError() != cudaSuccess) rc = -1;
         pb_diag_count_launch(3);
+        cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
     }
     cudaFreeAsync(d_mat, st); cudaFreeAsync(idx, st); cudaFreeAsync(order, st);
     cudaFreeAsync(cells, st); cudaFreeAsync(cells_sorted, st); cudaFreeAsync(counter, st);
     cudaFreeAsync(tmp, st);
     if (scratch) cudaFreeAsync(scratch, st);
+    cudaFreeAsync(d_err, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
+    if (herr) {
+        fprintf(stderr, "pb_cuda_nw_long: a pipeline wait exceeded its bound; pair abandoned\n");
+        rc = -1;
+    }
     cudaStreamDestroy(st);
     return rc;
 }
