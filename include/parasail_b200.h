@@ -57,6 +57,40 @@ extern int parasail_b200_batch_profile_device(
         const uint8_t *d_codes, const int64_t *d_offsets, const int *d_lengths, int n,
         int open, int gap, parasail_b200_record_t *d_records);
 
+/** parasail_b200_batch_profile_device without any device allocation. No
+ * counterpart in the reference (its CPU kernels allocate per call with
+ * parasail_memalign, src/memory.c); it exists for callers that may not
+ * allocate device memory while they run, e.g. a process whose device memory
+ * is reserved up front by another allocator, or a latency-bound loop in which
+ * a cudaMalloc/cudaFree would synchronise the device.
+ *
+ * Scratch comes from one fixed file-scope device array of
+ * parasail_b200_noalloc_scratch_bytes() bytes (32 MiB) per device; the
+ * profile (parasail_profile_create_*), d_codes, d_offsets, d_lengths and
+ * d_records are the caller's and must live on the current device. The
+ * batch must fit: n <= 190650 pairs, and 88 bytes per pair plus 8 bytes per
+ * target residue (32 with statistics), each region rounded up to 256 bytes,
+ * within the array (about 3.5 million residues score-only); a larger batch
+ * is rejected (-1 and a message naming the bytes it needs), never
+ * truncated. Functions that need the two-pass statistics
+ * pipeline (sw_stats_striped_*) are rejected. Records equal those of
+ * parasail_b200_batch_profile_device.
+ *
+ * The first call on a device does a one-time set-up (the array's address is
+ * looked up with cudaGetSymbolAddress, and a stream is created for the
+ * calling thread); make that first call before any stream capture begins.
+ * The array is shared by all calls on the device: calls that overlap in time
+ * on one device race on it and must be serialised by the caller. It keeps
+ * the last call's contents, none of which a later call reads. */
+extern int parasail_b200_batch_profile_device_noalloc(
+        const char *funcname, const parasail_profile_t *profile,
+        const uint8_t *d_codes, const int64_t *d_offsets, const int *d_lengths, int n,
+        int open, int gap, parasail_b200_record_t *d_records);
+
+/** Size in bytes of the per-device static scratch array of
+ * parasail_b200_batch_profile_device_noalloc. */
+extern size_t parasail_b200_noalloc_scratch_bytes(void);
+
 /** Database search: every one of nq query profiles (sharing one matrix)
  * against every target, in one pipeline; a Smith-Waterman score batch runs
  * all queries in a single kernel launch. records[q * n + i] is query q

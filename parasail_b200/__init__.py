@@ -178,6 +178,10 @@ lib.parasail_b200_batch_profile_device.restype = ctypes.c_int
 lib.parasail_b200_batch_profile_device.argtypes = [ctypes.c_char_p, _PP, ctypes.c_void_p, ctypes.c_void_p,
                                                    ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                                    ctypes.c_int, ctypes.c_void_p]
+lib.parasail_b200_batch_profile_device_noalloc.restype = ctypes.c_int
+lib.parasail_b200_batch_profile_device_noalloc.argtypes = lib.parasail_b200_batch_profile_device.argtypes
+lib.parasail_b200_noalloc_scratch_bytes.restype = ctypes.c_size_t
+lib.parasail_b200_noalloc_scratch_bytes.argtypes = []
 lib.parasail_b200_batch_pairs.restype = ctypes.c_int
 lib.parasail_b200_batch_pairs.argtypes = [ctypes.c_char_p, _MP] + [ctypes.c_void_p] * 6 + \
     [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]

@@ -153,6 +153,49 @@ int parasail_b200_batch_profile_device(const char *funcname, const parasail_prof
     return pb_cuda_batch_run(&job, &b, (pb_record *)d_records);
 }
 
+int parasail_b200_batch_profile_device_noalloc(const char *funcname, const parasail_profile_t *profile,
+                                               const uint8_t *d_codes, const int64_t *d_offsets,
+                                               const int *d_lengths, int n, int open, int gap,
+                                               parasail_b200_record_t *d_records)
+{
+    pb_job job;
+    pb_batch b;
+    const pb_device_profile *profs[1];
+    if (check_common(__func__, profile, n, open, gap) != 0) return -1;
+    if (n == 0) return 0;
+    if (!d_codes || !d_offsets || !d_lengths || !d_records) { fprintf(stderr, "%s: missing arrays\n", __func__); return -1; }
+    if (parse_job(funcname, 1, open, gap, profile->matrix, &job) != 0) {
+        fprintf(stderr, "%s: unknown profile function '%s'\n", __func__, funcname ? funcname : "(null)");
+        return -1;
+    }
+    if (pb_job_is_faststats(&job)) {
+        fprintf(stderr, "%s: '%s' needs the two-pass statistics pipeline, which this entry point does not run\n",
+                __func__, funcname);
+        return -1;
+    }
+    if (n > pb_cuda_noalloc_max_pairs()) {
+        fprintf(stderr, "%s: %d pairs exceed the limit of %d\n", __func__, n, pb_cuda_noalloc_max_pairs());
+        return -1;
+    }
+    if (!pb_gpu_ready(__func__)) return -1;
+    memset(&b, 0, sizeof b);
+    profs[0] = pb_profile_device(profile);
+    b.alg = job.mode.alg; b.sgflags = job.mode.sgflags; b.stats = job.mode.stats;
+    b.open = open; b.gap = gap; b.profs = profs; b.nprofs = 1; b.npairs = n;
+    /* padded rows of the width whose saturation checks the records carry
+     * (serial forms and Smith-Waterman score-only need none) */
+    b.pad_rows = (job.bits < 0 || (job.mode.alg == PB_SW && !job.mode.stats)) ? 0
+               : (job.bits == 0 || job.bits == 8) ? 32 : job.bits == 16 ? 16 : 8;
+    b.d_targets = d_codes; b.d_toff = d_offsets; b.d_tlen = d_lengths;
+    if (pb_cuda_noalloc_run(&job, &b, (pb_record *)d_records) != 0) {
+        fprintf(stderr, "%s: %s\n", __func__, pb_cuda_noalloc_last_error());
+        return -1;
+    }
+    return 0;
+}
+
+size_t parasail_b200_noalloc_scratch_bytes(void) { return pb_cuda_noalloc_capacity(); }
+
 int parasail_b200_batch_pairs(const char *funcname, const parasail_matrix_t *matrix,
                               const char *queries, const int64_t *qoffsets, const int *qlengths,
                               const char *targets, const int64_t *toffsets, const int *tlengths,

@@ -139,6 +139,15 @@ int pb_cuda_batch_host(const struct pb_job *job, const pb_batch *tmpl, const uin
                        const char *h_queries, const int64_t *h_qoff, const int *h_qlen,
                        int n, struct pb_record *h_rec);
 
+/* One profile against device-resident targets with no device allocation
+ * (pb_noalloc.cu): the exact kernel and the width resolution with their
+ * scratch in a fixed-size file-scope device array. Jobs that need the
+ * FASTSTATS prefix pass are not handled. */
+int pb_cuda_noalloc_run(const struct pb_job *job, const pb_batch *b, struct pb_record *d_rec);
+size_t pb_cuda_noalloc_capacity(void);
+int pb_cuda_noalloc_max_pairs(void);
+const char *pb_cuda_noalloc_last_error(void);
+
 /* Global alignment scores of long pairs (pb_nwlong.cu): one warp per pair,
  * device-resident codes, square matrix h_mat (msize x msize, row = target
  * letter, |values| <= 127, msize <= 32); optional per-pair band of
