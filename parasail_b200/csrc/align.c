@@ -103,7 +103,20 @@ int pb_run_job_pair(const pb_device_profile *dp, const pb_job *job, const uint8_
         rc = run_pair(0, dp, m, 1, 32, codes, tlen, o1.end_query + 1, o1.end_ref + 1, &o2);
         if (rc != 0) return rc;
     }
-    *rec = pb_chain_resolve(job, &o1, &o2, dp->qlen, tlen);
+    {
+        pb_lane_res e8, e16;
+        int round;
+        memset(&e8, 0, sizeof e8);
+        memset(&e16, 0, sizeof e16);
+        *rec = pb_chain_resolve(job, &o1, &o2, dp->qlen, tlen, &e8, &e16);
+        /* narrow striped widths the exact values cannot settle: the
+         * lane-exact kernel of that width, then resolve again */
+        for (round = 0; round < 2 && (rec->ambig == 8 || rec->ambig == 16); ++round) {
+            pb_lane_res *e = rec->ambig == 8 ? &e8 : &e16;
+            if (pb_cuda_lane_pair(rec->ambig, dp, &job->mode, codes, tlen, &o1, e) != 0) return -1;
+            *rec = pb_chain_resolve(job, &o1, &o2, dp->qlen, tlen, &e8, &e16);
+        }
+    }
     return 0;
 }
 

@@ -5,6 +5,7 @@
  */
 #include <cstdio>
 #include <cstdint>
+#include <cstring>
 #include <cuda_runtime.h>
 
 #include "pb_cuda.h"
@@ -16,14 +17,29 @@ namespace pb {
 __global__ void k_resolve(pb_job job, const pb_pair_out *__restrict__ o1,
                           const pb_pair_out *__restrict__ o2, const int *__restrict__ qlen,
                           int qlen_all, const int *__restrict__ tlen, int n,
-                          pb_record *__restrict__ rec)
+                          const int *__restrict__ list, const pb_lane_res *__restrict__ e8,
+                          const pb_lane_res *__restrict__ e16, pb_record *__restrict__ rec,
+                          int *__restrict__ need8, int *__restrict__ need16, int *__restrict__ counts)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = list ? list[k] : k;
     const pb_pair_out a = o1[i];
     pb_pair_out b;
     if (o2) b = o2[i];
-    rec[i] = pb_chain_resolve(&job, &a, o2 ? &b : nullptr, qlen ? qlen[i] : qlen_all, tlen[i]);
+    const pb_record r = pb_chain_resolve(&job, &a, o2 ? &b : nullptr, qlen ? qlen[i] : qlen_all, tlen[i],
+                                         e8 ? &e8[i] : nullptr, e16 ? &e16[i] : nullptr);
+    rec[i] = r;
+    if (counts && r.ambig == 8) need8[atomicAdd(&counts[0], 1)] = i;
+    else if (counts && r.ambig == 16) need16[atomicAdd(&counts[1], 1)] = i;
+}
+
+__global__ void k_max_int(const int *__restrict__ v, int n, int *__restrict__ out)
+{
+    int m = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = max(m, v[i]);
+    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
 /* prefix limits of the FASTSTATS stats pass; pairs that need none get a
@@ -39,10 +55,102 @@ __global__ void k_prefix_limits(pb_job job, const pb_pair_out *__restrict__ o1, 
     tlim[i] = need ? a.end_ref + 1 : 1;
 }
 
-void launch_resolve(const pb_job &job, const pb_pair_out *o1, const pb_pair_out *o2, const int *qlen,
-                    int qlen_all, const int *tlen, int n, pb_record *rec, cudaStream_t st)
+/*
+ * Resolution of n pairs with the lane-exact rounds: resolve every pair; the
+ * pairs that need the 8- or 16-bit lane kernel are listed, emulated and
+ * resolved again, until none is left (at most one round per width).
+ * `la` describes the query side (profile or matrix mode) and the targets.
+ * Work memory: from `work` (work_bytes, 256-byte aligned) when given,
+ * otherwise from the stream's pool. Synchronises the stream once per round.
+ */
+int resolve_rounds(const pb_job &job, const pb_lane_args &la, const pb_pair_out *o1, const pb_pair_out *o2,
+                   const int *qlen, int qlen_all, const int *tlen, int n, pb_record *rec, cudaStream_t st,
+                   void *work, size_t work_bytes)
 {
-    k_resolve<<<(n + 255) / 256, 256, 0, st>>>(job, o1, o2, qlen, qlen_all, tlen, n, rec);
+    if (n <= 0) return 0;
+    /* work layout: counts[2] | lists A (2n) | lists B (2n) | e8 (n) | e16 (n) | lane scratch */
+    const size_t b_counts = 256;
+    const size_t b_lists = ((sizeof(int) * 2 * (size_t)n) + 255) & ~(size_t)255;
+    const size_t b_res = ((sizeof(pb_lane_res) * (size_t)n) + 255) & ~(size_t)255;
+    const size_t fixed = b_counts + 2 * b_lists + 2 * b_res;
+    unsigned char *base = (unsigned char *)work;
+    bool own = false;
+    if (!base) {
+        if (cudaMallocAsync((void **)&base, fixed, st) != cudaSuccess) return -1;
+        own = true;
+    } else if (work_bytes < fixed) {
+        return -2;
+    }
+    int *counts = (int *)base;
+    int *lists[2] = {(int *)(base + b_counts), (int *)(base + b_counts + b_lists)};
+    pb_lane_res *e8 = (pb_lane_res *)(base + b_counts + 2 * b_lists);
+    pb_lane_res *e16 = (pb_lane_res *)(base + b_counts + 2 * b_lists + b_res);
+    unsigned char *lane_scratch = own ? nullptr : base + fixed;
+    const size_t lane_bytes = own ? 0 : work_bytes - fixed;
+    int rc = 0;
+    cudaMemsetAsync(counts, 0, 2 * sizeof(int), st);
+    cudaMemsetAsync(e8, 0, b_res, st);
+    cudaMemsetAsync(e16, 0, b_res, st);
+    k_resolve<<<(n + 255) / 256, 256, 0, st>>>(job, o1, o2, qlen, qlen_all, tlen, n, nullptr, nullptr, nullptr,
+                                               rec, lists[0], lists[0] + n, counts);
+    pb_diag_count_launch(1);
+    int cur = 0;
+    pb_lane_args a = la;
+    bool have_max = a.max_qlen > 0;
+    for (int round = 0; round < 3 && rc == 0; ++round) {
+        int hc[2] = {0, 0};
+        if (cudaMemcpyAsync(hc, counts, sizeof hc, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) { rc = -1; break; }
+        if (hc[0] + hc[1] == 0) break;
+        if (!have_max) {
+            /* matrix mode: the longest query sizes the lane scratch */
+            int *dm = counts + 2;
+            int hm = 0;
+            cudaMemsetAsync(dm, 0, sizeof(int), st);
+            k_max_int<<<64, 256, 0, st>>>(a.qlens, n, dm);
+            pb_diag_count_launch(1);
+            cudaMemcpyAsync(&hm, dm, sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (cudaStreamSynchronize(st) != cudaSuccess) { rc = -1; break; }
+            a.max_qlen = hm;
+            have_max = true;
+        }
+        a.kind = pb_lane_kind(&job.mode);
+        a.sgflags = job.mode.sgflags;
+        a.open = job.mode.open; a.gap = job.mode.gap;
+        if (hc[0] && pb_cuda_lane_run(8, &a, lists[cur], hc[0], e8, lane_scratch, lane_bytes, st) != 0) { rc = -1; break; }
+        if (hc[1] && pb_cuda_lane_run(16, &a, lists[cur] + n, hc[1], e16, lane_scratch, lane_bytes, st) != 0) { rc = -1; break; }
+        const int nxt = cur ^ 1;
+        cudaMemsetAsync(counts, 0, 2 * sizeof(int), st);
+        if (hc[0])
+            k_resolve<<<(hc[0] + 255) / 256, 256, 0, st>>>(job, o1, o2, qlen, qlen_all, tlen, hc[0], lists[cur], e8,
+                                                           e16, rec, lists[nxt], lists[nxt] + n, counts);
+        if (hc[1])
+            k_resolve<<<(hc[1] + 255) / 256, 256, 0, st>>>(job, o1, o2, qlen, qlen_all, tlen, hc[1], lists[cur] + n,
+                                                           e8, e16, rec, lists[nxt], lists[nxt] + n, counts);
+        pb_diag_count_launch((hc[0] ? 1 : 0) + (hc[1] ? 1 : 0));
+        if (cudaGetLastError() != cudaSuccess) { rc = -1; break; }
+        cur = nxt;
+    }
+    if (own) cudaFreeAsync(base, st);
+    return rc;
+}
+
+/* the lane arguments of query q of a batch */
+pb_lane_args lane_args_of(const pb_batch *b, int q, const pb_pair_out *o1)
+{
+    pb_lane_args a;
+    memset(&a, 0, sizeof a);
+    if (b->nprofs > 0) {
+        const pb_device_profile *p = b->profs[q];
+        a.prof = p->d_prof32; a.qcodes = p->d_qcodes; a.lp = p->lp; a.qlen = p->qlen; a.size = p->size;
+        a.mmax = p->mmax; a.mmin = p->mmin; a.max_qlen = p->qlen;
+    } else {
+        a.mat = b->d_mat; a.msize = b->msize; a.qall = b->d_qall; a.qoff = b->d_qoff; a.qlens = b->d_qlen;
+        a.mmax = b->mmax; a.mmin = b->mmin; a.max_qlen = 0;
+    }
+    a.targets = b->d_targets; a.toff = b->d_toff; a.tlen = b->d_tlen;
+    a.o1 = o1;
+    return a;
 }
 
 }  // namespace pb
@@ -102,11 +210,10 @@ extern "C" int pb_cuda_batch_run(const pb_job *job, const pb_batch *tmpl, pb_rec
     }
     for (int q = 0; q < nq && rc == 0; ++q) {
         const int qall = tmpl->nprofs > 0 ? tmpl->profs[q]->qlen : 0;
-        pb::launch_resolve(*job, o1 + (size_t)q * n, o2 ? o2 + (size_t)q * n : nullptr,
-                           tmpl->nprofs > 0 ? nullptr : tmpl->d_qlen, qall, tmpl->d_tlen, n,
-                           d_rec + (size_t)q * n, st);
-        pb_diag_count_launch(1);
-        if (cudaGetLastError() != cudaSuccess) rc = -1;
+        const pb_lane_args la = pb::lane_args_of(tmpl, q, o1 + (size_t)q * n);
+        rc = pb::resolve_rounds(*job, la, o1 + (size_t)q * n, o2 ? o2 + (size_t)q * n : nullptr,
+                                tmpl->nprofs > 0 ? nullptr : tmpl->d_qlen, qall, tmpl->d_tlen, n,
+                                d_rec + (size_t)q * n, st, nullptr, 0);
     }
     cudaFreeAsync(o1, st);
     if (o2) cudaFreeAsync(o2, st);

@@ -139,6 +139,35 @@ int pb_cuda_batch_host(const struct pb_job *job, const pb_batch *tmpl, const uin
                        const char *h_queries, const int64_t *h_qoff, const int *h_qlen,
                        int n, struct pb_record *h_rec);
 
+/* Lane-exact emulation of the reference's 8/16-bit striped kernels
+ * (pb_lane.cu) for the pairs listed in d_list. kind: 0 nw/sg score-only,
+ * 1 nw/sg with statistics, 2 the SW statistics kernel on the FASTSTATS prefix
+ * [0, o1.end_query] x [0, o1.end_ref]. Profile mode (prof, qcodes, lp, qlen)
+ * or matrix mode (mat, msize, qall, qoff, qlens). */
+typedef struct pb_lane_res {
+    int score, end_query, end_ref, matches, similar, length, saturated, valid;
+} pb_lane_res;
+
+typedef struct pb_lane_args {
+    int kind, sgflags, open, gap, mmax, mmin, max_qlen;
+    const int32_t *prof; const uint8_t *qcodes; int lp, qlen, size;
+    const int32_t *mat; int msize; const uint8_t *qall; const int64_t *qoff; const int *qlens;
+    const uint8_t *targets; const int64_t *toff; const int *tlen;
+    const pb_pair_out *o1;
+} pb_lane_args;
+
+/* scratch: NULL to allocate from the stream's pool, else at least
+ * pb_cuda_lane_scratch_per_warp bytes (fewer warps run when it is small).
+ * stream: a cudaStream_t. Asynchronous. */
+int pb_cuda_lane_run(int bits, const pb_lane_args *a, const int *d_list, int nlist, pb_lane_res *d_res,
+                     void *scratch, size_t scratch_bytes, void *stream);
+size_t pb_cuda_lane_scratch_per_warp(int bits, int kind, int max_qlen);
+/* One pair from host memory (the single-call entry points): target codes
+ * and the score pass's output on the host, result to *res. Synchronous. */
+struct pb_mode;
+int pb_cuda_lane_pair(int bits, const pb_device_profile *dp, const struct pb_mode *m, const uint8_t *h_codes,
+                      int tlen, const pb_pair_out *h_o1, pb_lane_res *h_res);
+
 /* One profile against device-resident targets with no device allocation
  * (pb_noalloc.cu): the exact kernel and the width resolution with their
  * scratch in a fixed-size file-scope device array. Jobs that need the

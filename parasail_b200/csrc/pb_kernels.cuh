@@ -66,8 +66,11 @@ struct Sw16Params {
 };
 
 void launch_exact(const ExactParams &p, int alg, bool stats, cudaStream_t st);
-void launch_resolve(const pb_job &job, const pb_pair_out *o1, const pb_pair_out *o2, const int *qlen,
-                    int qlen_all, const int *tlen, int n, pb_record *rec, cudaStream_t st);
+/* resolution with the lane-exact rounds (pb_batch.cu) */
+int resolve_rounds(const pb_job &job, const pb_lane_args &la, const pb_pair_out *o1, const pb_pair_out *o2,
+                   const int *qlen, int qlen_all, const int *tlen, int n, pb_record *rec, cudaStream_t st,
+                   void *work, size_t work_bytes);
+pb_lane_args lane_args_of(const pb_batch *b, int q, const pb_pair_out *o1);
 void launch_sw16(const Sw16Params &p, cudaStream_t st);
 
 }  // namespace pb

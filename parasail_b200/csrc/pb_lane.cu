@@ -1,5 +1,262 @@
 /*
- * pb_lane.cu -- lane-exact striped kernels (see pb_cuda.h).
+ * pb_lane.cu -- the lane-exact striped kernels (pb_lane.cuh) on the GPU: one
+ * warp per pair, AVX2 lane l = warp lane l. The vector shift of the
+ * reference's striped loop (_mm256_slli_si256 by one lane) is a warp shuffle,
+ * _mm256_movemask_epi8 of a comparison is a warp vote, and each of the
+ * kernel's per-segment vector arrays (pvHStore, pvE, ...) is a [segLen][32]
+ * int16 array in this warp's slice of a scratch buffer, so every thread only
+ * touches its own lane's elements.
+ *
+ * Runs only on the pairs whose narrow-width result the exact values cannot
+ * settle (pb_resolve.h), so it is built for exactness, not speed.
  */
+#include <cstdio>
+#include <cstdint>
+#include <climits>
+#include <cstring>
 #include <cuda_runtime.h>
+
 #include "pb_cuda.h"
+#include "pb_lane.cuh"
+#include "pb_resolve.h"
+
+namespace pb {
+namespace lane {
+
+template <int W> struct WarpVec {
+    static constexpr int L = Lim<W>::LANES;
+    typedef int V;
+    struct Arr { int16_t *p; };
+    int lane;
+    int16_t *scratch;
+
+    __device__ __forceinline__ Arr arr(int a, int segLen) { return Arr{scratch + (size_t)a * segLen * 32}; }
+    __device__ __forceinline__ V load(Arr a, int i) { return a.p[i * 32 + lane]; }
+    __device__ __forceinline__ void store(Arr a, int i, V x) { a.p[i * 32 + lane] = (int16_t)x; }
+    __device__ __forceinline__ V set1(int x) { return x; }
+    template <int W2> __device__ __forceinline__ V adds(V a, V b) { return clampw<W2>((long long)a + b); }
+    template <int W2> __device__ __forceinline__ V subs(V a, V b) { return clampw<W2>((long long)a - b); }
+    __device__ __forceinline__ V max(V a, V b) { return a > b ? a : b; }
+    __device__ __forceinline__ V min(V a, V b) { return a < b ? a : b; }
+    __device__ __forceinline__ V cmpgt(V a, V b) { return a > b ? -1 : 0; }
+    __device__ __forceinline__ V cmpeq(V a, V b) { return a == b ? -1 : 0; }
+    __device__ __forceinline__ V blend(V a, V b, V m) { return m ? b : a; }
+    __device__ __forceinline__ V and_(V a, V b) { return a & b; }
+    __device__ __forceinline__ V or_(V a, V b) { return a | b; }
+    __device__ __forceinline__ V andnot(V a, V b) { return ~a & b; }
+    __device__ __forceinline__ V shift1(V a)
+    {
+        const int y = __shfl_up_sync(0xffffffffu, a, 1);
+        return lane == 0 ? 0 : y;
+    }
+    __device__ __forceinline__ V insert0(V a, int x) { return lane == 0 ? x : a; }
+    __device__ __forceinline__ bool any(V m) { return __any_sync(0xffffffffu, lane < L && m != 0) != 0; }
+    __device__ __forceinline__ int extract(V a, int l) { return __shfl_sync(0xffffffffu, a, l); }
+    __device__ __forceinline__ int hmax(V a)
+    {
+        int m = lane < L ? a : INT_MIN;
+        for (int o = 16; o; o >>= 1) {
+            const int y = __shfl_xor_sync(0xffffffffu, m, o);
+            m = y > m ? y : m;
+        }
+        return m;
+    }
+    __device__ __forceinline__ V lane_eq(int k) { return lane == k ? -1 : 0; }
+    template <int W2> __device__ __forceinline__ void init_he(V &h, V &e, int i, int segLen, int s1_beg, int open, int gap)
+    {
+        long long tmp = s1_beg ? 0 : (-(long long)open - (long long)gap * (lane * segLen + i));
+        h = tmp < Lim<W2>::MIN ? Lim<W2>::MIN : (int)tmp;
+        tmp = tmp - open;
+        e = tmp < Lim<W2>::MIN ? Lim<W2>::MIN : (int)tmp;
+    }
+    template <int W2> __device__ __forceinline__ int boundary(const Problem &pr, int j)
+    {
+        if (j == 0) return 0;
+        const long long tmp = pr.s2_beg ? 0 : (-(long long)pr.open - (long long)pr.gap * (j - 1));
+        return tmp < Lim<W2>::MIN ? Lim<W2>::MIN : (int)tmp;
+    }
+    template <int W2> __device__ __forceinline__ V prof(const Problem &pr, int k, int i, int segLen)
+    {
+        const int row = lane * segLen + i;
+        return (lane < L && row < pr.qlen) ? wrap<W2>(prof_value(pr, k, row)) : 0;
+    }
+    template <int W2> __device__ __forceinline__ V match(const Problem &pr, int k, int i, int segLen)
+    {
+        const int row = lane * segLen + i;
+        return (lane < L && row < pr.qlen) ? (k == pr.qcodes[row] ? 1 : 0) : 0;
+    }
+    template <int W2> __device__ __forceinline__ V similar(const Problem &pr, int k, int i, int segLen)
+    {
+        return prof<W2>(pr, k, i, segLen) > 0 ? 1 : 0;
+    }
+};
+
+struct LaneJob {
+    int kind;                                  /* 0 nw/sg, 1 nw/sg stats, 2 sw stats prefix */
+    int open, gap, mmax, mmin;
+    int s1_beg, s1_end, s2_beg, s2_end;
+    /* profile mode */
+    const int32_t *prof; const uint8_t *qcodes; int lp; int qlen; int size;
+    /* matrix (pairs) mode */
+    const int32_t *mat; int msize; const uint8_t *qall; const int64_t *qoff; const int *qlens;
+    const uint8_t *targets; const int64_t *toff; const int *tlen;
+    const pb_pair_out *o1;                     /* kind 2: prefix = o1 ends */
+    const int *list; int nlist;
+    pb_lane_res *res;                          /* indexed by pair id */
+    int16_t *scratch; int seg_max; int narr;
+};
+
+constexpr int LANE_THREADS = 256;
+
+template <int W>
+__global__ void __launch_bounds__(LANE_THREADS) k_lane(LaneJob J)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    WarpVec<W> v;
+    v.lane = lane;
+    v.scratch = J.scratch + (size_t)warp * J.narr * J.seg_max * 32;
+    for (int k = warp; k < J.nlist; k += nwarps) {
+        const int pid = J.list[k];
+        Problem pr;
+        pr.open = J.open; pr.gap = J.gap; pr.mmax = J.mmax; pr.mmin = J.mmin;
+        pr.s1_beg = J.s1_beg; pr.s1_end = J.s1_end; pr.s2_beg = J.s2_beg; pr.s2_end = J.s2_end;
+        if (J.mat) {
+            pr.prof = nullptr; pr.lp = 0; pr.mat = J.mat; pr.msize = J.msize; pr.size = J.msize;
+            pr.qcodes = J.qall + J.qoff[pid]; pr.qlen = J.qlens[pid];
+        } else {
+            pr.prof = J.prof; pr.lp = J.lp; pr.mat = nullptr; pr.msize = 0; pr.size = J.size;
+            pr.qcodes = J.qcodes; pr.qlen = J.qlen;
+        }
+        pr.t = J.targets + J.toff[pid];
+        pr.tlen = J.tlen[pid];
+        if (J.kind == 2) {
+            pr.qlen = J.o1[pid].end_query + 1;
+            pr.tlen = J.o1[pid].end_ref + 1;
+        }
+        Out o;
+        if (J.kind == 0) striped_nwsg<WarpVec<W>, W>(v, pr, o);
+        else if (J.kind == 1) striped_nwsg_stats<WarpVec<W>, W>(v, pr, o);
+        else striped_sw_stats_bias<WarpVec<W>, W>(v, pr, o);
+        if (lane == 0) {
+            pb_lane_res r;
+            r.score = o.score; r.end_query = o.end_query; r.end_ref = o.end_ref;
+            r.matches = o.matches; r.similar = o.similar; r.length = o.length;
+            r.saturated = o.saturated; r.valid = 1;
+            J.res[pid] = r;
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace lane
+}  // namespace pb
+
+extern "C" {
+
+size_t pb_cuda_lane_scratch_per_warp(int bits, int kind, int max_qlen)
+{
+    const int L = 256 / bits;
+    const int seg = (max_qlen + L - 1) / L;
+    const int narr = kind == 0 ? 3 : kind == 1 ? 12 : 16;
+    return sizeof(int16_t) * (size_t)narr * seg * 32;
+}
+
+int pb_cuda_lane_run(int bits, const pb_lane_args *a, const int *d_list, int nlist, pb_lane_res *d_res,
+                     void *scratch, size_t scratch_bytes, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    using namespace pb::lane;
+    if (nlist <= 0) return 0;
+    if (bits != 8 && bits != 16) return -1;
+    LaneJob J;
+    J.kind = a->kind; J.open = a->open; J.gap = a->gap; J.mmax = a->mmax; J.mmin = a->mmin;
+    J.s1_beg = (a->sgflags & PB_S1_BEG) != 0; J.s1_end = (a->sgflags & PB_S1_END) != 0;
+    J.s2_beg = (a->sgflags & PB_S2_BEG) != 0; J.s2_end = (a->sgflags & PB_S2_END) != 0;
+    J.prof = a->prof; J.qcodes = a->qcodes; J.lp = a->lp; J.qlen = a->qlen; J.size = a->size;
+    J.mat = a->mat; J.msize = a->msize; J.qall = a->qall; J.qoff = a->qoff; J.qlens = a->qlens;
+    J.targets = a->targets; J.toff = a->toff; J.tlen = a->tlen; J.o1 = a->o1;
+    J.list = d_list; J.nlist = nlist; J.res = d_res;
+    const int L = 256 / bits;
+    J.seg_max = (a->max_qlen + L - 1) / L;
+    if (J.seg_max < 1) J.seg_max = 1;
+    J.narr = a->kind == 0 ? 3 : a->kind == 1 ? 12 : 16;
+    const size_t per_warp = sizeof(int16_t) * (size_t)J.narr * J.seg_max * 32;
+    int nsm = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int wpb = LANE_THREADS / 32;
+    /* warps launched: one per listed pair up to 8 per SM; every launched warp
+     * owns one per_warp slice of the scratch */
+    long long warps = nlist < nsm * 8 ? nlist : (long long)nsm * 8;
+    int threads = LANE_THREADS;
+    bool own = false;
+    if (scratch) {
+        const long long fit = (long long)(scratch_bytes / per_warp);
+        if (fit < 1) return -1;
+        if (warps > fit) warps = fit;
+    }
+    if (warps >= wpb) {
+        warps = (warps / wpb) * wpb;
+    } else {
+        threads = 32;
+    }
+    if (!scratch) {
+        if (cudaMallocAsync(&scratch, per_warp * warps, st) != cudaSuccess) return -1;
+        own = true;
+    }
+    J.scratch = (int16_t *)scratch;
+    const int blocks = (int)(warps * 32 / threads);
+    if (bits == 8) k_lane<8><<<blocks, threads, 0, st>>>(J);
+    else k_lane<16><<<blocks, threads, 0, st>>>(J);
+    pb_diag_count_launch(1);
+    const cudaError_t e = cudaGetLastError();
+    if (own) cudaFreeAsync(scratch, st);
+    return e == cudaSuccess ? 0 : -1;
+}
+
+int pb_cuda_lane_pair(int bits, const pb_device_profile *dp, const struct pb_mode *m, const uint8_t *h_codes,
+                      int tlen, const pb_pair_out *h_o1, pb_lane_res *h_res)
+{
+    if (pb_cuda_init() != 0) return -1;
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    uint8_t *d_t = nullptr;
+    int64_t *d_off = nullptr;
+    int *d_len = nullptr, *d_list = nullptr;
+    pb_pair_out *d_o1 = nullptr;
+    pb_lane_res *d_res = nullptr;
+    const int64_t zero = 0;
+    const int list0 = 0;
+    int rc = 0;
+    if (cudaMallocAsync((void **)&d_t, (size_t)tlen + 16, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_off, sizeof(int64_t), st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_len, sizeof(int), st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_list, sizeof(int), st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_o1, sizeof(pb_pair_out), st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_res, sizeof(pb_lane_res), st) != cudaSuccess)
+        rc = -1;
+    if (rc == 0) {
+        cudaMemcpyAsync(d_t, h_codes, tlen, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_off, &zero, sizeof zero, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_len, &tlen, sizeof tlen, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_list, &list0, sizeof list0, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_o1, h_o1, sizeof(pb_pair_out), cudaMemcpyHostToDevice, st);
+        pb_lane_args a;
+        memset(&a, 0, sizeof a);
+        a.kind = pb_lane_kind(m); a.sgflags = m->sgflags; a.open = m->open; a.gap = m->gap;
+        a.mmax = dp->mmax; a.mmin = dp->mmin; a.max_qlen = dp->qlen;
+        a.prof = dp->d_prof32; a.qcodes = dp->d_qcodes; a.lp = dp->lp; a.qlen = dp->qlen; a.size = dp->size;
+        a.targets = d_t; a.toff = d_off; a.tlen = d_len; a.o1 = d_o1;
+        rc = pb_cuda_lane_run(bits, &a, d_list, 1, d_res, nullptr, 0, st);
+        if (rc == 0) cudaMemcpyAsync(h_res, d_res, sizeof(pb_lane_res), cudaMemcpyDeviceToHost, st);
+    }
+    cudaFreeAsync(d_t, st); cudaFreeAsync(d_off, st); cudaFreeAsync(d_len, st);
+    cudaFreeAsync(d_list, st); cudaFreeAsync(d_o1, st); cudaFreeAsync(d_res, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
+    cudaStreamDestroy(st);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,544 @@
+/*
+ * pb_lane.cuh -- lane-exact restatement of the reference's 8- and 16-bit
+ * AVX2 striped kernels, for the pairs whose narrow-width result the exact
+ * DP values cannot settle.
+ *
+ * A narrow striped kernel computes with saturating W-bit lanes, starts every
+ * stripe's vertical gap at NEG_LIMIT and checks only some of its values
+ * against the limits, so near the limits its result (score, statistics and
+ * whether it reports saturation) is a function of its own arithmetic, not of
+ * the exact DP. This file restates that arithmetic step by step:
+ *
+ *   nw/sg score-only:  util/templates/nw_striped.c:186-300,
+ *                      util/templates/sg_striped.c (column maximum, s1_end
+ *                      scan of the last column in memory order, ends)
+ *   nw/sg statistics:  util/templates/nw_stats_striped.c:226-470,
+ *                      util/templates/sg_stats_striped.c (vMaxH* blends)
+ *   sw statistics:     util/templates/sw_stats_striped_bias.c:226-637 (the
+ *                      biased kernel the FASTSTATS wrapper :644-730 runs on
+ *                      the prefix [0, end_query] x [0, end_ref])
+ *
+ * with the profile of src/memory_avx2.c:28-253 / :255-528 (values truncated
+ * to W bits, padded rows 0; similar = truncated value > 0).
+ *
+ * The code is written against a vector policy P: the device policy maps one
+ * AVX2 lane to one lane of a warp (lane shift = warp shuffle, movemask = warp
+ * vote), so a warp runs one pair with the reference's own data movement.
+ */
+#ifndef PARASAIL_B200_PB_LANE_CUH
+#define PARASAIL_B200_PB_LANE_CUH
+
+#include <stdint.h>
+
+#ifdef __CUDACC__
+#define PB_LHD __host__ __device__ __forceinline__
+#else
+#define PB_LHD inline
+#endif
+
+namespace pb {
+namespace lane {
+
+template <int W> struct Lim {
+    static constexpr int LANES = 256 / W;
+    static constexpr int MIN = W == 8 ? -128 : -32768;
+    static constexpr int MAX = W == 8 ? 127 : 32767;
+};
+
+/* (intW_t)x: two's-complement wrap, as a C conversion to int8_t/int16_t */
+template <int W> PB_LHD int wrap(long long x)
+{
+    return W == 8 ? (int)(int8_t)(uint8_t)(x & 0xff) : (int)(int16_t)(uint16_t)(x & 0xffff);
+}
+
+template <int W> PB_LHD int clampw(long long x)
+{
+    return x < Lim<W>::MIN ? Lim<W>::MIN : (x > Lim<W>::MAX ? Lim<W>::MAX : (int)x);
+}
+
+/* One pair as the emulation sees it. Profile values come from the exact
+ * 32-bit profile (vector orientation: prof[k * lp + row], k = target code),
+ * queries' codes for the match plane. */
+struct Problem {
+    int qlen, tlen;                /* s1Len, s2Len of the kernel call */
+    int open, gap, mmax, mmin;
+    int s1_beg, s1_end, s2_beg, s2_end;
+    const int32_t *prof;           /* [size][lp], or nullptr in matrix mode */
+    const uint8_t *qcodes;         /* [>= qlen] */
+    int lp;
+    const int32_t *mat;            /* matrix mode: mat[k * msize + query code] */
+    int msize;
+    int size;                      /* alphabet size: codes >= size read as code 0 */
+    const uint8_t *t;              /* target codes */
+};
+
+/* profile value of target code k at query row `row` (row < qlen); an
+ * out-of-alphabet code reads as code 0, as in the exact kernel */
+PB_LHD int prof_value(const Problem &pr, int k, int row)
+{
+    if (k >= pr.size) k = 0;
+    if (pr.mat) {
+        int c = pr.qcodes[row];
+        if (c >= pr.msize) c = 0;
+        return pr.mat[k * pr.msize + c];
+    }
+    return pr.prof[(size_t)k * pr.lp + row];
+}
+
+struct Out {
+    int score, end_query, end_ref, matches, similar, length, saturated;
+};
+
+/* ---- nw / sg, score only (NW == SG with no free ends) ---- */
+template <class P, int W>
+PB_LHD void striped_nwsg(P &v, const Problem &pr, Out &o)
+{
+    typedef typename P::V V;
+    constexpr int L = Lim<W>::LANES;
+    const int s1Len = pr.qlen, s2Len = pr.tlen;
+    const int segLen = (s1Len + L - 1) / L;
+    const int offset = (s1Len - 1) % segLen;
+    const int lastLane = (s1Len - 1) / segLen;          /* lane of row s1Len-1 */
+    const int open = pr.open, gap = pr.gap;
+    const int NEG_LIMIT = wrap<W>((-open < pr.mmin ? (long long)Lim<W>::MIN + open : (long long)Lim<W>::MIN - pr.mmin) + 1);
+    const int POS_LIMIT = wrap<W>((long long)Lim<W>::MAX - pr.mmax - 1);
+    const V vGapO = v.set1(wrap<W>(open)), vGapE = v.set1(wrap<W>(gap));
+    const V vNegLimit = v.set1(NEG_LIMIT), vPosLimit = v.set1(POS_LIMIT);
+    V vSatMin = vPosLimit, vSatMax = vNegLimit, vMaxH = vNegLimit;
+    const V vPosMask = v.lane_eq(lastLane);
+    int end_query = s1Len - 1, end_ref = s2Len - 1;
+    int score = NEG_LIMIT;
+
+    typename P::Arr hs = v.arr(0, segLen), hl = v.arr(1, segLen), pe = v.arr(2, segLen);
+    /* initialize H and E */
+    for (int i = 0; i < segLen; ++i) {
+        V h, e;
+        v.template init_he<W>(h, e, i, segLen, pr.s1_beg, open, gap);
+        v.store(hs, i, h);
+        v.store(pe, i, e);
+    }
+    for (int j = 0; j < s2Len; ++j) {
+        const int bj = v.template boundary<W>(pr, j), bj1 = v.template boundary<W>(pr, j + 1);
+        const int k_t = pr.t[j];
+        V vE;
+        V vF = vNegLimit;
+        V vH = v.shift1(v.load(hs, segLen - 1));
+        { typename P::Arr tmp = hl; hl = hs; hs = tmp; }
+        vH = v.insert0(vH, bj);
+        for (int i = 0; i < segLen; ++i) {
+            vH = v.template adds<W>(vH, v.template prof<W>(pr, k_t, i, segLen));
+            vE = v.load(pe, i);
+            vH = v.max(vH, vE);
+            vH = v.max(vH, vF);
+            v.store(hs, i, vH);
+            vSatMax = v.max(vSatMax, vH);
+            vSatMin = v.min(vSatMin, vH);
+            vSatMin = v.min(vSatMin, vE);
+            vSatMin = v.min(vSatMin, vF);
+            vH = v.template subs<W>(vH, vGapO);
+            vE = v.template subs<W>(vE, vGapE);
+            vE = v.max(vE, vH);
+            v.store(pe, i, vE);
+            vF = v.template subs<W>(vF, vGapE);
+            vF = v.max(vF, vH);
+            vH = v.load(hl, i);
+        }
+        {
+            long long tmp = pr.s2_beg ? -(long long)open : (long long)bj1 - open;
+            const int tmp2 = tmp < Lim<W>::MIN ? Lim<W>::MIN : wrap<W>(tmp);
+            bool done = false;
+            for (int k = 0; k < L && !done; ++k) {
+                vF = v.insert0(v.shift1(vF), tmp2);
+                for (int i = 0; i < segLen; ++i) {
+                    vH = v.load(hs, i);
+                    vH = v.max(vH, vF);
+                    v.store(hs, i, vH);
+                    vSatMin = v.min(vSatMin, vH);
+                    vSatMax = v.max(vSatMax, vH);
+                    vH = v.template subs<W>(vH, vGapO);
+                    vF = v.template subs<W>(vF, vGapE);
+                    if (!v.any(v.cmpgt(vF, vH))) { done = true; break; }
+                }
+            }
+        }
+        {
+            vH = v.load(hs, offset);
+            const V vCompare = v.and_(vPosMask, v.cmpgt(vH, vMaxH));
+            vMaxH = v.max(vH, vMaxH);
+            if (v.any(vCompare)) end_ref = j;
+        }
+        /* the limit checks only accumulate: once one trips, the kernel's
+         * result is the saturated one whatever follows */
+        if (v.any(v.or_(v.cmpgt(vNegLimit, vSatMin), v.cmpgt(vSatMax, vPosLimit)))) break;
+    }
+    if (pr.s2_end) {
+        score = v.extract(vMaxH, lastLane);
+        end_query = s1Len - 1;
+    }
+    if (pr.s1_end) {
+        /* the last column in memory order: segment-major, lane-minor */
+        for (int i = 0; i < segLen; ++i) {
+            for (int l = 0; l < L; ++l) {
+                const int temp = i + l * segLen;
+                if (temp >= s1Len) continue;
+                const int t = v.extract(v.load(hs, i), l);
+                if (t > score) {
+                    score = t; end_query = temp; end_ref = s2Len - 1;
+                } else if (t == score && end_ref == s2Len - 1 && temp < end_query) {
+                    end_query = temp;
+                }
+            }
+        }
+    }
+    if (!pr.s1_end && !pr.s2_end) {
+        score = v.extract(v.load(hs, offset), lastLane);
+        end_ref = s2Len - 1;
+        end_query = s1Len - 1;
+    }
+    o.saturated = v.any(v.or_(v.cmpgt(vNegLimit, vSatMin), v.cmpgt(vSatMax, vPosLimit))) ? 1 : 0;
+    if (o.saturated) { score = 0; end_query = 0; end_ref = 0; }
+    o.score = score; o.end_query = end_query; o.end_ref = end_ref;
+    o.matches = o.similar = o.length = 0;
+}
+
+/* ---- nw / sg with statistics ---- */
+template <class P, int W>
+PB_LHD void striped_nwsg_stats(P &v, const Problem &pr, Out &o)
+{
+    typedef typename P::V V;
+    constexpr int L = Lim<W>::LANES;
+    const int s1Len = pr.qlen, s2Len = pr.tlen;
+    const int segLen = (s1Len + L - 1) / L;
+    const int offset = (s1Len - 1) % segLen;
+    const int lastLane = (s1Len - 1) / segLen;
+    const int open = pr.open, gap = pr.gap;
+    const int NEG_LIMIT = wrap<W>((-open < pr.mmin ? (long long)Lim<W>::MIN + open : (long long)Lim<W>::MIN - pr.mmin) + 1);
+    const int POS_LIMIT = wrap<W>((long long)Lim<W>::MAX - pr.mmax - 1);
+    const V vGapO = v.set1(wrap<W>(open)), vGapE = v.set1(wrap<W>(gap));
+    const V vZero = v.set1(0), vOne = v.set1(1);
+    const V vNegLimit = v.set1(NEG_LIMIT), vPosLimit = v.set1(POS_LIMIT);
+    V vSatMin = vPosLimit, vSatMax = vNegLimit;
+    V vMaxH = vNegLimit, vMaxHM = vNegLimit, vMaxHS = vNegLimit, vMaxHL = vNegLimit;
+    const V vPosMask = v.lane_eq(lastLane);
+    int end_query = s1Len - 1, end_ref = s2Len - 1;
+    int score = NEG_LIMIT, matches = 0, similar = 0, length = 0;
+
+    typename P::Arr hs = v.arr(0, segLen), hl = v.arr(1, segLen);
+    typename P::Arr hms = v.arr(2, segLen), hml = v.arr(3, segLen);
+    typename P::Arr hss = v.arr(4, segLen), hsl = v.arr(5, segLen);
+    typename P::Arr hls = v.arr(6, segLen), hll = v.arr(7, segLen);
+    typename P::Arr pe = v.arr(8, segLen), pem = v.arr(9, segLen), pes = v.arr(10, segLen), pel = v.arr(11, segLen);
+    for (int i = 0; i < segLen; ++i) {
+        v.store(hms, i, vZero); v.store(hss, i, vZero); v.store(hls, i, vZero);
+        v.store(pem, i, vZero); v.store(pes, i, vZero); v.store(pel, i, vOne);
+        V h, e;
+        v.template init_he<W>(h, e, i, segLen, pr.s1_beg, open, gap);
+        v.store(hs, i, h);
+        v.store(pe, i, e);
+    }
+    for (int j = 0; j < s2Len; ++j) {
+        const int bj = v.template boundary<W>(pr, j), bj1 = v.template boundary<W>(pr, j + 1);
+        const int k_t = pr.t[j];
+        V vF = vNegLimit, vFM = vZero, vFS = vZero, vFL = vOne;
+        V vH = v.shift1(v.load(hs, segLen - 1));
+        V vHM = v.shift1(v.load(hms, segLen - 1));
+        V vHS = v.shift1(v.load(hss, segLen - 1));
+        V vHL = v.shift1(v.load(hls, segLen - 1));
+        vH = v.insert0(vH, bj);
+        { typename P::Arr t0 = hl; hl = hs; hs = t0; }
+        { typename P::Arr t0 = hml; hml = hms; hms = t0; }
+        { typename P::Arr t0 = hsl; hsl = hss; hss = t0; }
+        { typename P::Arr t0 = hll; hll = hls; hls = t0; }
+        for (int i = 0; i < segLen; ++i) {
+            V vE = v.load(pe, i), vEM = v.load(pem, i), vES = v.load(pes, i), vEL = v.load(pel, i);
+            const V vH_dag = v.template adds<W>(vH, v.template prof<W>(pr, k_t, i, segLen));
+            vH = v.max(vH_dag, vE);
+            vH = v.max(vH, vF);
+            v.store(hs, i, vH);
+            V case1 = v.cmpeq(vH, vH_dag);
+            const V case2 = v.cmpeq(vH, vF);
+            vHM = v.blend(v.blend(vEM, vFM, case2), v.template adds<W>(vHM, v.template match<W>(pr, k_t, i, segLen)), case1);
+            v.store(hms, i, vHM);
+            vHS = v.blend(v.blend(vES, vFS, case2), v.template adds<W>(vHS, v.template similar<W>(pr, k_t, i, segLen)), case1);
+            v.store(hss, i, vHS);
+            vHL = v.blend(v.blend(vEL, vFL, case2), v.template adds<W>(vHL, vOne), case1);
+            v.store(hls, i, vHL);
+            vSatMin = v.min(vSatMin, vH);
+            vSatMax = v.max(vSatMax, vH);
+            vSatMax = v.max(vSatMax, vHM);
+            vSatMax = v.max(vSatMax, vHS);
+            vSatMax = v.max(vSatMax, vHL);
+            const V vEF_opn = v.template subs<W>(vH, vGapO);
+            const V vE_ext = v.template subs<W>(vE, vGapE);
+            vE = v.max(vEF_opn, vE_ext);
+            case1 = v.cmpgt(vEF_opn, vE_ext);
+            vEM = v.blend(vEM, vHM, case1);
+            vES = v.blend(vES, vHS, case1);
+            vEL = v.blend(v.template adds<W>(vEL, vOne), v.template adds<W>(vHL, vOne), case1);
+            v.store(pe, i, vE); v.store(pem, i, vEM); v.store(pes, i, vES); v.store(pel, i, vEL);
+            const V vF_ext = v.template subs<W>(vF, vGapE);
+            vF = v.max(vEF_opn, vF_ext);
+            case1 = v.cmpgt(vEF_opn, vF_ext);
+            vFM = v.blend(vFM, vHM, case1);
+            vFS = v.blend(vFS, vHS, case1);
+            vFL = v.blend(v.template adds<W>(vFL, vOne), v.template adds<W>(vHL, vOne), case1);
+            vH = v.load(hl, i); vHM = v.load(hml, i); vHS = v.load(hsl, i); vHL = v.load(hll, i);
+        }
+        {
+            long long tmp = pr.s2_beg ? -(long long)open : (long long)bj1 - open;
+            const int tmp2 = tmp < Lim<W>::MIN ? Lim<W>::MIN : wrap<W>(tmp);
+            bool done = false;
+            for (int k = 0; k < L && !done; ++k) {
+                V vHp = v.shift1(v.load(hl, segLen - 1));
+                vF = v.shift1(vF); vFM = v.shift1(vFM); vFS = v.shift1(vFS); vFL = v.shift1(vFL);
+                vHp = v.insert0(vHp, bj);
+                vF = v.insert0(vF, tmp2);
+                vFL = v.insert0(vFL, 1);
+                for (int i = 0; i < segLen; ++i) {
+                    vHp = v.template adds<W>(vHp, v.template prof<W>(pr, k_t, i, segLen));
+                    vH = v.load(hs, i);
+                    vH = v.max(vH, vF);
+                    v.store(hs, i, vH);
+                    const V case1 = v.cmpeq(vH, vHp);
+                    const V case2 = v.cmpeq(vH, vF);
+                    V cond = v.andnot(case1, case2);
+                    vHM = v.blend(v.load(hms, i), vFM, cond); v.store(hms, i, vHM);
+                    vHS = v.blend(v.load(hss, i), vFS, cond); v.store(hss, i, vHS);
+                    vHL = v.blend(v.load(hls, i), vFL, cond); v.store(hls, i, vHL);
+                    vSatMin = v.min(vSatMin, vH);
+                    vSatMax = v.max(vSatMax, vH);
+                    vSatMax = v.max(vSatMax, vHM);
+                    vSatMax = v.max(vSatMax, vHS);
+                    vSatMax = v.max(vSatMax, vHL);
+                    const V vEF_opn = v.template subs<W>(vH, vGapO);
+                    const V vF_ext = v.template subs<W>(vF, vGapE);
+                    if (!v.any(v.or_(v.cmpgt(vF_ext, vEF_opn), v.cmpeq(vF_ext, vEF_opn)))) { done = true; break; }
+                    vF = vF_ext;
+                    cond = v.cmpgt(vEF_opn, vF_ext);
+                    vFM = v.blend(vFM, vHM, cond);
+                    vFS = v.blend(vFS, vHS, cond);
+                    vFL = v.blend(v.template adds<W>(vFL, vOne), v.template adds<W>(vHL, vOne), cond);
+                    vHp = v.load(hl, i);
+                }
+            }
+        }
+        {
+            vH = v.load(hs, offset); vHM = v.load(hms, offset); vHS = v.load(hss, offset); vHL = v.load(hls, offset);
+            const V cond_max = v.cmpgt(vH, vMaxH);
+            vMaxH = v.blend(vMaxH, vH, cond_max);
+            vMaxHM = v.blend(vMaxHM, vHM, cond_max);
+            vMaxHS = v.blend(vMaxHS, vHS, cond_max);
+            vMaxHL = v.blend(vMaxHL, vHL, cond_max);
+            if (v.any(v.and_(vPosMask, cond_max))) end_ref = j;
+        }
+        if (v.any(v.or_(v.cmpgt(vNegLimit, vSatMin), v.cmpgt(vSatMax, vPosLimit)))) break;
+    }
+    if (pr.s2_end) {
+        end_query = s1Len - 1;
+        score = v.extract(vMaxH, lastLane);
+        matches = v.extract(vMaxHM, lastLane);
+        similar = v.extract(vMaxHS, lastLane);
+        length = v.extract(vMaxHL, lastLane);
+    }
+    if (pr.s1_end) {
+        for (int i = 0; i < segLen; ++i) {
+            const V th = v.load(hs, i), tm = v.load(hms, i), ts = v.load(hss, i), tl = v.load(hls, i);
+            for (int l = 0; l < L; ++l) {
+                const int temp = i + l * segLen;
+                if (temp >= s1Len) continue;
+                const int t = v.extract(th, l);
+                if (t > score) {
+                    score = t; end_query = temp; end_ref = s2Len - 1;
+                    matches = v.extract(tm, l); similar = v.extract(ts, l); length = v.extract(tl, l);
+                } else if (t == score && end_ref == s2Len - 1 && temp < end_query) {
+                    end_query = temp;
+                    matches = v.extract(tm, l); similar = v.extract(ts, l); length = v.extract(tl, l);
+                }
+            }
+        }
+    }
+    if (!pr.s1_end && !pr.s2_end) {
+        score = v.extract(v.load(hs, offset), lastLane);
+        matches = v.extract(v.load(hms, offset), lastLane);
+        similar = v.extract(v.load(hss, offset), lastLane);
+        length = v.extract(v.load(hls, offset), lastLane);
+        end_ref = s2Len - 1;
+        end_query = s1Len - 1;
+    }
+    o.saturated = v.any(v.or_(v.cmpgt(vNegLimit, vSatMin), v.cmpgt(vSatMax, vPosLimit))) ? 1 : 0;
+    if (o.saturated) { score = matches = similar = length = 0; end_query = end_ref = 0; }
+    o.score = score; o.end_query = end_query; o.end_ref = end_ref;
+    o.matches = matches; o.similar = similar; o.length = length;
+}
+
+/* ---- sw with statistics, biased lanes (the FASTSTATS prefix kernel) ---- */
+template <class P, int W>
+PB_LHD void striped_sw_stats_bias(P &v, const Problem &pr, Out &o)
+{
+    typedef typename P::V V;
+    constexpr int L = Lim<W>::LANES;
+    const int s1Len = pr.qlen, s2Len = pr.tlen;
+    const int segLen = (s1Len + L - 1) / L;
+    const int open = pr.open, gap = pr.gap;
+    const int bias = Lim<W>::MIN;
+    const V vGapO = v.set1(wrap<W>(open)), vGapE = v.set1(wrap<W>(gap));
+    const V vOne = v.set1(1);
+    const V vBias = v.set1(bias);
+    const V vBias1 = v.template adds<W>(vBias, vOne);
+    const V insert_mask = v.lane_eq(0);
+    const V vPosLimit = v.set1(Lim<W>::MAX);
+    const int maxp = wrap<W>((long long)Lim<W>::MAX - wrap<W>((long long)pr.mmax + 1));
+    V vMaxH = vBias, vMaxHUnit = vBias, vSatMax = vBias;
+    int score = bias, matches = bias, similar = bias, length = bias;
+    int end_query = 0, end_ref = 0;
+    int saturated = 0;
+
+    typename P::Arr hs = v.arr(0, segLen), hl = v.arr(1, segLen), hx = v.arr(2, segLen);
+    typename P::Arr hms = v.arr(3, segLen), hml = v.arr(4, segLen), hmx = v.arr(5, segLen);
+    typename P::Arr hss = v.arr(6, segLen), hsl = v.arr(7, segLen), hsx = v.arr(8, segLen);
+    typename P::Arr hls = v.arr(9, segLen), hll = v.arr(10, segLen), hlx = v.arr(11, segLen);
+    typename P::Arr pe = v.arr(12, segLen), pem = v.arr(13, segLen), pes = v.arr(14, segLen), pel = v.arr(15, segLen);
+    for (int i = 0; i < segLen; ++i) {
+        v.store(hs, i, vBias); v.store(hms, i, vBias); v.store(hss, i, vBias); v.store(hls, i, vBias);
+        v.store(pe, i, vBias); v.store(pem, i, vBias); v.store(pes, i, vBias); v.store(pel, i, vBias1);
+    }
+    int j;
+    for (j = 0; j < s2Len; ++j) {
+        const int k_t = pr.t[j];
+        V vF = vBias, vFM = vBias, vFS = vBias, vFL = vBias1;
+        V vH = v.blend(v.shift1(v.load(hs, segLen - 1)), vBias, insert_mask);
+        V vHM = v.blend(v.shift1(v.load(hms, segLen - 1)), vBias, insert_mask);
+        V vHS = v.blend(v.shift1(v.load(hss, segLen - 1)), vBias, insert_mask);
+        V vHL = v.blend(v.shift1(v.load(hls, segLen - 1)), vBias, insert_mask);
+        if (end_ref == j - 2) {
+            /* SWAP3(Max, Load, Store): Max <- Load, Load <- Store, Store <- old Max */
+            typename P::Arr t0;
+            t0 = hx; hx = hl; hl = hs; hs = t0;
+            t0 = hmx; hmx = hml; hml = hms; hms = t0;
+            t0 = hsx; hsx = hsl; hsl = hss; hss = t0;
+            t0 = hlx; hlx = hll; hll = hls; hls = t0;
+        } else {
+            typename P::Arr t0;
+            t0 = hl; hl = hs; hs = t0;
+            t0 = hml; hml = hms; hms = t0;
+            t0 = hsl; hsl = hss; hss = t0;
+            t0 = hll; hll = hls; hls = t0;
+        }
+        for (int i = 0; i < segLen; ++i) {
+            V vE = v.load(pe, i), vEM = v.load(pem, i), vES = v.load(pes, i), vEL = v.load(pel, i);
+            const V vH_dag = v.template adds<W>(vH, v.template prof<W>(pr, k_t, i, segLen));
+            vH = v.max(vH_dag, vE);
+            vH = v.max(vH, vF);
+            v.store(hs, i, vH);
+            const V cond_zero = v.cmpeq(vH, vBias);
+            V case1 = v.cmpeq(vH, vH_dag);
+            const V case2 = v.cmpeq(vH, vF);
+            vHM = v.blend(v.blend(vEM, vFM, case2), v.template adds<W>(vHM, v.template match<W>(pr, k_t, i, segLen)), case1);
+            vHM = v.blend(vHM, vBias, cond_zero);
+            v.store(hms, i, vHM);
+            vHS = v.blend(v.blend(vES, vFS, case2), v.template adds<W>(vHS, v.template similar<W>(pr, k_t, i, segLen)), case1);
+            vHS = v.blend(vHS, vBias, cond_zero);
+            v.store(hss, i, vHS);
+            vHL = v.blend(v.blend(vEL, vFL, case2), v.template adds<W>(vHL, vOne), case1);
+            vHL = v.blend(vHL, vBias, cond_zero);
+            v.store(hls, i, vHL);
+            vSatMax = v.max(vSatMax, vHM);
+            vSatMax = v.max(vSatMax, vHS);
+            vSatMax = v.max(vSatMax, vHL);
+            vMaxH = v.max(vH, vMaxH);
+            const V vEF_opn = v.template subs<W>(vH, vGapO);
+            const V vE_ext = v.template subs<W>(vE, vGapE);
+            vE = v.max(vEF_opn, vE_ext);
+            case1 = v.cmpgt(vEF_opn, vE_ext);
+            vEM = v.blend(vEM, vHM, case1);
+            vES = v.blend(vES, vHS, case1);
+            vEL = v.blend(v.template adds<W>(vEL, vOne), v.template adds<W>(vHL, vOne), case1);
+            v.store(pe, i, vE); v.store(pem, i, vEM); v.store(pes, i, vES); v.store(pel, i, vEL);
+            const V vF_ext = v.template subs<W>(vF, vGapE);
+            vF = v.max(vEF_opn, vF_ext);
+            case1 = v.cmpgt(vEF_opn, vF_ext);
+            vFM = v.blend(vFM, vHM, case1);
+            vFS = v.blend(vFS, vHS, case1);
+            vFL = v.blend(v.template adds<W>(vFL, vOne), v.template adds<W>(vHL, vOne), case1);
+            vH = v.load(hl, i); vHM = v.load(hml, i); vHS = v.load(hsl, i); vHL = v.load(hll, i);
+        }
+        {
+            bool done = false;
+            for (int k = 0; k < L && !done; ++k) {
+                V vHp = v.shift1(v.load(hl, segLen - 1));
+                vF = v.shift1(vF); vFM = v.shift1(vFM); vFS = v.shift1(vFS); vFL = v.shift1(vFL);
+                vHp = v.blend(vHp, vBias, insert_mask);
+                vF = v.blend(vF, vBias, insert_mask);
+                vFM = v.blend(vFM, vBias, insert_mask);
+                vFS = v.blend(vFS, vBias, insert_mask);
+                vFL = v.blend(vFL, vBias1, insert_mask);
+                for (int i = 0; i < segLen; ++i) {
+                    vHp = v.template adds<W>(vHp, v.template prof<W>(pr, k_t, i, segLen));
+                    vH = v.load(hs, i);
+                    vH = v.max(vH, vF);
+                    v.store(hs, i, vH);
+                    const V case1 = v.cmpeq(vH, vHp);
+                    const V case2 = v.cmpeq(vH, vF);
+                    V cond = v.andnot(case1, case2);
+                    vHM = v.blend(v.load(hms, i), vFM, cond); v.store(hms, i, vHM);
+                    vHS = v.blend(v.load(hss, i), vFS, cond); v.store(hss, i, vHS);
+                    vHL = v.blend(v.load(hls, i), vFL, cond); v.store(hls, i, vHL);
+                    vSatMax = v.max(vSatMax, vHM);
+                    vSatMax = v.max(vSatMax, vHS);
+                    vSatMax = v.max(vSatMax, vHL);
+                    vMaxH = v.max(vH, vMaxH);
+                    const V vEF_opn = v.template subs<W>(vH, vGapO);
+                    const V vF_ext = v.template subs<W>(vF, vGapE);
+                    if (!v.any(v.or_(v.cmpgt(vF_ext, vEF_opn),
+                                     v.and_(v.cmpeq(vF_ext, vEF_opn), v.cmpgt(vF_ext, vBias))))) { done = true; break; }
+                    vF = vF_ext;
+                    cond = v.cmpgt(vEF_opn, vF_ext);
+                    vFM = v.blend(vFM, vHM, cond);
+                    vFS = v.blend(vFS, vHS, cond);
+                    vFL = v.blend(v.template adds<W>(vFL, vOne), v.template adds<W>(vHL, vOne), cond);
+                    vHp = v.load(hl, i);
+                }
+            }
+        }
+        if (v.any(v.cmpgt(vMaxH, vMaxHUnit))) {
+            score = v.hmax(vMaxH);
+            if (score > maxp) { saturated = 1; break; }
+            vMaxHUnit = v.set1(score);
+            end_ref = j;
+        }
+        if (v.any(v.cmpeq(vSatMax, vPosLimit))) { saturated = 1; break; }
+    }
+    if (score == Lim<W>::MAX || v.any(v.cmpeq(vSatMax, vPosLimit))) saturated = 1;
+    if (saturated) {
+        score = end_query = end_ref = matches = similar = length = 0;
+    } else {
+        typename P::Arr tx = hx, tmx = hmx, tsx = hsx, tlx = hlx;
+        if (end_ref == j - 1) { tx = hs; tmx = hms; tsx = hss; tlx = hls; }
+        else if (end_ref == j - 2) { tx = hl; tmx = hml; tsx = hsl; tlx = hll; }
+        end_query = s1Len;
+        for (int i = 0; i < segLen; ++i) {
+            const V th = v.load(tx, i), tm = v.load(tmx, i), ts = v.load(tsx, i), tl = v.load(tlx, i);
+            for (int l = 0; l < L; ++l) {
+                if (v.extract(th, l) == score) {
+                    const int temp = i + l * segLen;
+                    if (temp < end_query) {
+                        end_query = temp;
+                        matches = v.extract(tm, l); similar = v.extract(ts, l); length = v.extract(tl, l);
+                    }
+                }
+            }
+        }
+    }
+    o.saturated = saturated;
+    o.score = score - bias;
+    o.end_query = end_query;
+    o.end_ref = end_ref;
+    o.matches = matches - bias;
+    o.similar = similar - bias;
+    o.length = length - bias;
+}
+
+}  // namespace lane
+}  // namespace pb
+
+#endif

@@ -7,6 +7,9 @@
  * Layout of the array for a call of n pairs (each region 256-byte aligned):
  *   [profile descriptor | n per-pair kernel outputs | n + 1 strip offsets |
  *    strip buffers: (target length) x (2 ints score-only, 8 with statistics)]
+ * Once the exact kernel is done, the strip region is reused for the
+ * resolution's work area (lists and results of the lane-exact rounds, and
+ * the lane kernel's per-warp arrays).
  * Every region is written by the call before it is read (descriptor copy,
  * offset scan, the exact kernel's per-pair outputs; a strip buffer's first
  * strip reads the top boundary, not the buffer), so nothing has to start at
@@ -169,8 +172,19 @@ int pb_cuda_noalloc_run(const pb_job *job, const pb_batch *b, pb_record *d_rec)
         p.scratch = d_strip; p.soff = d_soff; p.out = d_out;
         p.mat = nullptr; p.msize = 0; p.qall = nullptr; p.qoff = nullptr; p.qlen = nullptr;
         pb::launch_exact(p, b->alg, b->stats != 0, st);
-        pb::launch_resolve(*job, d_out, nullptr, nullptr, prof->qlen, b->d_tlen, n, d_rec, st);
-        pb_diag_count_launch(2);
+        pb_diag_count_launch(1);
+        if (cudaGetLastError() != cudaSuccess) goto fail;
+        /* the resolution's work area (lane-exact rounds) reuses the strip
+         * region: the exact kernel is done with it, in stream order */
+        const pb_lane_args la = pb::lane_args_of(b, 0, d_out);
+        const int rr = pb::resolve_rounds(*job, la, d_out, nullptr, nullptr, prof->qlen, b->d_tlen, n, d_rec, st,
+                                          base + off_strip, PB_NOALLOC_SCRATCH_BYTES - off_strip);
+        if (rr == -2) {
+            snprintf(g_noalloc_err, sizeof g_noalloc_err,
+                     "%d pairs need more resolution work space than the static scratch has left", n);
+            return -1;
+        }
+        if (rr != 0) goto fail;
     }
     if (cudaGetLastError() != cudaSuccess) goto fail;
     if (cudaStreamSynchronize(st) != cudaSuccess) goto fail;

@@ -28,8 +28,10 @@
  * rows up to ceil(qlen/lanes)*lanes (lanes = 32, 16, 8 for 8, 16, 32 bits);
  * the exact kernel reports those rows' extremes separately. Checks that read
  * the striped first pass (values before the lazy-F correction) are decided
- * here from sound bounds; a pair whose verdict the bounds cannot settle is
- * PB_AMBIG and goes to the lane-exact striped kernel.
+ * here from sound bounds where the bounds show a CLEAN run; any other verdict
+ * of an 8/16-bit striped kernel comes from the lane-exact restatement of that
+ * kernel (pb_lane.cuh), which also reproduces the reference's results in the
+ * cases where its narrow kernels return unflagged wrong values.
  */
 #ifndef PARASAIL_B200_PB_RESOLVE_H
 #define PARASAIL_B200_PB_RESOLVE_H
@@ -152,12 +154,31 @@ typedef struct pb_job {
     int base_flags;
 } pb_job;
 
-/* Compact per-pair result; `ambig` counts widths decided by the bounds'
- * fallback rule rather than exactly (see pb_resolve_tier). */
+/* Compact per-pair result. `ambig`: 0 when every width was decided
+ * exactly; PB_REC_FALLBACK when a scan or 32-bit verdict came from the
+ * bounds' fallback rule (pb_ambig_fallback); 8 or 16 while the pair still
+ * waits for the lane-exact kernel of that width (never in a finished
+ * record). */
 typedef struct pb_record {
     int score, end_query, end_ref, flag;
     int matches, similar, length, ambig;
 } pb_record;
+
+enum { PB_REC_FALLBACK = 1 };
+
+/* Widths whose verdict the lane-exact kernels (pb_lane.cuh) give whenever
+ * the exact values do not show a CLEAN run: the 8/16-bit striped nw/sg
+ * kernels and the 8/16-bit SW statistics kernel of the FASTSTATS wrapper. */
+PB_HD static inline int pb_lane_applies(const pb_mode *m, int bits)
+{
+    return m->striped && (bits == 8 || bits == 16) && (m->alg != PB_SW || m->stats);
+}
+
+/* lane kernel kind for a mode (pb_lane_args.kind) */
+PB_HD static inline int pb_lane_kind(const pb_mode *m)
+{
+    return m->alg == PB_SW ? 2 : (m->stats ? 1 : 0);
+}
 
 PB_HD static inline int pb_bits_flag(int bits)
 {
@@ -215,16 +236,21 @@ PB_HD static inline int pb_ambig_fallback(const pb_mode *m, int bits, const pb_p
 
 /* The result the reference returns for one pair (src/satcheck.c chains,
  * the kernels' sentinel values, the FASTSTATS wrapper). o2 is the prefix
- * pass (FASTSTATS only, may be NULL when pb_needs_pass2 said no). */
+ * pass (FASTSTATS only, may be NULL when pb_needs_pass2 said no). e8/e16 are
+ * the lane-exact kernels' results for the pair (NULL or not valid when they
+ * have not run); when a width needs one that is missing, the returned record
+ * has ambig = that width and nothing else in it is final. */
 PB_HD static inline pb_record pb_chain_resolve(const pb_job *j, const pb_pair_out *o1,
-                                               const pb_pair_out *o2, int qlen, int tlen)
+                                               const pb_pair_out *o2, int qlen, int tlen,
+                                               const pb_lane_res *e8, const pb_lane_res *e16)
 {
     const int w3[3] = {8, 16, 32};
     const pb_mode *m = &j->mode;
     pb_record r;
-    int f, l, t;
+    int f, l, t, fallback = 0;
     r.score = r.end_query = r.end_ref = r.matches = r.similar = r.length = 0;
     r.ambig = 0;
+    r.flag = 0;
     if (j->bits < 0) {   /* serial forms: exact 32-bit, flags given */
         r.score = o1->score; r.end_query = o1->end_query; r.end_ref = o1->end_ref;
         r.matches = o1->matches; r.similar = o1->similar; r.length = o1->length;
@@ -235,6 +261,7 @@ PB_HD static inline pb_record pb_chain_resolve(const pb_job *j, const pb_pair_ou
     for (t = f; t <= l; ++t) {
         const int w = w3[t];
         const int fl = j->base_flags | pb_bits_flag(w) | pb_lanes_flag(w);
+        const pb_lane_res *e = w == 8 ? e8 : w == 16 ? e16 : (const pb_lane_res *)0;
         int v;
         if (pb_job_is_faststats(j)) {
             if (pb_resolve_faststats_pass1(m, w, o1) == PB_SAT) {
@@ -242,33 +269,62 @@ PB_HD static inline pb_record pb_chain_resolve(const pb_job *j, const pb_pair_ou
                 /* the score-only pass's saturated result, without stats */
                 r.score = w == 8 ? 255 : w == 16 ? 65535 : 0x7fffffff;
                 r.flag = fl | PARASAIL_FLAG_SATURATED;
+                r.ambig = fallback;
                 return r;
             }
             v = pb_resolve_tier(m, w, o2, o1->end_query + 1, o1->end_ref + 1);
-            if (v == PB_AMBIG) { r.ambig++; v = pb_ambig_fallback(m, w, o2, o1->end_query + 1, o1->end_ref + 1); }
+            if (v != PB_CLEAN && pb_lane_applies(m, w)) {
+                /* the prefix kernel's own result, ends from the score pass */
+                if (!e || !e->valid) { r.ambig = w; return r; }
+                if (e->saturated && t < l) continue;
+                r.score = e->score; r.end_query = o1->end_query; r.end_ref = o1->end_ref;
+                r.matches = e->matches; r.similar = e->similar; r.length = e->length;
+                r.flag = fl | PARASAIL_FLAG_STATS | (e->saturated ? PARASAIL_FLAG_SATURATED : 0);
+                r.ambig = fallback;
+                return r;
+            }
+            if (v == PB_AMBIG) { fallback = PB_REC_FALLBACK; v = pb_ambig_fallback(m, w, o2, o1->end_query + 1, o1->end_ref + 1); }
             if (v == PB_SAT) {
                 if (t < l) continue;
                 r.end_query = o1->end_query; r.end_ref = o1->end_ref;
                 r.flag = fl | PARASAIL_FLAG_SATURATED | PARASAIL_FLAG_STATS;
+                r.ambig = fallback;
                 return r;
             }
             r.score = o1->score; r.end_query = o1->end_query; r.end_ref = o1->end_ref;
             r.matches = o2->matches; r.similar = o2->similar; r.length = o2->length;
             r.flag = fl | PARASAIL_FLAG_STATS;
+            r.ambig = fallback;
             return r;
         }
         v = pb_resolve_tier(m, w, o1, qlen, tlen);
-        if (v == PB_AMBIG) { r.ambig++; v = pb_ambig_fallback(m, w, o1, qlen, tlen); }
+        if (v != PB_CLEAN && pb_lane_applies(m, w)) {
+            if (!e || !e->valid) { r.ambig = w; return r; }
+            if (e->saturated) {
+                if (t < l) continue;
+                r.flag = fl | PARASAIL_FLAG_SATURATED | (m->stats ? PARASAIL_FLAG_STATS : 0);
+                r.ambig = fallback;
+                return r;
+            }
+            r.score = e->score; r.end_query = e->end_query; r.end_ref = e->end_ref;
+            if (m->stats) { r.matches = e->matches; r.similar = e->similar; r.length = e->length; }
+            r.flag = fl | (m->stats ? PARASAIL_FLAG_STATS : 0);
+            r.ambig = fallback;
+            return r;
+        }
+        if (v == PB_AMBIG) { fallback = PB_REC_FALLBACK; v = pb_ambig_fallback(m, w, o1, qlen, tlen); }
         if (v == PB_SAT) {
             if (t < l) continue;
             if (m->alg == PB_SW && m->striped && !m->stats)
                 r.score = w == 8 ? 255 : w == 16 ? 65535 : 0x7fffffff;
             r.flag = fl | PARASAIL_FLAG_SATURATED | (m->stats ? PARASAIL_FLAG_STATS : 0);
+            r.ambig = fallback;
             return r;
         }
         r.score = o1->score; r.end_query = o1->end_query; r.end_ref = o1->end_ref;
         r.matches = o1->matches; r.similar = o1->similar; r.length = o1->length;
         r.flag = fl | (m->stats ? PARASAIL_FLAG_STATS : 0);
+        r.ambig = fallback;
         return r;
     }
     return r;

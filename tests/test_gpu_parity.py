@@ -153,3 +153,35 @@ def test_nw_banded_vs_oracle():
         exp = O.nw_banded(q, t, 5, 2, k, om)
         assert (got["score"], got["end_query"], got["end_ref"]) == (exp["score"], exp["end_query"], exp["end_ref"])
         assert got["flag"] & pb.FLAG_BANDED
+
+
+@pytest.mark.skipif(O.ref() is None, reason="reference library not built")
+@pytest.mark.parametrize("width", ["8", "16", "sat"])
+def test_batch_striped_narrow_vs_live_reference(width):
+    """Batches through the device pipeline, including its lane-exact rounds
+    for the 8/16-bit striped kernels, against the reference's AVX2 kernels on
+    every pair: score, ends, statistics and flags."""
+    rng = random.Random({"8": 81, "16": 161, "sat": 7}[width])
+    b62 = pb.matrix_lookup("blosum62")
+    dna = pb.matrix_create("ACGT", 2, -3)
+    bad, total = [], 0
+    for alg_name in ("nw", "sg_qx", "sg_qe_db", "sg_de", "sw"):
+        for stats in (0, 1):
+            if alg_name == "sw" and not stats:
+                continue
+            for key, m, a, op, gp in (("blosum62", b62, AA, 11, 1), (("ACGT", 2, -3), dna, DNA, 5, 2)):
+                q = rand_seq(rng, rng.randint(10, 220), a)
+                targets = [mutate(rng, q, a, 0.25, 0.04) if k % 3 == 0 else rand_seq(rng, rng.randint(5, 260), a)
+                           for k in range(60)]
+                st = "_stats" if stats else ""
+                prof = pb.ProfileHandle("parasail_profile_create%s_%s" % (st, width), q, m)
+                name = "%s%s_striped_profile_%s" % (alg_name, st, width)
+                recs = pb.records_to_dicts(pb.batch_profile(name, prof, targets, op, gp), stats)
+                prof.close()
+                for t, r in zip(targets, recs):
+                    exp = O.ref_vector(alg_name, stats, "striped", width, q, t, op, gp, key)
+                    total += 1
+                    if any(r.get(k) != v for k, v in exp.items()):
+                        bad.append((name, key, q, t, r, exp))
+    assert total >= 500
+    assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])
