@@ -134,14 +134,30 @@ k_sw16(Sw16Params p, int *task_counter)
             const int8_t *pa_base = prof + r0;
             const int8_t *pb_base = prof + r0 + SW16_R;
             const bool more = r0 + 2 * SW16_R < ql;
+            /* the residue and the previous pass's boundary of a column are
+             * loaded two columns ahead: both come from L2 or DRAM, and the
+             * two-op chain of one column is too short to cover that latency
+             * (this pass overwrites buf[j-1] at column j, never buf[j+2]) */
+            const uint2 vnone = make_uint2(0u, gapO);
+            int c_n1 = 0 < len ? tseq[0] : 0;
+            int c_n2 = 1 < len ? tseq[1] : 0;
+            uint2 v_n1 = vnone, v_n2 = vnone;
+            if (r0 != 0) {
+                if (0 < wmax) v_n1 = buf[lane];
+                if (1 < wmax) v_n2 = buf[32 + lane];
+            }
             for (int j = 0; j <= wmax; ++j) {
-                const int ca = j < len ? tseq[j] : 0;
+                const int ca = c_n1;
+                c_n1 = c_n2;
+                c_n2 = j + 2 < len ? tseq[j + 2] : 0;
                 uint32_t hu, fu;
                 if (r0 == 0) {
                     hu = prev_h << 16;                      /* top row H = 0 */
                     fu = prmt(gapO, prev_f, 0x5410u);       /* top row F = -inf */
                 } else {
-                    const uint2 v = j < wmax ? buf[(size_t)j * 32 + lane] : make_uint2(0u, gapO);
+                    const uint2 v = v_n1;
+                    v_n1 = v_n2;
+                    v_n2 = j + 2 < wmax ? buf[(size_t)(j + 2) * 32 + lane] : vnone;
                     hu = prmt(v.x, prev_h, 0x5432u);        /* lo <- previous pass's strip B bottom */
                     fu = prmt(v.y, prev_f, 0x5432u);
                 }
