@@ -68,8 +68,8 @@ __device__ __forceinline__ int sext_byte(uint32_t lo, uint32_t hi, int k)
  */
 static constexpr long long NWL_SPIN = 1ll << 26;
 
-template <bool BANDED>
-__global__ void __launch_bounds__(NWL_WARPS * 32)
+template <bool BANDED, bool GE>
+__global__ void __launch_bounds__(NWL_WARPS * 32, 3)
 k_nw_wave(NwWaveParams p, int *counter, int *error)
 {
     __shared__ __align__(16) int8_t s_mat[32 * 32];
@@ -161,71 +161,97 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
             }
             int sh_h = NWL_NEG, sh_f = NWL_NEG;
             const int tend = jhi + 31;
-            /* residue and score row of this lane's next column, loaded one
-             * iteration ahead */
-            int jn = jlo - lane;
-            int tc_next = (jn >= jlo && jn <= jhi) ? ts[jn] : 0;
+            /* this lane's target residues, loaded two columns ahead */
+            auto res_at = [&](int c) -> int { return (c >= jlo && c <= jhi) ? (int)ts[c] : 0; };
+            int tc_n1 = res_at(jlo - lane), tc_n2 = res_at(jlo - lane + 1);
+            /* the previous pass's bottom row, one 32-column chunk per
+             * register (lane l holds column chunk start + l; lane 0 takes its
+             * column by shuffle), loaded one chunk ahead so that the L2
+             * latency is off the column loop. A chunk is read only after the
+             * previous pass has published the next one. */
+            auto ring_at = [&](int c) -> int2 {
+                return (pass > 0 && c >= prev_jlo && c <= prev_jhi) ? __ldcg(&in_buf[c])
+                                                                      : make_int2(NWL_NEG, NWL_NEG);
+            };
+            int2 cur_v = make_int2(NWL_NEG, NWL_NEG), nxt_v = cur_v;
             bool aborted = false;
             for (int it = jlo; it <= tend; ++it) {
                 const int j = it - lane;
-                if (((it - jlo) & 31) == 0) {
+                const int cpos = (it - jlo) & 31;
+                if (cpos == 0) {
                     bool ok = true;
-                    if (lane == 0) ok = wait_for(min(it + 31, jhi));
+                    if (lane == 0) ok = wait_for(it + 63);
                     ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0);
                     if (!ok) { aborted = true; break; }
+                    cur_v = it == jlo ? ring_at(it + lane) : nxt_v;
+                    nxt_v = ring_at(it + 32 + lane);
                 }
+                const int vh = __shfl_sync(0xffffffffu, cur_v.x, cpos);
+                const int vf = __shfl_sync(0xffffffffu, cur_v.y, cpos);
                 int up_h = __shfl_up_sync(0xffffffffu, sh_h, 1);
                 int up_f = __shfl_up_sync(0xffffffffu, sh_f, 1);
                 const bool active = j >= jlo && j <= jhi;
-                const int tc = tc_next;
-                jn = j + 1;
-                tc_next = (jn >= jlo && jn <= jhi) ? ts[jn] : 0;
+                const int tc = tc_n1;
+                tc_n1 = tc_n2;
+                tc_n2 = res_at(j + 2);
                 if (lane == 0 && active) {
                     if (r0 == 0) {
                         const bool inb = !BANDED || (-1 - j >= lo && -1 - j <= hi);
                         up_h = inb ? -open - j * gap : NWL_NEG;
                         up_f = NWL_NEG;
-                    } else if (j <= prev_jhi && j >= prev_jlo) {
-                        const int2 v = __ldcg(&in_buf[j]);
-                        up_h = v.x;
-                        up_f = v.y;
                     } else {
-                        up_h = NWL_NEG;
-                        up_f = NWL_NEG;
+                        up_h = vh;
+                        up_f = vf;
                     }
                 }
                 if (active) {
                     int hd = dg;
-                    int hu = up_h, fu = up_f;
                     uint32_t row_lo = 0, row_hi = 0;
                     if (p.small_alpha) {
                         row_lo = *reinterpret_cast<const uint32_t *>(s_mat + tc * 32);
                         row_hi = *reinterpret_cast<const uint32_t *>(s_mat + tc * 32 + 4);
                     }
+                    /* F of row R0 from the row above (previous lane or pass) */
+                    int f = max(up_f - gap, up_h - open);
+                    /* row R0 + r lies in the band iff 0 <= R0 + r - j - lo <= hi - lo */
+                    const int dlo = R0 - j - lo;
+                    const unsigned bw = (unsigned)(hi - lo);
+                    int last_h = 0, last_f = 0;
 #pragma unroll
                     for (int r = 0; r < NWL_RL; ++r) {
-                        const int i = R0 + r;
                         const int sc = p.small_alpha ? sext_byte(row_lo, row_hi, qc[r]) : (int)s_mat[tc * 32 + qc[r]];
-                        const int e = max(E[r] - gap, Hl[r] - open);
-                        const int f = max(fu - gap, hu - open);
-                        int h = max(max(hd + sc, e), f);
-                        int ee = e, ff = f;
+                        /* E and the diagonal/E part a are off the row-to-row chain */
+                        int e = max(E[r] - gap, Hl[r] - open);
+                        int a = __viaddmax_s32(hd, sc, e);
                         if (BANDED) {
-                            const int d = i - j;
-                            if (d < lo || d > hi) { h = NWL_NEG; ee = NWL_NEG; ff = NWL_NEG; }
+                            const bool in = (unsigned)(dlo + r) <= bw;
+                            e = in ? e : NWL_NEG;
+                            a = in ? a : NWL_NEG;
+                            f = in ? f : NWL_NEG;
                         }
-                        if (i == n - 1 && j == m - 1) { result = h; have_result = true; }
-                        E[r] = ee;
+                        const int h = max(a, f);
+                        last_h = h;
+                        last_f = f;
+                        /* F of the next row: max(F - gap, H - open). With
+                         * open >= gap, H - open = max(a, F) - open and
+                         * F - open <= F - gap, so only a - open is needed:
+                         * one dependent operation per row */
+                        if (GE) f = __viaddmax_s32(f, -gap, a - open);
+                        else f = max(f - gap, h - open);
+                        E[r] = e;
                         hd = Hl[r];
                         Hl[r] = h;
-                        hu = h;
-                        fu = ff;
+                    }
+                    if (j == m - 1 && R0 <= n - 1 && n - 1 < R0 + NWL_RL) {
+#pragma unroll
+                        for (int r = 0; r < NWL_RL; ++r)
+                            if (R0 + r == n - 1) { result = Hl[r]; have_result = true; }
                     }
                     dg = up_h;
-                    sh_h = hu;
-                    sh_f = fu;
+                    sh_h = last_h;
+                    sh_f = last_f;
                     if (lane == 31 && pass + 1 < npass) {
-                        out_buf[j] = make_int2(hu, fu);
+                        out_buf[j] = make_int2(last_h, last_f);
                         if (((j - jlo) & 31) == 31 || j == jhi) {
                             __threadfence_block();
                             *out_prog = out_base + j;
@@ -299,8 +325,12 @@ extern "C" int pb_cuda_nw_long(int npairs, int open, int gap, const int32_t *h_m
     int nsm = 0, dev = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (d_lo) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pb::k_nw_wave<true>, pb::NWL_WARPS * 32, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pb::k_nw_wave<false>, pb::NWL_WARPS * 32, 0);
+    /* the one-operation F chain needs open >= gap */
+    const bool ge = open >= gap;
+    void (*kern)(pb::NwWaveParams, int *, int *) =
+        d_lo ? (ge ? pb::k_nw_wave<true, true> : pb::k_nw_wave<true, false>)
+             : (ge ? pb::k_nw_wave<false, true> : pb::k_nw_wave<false, false>);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, pb::NWL_WARPS * 32, 0);
     if (per_sm < 1) per_sm = 1;
     int blocks = per_sm * nsm;
     if (blocks > npairs) blocks = npairs;
@@ -317,8 +347,7 @@ extern "C" int pb_cuda_nw_long(int npairs, int open, int gap, const int32_t *h_m
         p.mat = d_mat; p.q = d_q; p.qoff = d_qoff; p.qlen = d_qlen;
         p.t = d_t; p.toff = d_toff; p.tlen = d_tlen; p.lo = d_lo; p.hi = d_hi;
         p.order = order; p.scratch = scratch; p.maxlen = maxlen + 1; p.score = d_score;
-        if (d_lo) pb::k_nw_wave<true><<<blocks, pb::NWL_WARPS * 32, 0, st>>>(p, counter, d_err);
-        else pb::k_nw_wave<false><<<blocks, pb::NWL_WARPS * 32, 0, st>>>(p, counter, d_err);
+        kern<<<blocks, pb::NWL_WARPS * 32, 0, st>>>(p, counter, d_err);
         if (cudaGetLastError() != cudaSuccess) rc = -1;
         pb_diag_count_launch(3);
         cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st);

@@ -56,6 +56,9 @@ def test_nw_long_vs_oracle_dna_and_protein():
     pt = [mutate(rng, p, AA, 0.3, 0.05) for p in ps]
     got = pb.nw_long(b62, *_pack(ps), *_pack(pt), 11, 1)
     assert got.tolist() == [O.align(O.NW, 0, 0, q, t, 11, 1, ob)["score"] for q, t in zip(ps, pt)]
+    # open < gap takes the kernel's general F recurrence
+    got = pb.nw_long(dna, *_pack(qs[:40]), *_pack(ts[:40]), 1, 3)
+    assert got.tolist() == [O.align(O.NW, 0, 0, q, t, 1, 3, om)["score"] for q, t in zip(qs[:40], ts[:40])]
 
 
 def test_banded_vs_oracle_and_certificate_soundness():
