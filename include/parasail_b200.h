@@ -162,14 +162,21 @@ extern int parasail_b200_band_model_gradients(
         const parasail_b200_band_model_t *model, const float *x, const float *target, int n, float tau,
         float *grad_weights, float *grad_biases, float *loss);
 /** Trains on the GPU with Adam: labels are the smallest certifiable band of
- * each pair's optimal score from the full-DP kernel. */
+ * each pair's optimal score from the full-DP kernel. The last tenth of the
+ * pairs (when n >= 20) is held out of the gradient steps and then chooses
+ * the band scaling: the widen factor (of 1.0 ... 3.0) with the least
+ * expected DP work, band cells plus a full DP for every pair whose band
+ * would fail the certificate. */
 extern int parasail_b200_band_model_train(
         parasail_b200_band_model_t *model, const parasail_matrix_t *matrix,
         const char *queries, const int64_t *qoffsets, const int *qlengths,
         const char *targets, const int64_t *toffsets, const int *tlengths, int n,
         int open, int gap, int epochs, int batch, float lr, float *final_loss);
+/** The band scaling chosen at training (widen factor, slack diagonals). */
+extern void parasail_b200_band_model_scaling(const parasail_b200_band_model_t *model, float *widen, int *slack);
 /** Global alignment scores through the learned band: predicted band
- * (half-width scaled by `widen`, plus `slack` diagonals), banded DP,
+ * (half-width scaled by `widen`, plus `slack` diagonals; widen <= 0 and
+ * slack < 0 take the scaling chosen at training), banded DP,
  * exactness certificate, full-DP fallback. scores[] always equals
  * parasail_b200_nw_long's; band_lo/band_hi receive the bands used (the
  * whole matrix for fallback pairs), either may be NULL. */

@@ -302,6 +302,8 @@ lib.parasail_b200_band_model_new.argtypes = [ctypes.c_uint]
 lib.parasail_b200_band_model_free.argtypes = [_V]
 lib.parasail_b200_band_model_sizes.argtypes = [ctypes.POINTER(ctypes.c_int)] * 5
 lib.parasail_b200_band_model_get.argtypes = [_V, _V, _V]
+lib.parasail_b200_band_model_scaling.restype = None
+lib.parasail_b200_band_model_scaling.argtypes = [_V, _V, _V]
 lib.parasail_b200_band_model_set.argtypes = [_V, _V, _V]
 lib.parasail_b200_band_features.argtypes = [_MP, _V, _V, _V, _V, _V, _V, ctypes.c_int, _V]
 lib.parasail_b200_band_model_gradients.argtypes = [_V, _V, _V, ctypes.c_int, ctypes.c_float, _V, _V,
@@ -363,6 +365,12 @@ class BandModel:
         b = np.ascontiguousarray(b, np.float32)
         if lib.parasail_b200_band_model_set(self.ptr, w.ctypes.data, b.ctypes.data) != 0:
             raise RuntimeError("set failed")
+
+    def scaling(self):
+        """(widen, slack) chosen at training on held-out pairs."""
+        w, sl = ctypes.c_float(), ctypes.c_int()
+        lib.parasail_b200_band_model_scaling(self.ptr, ctypes.byref(w), ctypes.byref(sl))
+        return float(w.value), int(sl.value)
 
     def gradients(self, x, target, tau):
         np = _np()

@@ -34,6 +34,9 @@ int pb_cuda_band_from_pred(int npairs, const int *d_qlen, const int *d_tlen, con
                            float widen, int slack, int *d_lo, int *d_hi);
 int pb_cuda_band_certify(int npairs, int a, int open, int ext, const int *d_qlen, const int *d_tlen,
                          const int *d_lo, const int *d_hi, const int *d_score, int *d_cert, int *h_failures);
+int pb_cuda_band_tune(struct pb_band_model *m, int n, const float *d_x, const int *d_qlen, const int *d_tlen,
+                      const int *d_lab_lo, const int *d_lab_hi, float *chosen);
+void pb_cuda_band_scaling(const struct pb_band_model *m, float *widen, int *slack);
 int pb_cuda_band_cells(int npairs, const int *d_qlen, const int *d_tlen, const int *d_lo, const int *d_hi,
                        unsigned long long *h_cells);
 
@@ -157,6 +160,11 @@ int parasail_b200_band_model_get(const parasail_b200_band_model_t *model, float 
     return model ? pb_cuda_band_model_get((const struct pb_band_model *)model, weights, biases) : -1;
 }
 
+void parasail_b200_band_model_scaling(const parasail_b200_band_model_t *model, float *widen, int *slack)
+{
+    if (model) pb_cuda_band_scaling((const struct pb_band_model *)model, widen, slack);
+}
+
 int parasail_b200_band_model_set(parasail_b200_band_model_t *model, const float *weights, const float *biases)
 {
     return (model && weights && biases) ? pb_cuda_band_model_set((struct pb_band_model *)model, weights, biases) : -1;
@@ -211,9 +219,9 @@ int parasail_b200_band_model_train(parasail_b200_band_model_t *model, const para
                                    int open, int gap, int epochs, int batch, float lr, float *final_loss)
 {
     dev_pairs d;
-    int nin, nh, no, nw, nb, rc, e, s;
+    int nin, nh, no, nw, nb, rc, e, s, n_tr, n_tune;
     float *d_feat, *d_tgt, *d_gw, *d_gb, loss = 0.0f;
-    int *d_score;
+    int *d_score, *d_lab_lo, *d_lab_hi;
     if (!model || !long_ok(__func__, matrix, open, gap)) return -1;
     if (n <= 0 || epochs <= 0 || batch <= 0) return -1;
     pb_cuda_band_sizes(&nin, &nh, &no, &nw, &nb);
@@ -223,16 +231,22 @@ int parasail_b200_band_model_train(parasail_b200_band_model_t *model, const para
     d_score = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
     d_gw = (float *)pb_cuda_malloc(sizeof(float) * (size_t)nw);
     d_gb = (float *)pb_cuda_malloc(sizeof(float) * (size_t)nb);
+    d_lab_lo = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    d_lab_hi = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
     pb_cuda_sync();
+    /* the last tenth of the pairs is held out of the gradient steps and
+     * chooses the band scaling afterwards */
+    n_tune = n >= 20 ? n / 10 : 0;
+    n_tr = n - n_tune;
     /* labels: the smallest certifiable band of the full-DP optimum */
     rc = pb_cuda_band_features(n, d.q, d.qoff, d.qlen, d.t, d.toff, d.tlen, d_feat);
     if (rc == 0) rc = run_full(matrix, &d, open, gap, d_score);
-    if (rc == 0) rc = pb_cuda_band_labels(n, matrix->max, open, gap, d.qlen, d.tlen, d_score, d_tgt, NULL, NULL);
+    if (rc == 0) rc = pb_cuda_band_labels(n, matrix->max, open, gap, d.qlen, d.tlen, d_score, d_tgt, d_lab_lo, d_lab_hi);
     for (e = 0; rc == 0 && e < epochs; ++e) {
         double tot = 0.0;
         int nbat = 0;
-        for (s = 0; rc == 0 && s < n; s += batch) {
-            const int bn = (n - s) < batch ? (n - s) : batch;
+        for (s = 0; rc == 0 && s < n_tr; s += batch) {
+            const int bn = (n_tr - s) < batch ? (n_tr - s) : batch;
             float l = 0.0f;
             rc = pb_cuda_band_gradients((const struct pb_band_model *)model, bn, d_feat + (size_t)s * nin,
                                         d_tgt + (size_t)s * no, BAND_TAU, d_gw, d_gb, &l);
@@ -242,8 +256,12 @@ int parasail_b200_band_model_train(parasail_b200_band_model_t *model, const para
         }
         loss = (float)(tot / (nbat ? nbat : 1));
     }
+    if (rc == 0 && n_tune > 0)
+        rc = pb_cuda_band_tune((struct pb_band_model *)model, n_tune, d_feat + (size_t)n_tr * nin, d.qlen + n_tr,
+                               d.tlen + n_tr, d_lab_lo + n_tr, d_lab_hi + n_tr, NULL);
     if (final_loss) *final_loss = loss;
     pb_cuda_free(d_feat); pb_cuda_free(d_tgt); pb_cuda_free(d_score); pb_cuda_free(d_gw); pb_cuda_free(d_gb);
+    pb_cuda_free(d_lab_lo); pb_cuda_free(d_lab_hi);
     dev_pairs_free(&d);
     return rc;
 }
@@ -258,6 +276,14 @@ static int learned_run(const struct pb_band_model *model, const parasail_matrix_
     int *d_cert;
     const int n = d->n;
     pb_cuda_band_sizes(&nin, &nh, &no, &nw, &nb);
+    {
+        /* widen <= 0 / slack < 0: the scaling tuned at training */
+        float tw;
+        int ts;
+        pb_cuda_band_scaling(model, &tw, &ts);
+        if (widen <= 0.0f) widen = tw;
+        if (slack < 0) slack = ts;
+    }
     d_feat = (float *)pb_cuda_malloc(sizeof(float) * (size_t)n * nin);
     d_y = (float *)pb_cuda_malloc(sizeof(float) * (size_t)n * no);
     d_cert = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);

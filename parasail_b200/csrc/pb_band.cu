@@ -348,6 +348,27 @@ __global__ void k_band_cells(int npairs, const int *qlen, const int *tlen, const
     atomicAdd(cells, (unsigned long long)tot);
 }
 
+/* expected DP work of a band choice: the band's cells, plus a full DP for
+ * every pair whose band does not contain its label band (the smallest band
+ * the certificate accepts for the optimum, so the certificate would fail) */
+__global__ void k_tune_cost(int npairs, const int *qlen, const int *tlen, const int *lo, const int *hi,
+                            const int *lab_lo, const int *lab_hi, unsigned long long *cost)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const long long n = qlen[p], m = tlen[p];
+    long long tot = 0;
+    const long long dlo = lo[p] > -(m - 1) ? lo[p] : -(m - 1);
+    const long long dhi = hi[p] < n - 1 ? hi[p] : n - 1;
+    for (long long d = dlo; d <= dhi; ++d) {
+        const long long jmin = d < 0 ? -d : 0;
+        const long long jmax = (n - 1 - d) < (m - 1) ? (n - 1 - d) : (m - 1);
+        if (jmax >= jmin) tot += jmax - jmin + 1;
+    }
+    if (lo[p] > lab_lo[p] || hi[p] < lab_hi[p]) tot += n * m;
+    atomicAdd(cost, (unsigned long long)tot);
+}
+
 }  // namespace pb
 
 /* ======================================================================== */
@@ -359,6 +380,9 @@ struct pb_band_model {
     float *mw1, *mw2, *mb1, *mb2;
     __nv_bfloat16 *wb;
     int step;
+    /* band scaling chosen on held-out pairs after training */
+    float widen;
+    int slack;
 };
 
 static const int NW1 = pb::MLP_H * pb::MLP_IN, NW2 = pb::MLP_H * pb::MLP_H, NW3 = pb::MLP_OUT * pb::MLP_H;
@@ -381,6 +405,8 @@ extern "C" pb_band_model *pb_cuda_band_model_new(unsigned seed)
 {
     if (pb_cuda_init() != 0) return nullptr;
     pb_band_model *m = new pb_band_model();
+    m->widen = 1.1f;
+    m->slack = 32;
     std::vector<float> hw(NWT), hb(NBT, 0.0f);
     /* He-uniform initialisation from a fixed LCG (reproducible) */
     uint64_t s = 0x9E3779B97F4A7C15ull ^ seed;
@@ -564,6 +590,45 @@ extern "C" int pb_cuda_band_cells(int npairs, const int *d_qlen, const int *d_tl
     cudaMemcpy(h_cells, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
     cudaFree(d);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+/* Chooses the model's band scaling on n held-out pairs (features d_x,
+ * label bands d_lab_lo/d_lab_hi): the widen factor of a fixed grid with the
+ * least expected DP work (k_tune_cost). */
+extern "C" int pb_cuda_band_tune(pb_band_model *m, int n, const float *d_x, const int *d_qlen, const int *d_tlen,
+                                 const int *d_lab_lo, const int *d_lab_hi, float *chosen)
+{
+    static const float grid[] = {1.0f, 1.1f, 1.25f, 1.5f, 1.75f, 2.0f, 2.5f, 3.0f};
+    if (n <= 0) return -1;
+    float *y = nullptr;
+    int *lo = nullptr, *hi = nullptr;
+    unsigned long long *cost = nullptr;
+    cudaMalloc(&y, sizeof(float) * n * pb::MLP_OUT);
+    cudaMalloc(&lo, sizeof(int) * n);
+    cudaMalloc(&hi, sizeof(int) * n);
+    cudaMalloc(&cost, sizeof(unsigned long long));
+    int rc = pb_cuda_band_forward(m, n, d_x, nullptr, nullptr, y);
+    unsigned long long best = ~0ull;
+    float bw = m->widen;
+    for (unsigned g = 0; rc == 0 && g < sizeof grid / sizeof grid[0]; ++g) {
+        unsigned long long c = 0;
+        rc = pb_cuda_band_from_pred(n, d_qlen, d_tlen, y, grid[g], m->slack, lo, hi);
+        cudaMemset(cost, 0, sizeof(unsigned long long));
+        pb::k_tune_cost<<<(n + 127) / 128, 128>>>(n, d_qlen, d_tlen, lo, hi, d_lab_lo, d_lab_hi, cost);
+        pb_diag_count_launch(1);
+        if (cudaMemcpy(&c, cost, sizeof c, cudaMemcpyDeviceToHost) != cudaSuccess) rc = -1;
+        if (rc == 0 && c < best) { best = c; bw = grid[g]; }
+    }
+    if (rc == 0) m->widen = bw;
+    if (chosen) *chosen = m->widen;
+    cudaFree(y); cudaFree(lo); cudaFree(hi); cudaFree(cost);
+    return rc;
+}
+
+extern "C" void pb_cuda_band_scaling(const pb_band_model *m, float *widen, int *slack)
+{
+    if (widen) *widen = m->widen;
+    if (slack) *slack = m->slack;
 }
 
 /* host mirror of the certificate arithmetic, for the C host code */

@@ -27,14 +27,18 @@
 #include <algorithm>
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
+#include <cooperative_groups.h>
+#include <cuda/atomic>
 #include <cstdio>
+#include <type_traits>
 
 #include "pb_cuda.h"
 
 namespace pb {
 
 static constexpr int NWL_RL = 8;          /* query rows per lane */
-static constexpr int NWL_WARPS = 8;       /* warps per CTA, one CTA per pair */
+static constexpr int NWL_WARPS = 8;       /* warps per CTA */
+static constexpr int NWL_CLUSTER = 4;     /* CTAs per cluster for the largest pairs */
 static constexpr int NWL_NEG = INT32_MIN / 4;
 
 struct NwWaveParams {
@@ -43,11 +47,15 @@ struct NwWaveParams {
     const uint8_t *q; const int64_t *qoff; const int *qlen;
     const uint8_t *t; const int64_t *toff; const int *tlen;
     const int *lo; const int *hi; /* per pair band (diagonal i - j), or nullptr */
-    const int *order;             /* pairs, most cells first */
-    int2 *scratch;                /* per CTA: NWL_WARPS ring buffers of [maxlen] (H, F) */
+    const int *order;             /* pairs, cooperative ones first, then most cells first */
+    const unsigned long long *keys; /* sorted keys; bit 62 set: run by a whole cluster */
+    int2 *scratch;                /* per warp slot: a ring buffer of [maxlen] (H, F) */
+    long long *prog;              /* per warp slot: publication progress of its ring */
     int maxlen;
     int *score;                   /* per pair */
 };
+
+static constexpr unsigned long long NWL_COOP_BIT = 1ull << 62;
 
 __device__ __forceinline__ int sext_byte(uint32_t lo, uint32_t hi, int k)
 {
@@ -59,42 +67,73 @@ __device__ __forceinline__ int sext_byte(uint32_t lo, uint32_t hi, int k)
 }
 
 /*
- * One CTA of NWL_WARPS warps per pair. Pass p (rows p*256 .. p*256+255) is
- * run by warp p % NWL_WARPS; its lane 0 reads pass p-1's bottom row from
- * ring buffer (p-1) % NWL_WARPS, which pass p-1's lane 31 fills column by
- * column and publishes through a progress counter in shared memory every 32
- * columns. Waits are bounded: a spin that exceeds NWL_SPIN polls sets the
- * error flag and abandons the pair (the host reports the failure).
+ * A team of warps per pair: the NWL_WARPS warps of one CTA, or, for pairs
+ * flagged cooperative, the warps of all CTAs of a thread-block cluster
+ * (which the hardware schedules together). Pass p (rows p*256 .. p*256+255)
+ * runs on team warp p % T; its lane 0 reads pass p-1's bottom row from that
+ * warp slot's ring buffer, which pass p-1's lane 31 fills column by column
+ * and publishes every 32 columns through the slot's progress counter
+ * (device-scope release / acquire, so it works across the cluster's CTAs).
+ * Waits are bounded: a wait that exceeds NWL_SPIN_CYCLES, or sees the
+ * launch's error flag set, gives up; the host reports the failure.
  */
-static constexpr long long NWL_SPIN = 1ll << 26;
+static constexpr long long NWL_SPIN_CYCLES = 1ll << 32;
 
 template <bool BANDED, bool GE>
 __global__ void __launch_bounds__(NWL_WARPS * 32, 3)
 k_nw_wave(NwWaveParams p, int *counter, int *error)
 {
+    namespace cg = cooperative_groups;
     __shared__ __align__(16) int8_t s_mat[32 * 32];
-    /* progress of ring buffer k: g * (m + 1) + j + 1 once generation g (the
-     * pass g * NWL_WARPS + k) has published column j; monotone, so a reader
-     * never mistakes an older pass's progress for its predecessor's */
-    __shared__ volatile long long s_prog[NWL_WARPS];
     __shared__ int s_pair;
-    __shared__ volatile int s_abort;
     for (int k = threadIdx.x; k < p.msize * p.msize; k += blockDim.x) {
         const int r = k / p.msize, c = k % p.msize;
         s_mat[r * 32 + c] = p.mat[k];
     }
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = (int)cluster.num_blocks();
+    const int crank = (int)cluster.block_rank();
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int open = p.open, gap = p.gap;
-    int2 *ring = p.scratch + (size_t)blockIdx.x * NWL_WARPS * p.maxlen;
+    volatile int *verr = error;
+    bool coop = C > 1;
 
     for (;;) {
-        __syncthreads();
-        if (threadIdx.x == 0) { s_pair = atomicAdd(counter, 1); s_abort = 0; }
-        if (threadIdx.x < NWL_WARPS) s_prog[threadIdx.x] = 0;
-        __syncthreads();
-        const int w = s_pair;
+        int w;
+        if (coop) {
+            cluster.sync();
+            if (crank == 0 && threadIdx.x == 0) s_pair = atomicAdd(counter, 1);
+            cluster.sync();
+            w = *cluster.map_shared_rank(&s_pair, 0);
+            /* every CTA has read rank 0's pair before it is overwritten */
+            cluster.sync();
+            if (w < p.npairs && !(p.keys[w] & NWL_COOP_BIT)) {
+                /* the cooperative pairs are done: from here on each CTA
+                 * takes pairs of its own (rank 0 keeps this one) */
+                coop = false;
+                if (crank != 0) {
+                    if (threadIdx.x == 0) s_pair = atomicAdd(counter, 1);
+                    __syncthreads();
+                    w = s_pair;
+                }
+            }
+        } else {
+            __syncthreads();
+            if (threadIdx.x == 0) s_pair = atomicAdd(counter, 1);
+            __syncthreads();
+            w = s_pair;
+        }
         if (w >= p.npairs) break;
+        const int T = coop ? C * NWL_WARPS : NWL_WARPS;           /* warps of the team */
+        const int tw = coop ? crank * NWL_WARPS + warp : warp;    /* this warp in the team */
+        const long long slot0 = coop ? (long long)(blockIdx.x / C) * C * NWL_WARPS
+                                     : (long long)blockIdx.x * NWL_WARPS;
+        /* this CTA's slots start the pair unpublished */
+        if (threadIdx.x < NWL_WARPS)
+            cuda::atomic_ref<long long, cuda::thread_scope_device>(p.prog[(long long)blockIdx.x * NWL_WARPS + threadIdx.x])
+                .store(0, cuda::memory_order_relaxed);
+        if (coop) cluster.sync(); else __syncthreads();
         const int pid = p.order[w];
         const int n = p.qlen[pid], m = p.tlen[pid];
         const uint8_t *qs = p.q + p.qoff[pid];
@@ -105,16 +144,17 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
         int result = NWL_NEG;
         bool have_result = false;
 
-        for (int pass = warp; pass < npass; pass += NWL_WARPS) {
+        for (int pass = tw; pass < npass; pass += T) {
             const int r0 = pass * 32 * NWL_RL;
             const int R0 = r0 + lane * NWL_RL;
-            int2 *in_buf = ring + (size_t)((pass + NWL_WARPS - 1) % NWL_WARPS) * p.maxlen;
-            int2 *out_buf = ring + (size_t)(pass % NWL_WARPS) * p.maxlen;
+            const long long in_slot = slot0 + (pass + T - 1) % T, out_slot = slot0 + pass % T;
+            int2 *in_buf = p.scratch + in_slot * p.maxlen;
+            int2 *out_buf = p.scratch + out_slot * p.maxlen;
             const long long stride = (long long)m + 1;
-            volatile long long *in_prog = &s_prog[(pass + NWL_WARPS - 1) % NWL_WARPS];
-            volatile long long *out_prog = &s_prog[pass % NWL_WARPS];
-            const long long in_base = pass > 0 ? (long long)((pass - 1) / NWL_WARPS) * stride + 1 : 0;
-            const long long out_base = (long long)(pass / NWL_WARPS) * stride + 1;
+            cuda::atomic_ref<long long, cuda::thread_scope_device> in_prog(p.prog[in_slot]);
+            cuda::atomic_ref<long long, cuda::thread_scope_device> out_prog(p.prog[out_slot]);
+            const long long in_base = pass > 0 ? (long long)((pass - 1) / T) * stride + 1 : 0;
+            const long long out_base = (long long)(pass / T) * stride + 1;
             int qc[NWL_RL];
 #pragma unroll
             for (int r = 0; r < NWL_RL; ++r) qc[r] = (R0 + r < n) ? qs[R0 + r] : 0;
@@ -131,12 +171,16 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
                 if (pass == 0) return true;
                 const int need = min(c, prev_jhi);
                 if (need < 0) return true;
-                long long spins = 0;
-                while (*in_prog < in_base + need) {
-                    if (s_abort) return false;
-                    if (++spins > NWL_SPIN) { s_abort = 1; atomicExch(error, 1); return false; }
+                const long long t0 = clock64();
+                unsigned ns = 32;
+                while (in_prog.load(cuda::memory_order_acquire) < in_base + need) {
+                    if (*verr) return false;
+                    if (clock64() - t0 > NWL_SPIN_CYCLES) { atomicExch(error, 1); return false; }
+                    /* back off, so that waiting warps leave the memory
+                     * system and the issue slots to the producers */
+                    __nanosleep(ns);
+                    if (ns < 1024) ns <<= 1;
                 }
-                __threadfence_block();
                 return true;
             };
             int Hl[NWL_RL], E[NWL_RL];
@@ -204,6 +248,14 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
                         up_f = vf;
                     }
                 }
+                /* banded: do all active lanes of the warp hold all their
+                 * rows inside the band at this column? */
+                bool full_in = true;
+                if (BANDED) {
+                    const unsigned bwl = (unsigned)(hi - lo);
+                    const bool mine = !active || (bwl >= NWL_RL - 1 && (unsigned)(R0 - j - lo) <= bwl - (NWL_RL - 1));
+                    full_in = __all_sync(0xffffffffu, mine);
+                }
                 if (active) {
                     int hd = dg;
                     uint32_t row_lo = 0, row_hi = 0;
@@ -217,30 +269,42 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
                     const int dlo = R0 - j - lo;
                     const unsigned bw = (unsigned)(hi - lo);
                     int last_h = 0, last_f = 0;
+                    /* one column of this lane's rows; MASK: rows outside the
+                     * band are -infinity */
+                    auto rows = [&](auto mask_tag) {
+                        constexpr bool MASK = decltype(mask_tag)::value;
 #pragma unroll
-                    for (int r = 0; r < NWL_RL; ++r) {
-                        const int sc = p.small_alpha ? sext_byte(row_lo, row_hi, qc[r]) : (int)s_mat[tc * 32 + qc[r]];
-                        /* E and the diagonal/E part a are off the row-to-row chain */
-                        int e = max(E[r] - gap, Hl[r] - open);
-                        int a = __viaddmax_s32(hd, sc, e);
-                        if (BANDED) {
-                            const bool in = (unsigned)(dlo + r) <= bw;
-                            e = in ? e : NWL_NEG;
-                            a = in ? a : NWL_NEG;
-                            f = in ? f : NWL_NEG;
+                        for (int r = 0; r < NWL_RL; ++r) {
+                            const int sc = p.small_alpha ? sext_byte(row_lo, row_hi, qc[r]) : (int)s_mat[tc * 32 + qc[r]];
+                            /* E and the diagonal/E part a are off the row-to-row chain */
+                            int e = max(E[r] - gap, Hl[r] - open);
+                            int a = __viaddmax_s32(hd, sc, e);
+                            if (MASK) {
+                                const bool in = (unsigned)(dlo + r) <= bw;
+                                e = in ? e : NWL_NEG;
+                                a = in ? a : NWL_NEG;
+                                f = in ? f : NWL_NEG;
+                            }
+                            const int h = max(a, f);
+                            last_h = h;
+                            last_f = f;
+                            /* F of the next row: max(F - gap, H - open). With
+                             * open >= gap, H - open = max(a, F) - open and
+                             * F - open <= F - gap, so only a - open is needed:
+                             * one dependent operation per row */
+                            if (GE) f = __viaddmax_s32(f, -gap, a - open);
+                            else f = max(f - gap, h - open);
+                            E[r] = e;
+                            hd = Hl[r];
+                            Hl[r] = h;
                         }
-                        const int h = max(a, f);
-                        last_h = h;
-                        last_f = f;
-                        /* F of the next row: max(F - gap, H - open). With
-                         * open >= gap, H - open = max(a, F) - open and
-                         * F - open <= F - gap, so only a - open is needed:
-                         * one dependent operation per row */
-                        if (GE) f = __viaddmax_s32(f, -gap, a - open);
-                        else f = max(f - gap, h - open);
-                        E[r] = e;
-                        hd = Hl[r];
-                        Hl[r] = h;
+                    };
+                    if (BANDED && !full_in) {
+                        rows(std::integral_constant<bool, true>());
+                    } else {
+                        /* unbanded, or a column where every active lane of a
+                         * wide band holds all its rows: no masks */
+                        rows(std::integral_constant<bool, false>());
                     }
                     if (j == m - 1 && R0 <= n - 1 && n - 1 < R0 + NWL_RL) {
 #pragma unroll
@@ -252,10 +316,8 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
                     sh_f = last_f;
                     if (lane == 31 && pass + 1 < npass) {
                         out_buf[j] = make_int2(last_h, last_f);
-                        if (((j - jlo) & 31) == 31 || j == jhi) {
-                            __threadfence_block();
-                            *out_prog = out_base + j;
-                        }
+                        if (((j - jlo) & 31) == 31 || j == jhi)
+                            out_prog.store(out_base + j, cuda::memory_order_release);
                     }
                 }
             }
@@ -263,11 +325,10 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
             __syncwarp();
         }
         /* the corner's owner publishes the result */
-        __shared__ int s_result;
-        if (have_result) s_result = result;
-        __syncthreads();
-        if (threadIdx.x == 0) p.score[pid] = s_abort ? NWL_NEG : s_result;
+        if (have_result) p.score[pid] = result;
     }
+    /* no CTA leaves while another of its cluster may still read its pair */
+    if (coop) cluster.sync();
 }
 
 __global__ void k_iota_nw(int *v, int n)
@@ -276,10 +337,40 @@ __global__ void k_iota_nw(int *v, int n)
     if (i < n) v[i] = i;
 }
 
-__global__ void k_cells(const int *ql, const int *tl, int n, int64_t *cells)
+/* sort key: the pair's work (cells, or for a band its rows x the columns
+ * its passes sweep); the total goes to *total for k_coop_flag */
+__global__ void k_cells(const int *ql, const int *tl, const int *lo, const int *hi, int n,
+                        unsigned long long *keys, unsigned long long *total)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) cells[i] = (int64_t)ql[i] * tl[i];
+    unsigned long long k = 0;
+    if (i < n) {
+        const unsigned long long cols = lo ? (unsigned long long)min((long long)tl[i],
+                                                  (long long)hi[i] - lo[i] + 32 * NWL_RL)
+                                           : (unsigned long long)tl[i];
+        k = (unsigned long long)ql[i] * cols;
+        keys[i] = k;
+    }
+    for (int o = 16; o; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
+    if ((threadIdx.x & 31) == 0 && k) atomicAdd(total, k);
+}
+
+/* NWL_COOP_BIT for the pairs a whole cluster should run: those whose work
+ * is above a fair share of the total per CTA (left to one CTA, they would
+ * finish last), that give every warp of the team a pass, and, banded, whose
+ * band is at least 1024 diagonals wide (narrower, consecutive passes overlap
+ * too little to keep a team busy) */
+__global__ void k_coop_flag(const int *ql, const int *lo, const int *hi, int n, int nctas, int coop_pass,
+                            const unsigned long long *total, unsigned long long *keys, int *ncoop)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int npass = (ql[i] + 32 * NWL_RL - 1) / (32 * NWL_RL);
+    const unsigned long long k = keys[i];
+    if (npass >= coop_pass && (!lo || hi[i] - lo[i] >= 1024) && k * (unsigned long long)nctas > *total) {
+        keys[i] = k | NWL_COOP_BIT;
+        atomicAdd(ncoop, 1);
+    }
 }
 
 }  // namespace pb
@@ -306,22 +397,9 @@ extern "C" int pb_cuda_nw_long(int npairs, int open, int gap, const int32_t *h_m
     }
     int8_t *d_mat = nullptr;
     int *idx = nullptr, *order = nullptr, *counter = nullptr;
-    int64_t *cells = nullptr, *cells_sorted = nullptr;
+    unsigned long long *keys = nullptr, *keys_sorted = nullptr;
     void *tmp = nullptr;
     size_t tmpb = 0;
-    cudaMallocAsync((void **)&d_mat, hm.size(), st);
-    cudaMemcpyAsync(d_mat, hm.data(), hm.size(), cudaMemcpyHostToDevice, st);
-    cudaMallocAsync((void **)&idx, sizeof(int) * npairs, st);
-    cudaMallocAsync((void **)&order, sizeof(int) * npairs, st);
-    cudaMallocAsync((void **)&cells, sizeof(int64_t) * npairs, st);
-    cudaMallocAsync((void **)&cells_sorted, sizeof(int64_t) * npairs, st);
-    cudaMallocAsync((void **)&counter, sizeof(int), st);
-    cudaMemsetAsync(counter, 0, sizeof(int), st);
-    pb::k_iota_nw<<<(npairs + 255) / 256, 256, 0, st>>>(idx, npairs);
-    pb::k_cells<<<(npairs + 255) / 256, 256, 0, st>>>(d_qlen, d_tlen, npairs, cells);
-    cub::DeviceRadixSort::SortPairsDescending(nullptr, tmpb, cells, cells_sorted, idx, order, npairs, 0, 64, st);
-    cudaMallocAsync(&tmp, tmpb, st);
-    cub::DeviceRadixSort::SortPairsDescending(tmp, tmpb, cells, cells_sorted, idx, order, npairs, 0, 64, st);
     int nsm = 0, dev = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -332,32 +410,105 @@ extern "C" int pb_cuda_nw_long(int npairs, int open, int gap, const int32_t *h_m
              : (ge ? pb::k_nw_wave<false, true> : pb::k_nw_wave<false, false>);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, pb::NWL_WARPS * 32, 0);
     if (per_sm < 1) per_sm = 1;
-    int blocks = per_sm * nsm;
-    if (blocks > npairs) blocks = npairs;
+    /* clusters of NWL_CLUSTER CTAs run the largest pairs as one team */
+    int C = pb::NWL_CLUSTER, nclusters = 0;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(C * nsm);
+    cfg.blockDim = dim3(pb::NWL_WARPS * 32);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, (const void *)kern, &cfg) != cudaSuccess || nclusters < 1) {
+        cudaGetLastError();
+        C = 1;
+    }
+    const int plain_max = per_sm * nsm;
+    cudaMallocAsync((void **)&d_mat, hm.size(), st);
+    cudaMemcpyAsync(d_mat, hm.data(), hm.size(), cudaMemcpyHostToDevice, st);
+    cudaMallocAsync((void **)&idx, sizeof(int) * npairs, st);
+    cudaMallocAsync((void **)&order, sizeof(int) * npairs, st);
+    cudaMallocAsync((void **)&keys, sizeof(unsigned long long) * npairs, st);
+    cudaMallocAsync((void **)&keys_sorted, sizeof(unsigned long long) * npairs, st);
+    cudaMallocAsync((void **)&counter, sizeof(int) * 8, st);
+    cudaMemsetAsync(counter, 0, sizeof(int) * 8, st);
+    /* counter[0], [1]: pair counters of the two launches; [2..3]: total
+     * work; [4]: cooperative pairs */
+    unsigned long long *total = reinterpret_cast<unsigned long long *>(counter + 2);
+    pb::k_iota_nw<<<(npairs + 255) / 256, 256, 0, st>>>(idx, npairs);
+    pb::k_cells<<<(npairs + 255) / 256, 256, 0, st>>>(d_qlen, d_tlen, d_lo, d_hi, npairs, keys, total);
+    if (C > 1)
+        pb::k_coop_flag<<<(npairs + 255) / 256, 256, 0, st>>>(d_qlen, d_lo, d_hi, npairs, plain_max,
+                                                              C * pb::NWL_WARPS, total, keys, counter + 4);
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, tmpb, keys, keys_sorted, idx, order, npairs, 0, 64, st);
+    cudaMallocAsync(&tmp, tmpb, st);
+    cub::DeviceRadixSort::SortPairsDescending(tmp, tmpb, keys, keys_sorted, idx, order, npairs, 0, 64, st);
+    /* the cooperative pairs (sorted first) go to a cluster launch, the rest
+     * to a plain launch on a second stream; the two never wait on each other */
+    int ncoop = 0;
+    cudaMemcpyAsync(&ncoop, counter + 4, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    const int cblocks = ncoop > 0 ? (ncoop < nclusters ? ncoop : nclusters) * C : 0;
+    const int pblocks = npairs - ncoop < plain_max ? npairs - ncoop : plain_max;
+    const int blocks = cblocks + pblocks;
     int2 *scratch = nullptr;
+    long long *prog = nullptr;
     int *d_err = nullptr;
     int rc = 0, herr = 0;
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev = nullptr;
     cudaMallocAsync((void **)&d_err, sizeof(int), st);
     cudaMemsetAsync(d_err, 0, sizeof(int), st);
-    if (cudaMallocAsync((void **)&scratch, sizeof(int2) * (size_t)(maxlen + 1) * blocks * pb::NWL_WARPS, st) != cudaSuccess)
+    if (cudaMallocAsync((void **)&scratch, sizeof(int2) * (size_t)(maxlen + 1) * blocks * pb::NWL_WARPS, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&prog, sizeof(long long) * (size_t)blocks * pb::NWL_WARPS, st) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
         rc = -1;
     if (rc == 0) {
+        cudaMemsetAsync(prog, 0, sizeof(long long) * (size_t)blocks * pb::NWL_WARPS, st);
+        cudaEventRecord(ev, st);
+        cudaStreamWaitEvent(st2, ev, 0);
         pb::NwWaveParams p;
-        p.npairs = npairs; p.open = open; p.gap = gap; p.msize = msize; p.small_alpha = small;
+        p.open = open; p.gap = gap; p.msize = msize; p.small_alpha = small;
         p.mat = d_mat; p.q = d_q; p.qoff = d_qoff; p.qlen = d_qlen;
         p.t = d_t; p.toff = d_toff; p.tlen = d_tlen; p.lo = d_lo; p.hi = d_hi;
-        p.order = order; p.scratch = scratch; p.maxlen = maxlen + 1; p.score = d_score;
-        kern<<<blocks, pb::NWL_WARPS * 32, 0, st>>>(p, counter, d_err);
+        p.maxlen = maxlen + 1; p.score = d_score;
+        if (cblocks > 0) {
+            pb::NwWaveParams pc = p;
+            pc.npairs = ncoop; pc.order = order; pc.keys = keys_sorted;
+            pc.scratch = scratch; pc.prog = prog;
+            cfg.gridDim = dim3(cblocks);
+            if (cudaLaunchKernelEx(&cfg, kern, pc, counter, d_err) != cudaSuccess) rc = -1;
+            pb_diag_count_launch(1);
+        }
+        if (pblocks > 0) {
+            pb::NwWaveParams pp = p;
+            pp.npairs = npairs - ncoop; pp.order = order + ncoop; pp.keys = keys_sorted + ncoop;
+            pp.scratch = scratch + (size_t)cblocks * pb::NWL_WARPS * p.maxlen;
+            pp.prog = prog + (size_t)cblocks * pb::NWL_WARPS;
+            kern<<<pblocks, pb::NWL_WARPS * 32, 0, st2>>>(pp, counter + 1, d_err);
+            pb_diag_count_launch(1);
+        }
         if (cudaGetLastError() != cudaSuccess) rc = -1;
-        pb_diag_count_launch(3);
+        pb_diag_count_launch(C > 1 ? 3 : 2);   /* k_iota_nw, k_cells, k_coop_flag */
+        cudaEventRecord(ev, st2);
+        cudaStreamWaitEvent(st, ev, 0);
         cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
     }
     cudaFreeAsync(d_mat, st); cudaFreeAsync(idx, st); cudaFreeAsync(order, st);
-    cudaFreeAsync(cells, st); cudaFreeAsync(cells_sorted, st); cudaFreeAsync(counter, st);
+    cudaFreeAsync(keys, st); cudaFreeAsync(keys_sorted, st); cudaFreeAsync(counter, st);
     cudaFreeAsync(tmp, st);
     if (scratch) cudaFreeAsync(scratch, st);
+    if (prog) cudaFreeAsync(prog, st);
     cudaFreeAsync(d_err, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
+    if (st2) cudaStreamDestroy(st2);
+    if (ev) cudaEventDestroy(ev);
     if (herr) {
         fprintf(stderr, "pb_cuda_nw_long: a pipeline wait exceeded its bound; pair abandoned\n");
         rc = -1;

@@ -183,8 +183,10 @@ def test_learned_band_trains_certifies_and_beats_fixed_band():
     l0 = m.train(dna, *tr[:6], OPEN, GAP, epochs=1, batch=128, lr=2e-3)
     l1 = m.train(dna, *tr[:6], OPEN, GAP, epochs=60, batch=128, lr=2e-3)
     assert l1 < l0
+    widen, slack = m.scaling()                     # tuned on the held-out tenth
+    assert 1.0 <= widen <= 3.0 and slack == 32
     full = pb.nw_long(dna, *te[:6], OPEN, GAP)
-    sc, lo, hi, st = m.align(dna, *te[:6], OPEN, GAP, widen=1.1, slack=32)
+    sc, lo, hi, st = m.align(dna, *te[:6], OPEN, GAP, widen=0.0, slack=-1)
     assert (sc == full).all()                      # every reported score equals full DP
     assert st.pairs == 120 and st.certified + st.fallback == 120
     assert st.certified >= 0.8 * 120
