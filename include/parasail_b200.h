@@ -138,8 +138,8 @@ typedef struct parasail_b200_band_model parasail_b200_band_model_t;
 typedef struct parasail_b200_band_stats {
     long long pairs;        /**< pairs aligned */
     long long certified;    /**< pairs whose banded score passed the certificate */
-    long long fallback;     /**< pairs rerun on the full DP */
-    double band_cells;      /**< DP cells inside the predicted bands */
+    long long fallback;     /**< pairs whose first band failed the certificate and reran on a wider one */
+    double band_cells;      /**< DP cells computed: first bands of all pairs, second bands of the reruns */
 } parasail_b200_band_stats_t;
 
 extern parasail_b200_band_model_t *parasail_b200_band_model_new(unsigned seed);
@@ -176,10 +176,13 @@ extern int parasail_b200_band_model_train(
 extern void parasail_b200_band_model_scaling(const parasail_b200_band_model_t *model, float *widen, int *slack);
 /** Global alignment scores through the learned band: predicted band
  * (half-width scaled by `widen`, plus `slack` diagonals; widen <= 0 and
- * slack < 0 take the scaling chosen at training), banded DP,
- * exactness certificate, full-DP fallback. scores[] always equals
- * parasail_b200_nw_long's; band_lo/band_hi receive the bands used (the
- * whole matrix for fallback pairs), either may be NULL. */
+ * slack < 0 take the scaling chosen at training), banded DP with the
+ * exactness certificate checked inside the launch. A pair whose band fails
+ * it reruns at once, in the same launch, on its band widened by the label
+ * band of its own banded cost, which always passes. scores[] always equals
+ * parasail_b200_nw_long's; band_lo/band_hi receive the band each pair
+ * finally used, either may be NULL; stats->fallback counts the reruns and
+ * stats->band_cells every DP cell the call computed. */
 extern int parasail_b200_nw_learned_band(
         const parasail_b200_band_model_t *model, const parasail_matrix_t *matrix,
         const char *queries, const int64_t *qoffsets, const int *qlengths,
@@ -201,6 +204,11 @@ extern long parasail_b200_kernel_launches(void);
 extern double parasail_b200_sw16_kernel_ms(long *launches);
 /** Diagnostics: zero the two counters above. */
 extern void parasail_b200_reset_counters(void);
+/** Host wall time (ms) of the phases of this thread's last
+ * parasail_b200_nw_learned_band call: [0] features, MLP and bands, [1]
+ * banded DP with the in-launch certificate and reruns, [2] cell counting,
+ * [3] unused (0), [4] upload of the pairs. */
+extern void parasail_b200_band_phase_ms(double *out5);
 /** Measured lane-operations per second of the DPX int16x2 add-max pipe on
  * the current device (the integer roofline of the DP kernels). */
 extern double parasail_b200_dpx_peak(void);

@@ -10,6 +10,7 @@
  * its scores therefore always equal the plain path's.
  */
 #include <stdlib.h>
+#include <time.h>
 #include <string.h>
 
 #include "pb_internal.h"
@@ -37,6 +38,7 @@ int pb_cuda_band_certify(int npairs, int a, int open, int ext, const int *d_qlen
 int pb_cuda_band_tune(struct pb_band_model *m, int n, const float *d_x, const int *d_qlen, const int *d_tlen,
                       const int *d_lab_lo, const int *d_lab_hi, float *chosen);
 void pb_cuda_band_scaling(const struct pb_band_model *m, float *widen, int *slack);
+int pb_cuda_band_select(int npairs, const int *d_rounds, const int *d_lo, const int *d_hi, int *sel_lo, int *sel_hi);
 int pb_cuda_band_cells(int npairs, const int *d_qlen, const int *d_tlen, const int *d_lo, const int *d_hi,
                        unsigned long long *h_cells);
 
@@ -267,6 +269,23 @@ int parasail_b200_band_model_train(parasail_b200_band_model_t *model, const para
 }
 
 /* shared by the host and device entry points */
+/* host wall time of the phases of the last parasail_b200_nw_learned_band
+ * call on this thread (diagnostics) */
+static __thread double g_phase_ms[5];
+
+static double now_ms(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
+}
+
+void parasail_b200_band_phase_ms(double *out)
+{
+    int k;
+    for (k = 0; k < 5; ++k) out[k] = g_phase_ms[k];
+}
+
 static int learned_run(const struct pb_band_model *model, const parasail_matrix_t *matrix, const dev_pairs *d,
                        int open, int gap, float widen, int slack, int *d_score, int *d_lo, int *d_hi,
                        parasail_b200_band_stats_t *stats)
@@ -286,79 +305,52 @@ static int learned_run(const struct pb_band_model *model, const parasail_matrix_
     }
     d_feat = (float *)pb_cuda_malloc(sizeof(float) * (size_t)n * nin);
     d_y = (float *)pb_cuda_malloc(sizeof(float) * (size_t)n * no);
-    d_cert = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    d_cert = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);   /* rounds per pair */
     pb_cuda_sync();
-    rc = pb_cuda_band_features(n, d->q, d->qoff, d->qlen, d->t, d->toff, d->tlen, d_feat);
-    if (rc == 0) rc = pb_cuda_band_forward(model, n, d_feat, NULL, NULL, d_y);
-    if (rc == 0) rc = pb_cuda_band_from_pred(n, d->qlen, d->tlen, d_y, widen, slack, d_lo, d_hi);
-    if (rc == 0) rc = pb_cuda_nw_long(n, open, gap, matrix->matrix, matrix->size, d->q, d->qoff, d->qlen,
-                                      d->t, d->toff, d->tlen, d_lo, d_hi, d->maxlen, d_score);
-    if (rc == 0) rc = pb_cuda_band_certify(n, matrix->max, open, gap, d->qlen, d->tlen, d_lo, d_hi, d_score,
-                                           d_cert, &nfail);
-    if (rc == 0 && stats) {
-        unsigned long long cells = 0;
-        pb_cuda_band_cells(n, d->qlen, d->tlen, d_lo, d_hi, &cells);
-        stats->band_cells = (double)cells;
+    {
+        double t0 = now_ms(), t1;
+        rc = pb_cuda_band_features(n, d->q, d->qoff, d->qlen, d->t, d->toff, d->tlen, d_feat);
+        if (rc == 0) rc = pb_cuda_band_forward(model, n, d_feat, NULL, NULL, d_y);
+        if (rc == 0) rc = pb_cuda_band_from_pred(n, d->qlen, d->tlen, d_y, widen, slack, d_lo, d_hi);
+        /* the MLP and band kernels run on the default stream, the DP on its
+         * own: the bands must be complete before the DP reads them */
+        if (rc == 0) rc = pb_cuda_device_sync();
+        t1 = now_ms();
+        g_phase_ms[0] = t1 - t0;
+        /* cells of the first bands (every pair runs them) */
+        if (rc == 0 && stats) {
+            unsigned long long cells = 0;
+            pb_cuda_band_cells(n, d->qlen, d->tlen, d_lo, d_hi, &cells);
+            stats->band_cells = (double)cells;
+        }
+        t0 = now_ms();
+        g_phase_ms[2] = t0 - t1;
+        /* banded DP with the certificate in the launch: a pair that fails it
+         * reruns at once on a band that passes */
+        if (rc == 0) rc = pb_cuda_memset(d_cert, 0, sizeof(int) * (size_t)n);
+        if (rc == 0) rc = pb_cuda_nw_long_cert(n, open, gap, matrix->matrix, matrix->size, matrix->max, d->q,
+                                               d->qoff, d->qlen, d->t, d->toff, d->tlen, d_lo, d_hi, d->maxlen,
+                                               d_score, d_cert);
+        g_phase_ms[1] = now_ms() - t0;
     }
-    if (rc == 0 && nfail > 0) {
-        /* the fallback: full DP for every pair that failed the certificate */
-        int *hc = (int *)malloc(sizeof(int) * (size_t)n);
-        int *hq = (int *)malloc(sizeof(int) * (size_t)n), *ht = (int *)malloc(sizeof(int) * (size_t)n);
-        int64_t *hqo = (int64_t *)malloc(sizeof(int64_t) * (size_t)n), *hto = (int64_t *)malloc(sizeof(int64_t) * (size_t)n);
-        int *hs = (int *)malloc(sizeof(int) * (size_t)n);
-        int *idx = (int *)malloc(sizeof(int) * (size_t)n);
-        int k, f = 0;
-        pb_cuda_d2h(hc, d_cert, sizeof(int) * n);
-        pb_cuda_d2h(hq, d->qlen, sizeof(int) * n);
-        pb_cuda_d2h(ht, d->tlen, sizeof(int) * n);
-        pb_cuda_d2h(hqo, d->qoff, sizeof(int64_t) * n);
-        pb_cuda_d2h(hto, d->toff, sizeof(int64_t) * n);
-        for (k = 0; k < n; ++k) {
-            if (!hc[k]) {
-                idx[f] = k; hq[f] = hq[k]; ht[f] = ht[k]; hqo[f] = hqo[k]; hto[f] = hto[k];
-                ++f;
-            }
+    g_phase_ms[3] = 0.0;
+    if (rc == 0) {
+        /* pairs that ran twice: count them, and add their second bands */
+        int *hr = (int *)malloc(sizeof(int) * (size_t)n);
+        int k;
+        rc = hr ? pb_cuda_d2h(hr, d_cert, sizeof(int) * n) : -1;
+        for (k = 0; rc == 0 && k < n; ++k) if (hr[k] == 2) ++nfail;
+        free(hr);
+        if (rc == 0 && stats && nfail > 0) {
+            /* second-round cells: the final bands of the pairs that reran */
+            int *sel_lo = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+            int *sel_hi = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+            unsigned long long cells = 0;
+            rc = pb_cuda_band_select(n, d_cert, d_lo, d_hi, sel_lo, sel_hi);
+            if (rc == 0) rc = pb_cuda_band_cells(n, d->qlen, d->tlen, sel_lo, sel_hi, &cells);
+            stats->band_cells += (double)cells;
+            pb_cuda_free(sel_lo); pb_cuda_free(sel_hi);
         }
-        {
-            dev_pairs sub = *d;
-            int *fs = (int *)pb_cuda_malloc(sizeof(int) * f);
-            sub.n = f;
-            sub.qlen = (int *)pb_cuda_malloc(sizeof(int) * f);
-            sub.tlen = (int *)pb_cuda_malloc(sizeof(int) * f);
-            sub.qoff = (int64_t *)pb_cuda_malloc(sizeof(int64_t) * f);
-            sub.toff = (int64_t *)pb_cuda_malloc(sizeof(int64_t) * f);
-            pb_cuda_h2d(sub.qlen, hq, sizeof(int) * f);
-            pb_cuda_h2d(sub.tlen, ht, sizeof(int) * f);
-            pb_cuda_h2d(sub.qoff, hqo, sizeof(int64_t) * f);
-            pb_cuda_h2d(sub.toff, hto, sizeof(int64_t) * f);
-            pb_cuda_sync();
-            rc = run_full(matrix, &sub, open, gap, fs);
-            if (rc == 0) {
-                pb_cuda_d2h(hs, fs, sizeof(int) * f);
-                /* scatter the fallback scores, widen the reported band */
-                {
-                    int *all = (int *)malloc(sizeof(int) * (size_t)n);
-                    int *alo = (int *)malloc(sizeof(int) * (size_t)n), *ahi = (int *)malloc(sizeof(int) * (size_t)n);
-                    pb_cuda_d2h(all, d_score, sizeof(int) * n);
-                    pb_cuda_d2h(alo, d_lo, sizeof(int) * n);
-                    pb_cuda_d2h(ahi, d_hi, sizeof(int) * n);
-                    for (k = 0; k < f; ++k) {
-                        all[idx[k]] = hs[k];
-                        alo[idx[k]] = -ht[k] - 1;
-                        ahi[idx[k]] = hq[k] + 1;
-                    }
-                    pb_cuda_h2d(d_score, all, sizeof(int) * n);
-                    pb_cuda_h2d(d_lo, alo, sizeof(int) * n);
-                    pb_cuda_h2d(d_hi, ahi, sizeof(int) * n);
-                    pb_cuda_sync();
-                    free(all); free(alo); free(ahi);
-                }
-            }
-            pb_cuda_free(fs); pb_cuda_free(sub.qlen); pb_cuda_free(sub.tlen);
-            pb_cuda_free(sub.qoff); pb_cuda_free(sub.toff);
-            pb_cuda_sync();
-        }
-        free(hc); free(hq); free(ht); free(hqo); free(hto); free(hs); free(idx);
     }
     if (stats) {
         stats->pairs = n;
@@ -380,7 +372,12 @@ int parasail_b200_nw_learned_band(const parasail_b200_band_model_t *model, const
     int *d_score, *d_lo, *d_hi, rc;
     if (!model || !long_ok(__func__, matrix, open, gap)) return -1;
     if (n <= 0) return n == 0 ? 0 : -1;
-    if (dev_pairs_upload(matrix, queries, qoffsets, qlengths, targets, toffsets, tlengths, n, &d) != 0) return -1;
+    {
+        const double tu = now_ms();
+        if (dev_pairs_upload(matrix, queries, qoffsets, qlengths, targets, toffsets, tlengths, n, &d) != 0) return -1;
+        pb_cuda_sync();
+        g_phase_ms[4] = now_ms() - tu;
+    }
     d_score = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
     d_lo = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
     d_hi = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);

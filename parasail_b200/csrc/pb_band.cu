@@ -33,6 +33,7 @@
 #include <cuda_bf16.h>
 
 #include "pb_cuda.h"
+#include "pb_cert.cuh"
 
 namespace pb {
 
@@ -238,42 +239,6 @@ __global__ void k_adam(int n, float *w, const float *g, float *m1, float *m2, __
 
 /* ---- 3. bands and labels ---------------------------------------------- */
 
-struct CostModel { int a, open, ext; };
-
-/* doubled minimum cost of any path leaving [lo, hi] */
-__host__ __device__ inline long long exit_cost2(const CostModel &c, int n, int m, int lo, int hi)
-{
-    const long long dend = (long long)n - m;
-    const long long unit2 = c.a + 2LL * c.ext;           /* 2 (a/2 + ext) */
-    const long long up = (2LL * (hi + 1) - dend) * unit2 + 4LL * (c.open - c.ext);
-    const long long dn = (dend - 2LL * (lo - 1)) * unit2 + 4LL * (c.open - c.ext);
-    return up < dn ? up : dn;
-}
-
-__host__ __device__ inline long long floor_div(long long x, long long d)
-{
-    long long q = x / d;
-    if ((x % d != 0) && ((x < 0) != (d < 0))) --q;
-    return q;
-}
-
-/* smallest band whose exit cost covers the doubled optimal cost c2 */
-__host__ __device__ inline void label_band(const CostModel &c, int n, int m, long long c2, int *lo, int *hi)
-{
-    const long long dend = (long long)n - m;
-    const long long unit2 = c.a + 2LL * c.ext;
-    const long long need = c2 - 4LL * (c.open - c.ext);
-    /* g = fewest gap columns an exit must have: (2(hi+1) - dend) >= g */
-    const long long g = need <= 0 ? 0 : -floor_div(-need, unit2);
-    long long h = -floor_div(-(g + dend), 2) - 1;       /* ceil((g + dend)/2) - 1 */
-    long long l = floor_div(dend + 2 - g, 2);           /* (dend - 2(lo-1)) >= g */
-    const long long lmin = dend < 0 ? dend : 0, hmax = dend > 0 ? dend : 0;
-    if (h < hmax) h = hmax;
-    if (l > lmin) l = lmin;
-    *lo = (int)(l < -(long long)m - 1 ? -(long long)m - 1 : l);
-    *hi = (int)(h > (long long)n + 1 ? (long long)n + 1 : h);
-}
-
 __global__ void k_labels(int npairs, CostModel c, const int *qlen, const int *tlen, const int *score,
                          float *target, int *lo_out, int *hi_out)
 {
@@ -348,24 +313,36 @@ __global__ void k_band_cells(int npairs, const int *qlen, const int *tlen, const
     atomicAdd(cells, (unsigned long long)tot);
 }
 
-/* expected DP work of a band choice: the band's cells, plus a full DP for
- * every pair whose band does not contain its label band (the smallest band
- * the certificate accepts for the optimum, so the certificate would fail) */
+/* cells (i, j) of an n x m matrix with lo <= i - j <= hi */
+__device__ inline long long band_cells_of(long long n, long long m, long long lo, long long hi)
+{
+    long long tot = 0;
+    const long long dlo = lo > -(m - 1) ? lo : -(m - 1);
+    const long long dhi = hi < n - 1 ? hi : n - 1;
+    for (long long d = dlo; d <= dhi; ++d) {
+        const long long jmin = d < 0 ? -d : 0;
+        const long long jmax = (n - 1 - d) < (m - 1) ? (n - 1 - d) : (m - 1);
+        if (jmax >= jmin) tot += jmax - jmin + 1;
+    }
+    return tot;
+}
+
+/* expected cost of a band choice, in cells: the band's cells, plus, for
+ * every pair whose band does not contain its label band (so the certificate
+ * fails), a rerun on (band) U (label band of the first run's cost). That
+ * cost is at least the optimum's, so the rerun band is at least the union
+ * with the label band; it counts twice that union's cells. */
+static constexpr int BAND_RERUN_WEIGHT = 2;
+
 __global__ void k_tune_cost(int npairs, const int *qlen, const int *tlen, const int *lo, const int *hi,
                             const int *lab_lo, const int *lab_hi, unsigned long long *cost)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npairs) return;
     const long long n = qlen[p], m = tlen[p];
-    long long tot = 0;
-    const long long dlo = lo[p] > -(m - 1) ? lo[p] : -(m - 1);
-    const long long dhi = hi[p] < n - 1 ? hi[p] : n - 1;
-    for (long long d = dlo; d <= dhi; ++d) {
-        const long long jmin = d < 0 ? -d : 0;
-        const long long jmax = (n - 1 - d) < (m - 1) ? (n - 1 - d) : (m - 1);
-        if (jmax >= jmin) tot += jmax - jmin + 1;
-    }
-    if (lo[p] > lab_lo[p] || hi[p] < lab_hi[p]) tot += n * m;
+    long long tot = band_cells_of(n, m, lo[p], hi[p]);
+    if (lo[p] > lab_lo[p] || hi[p] < lab_hi[p])
+        tot += BAND_RERUN_WEIGHT * band_cells_of(n, m, min(lo[p], lab_lo[p]), max(hi[p], lab_hi[p]));
     atomicAdd(cost, (unsigned long long)tot);
 }
 
@@ -629,6 +606,25 @@ extern "C" void pb_cuda_band_scaling(const pb_band_model *m, float *widen, int *
 {
     if (widen) *widen = m->widen;
     if (slack) *slack = m->slack;
+}
+
+/* bands of the pairs that ran twice (d_rounds == 2), empty bands (no
+ * cells) for the others */
+__global__ void k_band_select(int npairs, const int *rounds, const int *lo, const int *hi, int *slo, int *shi)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const bool twice = rounds[p] == 2;
+    slo[p] = twice ? lo[p] : 1;
+    shi[p] = twice ? hi[p] : 0;
+}
+
+extern "C" int pb_cuda_band_select(int npairs, const int *d_rounds, const int *d_lo, const int *d_hi, int *sel_lo,
+                                   int *sel_hi)
+{
+    k_band_select<<<(npairs + 255) / 256, 256>>>(npairs, d_rounds, d_lo, d_hi, sel_lo, sel_hi);
+    pb_diag_count_launch(1);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 /* host mirror of the certificate arithmetic, for the C host code */

@@ -105,6 +105,9 @@ void *pb_cuda_malloc(size_t bytes);
 void pb_cuda_free(void *p);
 int pb_cuda_h2d(void *dst, const void *src, size_t bytes);
 int pb_cuda_d2h(void *dst, const void *src, size_t bytes);
+/* all work on the device, including kernels on the legacy default stream */
+int pb_cuda_device_sync(void);
+int pb_cuda_memset(void *p, int v, size_t bytes);
 int pb_cuda_sync(void);
 
 /* --- alignment ------------------------------------------------------------- */
@@ -185,6 +188,16 @@ int pb_cuda_nw_long(int npairs, int open, int gap, const int32_t *h_mat, int msi
                     const uint8_t *d_q, const int64_t *d_qoff, const int *d_qlen,
                     const uint8_t *d_t, const int64_t *d_toff, const int *d_tlen,
                     const int *d_lo, const int *d_hi, int maxlen, int *d_score);
+/* The same with a band per pair and the exactness certificate inside the
+ * launch (a = the matrix's largest score): a pair whose banded score fails
+ * it is rerun at once, by the same team, on its band widened by the label
+ * band of its own cost, which always passes. d_lo/d_hi are updated to the
+ * band each pair finally used; d_rounds[i] is set to 2 for those pairs
+ * (and left untouched for the others). */
+int pb_cuda_nw_long_cert(int npairs, int open, int gap, const int32_t *h_mat, int msize, int a,
+                         const uint8_t *d_q, const int64_t *d_qoff, const int *d_qlen,
+                         const uint8_t *d_t, const int64_t *d_toff, const int *d_tlen,
+                         int *d_lo, int *d_hi, int maxlen, int *d_score, int *d_rounds);
 
 /* diagnostics (pb_diag.cu) */
 void pb_diag_count_launch(long n);

@@ -163,6 +163,20 @@ int pb_cuda_sync(void)
     return 0;
 }
 
+/* waits for all work on the device, the legacy default stream included */
+int pb_cuda_device_sync(void)
+{
+    CK(cudaDeviceSynchronize());
+    return 0;
+}
+
+int pb_cuda_memset(void *p, int v, size_t bytes)
+{
+    CK(cudaMemsetAsync(p, v, bytes, stream()));
+    CK(cudaStreamSynchronize(stream()));
+    return 0;
+}
+
 int pb_cuda_profile_create(const int *table, int is_pssm, int size,
                            const uint8_t *qcodes, int qlen, int mmax, int mmin,
                            pb_device_profile *out)

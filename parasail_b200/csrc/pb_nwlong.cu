@@ -33,12 +33,13 @@
 #include <type_traits>
 
 #include "pb_cuda.h"
+#include "pb_cert.cuh"
 
 namespace pb {
 
 static constexpr int NWL_RL = 8;          /* query rows per lane */
 static constexpr int NWL_WARPS = 8;       /* warps per CTA */
-static constexpr int NWL_CLUSTER = 4;     /* CTAs per cluster for the largest pairs */
+static constexpr int NWL_CLUSTER = 8;     /* CTAs per cluster for the largest pairs */
 static constexpr int NWL_NEG = INT32_MIN / 4;
 
 struct NwWaveParams {
@@ -47,6 +48,10 @@ struct NwWaveParams {
     const uint8_t *q; const int64_t *qoff; const int *qlen;
     const uint8_t *t; const int64_t *toff; const int *tlen;
     const int *lo; const int *hi; /* per pair band (diagonal i - j), or nullptr */
+    int cert;                     /* banded: certify each pair, widen and rerun on failure */
+    CostModel cm;
+    int *lo_out, *hi_out;         /* cert: the band of pairs that ran twice */
+    int *rounds;                  /* cert: 2 for pairs that ran twice */
     const int *order;             /* pairs, cooperative ones first, then most cells first */
     const unsigned long long *keys; /* sorted keys; bit 62 set: run by a whole cluster */
     int2 *scratch;                /* per warp slot: a ring buffer of [maxlen] (H, F) */
@@ -129,18 +134,23 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
         const int tw = coop ? crank * NWL_WARPS + warp : warp;    /* this warp in the team */
         const long long slot0 = coop ? (long long)(blockIdx.x / C) * C * NWL_WARPS
                                      : (long long)blockIdx.x * NWL_WARPS;
+        const int pid = p.order[w];
+        const int n = p.qlen[pid], m = p.tlen[pid];
+        const uint8_t *qs = p.q + p.qoff[pid];
+        const uint8_t *ts = p.t + p.toff[pid];
+        int lo = BANDED ? p.lo[pid] : -(m + 1);
+        int hi = BANDED ? p.hi[pid] : n + 1;
+        const int npass = (n + 32 * NWL_RL - 1) / (32 * NWL_RL);
+        /* with p.cert, a band whose score fails the certificate is widened
+         * to (its band) U (the label band of its own cost) and the pair runs
+         * once more: that band always passes (its optimum costs at most the
+         * first one's, and the label band of that cost covers it) */
+        for (int round = 0; round < (BANDED && p.cert ? 2 : 1); ++round) {
         /* this CTA's slots start the pair unpublished */
         if (threadIdx.x < NWL_WARPS)
             cuda::atomic_ref<long long, cuda::thread_scope_device>(p.prog[(long long)blockIdx.x * NWL_WARPS + threadIdx.x])
                 .store(0, cuda::memory_order_relaxed);
         if (coop) cluster.sync(); else __syncthreads();
-        const int pid = p.order[w];
-        const int n = p.qlen[pid], m = p.tlen[pid];
-        const uint8_t *qs = p.q + p.qoff[pid];
-        const uint8_t *ts = p.t + p.toff[pid];
-        const int lo = BANDED ? p.lo[pid] : -(m + 1);
-        const int hi = BANDED ? p.hi[pid] : n + 1;
-        const int npass = (n + 32 * NWL_RL - 1) / (32 * NWL_RL);
         int result = NWL_NEG;
         bool have_result = false;
 
@@ -326,6 +336,31 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
         }
         /* the corner's owner publishes the result */
         if (have_result) p.score[pid] = result;
+        if (!(BANDED && p.cert)) break;
+        /* every thread of the team reads the one published score, so all
+         * take the same branch (and the same barriers) below */
+        if (coop) cluster.sync(); else __syncthreads();
+        const int sc = *(volatile int *)&p.score[pid];
+        const bool whole = lo <= -(m + 1) && hi >= n + 1;
+        bool ok = whole;
+        if (!whole && cert_valid(p.cm) && sc > NWL_NEG / 2)
+            ok = cost2_of(p.cm, n, m, sc) <= exit_cost2(p.cm, n, m, lo, hi);
+        if (ok || round == 1) break;
+        if (cert_valid(p.cm) && sc > NWL_NEG / 2) {
+            int l2, h2;
+            label_band(p.cm, n, m, cost2_of(p.cm, n, m, sc), &l2, &h2);
+            lo = min(lo, l2);
+            hi = max(hi, h2);
+        } else {
+            lo = -(m + 1);
+            hi = n + 1;
+        }
+        if (threadIdx.x == 0 && (!coop || crank == 0)) {
+            p.lo_out[pid] = lo;
+            p.hi_out[pid] = hi;
+            p.rounds[pid] = 2;
+        }
+        }   /* rounds */
     }
     /* no CTA leaves while another of its cluster may still read its pair */
     if (coop) cluster.sync();
@@ -358,8 +393,10 @@ __global__ void k_cells(const int *ql, const int *tl, const int *lo, const int *
 /* NWL_COOP_BIT for the pairs a whole cluster should run: those whose work
  * is above a fair share of the total per CTA (left to one CTA, they would
  * finish last), that give every warp of the team a pass, and, banded, whose
- * band is at least 1024 diagonals wide (narrower, consecutive passes overlap
- * too little to keep a team busy) */
+ * band is at least 1024 diagonals wide. (A banded pass starts about 350
+ * columns after the one above it, the band moving with the rows, so a team
+ * of T warps is only fully busy on bands of about 350 T columns; below that
+ * the team still finishes a large pair sooner than one CTA would.) */
 __global__ void k_coop_flag(const int *ql, const int *lo, const int *hi, int n, int nctas, int coop_pass,
                             const unsigned long long *total, unsigned long long *keys, int *ncoop)
 {
@@ -379,10 +416,11 @@ __global__ void k_coop_flag(const int *ql, const int *lo, const int *hi, int n, 
  * q[qoff[i] ..+qlen[i]), target i likewise, scored through the square matrix
  * d_mat (msize x msize int32, row = target letter). d_lo/d_hi: optional
  * per-pair band. Scores to d_score. */
-extern "C" int pb_cuda_nw_long(int npairs, int open, int gap, const int32_t *h_mat, int msize,
-                               const uint8_t *d_q, const int64_t *d_qoff, const int *d_qlen,
-                               const uint8_t *d_t, const int64_t *d_toff, const int *d_tlen,
-                               const int *d_lo, const int *d_hi, int maxlen, int *d_score)
+static int nw_long_impl(int npairs, int open, int gap, const int32_t *h_mat, int msize,
+                        const uint8_t *d_q, const int64_t *d_qoff, const int *d_qlen,
+                        const uint8_t *d_t, const int64_t *d_toff, const int *d_tlen,
+                        const int *d_lo, const int *d_hi, int maxlen, int *d_score,
+                        int cert_a, int *d_lo_out, int *d_hi_out, int *d_rounds)
 {
     if (pb_cuda_init() != 0) return -1;
     if (npairs <= 0) return 0;
@@ -478,6 +516,9 @@ extern "C" int pb_cuda_nw_long(int npairs, int open, int gap, const int32_t *h_m
         p.mat = d_mat; p.q = d_q; p.qoff = d_qoff; p.qlen = d_qlen;
         p.t = d_t; p.toff = d_toff; p.tlen = d_tlen; p.lo = d_lo; p.hi = d_hi;
         p.maxlen = maxlen + 1; p.score = d_score;
+        p.cert = d_lo && d_rounds ? 1 : 0;
+        p.cm.a = cert_a; p.cm.open = open; p.cm.ext = gap;
+        p.lo_out = d_lo_out; p.hi_out = d_hi_out; p.rounds = d_rounds;
         if (cblocks > 0) {
             pb::NwWaveParams pc = p;
             pc.npairs = ncoop; pc.order = order; pc.keys = keys_sorted;
@@ -515,4 +556,22 @@ extern "C" int pb_cuda_nw_long(int npairs, int open, int gap, const int32_t *h_m
     }
     cudaStreamDestroy(st);
     return rc;
+}
+
+extern "C" int pb_cuda_nw_long(int npairs, int open, int gap, const int32_t *h_mat, int msize,
+                               const uint8_t *d_q, const int64_t *d_qoff, const int *d_qlen,
+                               const uint8_t *d_t, const int64_t *d_toff, const int *d_tlen,
+                               const int *d_lo, const int *d_hi, int maxlen, int *d_score)
+{
+    return nw_long_impl(npairs, open, gap, h_mat, msize, d_q, d_qoff, d_qlen, d_t, d_toff, d_tlen, d_lo, d_hi,
+                        maxlen, d_score, 0, nullptr, nullptr, nullptr);
+}
+
+extern "C" int pb_cuda_nw_long_cert(int npairs, int open, int gap, const int32_t *h_mat, int msize, int a,
+                                    const uint8_t *d_q, const int64_t *d_qoff, const int *d_qlen,
+                                    const uint8_t *d_t, const int64_t *d_toff, const int *d_tlen,
+                                    int *d_lo, int *d_hi, int maxlen, int *d_score, int *d_rounds)
+{
+    return nw_long_impl(npairs, open, gap, h_mat, msize, d_q, d_qoff, d_qlen, d_t, d_toff, d_tlen, d_lo, d_hi,
+                        maxlen, d_score, a, d_lo, d_hi, d_rounds);
 }
