@@ -53,6 +53,7 @@ struct Sw16Task {
 
 struct Sw16Params {
     int open, gap, npairs, nq, ntasks, maxlen;
+    int nteam;               /* tasks [0, nteam) are run by a whole block */
     const Sw16Query *queries;
     const int8_t *prof_all;  /* concatenated [size][lp] int8 profiles */
     int prof_bytes;

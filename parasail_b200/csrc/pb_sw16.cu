@@ -95,16 +95,53 @@ k_sw16(Sw16Params p, int *task_counter)
     __syncthreads();
 
     const int lane = threadIdx.x & 31;
-    const int slot = blockIdx.x * SW16_WARPS + (threadIdx.x >> 5);
-    uint2 *buf = reinterpret_cast<uint2 *>(p.scratch) + (size_t)slot * p.maxlen * 32;
+    const int wid = threadIdx.x >> 5;
+    /* the block's SW16_WARPS buffers: warp w's is team_buf + w * maxlen * 32 */
+    uint2 *team_buf = reinterpret_cast<uint2 *>(p.scratch) + (size_t)blockIdx.x * SW16_WARPS * p.maxlen * 32;
     const uint32_t gapO = splat16(-p.open);
     const uint32_t gapE = splat16(-p.gap);
+    /* team tasks: the tasks at the front of the list (the most expensive,
+     * each more than a fair share of the work per warp) are run by all
+     * warps of a block together, pass k of the task on warp k % SW16_WARPS;
+     * a pass reads the previous one's bottom row from that warp's buffer,
+     * published every 32 columns through s_prog (generation-tagged, so that
+     * it only grows) */
+    __shared__ volatile long long s_prog[SW16_WARPS];
+    __shared__ int s_task;
+    __shared__ Sw16Best s_best[SW16_WARPS][32];
+    __shared__ int s_have[SW16_WARPS][32];
+    __shared__ int s_status[SW16_WARPS][32];
+    volatile int *verr = task_counter + 2;
+    bool team = p.nteam > 0;
 
+    /* warp tasks: the first of each warp block-strided, so that the largest
+     * ones (the list is sorted by cost) are spread one per block instead of
+     * landing on the first blocks' SMs; then from the shared counter */
+    const int nwarps_total = gridDim.x * SW16_WARPS;
+    bool first = true;
     for (;;) {
-        int task = 0;
-        if (lane == 0) task = atomicAdd(task_counter, 1);
-        task = __shfl_sync(0xffffffffu, task, 0);
-        if (task >= p.ntasks) break;
+        int task = 0, trank = 0, tsize = 1;
+        if (team) {
+            __syncthreads();
+            if (threadIdx.x == 0) s_task = atomicAdd(task_counter + 1, 1);
+            if (threadIdx.x < SW16_WARPS) s_prog[threadIdx.x] = 0;
+            __syncthreads();
+            task = s_task;
+            if (task >= p.nteam) { team = false; continue; }
+            trank = wid;
+            tsize = SW16_WARPS;
+        } else {
+            if (first) {
+                task = p.nteam + blockIdx.x + gridDim.x * wid;
+                first = false;
+            } else {
+                if (lane == 0) task = p.nteam + nwarps_total + atomicAdd(task_counter, 1);
+                task = __shfl_sync(0xffffffffu, task, 0);
+            }
+            if (task >= p.ntasks) break;
+        }
+        uint2 *out_buf = team_buf + (size_t)(team ? trank : wid) * p.maxlen * 32;
+        const uint2 *in_buf = team ? team_buf + (size_t)((trank + tsize - 1) % tsize) * p.maxlen * 32 : out_buf;
         const Sw16Task T = p.tasks[task];
         const Sw16Query Q = p.queries[T.q];
         const int s = T.first + lane;
@@ -122,7 +159,30 @@ k_sw16(Sw16Params p, int *task_counter)
         bool have = false;
         int status = 0;
 
-        for (int r0 = 0; r0 < ql; r0 += 2 * SW16_R) {
+        const long long stride = (long long)wmax + 1;
+        for (int r0 = 2 * SW16_R * trank; r0 < ql; r0 += 2 * SW16_R * tsize) {
+            const int sp = r0 / (2 * SW16_R);            /* pass index */
+            /* team: the previous pass (warp trank-1) must have published
+             * column c before it is read */
+            const long long in_base = (long long)((sp - 1) / tsize) * stride + 1;
+            const long long out_base = (long long)(sp / tsize) * stride + 1;
+            auto wait_for = [&](int c) -> bool {
+                if (!team || sp == 0) return true;
+                const int need = min(c, wmax - 1);
+                bool ok = true;
+                if (lane == 0 && need >= 0) {
+                    const long long t0 = clock64();
+                    while (s_prog[(trank + tsize - 1) % tsize] < in_base + need) {
+                        if (*verr) { ok = false; break; }
+                        if (clock64() - t0 > (1ll << 32)) { atomicExch(task_counter + 2, 1); ok = false; break; }
+                    }
+                    __threadfence_block();
+                }
+                ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+                __syncwarp();
+                return ok;
+            };
+            if (!wait_for(33)) break;
             uint32_t H[SW16_R], E[SW16_R];
 #pragma unroll
             for (int r = 0; r < SW16_R; ++r) { H[r] = 0u; E[r] = gapO; }
@@ -143,10 +203,12 @@ k_sw16(Sw16Params p, int *task_counter)
             int c_n2 = 1 < len ? tseq[1] : 0;
             uint2 v_n1 = vnone, v_n2 = vnone;
             if (r0 != 0) {
-                if (0 < wmax) v_n1 = buf[lane];
-                if (1 < wmax) v_n2 = buf[32 + lane];
+                if (0 < wmax) v_n1 = __ldcg(&in_buf[lane]);
+                if (1 < wmax) v_n2 = __ldcg(&in_buf[32 + lane]);
             }
+            bool aborted = false;
             for (int j = 0; j <= wmax; ++j) {
+                if (team && j > 0 && (j & 31) == 0 && !wait_for(j + 33)) { aborted = true; break; }
                 const int ca = c_n1;
                 c_n1 = c_n2;
                 c_n2 = j + 2 < len ? tseq[j + 2] : 0;
@@ -157,7 +219,7 @@ k_sw16(Sw16Params p, int *task_counter)
                 } else {
                     const uint2 v = v_n1;
                     v_n1 = v_n2;
-                    v_n2 = j + 2 < wmax ? buf[(size_t)(j + 2) * 32 + lane] : vnone;
+                    v_n2 = j + 2 < wmax ? __ldcg(&in_buf[(size_t)(j + 2) * 32 + lane]) : vnone;
                     hu = prmt(v.x, prev_h, 0x5432u);        /* lo <- previous pass's strip B bottom */
                     fu = prmt(v.y, prev_f, 0x5432u);
                 }
@@ -190,7 +252,15 @@ k_sw16(Sw16Params p, int *task_counter)
                     fu = f;
                     if (r & 1) cmax = __vimax3_s16x2(cmax, H[r - 1], h);
                 }
-                if (j >= 1 && more) buf[(size_t)(j - 1) * 32 + lane] = make_uint2(hu, fu);
+                if (j >= 1 && more) {
+                    out_buf[(size_t)(j - 1) * 32 + lane] = make_uint2(hu, fu);
+                    /* team: publish every 32 columns and the last one */
+                    if (team && (((j - 1) & 31) == 31 || j - 1 == wmax - 1)) {
+                        __threadfence_block();
+                        __syncwarp();
+                        if (lane == 0) s_prog[trank] = out_base + (j - 1);
+                    }
+                }
                 prev_h = hu;
                 prev_f = fu;
                 cb = ca;
@@ -227,8 +297,30 @@ k_sw16(Sw16Params p, int *task_counter)
                     sbest = (uint32_t)(uint16_t)sa.score | ((uint32_t)(uint16_t)sb.score << 16);
                 }
             }
+            if (aborted) break;
             fold_best(best, have, sa);
             fold_best(best, have, sb);
+        }
+        if (team) {
+            /* merge the warps' per-lane bests: highest score, then smallest
+             * column, then smallest row (the reference's first maximum) */
+            s_best[wid][lane] = best;
+            s_have[wid][lane] = have ? 1 : 0;
+            s_status[wid][lane] = status;
+            __syncthreads();
+            if (wid != 0) continue;
+            have = false;
+            status = 0;
+            for (int w = 0; w < SW16_WARPS; ++w) {
+                status |= s_status[w][lane];
+                if (!s_have[w][lane]) continue;
+                const Sw16Best c = s_best[w][lane];
+                if (!have || c.score > best.score || (c.score == best.score && (c.j < best.j ||
+                                                        (c.j == best.j && c.i < best.i)))) {
+                    best = c;
+                    have = true;
+                }
+            }
         }
         /* no positive cell: score 0 at (0, 0), the first cell (src/sw.c:150-158) */
         if (valid) {
@@ -308,14 +400,14 @@ extern "C" int pb_cuda_align_sw16_multi(const pb_batch *b, pb_pair_out *d_out_al
     cudaMallocAsync((void **)&keys_sorted, sizeof(int) * n, st);
     cudaMallocAsync((void **)&idx, sizeof(int) * n, st);
     cudaMallocAsync((void **)&order, sizeof(int) * n, st);
-    cudaMallocAsync((void **)&counter, sizeof(int) * 2, st);
+    cudaMallocAsync((void **)&counter, sizeof(int) * 4, st);
     k_iota<<<(n + 255) / 256, 256, 0, st>>>(idx, n);
     cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_sort, b->d_tlen, keys_sorted, idx, order, n, 0, 32, st);
     cudaMallocAsync(&tmp, tmp_sort, st);
     cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_sort, b->d_tlen, keys_sorted, idx, order, n, 0, 32, st);
     std::vector<int> hlen(n);
     cudaMemcpyAsync(hlen.data(), keys_sorted, sizeof(int) * n, cudaMemcpyDeviceToHost, st);
-    cudaMemsetAsync(counter, 0, sizeof(int) * 2, st);
+    cudaMemsetAsync(counter, 0, sizeof(int) * 4, st);   /* warp tasks, team tasks, error */
     /* concatenated int8 profiles */
     std::vector<pb::Sw16Query> hq(nq);
     int8_t *prof_all = nullptr;
@@ -374,9 +466,20 @@ extern "C" int pb_cuda_align_sw16_multi(const pb_batch *b, pb_pair_out *d_out_al
         cudaStreamDestroy(st);
         return -1;
     }
+    /* team tasks: those above a fair share of the work per warp, which one
+     * warp alone would finish last */
+    int nteam = 0;
+    {
+        double total = 0.0;
+        for (const auto &t : sorted_tasks) total += (double)hq[t.q].qlen * hlen[t.first];
+        const double fair = total / ((double)blocks * pb::SW16_WARPS);
+        while (nteam < (int)sorted_tasks.size() &&
+               (double)hq[sorted_tasks[nteam].q].qlen * hlen[sorted_tasks[nteam].first] > fair)
+            ++nteam;
+    }
     pb::Sw16Params p;
     p.open = b->open; p.gap = b->gap; p.npairs = n; p.nq = nq;
-    p.ntasks = (int)sorted_tasks.size(); p.maxlen = maxlen;
+    p.ntasks = (int)sorted_tasks.size(); p.maxlen = maxlen; p.nteam = nteam;
     p.queries = d_q; p.prof_all = prof_all; p.prof_bytes = (int)prof_bytes;
     p.order = order; p.tasks = d_tasks;
     p.targets = b->d_targets; p.toff = b->d_toff; p.tlen = b->d_tlen;
@@ -389,7 +492,15 @@ extern "C" int pb_cuda_align_sw16_multi(const pb_batch *b, pb_pair_out *d_out_al
     cudaEventRecord(ev1, st);
     if (cudaGetLastError() != cudaSuccess) rc = -1;
     pb_diag_count_launch(2);   /* k_iota, k_sw16 */
-    cudaStreamSynchronize(st);
+    {
+        int herr = 0;
+        cudaMemcpyAsync(&herr, counter + 2, sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        if (herr) {
+            fprintf(stderr, "pb_cuda_align_sw16_multi: a pass wait exceeded its bound\n");
+            rc = -1;
+        }
+    }
     {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ev0, ev1);
