@@ -35,6 +35,9 @@ OPEN, GAP = 11, 1
 QUERY_LENGTHS = (100, 250, 500, 1000, 2000)
 N_TARGETS = 200_000
 OPS_PER_CELL = 6   # SW score-only algorithmic lane-operations per cell
+# DRAM bytes (read + write) per cell of k_sw16 on this workload, from one full-size ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum = 136.2 GB for 2.7213e11 cells; profiles/k_sw16_db_search.md)
+SW16_DRAM_BYTES_PER_CELL = 136.18e9 / 2.7213e11
 
 
 def parse():
@@ -349,7 +352,9 @@ def main():
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "roofline": {"bound": "int", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s",
-                     "frac": achieved / peak if peak > 0 else None, "traffic": None,
+                     "frac": achieved / peak if peak > 0 else None,
+                     "traffic": SW16_DRAM_BYTES_PER_CELL * cells_per_launch,
+                     "traffic_unit": "bytes per launch (ncu capture, scaled by cells)",
                      "kernel": "k_sw16", "peak_source": "live DPX viaddmax int16x2 microbenchmark",
                      "ops_per_cell": OPS_PER_CELL, "kernel_ms_per_launch": kernel_ms_per_launch},
         "roofline_hbm": {"bound": "hbm", "achieved": (int(lens.sum()) + 12 * n) / (kernel_ms_per_launch * 1e-3) / 1e9,
