@@ -460,15 +460,19 @@ extern "C" int pb_cuda_band_features(int npairs, const uint8_t *d_q, const int64
     const int blocks = std::min(npairs, nsm * 4);
     uint32_t *tables = nullptr;
     int *counter = nullptr;
-    if (cudaMalloc(&tables, sizeof(uint32_t) * ((size_t)1 << (2 * pb::KMER_K)) * blocks) != cudaSuccess) return -1;
-    cudaMemset(tables, 0xff, sizeof(uint32_t) * ((size_t)1 << (2 * pb::KMER_K)) * blocks);
-    cudaMalloc(&counter, sizeof(int));
-    cudaMemset(counter, 0, sizeof(int));
+    /* stream-ordered pool memory: a plain cudaMalloc/cudaFree of these
+     * tables (tens of MB per call) can stall while the pool holds most of
+     * the device's memory */
+    const size_t tbytes = sizeof(uint32_t) * ((size_t)1 << (2 * pb::KMER_K)) * blocks;
+    if (cudaMallocAsync((void **)&tables, tbytes, 0) != cudaSuccess) return -1;
+    if (cudaMallocAsync((void **)&counter, sizeof(int), 0) != cudaSuccess) { cudaFreeAsync(tables, 0); return -1; }
+    cudaMemsetAsync(tables, 0xff, tbytes, 0);
+    cudaMemsetAsync(counter, 0, sizeof(int), 0);
     pb::k_kmer_hist<<<blocks, 256>>>(npairs, d_q, d_qoff, d_qlen, d_t, d_toff, d_tlen, tables, d_feat, counter);
     pb_diag_count_launch(1);
+    cudaFreeAsync(tables, 0);
+    cudaFreeAsync(counter, 0);
     cudaError_t e = cudaDeviceSynchronize();
-    cudaFree(tables);
-    cudaFree(counter);
     return e == cudaSuccess ? 0 : -1;
 }
 
@@ -560,13 +564,14 @@ extern "C" int pb_cuda_band_cells(int npairs, const int *d_qlen, const int *d_tl
                                   const int *d_hi, unsigned long long *h_cells)
 {
     unsigned long long *d = nullptr;
-    cudaMalloc(&d, sizeof(unsigned long long));
-    cudaMemset(d, 0, sizeof(unsigned long long));
+    if (cudaMallocAsync((void **)&d, sizeof(unsigned long long), 0) != cudaSuccess) return -1;
+    cudaMemsetAsync(d, 0, sizeof(unsigned long long), 0);
     pb::k_band_cells<<<(npairs + 127) / 128, 128>>>(npairs, d_qlen, d_tlen, d_lo, d_hi, d);
     pb_diag_count_launch(1);
-    cudaMemcpy(h_cells, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
-    cudaFree(d);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    cudaMemcpyAsync(h_cells, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost, 0);
+    cudaFreeAsync(d, 0);
+    const cudaError_t e = cudaStreamSynchronize(0);
+    return e == cudaSuccess && cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 /* Chooses the model's band scaling on n held-out pairs (features d_x,

@@ -39,7 +39,11 @@ namespace pb {
 
 static constexpr int NWL_RL = 8;          /* query rows per lane */
 static constexpr int NWL_WARPS = 8;       /* warps per CTA */
-static constexpr int NWL_CLUSTER = 8;     /* CTAs per cluster for the largest pairs */
+static constexpr int NWL_CLUSTER = 8;     /* CTAs per cluster for the largest pairs, full DP */
+/* banded: consecutive passes start ~350 columns apart, so a team of T warps
+ * only keeps busy on bands of ~350 T columns; smaller clusters suit the band
+ * widths of long pairs better */
+static constexpr int NWL_CLUSTER_BANDED = 4;
 static constexpr int NWL_NEG = INT32_MIN / 4;
 
 struct NwWaveParams {
@@ -449,7 +453,7 @@ static int nw_long_impl(int npairs, int open, int gap, const int32_t *h_mat, int
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, pb::NWL_WARPS * 32, 0);
     if (per_sm < 1) per_sm = 1;
     /* clusters of NWL_CLUSTER CTAs run the largest pairs as one team */
-    int C = pb::NWL_CLUSTER, nclusters = 0;
+    int C = d_lo ? pb::NWL_CLUSTER_BANDED : pb::NWL_CLUSTER, nclusters = 0;
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
