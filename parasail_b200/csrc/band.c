@@ -66,7 +66,7 @@ static int dev_pairs_upload(const parasail_matrix_t *matrix, const char *queries
 {
     int64_t qb = 0, tb = 0, k;
     int i;
-    uint8_t *hq, *ht;
+    uint8_t map[256];
     memset(d, 0, sizeof *d);
     d->n = n;
     for (i = 0; i < n; ++i) {
@@ -75,11 +75,7 @@ static int dev_pairs_upload(const parasail_matrix_t *matrix, const char *queries
         if (toff[i] + tlen[i] > tb) tb = toff[i] + tlen[i];
         if (tlen[i] > d->maxlen) d->maxlen = tlen[i];
     }
-    hq = (uint8_t *)malloc((size_t)qb + 1);
-    ht = (uint8_t *)malloc((size_t)tb + 1);
-    if (!hq || !ht) { free(hq); free(ht); return -1; }
-    for (k = 0; k < qb; ++k) hq[k] = (uint8_t)matrix->mapper[(unsigned char)queries[k]];
-    for (k = 0; k < tb; ++k) ht[k] = (uint8_t)matrix->mapper[(unsigned char)targets[k]];
+    for (k = 0; k < 256; ++k) map[k] = (uint8_t)matrix->mapper[k];
     d->q = (uint8_t *)pb_cuda_malloc((size_t)qb + 16);
     d->t = (uint8_t *)pb_cuda_malloc((size_t)tb + 16);
     d->qoff = (int64_t *)pb_cuda_malloc(sizeof(int64_t) * n);
@@ -87,17 +83,17 @@ static int dev_pairs_upload(const parasail_matrix_t *matrix, const char *queries
     d->qlen = (int *)pb_cuda_malloc(sizeof(int) * n);
     d->tlen = (int *)pb_cuda_malloc(sizeof(int) * n);
     if (!d->q || !d->t || !d->qoff || !d->toff || !d->qlen || !d->tlen) {
-        free(hq); free(ht); dev_pairs_free(d); return -1;
+        dev_pairs_free(d); return -1;
     }
-    pb_cuda_h2d(d->q, hq, (size_t)qb);
-    pb_cuda_h2d(d->t, ht, (size_t)tb);
+    /* characters go up as they are and are mapped to codes on the device */
+    if (pb_cuda_h2d_mapped(d->q, queries, qb, map) != 0 || pb_cuda_h2d_mapped(d->t, targets, tb, map) != 0) {
+        dev_pairs_free(d); return -1;
+    }
     pb_cuda_h2d(d->qoff, qoff, sizeof(int64_t) * n);
     pb_cuda_h2d(d->toff, toff, sizeof(int64_t) * n);
     pb_cuda_h2d(d->qlen, qlen, sizeof(int) * n);
     pb_cuda_h2d(d->tlen, tlen, sizeof(int) * n);
     pb_cuda_sync();
-    free(hq);
-    free(ht);
     return 0;
 }
 

@@ -108,6 +108,8 @@ int pb_cuda_d2h(void *dst, const void *src, size_t bytes);
 /* all work on the device, including kernels on the legacy default stream */
 int pb_cuda_device_sync(void);
 int pb_cuda_memset(void *p, int v, size_t bytes);
+/* n host characters to the device, mapped to codes there through mapper256 */
+int pb_cuda_h2d_mapped(uint8_t *d_buf, const char *h_chars, int64_t n, const uint8_t *mapper256);
 int pb_cuda_sync(void);
 
 /* --- alignment ------------------------------------------------------------- */

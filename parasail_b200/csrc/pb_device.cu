@@ -80,6 +80,16 @@ __global__ void k_build_profile(const int *__restrict__ table, int is_pssm, int 
     }
 }
 
+/* bytes -> codes through a 256-entry table, in place */
+__global__ void k_map_bytes(uint8_t *__restrict__ buf, int64_t n, const uint8_t *__restrict__ map)
+{
+    __shared__ uint8_t smap[256];
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) smap[k] = map[k];
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        buf[i] = smap[buf[i]];
+}
+
 __global__ void k_scratch_sizes(const int *__restrict__ tlen, const int *__restrict__ tlim,
                                 int n, int nv, int64_t *__restrict__ sizes)
 {
@@ -160,6 +170,24 @@ int pb_cuda_d2h(void *dst, const void *src, size_t bytes)
 int pb_cuda_sync(void)
 {
     CK(cudaStreamSynchronize(stream()));
+    return 0;
+}
+
+/* copies n host characters to d_buf and maps them to codes there */
+int pb_cuda_h2d_mapped(uint8_t *d_buf, const char *h_chars, int64_t n, const uint8_t *mapper256)
+{
+    if (n <= 0) return 0;
+    cudaStream_t st = stream();
+    uint8_t *d_map = nullptr;
+    CK(cudaMallocAsync((void **)&d_map, 256, st));
+    CK(cudaMemcpyAsync(d_map, mapper256, 256, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_buf, h_chars, (size_t)n, cudaMemcpyHostToDevice, st));
+    k_map_bytes<<<296, 256, 0, st>>>(d_buf, n, d_map);
+    pb_diag_count_launch(1);
+    CK(cudaGetLastError());
+    CK(cudaFreeAsync(d_map, st));
+    /* the host mapper copy dies at return */
+    CK(cudaStreamSynchronize(st));
     return 0;
 }
 
