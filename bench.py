@@ -148,7 +148,7 @@ def cpu_baseline(queries, buf, offs, lens, target_seconds):
             "ntargets": nt, "checksum": chk, "saturated_32": nsat}, None
 
 
-def learned_band_leg(pb, n_train=2000, n_test=300, epochs=40):
+def learned_band_leg(pb, n_train=2000, n_test=300, epochs=120):
     """Config-5 leg: long DNA pairs (5-50 kbp, 1-15% divergence, a large
     indel in 30%), +1/-2, open 4, extend 1. Plain full-DP global alignment
     vs the learned band (features + MLP + banded DP + certificate + full-DP

@@ -331,8 +331,10 @@ __device__ inline long long band_cells_of(long long n, long long m, long long lo
  * every pair whose band does not contain its label band (so the certificate
  * fails), a rerun on (band) U (label band of the first run's cost). That
  * cost is at least the optimum's, so the rerun band is at least the union
- * with the label band; it counts twice that union's cells. */
-static constexpr int BAND_RERUN_WEIGHT = 2;
+ * with the label band. A rerun counts 6 times that union's cells: it starts
+ * only when its pair's first band is done, so it lengthens that pair's
+ * latency (often the batch's tail) rather than adding to throughput. */
+static constexpr int BAND_RERUN_WEIGHT = 6;
 
 __global__ void k_tune_cost(int npairs, const int *qlen, const int *tlen, const int *lo, const int *hi,
                             const int *lab_lo, const int *lab_hi, unsigned long long *cost)
