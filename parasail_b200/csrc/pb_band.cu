@@ -582,7 +582,7 @@ extern "C" int pb_cuda_band_cells(int npairs, const int *d_qlen, const int *d_tl
 extern "C" int pb_cuda_band_tune(pb_band_model *m, int n, const float *d_x, const int *d_qlen, const int *d_tlen,
                                  const int *d_lab_lo, const int *d_lab_hi, float *chosen)
 {
-    static const float grid[] = {1.0f, 1.1f, 1.25f, 1.5f, 1.75f, 2.0f, 2.5f, 3.0f};
+    static const float grid[] = {1.0f, 1.05f, 1.1f, 1.15f, 1.2f, 1.3f, 1.4f, 1.5f, 1.75f, 2.0f, 2.5f, 3.0f};
     if (n <= 0) return -1;
     float *y = nullptr;
     int *lo = nullptr, *hi = nullptr;

@@ -44,6 +44,9 @@ static constexpr int NWL_CLUSTER = 8;     /* CTAs per cluster for the largest pa
  * only keeps busy on bands of ~350 T columns; smaller clusters suit the band
  * widths of long pairs better */
 static constexpr int NWL_CLUSTER_BANDED = 4;
+/* banded: a team only pays off for the pairs well above a fair share of
+ * the work (it idles on bands narrower than ~350 columns per warp) */
+static constexpr int NWL_COOP_SHARE_BANDED = 1;
 static constexpr int NWL_NEG = INT32_MIN / 4;
 
 struct NwWaveParams {
@@ -395,20 +398,21 @@ __global__ void k_cells(const int *ql, const int *tl, const int *lo, const int *
 }
 
 /* NWL_COOP_BIT for the pairs a whole cluster should run: those whose work
- * is above a fair share of the total per CTA (left to one CTA, they would
- * finish last), that give every warp of the team a pass, and, banded, whose
+ * is above `share` fair shares of the total per CTA (left to one CTA, they
+ * would finish last), that give every warp of the team a pass, and, banded, whose
  * band is at least 1024 diagonals wide. (A banded pass starts about 350
  * columns after the one above it, the band moving with the rows, so a team
  * of T warps is only fully busy on bands of about 350 T columns; below that
  * the team still finishes a large pair sooner than one CTA would.) */
 __global__ void k_coop_flag(const int *ql, const int *lo, const int *hi, int n, int nctas, int coop_pass,
-                            const unsigned long long *total, unsigned long long *keys, int *ncoop)
+                            int share, const unsigned long long *total, unsigned long long *keys, int *ncoop)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int npass = (ql[i] + 32 * NWL_RL - 1) / (32 * NWL_RL);
     const unsigned long long k = keys[i];
-    if (npass >= coop_pass && (!lo || hi[i] - lo[i] >= 1024) && k * (unsigned long long)nctas > *total) {
+    if (npass >= coop_pass && (!lo || hi[i] - lo[i] >= 1024) &&
+        k * (unsigned long long)nctas > (unsigned long long)share * *total) {
         keys[i] = k | NWL_COOP_BIT;
         atomicAdd(ncoop, 1);
     }
@@ -486,7 +490,9 @@ static int nw_long_impl(int npairs, int open, int gap, const int32_t *h_mat, int
     pb::k_cells<<<(npairs + 255) / 256, 256, 0, st>>>(d_qlen, d_tlen, d_lo, d_hi, npairs, keys, total);
     if (C > 1)
         pb::k_coop_flag<<<(npairs + 255) / 256, 256, 0, st>>>(d_qlen, d_lo, d_hi, npairs, plain_max,
-                                                              C * pb::NWL_WARPS, total, keys, counter + 4);
+                                                              C * pb::NWL_WARPS,
+                                                              d_lo ? pb::NWL_COOP_SHARE_BANDED : 1, total, keys,
+                                                              counter + 4);
     cub::DeviceRadixSort::SortPairsDescending(nullptr, tmpb, keys, keys_sorted, idx, order, npairs, 0, 64, st);
     cudaMallocAsync(&tmp, tmpb, st);
     cub::DeviceRadixSort::SortPairsDescending(tmp, tmpb, keys, keys_sorted, idx, order, npairs, 0, 64, st);
