@@ -104,18 +104,18 @@ int pb_run_job_pair(const pb_device_profile *dp, const pb_job *job, const uint8_
         if (rc != 0) return rc;
     }
     {
-        pb_lane_res e8, e16;
+        pb_lane_res e[3];
         int round;
-        memset(&e8, 0, sizeof e8);
-        memset(&e16, 0, sizeof e16);
-        *rec = pb_chain_resolve(job, &o1, &o2, dp->qlen, tlen, &e8, &e16);
-        /* narrow striped widths the exact values cannot settle: the
-         * lane-exact kernel of that width, then resolve again */
-        for (round = 0; round < 2 && (rec->ambig == 8 || rec->ambig == 16); ++round) {
-            pb_lane_res *e = rec->ambig == 8 ? &e8 : &e16;
-            if (pb_cuda_lane_pair(rec->ambig, dp, &job->mode, codes, tlen, &o1, e) != 0) return -1;
-            *rec = pb_chain_resolve(job, &o1, &o2, dp->qlen, tlen, &e8, &e16);
+        memset(e, 0, sizeof e);
+        *rec = pb_chain_resolve(job, &o1, &o2, dp->qlen, tlen, &e[0], &e[1], &e[2]);
+        /* striped widths the exact values do not give: the lane-exact
+         * kernel of that width, then resolve again */
+        for (round = 0; round < 3 && (rec->ambig == 8 || rec->ambig == 16 || rec->ambig == 32); ++round) {
+            pb_lane_res *x = &e[rec->ambig == 8 ? 0 : rec->ambig == 16 ? 1 : 2];
+            if (pb_cuda_lane_pair(rec->ambig, dp, &job->mode, codes, tlen, &o1, x) != 0) return -1;
+            *rec = pb_chain_resolve(job, &o1, &o2, dp->qlen, tlen, &e[0], &e[1], &e[2]);
         }
+        if (rec->ambig == 8 || rec->ambig == 16 || rec->ambig == 32) return -1;
     }
     return 0;
 }

@@ -14,12 +14,30 @@
 
 namespace pb {
 
+/* The lane results of pair i as the chain reads them: `e` holds the last
+ * lane-exact result of the pair (valid = its width). The chain moves past a
+ * width whose lane result it read only when that result saturated, so every
+ * narrower width it read is given back as a saturated result. */
+__device__ inline void lane_views(const pb_lane_res *e, int i, pb_lane_res x[3])
+{
+    const int w3[3] = {8, 16, 32};
+    pb_lane_res s;
+    memset(x, 0, 3 * sizeof(pb_lane_res));
+    if (!e) return;
+    s = e[i];
+    for (int t = 0; t < 3; ++t) {
+        if (s.valid == w3[t]) x[t] = s;
+        else if (s.valid > w3[t]) { x[t].valid = w3[t]; x[t].saturated = 1; }
+    }
+}
+
+/* Resolves pairs (all n, or the n listed) and lists by width the pairs that
+ * still wait for a lane-exact kernel: need + w * n, counts[w]. */
 __global__ void k_resolve(pb_job job, const pb_pair_out *__restrict__ o1,
                           const pb_pair_out *__restrict__ o2, const int *__restrict__ qlen,
-                          int qlen_all, const int *__restrict__ tlen, int n,
-                          const int *__restrict__ list, const pb_lane_res *__restrict__ e8,
-                          const pb_lane_res *__restrict__ e16, pb_record *__restrict__ rec,
-                          int *__restrict__ need8, int *__restrict__ need16, int *__restrict__ counts)
+                          int qlen_all, const int *__restrict__ tlen, int n_all, int n,
+                          const int *__restrict__ list, const pb_lane_res *__restrict__ e,
+                          pb_record *__restrict__ rec, int *__restrict__ need, int *__restrict__ counts)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -27,11 +45,13 @@ __global__ void k_resolve(pb_job job, const pb_pair_out *__restrict__ o1,
     const pb_pair_out a = o1[i];
     pb_pair_out b;
     if (o2) b = o2[i];
+    pb_lane_res x[3];
+    lane_views(e, i, x);
     const pb_record r = pb_chain_resolve(&job, &a, o2 ? &b : nullptr, qlen ? qlen[i] : qlen_all, tlen[i],
-                                         e8 ? &e8[i] : nullptr, e16 ? &e16[i] : nullptr);
+                                         &x[0], &x[1], &x[2]);
     rec[i] = r;
-    if (counts && r.ambig == 8) need8[atomicAdd(&counts[0], 1)] = i;
-    else if (counts && r.ambig == 16) need16[atomicAdd(&counts[1], 1)] = i;
+    const int t = r.ambig == 8 ? 0 : r.ambig == 16 ? 1 : r.ambig == 32 ? 2 : -1;
+    if (t >= 0) need[(size_t)t * n_all + atomicAdd(&counts[t], 1)] = i;
 }
 
 __global__ void k_max_int(const int *__restrict__ v, int n, int *__restrict__ out)
@@ -57,22 +77,23 @@ __global__ void k_prefix_limits(pb_job job, const pb_pair_out *__restrict__ o1, 
 
 /*
  * Resolution of n pairs with the lane-exact rounds: resolve every pair; the
- * pairs that need the 8- or 16-bit lane kernel are listed, emulated and
- * resolved again, until none is left (at most one round per width).
- * `la` describes the query side (profile or matrix mode) and the targets.
- * Work memory: from `work` (work_bytes, 256-byte aligned) when given,
- * otherwise from the stream's pool. Synchronises the stream once per round.
+ * pairs that need the 8-, 16- or 32-bit lane kernel are listed by width,
+ * emulated and resolved again, until none is left (at most one round per
+ * width). `la` describes the query side (profile or matrix mode) and the
+ * targets. Work memory: from `work` (work_bytes, 256-byte aligned) when
+ * given, otherwise from the stream's pool. Synchronises the stream once per
+ * round.
  */
 int resolve_rounds(const pb_job &job, const pb_lane_args &la, const pb_pair_out *o1, const pb_pair_out *o2,
                    const int *qlen, int qlen_all, const int *tlen, int n, pb_record *rec, cudaStream_t st,
                    void *work, size_t work_bytes)
 {
     if (n <= 0) return 0;
-    /* work layout: counts[2] | lists A (2n) | lists B (2n) | e8 (n) | e16 (n) | lane scratch */
+    /* work layout: counts | lists A (3n) | lists B (3n) | results (n) | lane scratch */
     const size_t b_counts = 256;
-    const size_t b_lists = ((sizeof(int) * 2 * (size_t)n) + 255) & ~(size_t)255;
+    const size_t b_lists = ((sizeof(int) * 3 * (size_t)n) + 255) & ~(size_t)255;
     const size_t b_res = ((sizeof(pb_lane_res) * (size_t)n) + 255) & ~(size_t)255;
-    const size_t fixed = b_counts + 2 * b_lists + 2 * b_res;
+    const size_t fixed = b_counts + 2 * b_lists + b_res;
     unsigned char *base = (unsigned char *)work;
     bool own = false;
     if (!base) {
@@ -83,28 +104,28 @@ int resolve_rounds(const pb_job &job, const pb_lane_args &la, const pb_pair_out 
     }
     int *counts = (int *)base;
     int *lists[2] = {(int *)(base + b_counts), (int *)(base + b_counts + b_lists)};
-    pb_lane_res *e8 = (pb_lane_res *)(base + b_counts + 2 * b_lists);
-    pb_lane_res *e16 = (pb_lane_res *)(base + b_counts + 2 * b_lists + b_res);
+    pb_lane_res *res = (pb_lane_res *)(base + b_counts + 2 * b_lists);
     unsigned char *lane_scratch = own ? nullptr : base + fixed;
     const size_t lane_bytes = own ? 0 : work_bytes - fixed;
+    const int w3[3] = {8, 16, 32};
     int rc = 0;
-    cudaMemsetAsync(counts, 0, 2 * sizeof(int), st);
-    cudaMemsetAsync(e8, 0, b_res, st);
-    cudaMemsetAsync(e16, 0, b_res, st);
-    k_resolve<<<(n + 255) / 256, 256, 0, st>>>(job, o1, o2, qlen, qlen_all, tlen, n, nullptr, nullptr, nullptr,
-                                               rec, lists[0], lists[0] + n, counts);
+    cudaMemsetAsync(counts, 0, 3 * sizeof(int), st);
+    cudaMemsetAsync(res, 0, b_res, st);
+    k_resolve<<<(n + 255) / 256, 256, 0, st>>>(job, o1, o2, qlen, qlen_all, tlen, n, n, nullptr, nullptr,
+                                               rec, lists[0], counts);
     pb_diag_count_launch(1);
     int cur = 0;
     pb_lane_args a = la;
     bool have_max = a.max_qlen > 0;
-    for (int round = 0; round < 3 && rc == 0; ++round) {
-        int hc[2] = {0, 0};
+    for (int round = 0; rc == 0; ++round) {
+        int hc[3] = {0, 0, 0};
         if (cudaMemcpyAsync(hc, counts, sizeof hc, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess) { rc = -1; break; }
-        if (hc[0] + hc[1] == 0) break;
+        if (hc[0] + hc[1] + hc[2] == 0) break;
+        if (round == 3) { rc = -1; break; }   /* a width cannot be asked for twice */
         if (!have_max) {
             /* matrix mode: the longest query sizes the lane scratch */
-            int *dm = counts + 2;
+            int *dm = counts + 4;
             int hm = 0;
             cudaMemsetAsync(dm, 0, sizeof(int), st);
             k_max_int<<<64, 256, 0, st>>>(a.qlens, n, dm);
@@ -117,17 +138,20 @@ int resolve_rounds(const pb_job &job, const pb_lane_args &la, const pb_pair_out 
         a.kind = pb_lane_kind(&job.mode);
         a.sgflags = job.mode.sgflags;
         a.open = job.mode.open; a.gap = job.mode.gap;
-        if (hc[0] && pb_cuda_lane_run(8, &a, lists[cur], hc[0], e8, lane_scratch, lane_bytes, st) != 0) { rc = -1; break; }
-        if (hc[1] && pb_cuda_lane_run(16, &a, lists[cur] + n, hc[1], e16, lane_scratch, lane_bytes, st) != 0) { rc = -1; break; }
+        for (int t = 0; t < 3 && rc == 0; ++t)
+            if (hc[t] && pb_cuda_lane_run(w3[t], &a, lists[cur] + (size_t)t * n, hc[t], res, lane_scratch,
+                                          lane_bytes, st) != 0)
+                rc = -1;
+        if (rc) break;
         const int nxt = cur ^ 1;
-        cudaMemsetAsync(counts, 0, 2 * sizeof(int), st);
-        if (hc[0])
-            k_resolve<<<(hc[0] + 255) / 256, 256, 0, st>>>(job, o1, o2, qlen, qlen_all, tlen, hc[0], lists[cur], e8,
-                                                           e16, rec, lists[nxt], lists[nxt] + n, counts);
-        if (hc[1])
-            k_resolve<<<(hc[1] + 255) / 256, 256, 0, st>>>(job, o1, o2, qlen, qlen_all, tlen, hc[1], lists[cur] + n,
-                                                           e8, e16, rec, lists[nxt], lists[nxt] + n, counts);
-        pb_diag_count_launch((hc[0] ? 1 : 0) + (hc[1] ? 1 : 0));
+        cudaMemsetAsync(counts, 0, 3 * sizeof(int), st);
+        for (int t = 0; t < 3; ++t)
+            if (hc[t]) {
+                k_resolve<<<(hc[t] + 255) / 256, 256, 0, st>>>(job, o1, o2, qlen, qlen_all, tlen, n, hc[t],
+                                                               lists[cur] + (size_t)t * n, res, rec, lists[nxt],
+                                                               counts);
+                pb_diag_count_launch(1);
+            }
         if (cudaGetLastError() != cudaSuccess) { rc = -1; break; }
         cur = nxt;
     }

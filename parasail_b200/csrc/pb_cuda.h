@@ -149,6 +149,8 @@ int pb_cuda_batch_host(const struct pb_job *job, const pb_batch *tmpl, const uin
  * 1 nw/sg with statistics, 2 the SW statistics kernel on the FASTSTATS prefix
  * [0, o1.end_query] x [0, o1.end_ref]. Profile mode (prof, qcodes, lp, qlen)
  * or matrix mode (mat, msize, qall, qoff, qlens). */
+/* One lane-exact kernel result; valid = the width of the kernel that
+ * wrote it (0: none). */
 typedef struct pb_lane_res {
     int score, end_query, end_ref, matches, similar, length, saturated, valid;
 } pb_lane_res;

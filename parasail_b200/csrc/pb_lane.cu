@@ -23,19 +23,24 @@
 namespace pb {
 namespace lane {
 
+/* storage of one lane value: 16 bits hold the 8- and 16-bit kernels' lanes */
+template <int W> struct LaneElem { typedef int16_t T; };
+template <> struct LaneElem<32> { typedef int32_t T; };
+
 template <int W> struct WarpVec {
     static constexpr int L = Lim<W>::LANES;
     typedef int V;
-    struct Arr { int16_t *p; };
+    typedef typename LaneElem<W>::T E;
+    struct Arr { E *p; };
     int lane;
-    int16_t *scratch;
+    E *scratch;
 
     __device__ __forceinline__ Arr arr(int a, int segLen) { return Arr{scratch + (size_t)a * segLen * 32}; }
     __device__ __forceinline__ V load(Arr a, int i) { return a.p[i * 32 + lane]; }
-    __device__ __forceinline__ void store(Arr a, int i, V x) { a.p[i * 32 + lane] = (int16_t)x; }
+    __device__ __forceinline__ void store(Arr a, int i, V x) { a.p[i * 32 + lane] = (E)x; }
     __device__ __forceinline__ V set1(int x) { return x; }
-    template <int W2> __device__ __forceinline__ V adds(V a, V b) { return clampw<W2>((long long)a + b); }
-    template <int W2> __device__ __forceinline__ V subs(V a, V b) { return clampw<W2>((long long)a - b); }
+    template <int W2> __device__ __forceinline__ V adds(V a, V b) { return lane_arith<W2>((long long)a + b); }
+    template <int W2> __device__ __forceinline__ V subs(V a, V b) { return lane_arith<W2>((long long)a - b); }
     __device__ __forceinline__ V max(V a, V b) { return a > b ? a : b; }
     __device__ __forceinline__ V min(V a, V b) { return a < b ? a : b; }
     __device__ __forceinline__ V cmpgt(V a, V b) { return a > b ? -1 : 0; }
@@ -92,7 +97,7 @@ template <int W> struct WarpVec {
 };
 
 struct LaneJob {
-    int kind;                                  /* 0 nw/sg, 1 nw/sg stats, 2 sw stats prefix */
+    int kind;                                  /* 0 nw/sg, 1 nw/sg stats, 2 sw stats prefix, 3 sw */
     int open, gap, mmax, mmin;
     int s1_beg, s1_end, s2_beg, s2_end;
     /* profile mode */
@@ -103,8 +108,10 @@ struct LaneJob {
     const pb_pair_out *o1;                     /* kind 2: prefix = o1 ends */
     const int *list; int nlist;
     pb_lane_res *res;                          /* indexed by pair id */
-    int16_t *scratch; int seg_max; int narr;
+    void *scratch; int seg_max; int narr;
 };
+
+PB_LHD int lane_narr(int kind) { return kind == 0 ? 3 : kind == 1 ? 12 : kind == 2 ? 16 : 4; }
 
 constexpr int LANE_THREADS = 256;
 
@@ -116,7 +123,7 @@ __global__ void __launch_bounds__(LANE_THREADS) k_lane(LaneJob J)
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     WarpVec<W> v;
     v.lane = lane;
-    v.scratch = J.scratch + (size_t)warp * J.narr * J.seg_max * 32;
+    v.scratch = reinterpret_cast<typename WarpVec<W>::E *>(J.scratch) + (size_t)warp * J.narr * J.seg_max * 32;
     for (int k = warp; k < J.nlist; k += nwarps) {
         const int pid = J.list[k];
         Problem pr;
@@ -138,12 +145,13 @@ __global__ void __launch_bounds__(LANE_THREADS) k_lane(LaneJob J)
         Out o;
         if (J.kind == 0) striped_nwsg<WarpVec<W>, W>(v, pr, o);
         else if (J.kind == 1) striped_nwsg_stats<WarpVec<W>, W>(v, pr, o);
-        else striped_sw_stats_bias<WarpVec<W>, W>(v, pr, o);
+        else if (J.kind == 3) striped_sw<WarpVec<W>, W>(v, pr, o);
+        else if (W != 32) striped_sw_stats_bias<WarpVec<W>, W>(v, pr, o);
         if (lane == 0) {
             pb_lane_res r;
             r.score = o.score; r.end_query = o.end_query; r.end_ref = o.end_ref;
             r.matches = o.matches; r.similar = o.similar; r.length = o.length;
-            r.saturated = o.saturated; r.valid = 1;
+            r.saturated = o.saturated; r.valid = W;
             J.res[pid] = r;
         }
         __syncwarp();
@@ -159,8 +167,7 @@ size_t pb_cuda_lane_scratch_per_warp(int bits, int kind, int max_qlen)
 {
     const int L = 256 / bits;
     const int seg = (max_qlen + L - 1) / L;
-    const int narr = kind == 0 ? 3 : kind == 1 ? 12 : 16;
-    return sizeof(int16_t) * (size_t)narr * seg * 32;
+    return (bits == 32 ? 4 : 2) * (size_t)pb::lane::lane_narr(kind) * seg * 32;
 }
 
 int pb_cuda_lane_run(int bits, const pb_lane_args *a, const int *d_list, int nlist, pb_lane_res *d_res,
@@ -169,7 +176,7 @@ int pb_cuda_lane_run(int bits, const pb_lane_args *a, const int *d_list, int nli
     cudaStream_t st = (cudaStream_t)stream;
     using namespace pb::lane;
     if (nlist <= 0) return 0;
-    if (bits != 8 && bits != 16) return -1;
+    if ((bits != 8 && bits != 16 && bits != 32) || (bits == 32 && a->kind == 2)) return -1;
     LaneJob J;
     J.kind = a->kind; J.open = a->open; J.gap = a->gap; J.mmax = a->mmax; J.mmin = a->mmin;
     J.s1_beg = (a->sgflags & PB_S1_BEG) != 0; J.s1_end = (a->sgflags & PB_S1_END) != 0;
@@ -181,8 +188,8 @@ int pb_cuda_lane_run(int bits, const pb_lane_args *a, const int *d_list, int nli
     const int L = 256 / bits;
     J.seg_max = (a->max_qlen + L - 1) / L;
     if (J.seg_max < 1) J.seg_max = 1;
-    J.narr = a->kind == 0 ? 3 : a->kind == 1 ? 12 : 16;
-    const size_t per_warp = sizeof(int16_t) * (size_t)J.narr * J.seg_max * 32;
+    J.narr = lane_narr(a->kind);
+    const size_t per_warp = (bits == 32 ? 4 : 2) * (size_t)J.narr * J.seg_max * 32;
     int nsm = 0, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -206,10 +213,11 @@ int pb_cuda_lane_run(int bits, const pb_lane_args *a, const int *d_list, int nli
         if (cudaMallocAsync(&scratch, per_warp * warps, st) != cudaSuccess) return -1;
         own = true;
     }
-    J.scratch = (int16_t *)scratch;
+    J.scratch = scratch;
     const int blocks = (int)(warps * 32 / threads);
     if (bits == 8) k_lane<8><<<blocks, threads, 0, st>>>(J);
-    else k_lane<16><<<blocks, threads, 0, st>>>(J);
+    else if (bits == 16) k_lane<16><<<blocks, threads, 0, st>>>(J);
+    else k_lane<32><<<blocks, threads, 0, st>>>(J);
     pb_diag_count_launch(1);
     const cudaError_t e = cudaGetLastError();
     if (own) cudaFreeAsync(scratch, st);

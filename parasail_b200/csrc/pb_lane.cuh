@@ -41,19 +41,28 @@ namespace lane {
 
 template <int W> struct Lim {
     static constexpr int LANES = 256 / W;
-    static constexpr int MIN = W == 8 ? -128 : -32768;
-    static constexpr int MAX = W == 8 ? 127 : 32767;
+    static constexpr int MIN = W == 8 ? -128 : W == 16 ? -32768 : (int)0x80000000;
+    static constexpr int MAX = W == 8 ? 127 : W == 16 ? 32767 : 0x7fffffff;
 };
 
-/* (intW_t)x: two's-complement wrap, as a C conversion to int8_t/int16_t */
+/* (intW_t)x: two's-complement wrap, as a C conversion to int8/16/32_t */
 template <int W> PB_LHD int wrap(long long x)
 {
-    return W == 8 ? (int)(int8_t)(uint8_t)(x & 0xff) : (int)(int16_t)(uint16_t)(x & 0xffff);
+    return W == 8 ? (int)(int8_t)(uint8_t)(x & 0xff)
+         : W == 16 ? (int)(int16_t)(uint16_t)(x & 0xffff)
+                   : (int)(uint32_t)(x & 0xffffffffll);
 }
 
 template <int W> PB_LHD int clampw(long long x)
 {
     return x < Lim<W>::MIN ? Lim<W>::MIN : (x > Lim<W>::MAX ? Lim<W>::MAX : (int)x);
+}
+
+/* lane add/subtract of the W-bit kernels: saturating at 8 and 16 bits
+ * (_mm256_adds/subs_epi8/16), wrapping at 32 (_mm256_add/sub_epi32) */
+template <int W> PB_LHD int lane_arith(long long x)
+{
+    return W == 32 ? wrap<W>(x) : clampw<W>(x);
 }
 
 /* One pair as the emulation sees it. Profile values come from the exact
@@ -536,6 +545,113 @@ PB_LHD void striped_sw_stats_bias(P &v, const Problem &pr, Out &o)
     o.matches = matches - bias;
     o.similar = similar - bias;
     o.length = length - bias;
+}
+
+/* ---- sw, score only: biased lanes at 8/16 bits (util/templates/
+ * sw_striped_bias.c), plain lanes with an explicit 0 floor at 32
+ * (util/templates/sw_striped.c) ---- */
+template <class P, int W>
+PB_LHD void striped_sw(P &v, const Problem &pr, Out &o)
+{
+    typedef typename P::V V;
+    constexpr int L = Lim<W>::LANES;
+    constexpr bool BIAS = W != 32;
+    const int s1Len = pr.qlen, s2Len = pr.tlen;
+    const int segLen = (s1Len + L - 1) / L;
+    const int open = pr.open, gap = pr.gap;
+    const int bias = BIAS ? Lim<W>::MIN : 0;
+    const int neg_inf = BIAS ? Lim<W>::MIN : Lim<W>::MIN / 2;
+    const V vGapO = v.set1(wrap<W>(open)), vGapE = v.set1(wrap<W>(gap));
+    const V vZero = v.set1(0);
+    const V vBias = v.set1(bias);
+    const V insert_mask = v.lane_eq(0);
+    const int maxp = wrap<W>((long long)Lim<W>::MAX - wrap<W>((long long)pr.mmax + 1));
+    V vMaxH = v.set1(BIAS ? bias : neg_inf), vMaxHUnit = vMaxH;
+    int score = BIAS ? bias : neg_inf;
+    int end_query = 0, end_ref = 0, saturated = 0;
+
+    typename P::Arr hs = v.arr(0, segLen), hl = v.arr(1, segLen), hx = v.arr(2, segLen), pe = v.arr(3, segLen);
+    const V e0 = BIAS ? vBias : v.set1(wrap<W>(-(long long)open));
+    for (int i = 0; i < segLen; ++i) {
+        v.store(hs, i, BIAS ? vBias : vZero);
+        v.store(pe, i, e0);
+    }
+    int j;
+    for (j = 0; j < s2Len; ++j) {
+        const int k_t = pr.t[j];
+        V vE;
+        V vF = BIAS ? vBias : vZero;
+        V vH = v.shift1(v.load(hs, segLen - 1));
+        if (BIAS) vH = v.blend(vH, vBias, insert_mask);
+        if (end_ref == j - 2) {
+            typename P::Arr t0 = hx; hx = hl; hl = hs; hs = t0;
+        } else {
+            typename P::Arr t0 = hl; hl = hs; hs = t0;
+        }
+        for (int i = 0; i < segLen; ++i) {
+            vH = v.template adds<W>(vH, v.template prof<W>(pr, k_t, i, segLen));
+            vE = v.load(pe, i);
+            vH = v.max(vH, vE);
+            vH = v.max(vH, vF);
+            if (!BIAS) vH = v.max(vH, vZero);
+            v.store(hs, i, vH);
+            vMaxH = v.max(vH, vMaxH);
+            vH = v.template subs<W>(vH, vGapO);
+            vE = v.template subs<W>(vE, vGapE);
+            vE = v.max(vE, vH);
+            v.store(pe, i, vE);
+            vF = v.template subs<W>(vF, vGapE);
+            vF = v.max(vF, vH);
+            vH = v.load(hl, i);
+        }
+        {
+            bool done = false;
+            for (int k = 0; k < L && !done; ++k) {
+                vF = v.shift1(vF);
+                if (BIAS) vF = v.blend(vF, vBias, insert_mask);
+                for (int i = 0; i < segLen; ++i) {
+                    vH = v.load(hs, i);
+                    vH = v.max(vH, vF);
+                    v.store(hs, i, vH);
+                    vMaxH = v.max(vH, vMaxH);
+                    vH = v.template subs<W>(vH, vGapO);
+                    vF = v.template subs<W>(vF, vGapE);
+                    if (!v.any(v.cmpgt(vF, vH))) { done = true; break; }
+                }
+            }
+        }
+        if (v.any(v.cmpgt(vMaxH, vMaxHUnit))) {
+            score = v.hmax(vMaxH);
+            if (score > maxp) { saturated = 1; break; }
+            vMaxHUnit = v.set1(score);
+            end_ref = j;
+        }
+    }
+    if (score == Lim<W>::MAX) saturated = 1;
+    if (saturated) {
+        score = Lim<W>::MAX;
+        end_query = 0;
+        end_ref = 0;
+    } else {
+        typename P::Arr tx = hx;
+        if (end_ref == j - 1) tx = hs;
+        else if (end_ref == j - 2) tx = hl;
+        end_query = s1Len - 1;
+        for (int i = 0; i < segLen; ++i) {
+            const V th = v.load(tx, i);
+            for (int l = 0; l < L; ++l) {
+                if (v.extract(th, l) == score) {
+                    const int temp = i + l * segLen;
+                    if (temp < end_query) end_query = temp;
+                }
+            }
+        }
+    }
+    o.saturated = saturated;
+    o.score = (int)((long long)score - bias);
+    o.end_query = end_query;
+    o.end_ref = end_ref;
+    o.matches = o.similar = o.length = 0;
 }
 
 }  // namespace lane

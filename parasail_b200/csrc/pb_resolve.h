@@ -166,18 +166,36 @@ typedef struct pb_record {
 
 enum { PB_REC_FALLBACK = 1 };
 
-/* Widths whose verdict the lane-exact kernels (pb_lane.cuh) give whenever
- * the exact values do not show a CLEAN run: the 8/16-bit striped nw/sg
- * kernels and the 8/16-bit SW statistics kernel of the FASTSTATS wrapper. */
+/* Widths at which the reference's striped kernel computes something other
+ * than the exact DP for every pair, so that only the lane-exact kernel
+ * gives its result: a penalty that wraps in the lane width (set1 of open or
+ * gap above INT_w_MAX), in the score-only kernels open <= gap (their lazy-F
+ * loop stops on a tie between F - gap and H - open, which open <= gap makes
+ * common), and in the statistics kernels open < gap (they continue on ties,
+ * and agree with the exact DP at open == gap). The SW statistics kernels of
+ * the FASTSTATS wrapper are not emulated in these regimes. */
+PB_HD static inline int pb_lane_forced(const pb_mode *m, int bits)
+{
+    if (!m->striped || (m->alg == PB_SW && m->stats)) return 0;
+    if (bits < 32 && (m->open > int_max_w(bits) || m->gap > int_max_w(bits))) return 1;
+    return m->stats ? m->open < m->gap : m->open <= m->gap;
+}
+
+/* Widths whose verdict the lane-exact kernels (pb_lane.cuh) give: the
+ * 8/16-bit striped nw/sg kernels and the 8/16-bit SW statistics kernel of
+ * the FASTSTATS wrapper whenever the exact values do not show a CLEAN run,
+ * and every striped width pb_lane_forced names. */
 PB_HD static inline int pb_lane_applies(const pb_mode *m, int bits)
 {
-    return m->striped && (bits == 8 || bits == 16) && (m->alg != PB_SW || m->stats);
+    if (!m->striped) return 0;
+    if (m->alg == PB_SW) return m->stats ? (bits == 8 || bits == 16) : pb_lane_forced(m, bits);
+    return bits == 8 || bits == 16 || pb_lane_forced(m, bits);
 }
 
 /* lane kernel kind for a mode (pb_lane_args.kind) */
 PB_HD static inline int pb_lane_kind(const pb_mode *m)
 {
-    return m->alg == PB_SW ? 2 : (m->stats ? 1 : 0);
+    return m->alg == PB_SW ? (m->stats ? 2 : 3) : (m->stats ? 1 : 0);
 }
 
 PB_HD static inline int pb_bits_flag(int bits)
@@ -236,13 +254,14 @@ PB_HD static inline int pb_ambig_fallback(const pb_mode *m, int bits, const pb_p
 
 /* The result the reference returns for one pair (src/satcheck.c chains,
  * the kernels' sentinel values, the FASTSTATS wrapper). o2 is the prefix
- * pass (FASTSTATS only, may be NULL when pb_needs_pass2 said no). e8/e16 are
- * the lane-exact kernels' results for the pair (NULL or not valid when they
+ * pass (FASTSTATS only, may be NULL when pb_needs_pass2 said no). e8, e16
+ * and e32 the lane-exact kernels' results for the pair (NULL or not valid when they
  * have not run); when a width needs one that is missing, the returned record
  * has ambig = that width and nothing else in it is final. */
 PB_HD static inline pb_record pb_chain_resolve(const pb_job *j, const pb_pair_out *o1,
                                                const pb_pair_out *o2, int qlen, int tlen,
-                                               const pb_lane_res *e8, const pb_lane_res *e16)
+                                               const pb_lane_res *e8, const pb_lane_res *e16,
+                                               const pb_lane_res *e32)
 {
     const int w3[3] = {8, 16, 32};
     const pb_mode *m = &j->mode;
@@ -261,7 +280,7 @@ PB_HD static inline pb_record pb_chain_resolve(const pb_job *j, const pb_pair_ou
     for (t = f; t <= l; ++t) {
         const int w = w3[t];
         const int fl = j->base_flags | pb_bits_flag(w) | pb_lanes_flag(w);
-        const pb_lane_res *e = w == 8 ? e8 : w == 16 ? e16 : (const pb_lane_res *)0;
+        const pb_lane_res *e = w == 8 ? e8 : w == 16 ? e16 : e32;
         int v;
         if (pb_job_is_faststats(j)) {
             if (pb_resolve_faststats_pass1(m, w, o1) == PB_SAT) {
@@ -298,10 +317,12 @@ PB_HD static inline pb_record pb_chain_resolve(const pb_job *j, const pb_pair_ou
             return r;
         }
         v = pb_resolve_tier(m, w, o1, qlen, tlen);
-        if (v != PB_CLEAN && pb_lane_applies(m, w)) {
+        if ((v != PB_CLEAN || pb_lane_forced(m, w)) && pb_lane_applies(m, w)) {
             if (!e || !e->valid) { r.ambig = w; return r; }
             if (e->saturated) {
                 if (t < l) continue;
+                /* the kernel's saturated result: zeros, or the SW sentinel */
+                r.score = e->score; r.end_query = e->end_query; r.end_ref = e->end_ref;
                 r.flag = fl | PARASAIL_FLAG_SATURATED | (m->stats ? PARASAIL_FLAG_STATS : 0);
                 r.ambig = fallback;
                 return r;

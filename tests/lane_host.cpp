@@ -24,8 +24,8 @@ template <int W> struct HostVec {
     V load(Arr a, int i) { return a[i]; }
     void store(Arr a, int i, const V &x) { a[i] = x; }
     V set1(int x) { V r; for (int l = 0; l < 32; ++l) r.v[l] = x; return r; }
-    template <int W2> V adds(const V &a, const V &b) { V r; for (int l = 0; l < 32; ++l) r.v[l] = clampw<W2>((long long)a.v[l] + b.v[l]); return r; }
-    template <int W2> V subs(const V &a, const V &b) { V r; for (int l = 0; l < 32; ++l) r.v[l] = clampw<W2>((long long)a.v[l] - b.v[l]); return r; }
+    template <int W2> V adds(const V &a, const V &b) { V r; for (int l = 0; l < 32; ++l) r.v[l] = lane_arith<W2>((long long)a.v[l] + b.v[l]); return r; }
+    template <int W2> V subs(const V &a, const V &b) { V r; for (int l = 0; l < 32; ++l) r.v[l] = lane_arith<W2>((long long)a.v[l] - b.v[l]); return r; }
     V max(const V &a, const V &b) { V r; for (int l = 0; l < 32; ++l) r.v[l] = a.v[l] > b.v[l] ? a.v[l] : b.v[l]; return r; }
     V min(const V &a, const V &b) { V r; for (int l = 0; l < 32; ++l) r.v[l] = a.v[l] < b.v[l] ? a.v[l] : b.v[l]; return r; }
     V cmpgt(const V &a, const V &b) { V r; for (int l = 0; l < 32; ++l) r.v[l] = a.v[l] > b.v[l] ? -1 : 0; return r; }
@@ -86,12 +86,14 @@ template <int W> void run(int kind, const Problem &pr, Out &o)
     HostVec<W> v;
     if (kind == 0) striped_nwsg<HostVec<W>, W>(v, pr, o);
     else if (kind == 1) striped_nwsg_stats<HostVec<W>, W>(v, pr, o);
-    else striped_sw_stats_bias<HostVec<W>, W>(v, pr, o);
+    else if (kind == 2) striped_sw_stats_bias<HostVec<W>, W>(v, pr, o);
+    else striped_sw<HostVec<W>, W>(v, pr, o);
 }
 
 }  // namespace
 
-/* kind: 0 nw/sg score-only, 1 nw/sg statistics, 2 sw statistics (biased);
+/* kind: 0 nw/sg score-only, 1 nw/sg statistics, 2 sw statistics (biased),
+ * 3 sw score-only;
  * sg = {s1_beg, s1_end, s2_beg, s2_end}; out = {score, end_query, end_ref,
  * matches, similar, length, saturated} */
 extern "C" int lane_host_run(int kind, int bits, const int32_t *prof, int size, int lp, const uint8_t *qcodes, int qlen,
@@ -106,6 +108,7 @@ extern "C" int lane_host_run(int kind, int bits, const int32_t *prof, int size, 
     Out o;
     if (bits == 8) run<8>(kind, pr, o);
     else if (bits == 16) run<16>(kind, pr, o);
+    else if (bits == 32 && kind != 2) run<32>(kind, pr, o);
     else return -1;
     out[0] = o.score; out[1] = o.end_query; out[2] = o.end_ref;
     out[3] = o.matches; out[4] = o.similar; out[5] = o.length; out[6] = o.saturated;

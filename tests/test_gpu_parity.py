@@ -141,6 +141,66 @@ def test_vector_forms_vs_live_reference(width):
     assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])
 
 
+def _penalties(rng, width, protein):
+    """open == gap, open < gap, and penalties that wrap in a narrow lane"""
+    c = [(1, 1), (2, 2), (3, 3), (0, 1), (1, 2)]
+    if width in ("8", "sat"):
+        c.append((200, 1) if protein else (130, 2))
+    if width in ("16", "sat"):
+        c.append((40000, 1) if protein else (1, 33000))
+    return rng.choice(c)
+
+
+@pytest.mark.skipif(O.ref() is None, reason="reference library not built")
+@pytest.mark.parametrize("width", ["8", "16", "32", "sat"])
+def test_striped_linear_and_wrapped_penalties_vs_live_reference(width):
+    """Striped kernels where the reference departs from the exact DP (its
+    lazy-F loop stops on ties when open <= gap, and set1 of a penalty above
+    the lane maximum wraps): the direct and profile forms, and batches of
+    both kinds, against the reference's AVX2 kernels. Scan kernels are
+    checked at open == gap, where they follow the exact DP."""
+    rng = random.Random({"8": 18, "16": 116, "32": 132, "sat": 77}[width])
+    bad, total = [], 0
+    for alg_name, stats in (("sw", 0), ("nw", 0), ("sg", 0), ("sg_qx", 0), ("sg_de", 0), ("sg_qb_db", 0),
+                            ("nw", 1), ("sg_qe_db", 1)):
+        st = "_stats" if stats else ""
+        for it in range(6):
+            protein = it % 2 == 1
+            key, a = ("blosum62", AA) if protein else (("ACGT", 2, -3), DNA)
+            m = _pb_matrix(key)
+            op, gp = _penalties(rng, width, protein)
+            q = rand_seq(rng, rng.randint(1, 200), a)
+            targets = [mutate(rng, q, a, 0.2, 0.04) if k % 3 == 0 else rand_seq(rng, rng.randint(1, 220), a)
+                       for k in range(12)]
+            exp = [O.ref_vector(alg_name, stats, "striped", width, q, t, op, gp, key) for t in targets]
+            got = {}
+            got["direct"] = [pb.align("parasail_%s%s_striped_%s" % (alg_name, st, width), q, t, op, gp, m)
+                             for t in targets]
+            prof = pb.ProfileHandle("parasail_profile_create%s_%s" % (st, width), q, m)
+            got["profile"] = [pb.align_profile("parasail_%s%s_striped_profile_%s" % (alg_name, st, width),
+                                               prof, t, op, gp) for t in targets]
+            got["batch"] = pb.records_to_dicts(
+                pb.batch_profile("%s%s_striped_profile_%s" % (alg_name, st, width), prof, targets, op, gp), stats)
+            prof.close()
+            got["pairs"] = pb.records_to_dicts(
+                pb.batch_pairs("%s%s_striped_%s" % (alg_name, st, width), m, [q] * len(targets), targets, op, gp),
+                stats)
+            for form, rs in got.items():
+                for t, r, e in zip(targets, rs, exp):
+                    total += 1
+                    if any(r.get(k) != v for k, v in e.items()):
+                        bad.append((form, alg_name, stats, width, op, gp, q, t, r, e))
+            if op == gp and op < 128:
+                for t in targets[:4]:
+                    total += 1
+                    r = pb.align("parasail_%s%s_scan_%s" % (alg_name, st, width), q, t, op, gp, m)
+                    e = O.ref_vector(alg_name, stats, "scan", width, q, t, op, gp, key)
+                    if any(r.get(k) != v for k, v in e.items()):
+                        bad.append(("scan", alg_name, stats, width, op, gp, q, t, r, e))
+    assert total >= 8 * 6 * 12 * 4
+    assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])
+
+
 def test_nw_banded_vs_oracle():
     rng = random.Random(11)
     dna = pb.matrix_create("ACGT", 2, -3)

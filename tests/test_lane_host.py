@@ -114,3 +114,47 @@ def test_lane_emulation_vs_reference_kernels(lanelib, seed):
                         bad.append((name, bits, stats, key, op, gp, q, t, exp, got))
     assert total > 300 and nsat > 50
     assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_lane_emulation_linear_and_wrapped_penalties(lanelib, seed):
+    """open <= gap (the score-only kernels' lazy-F loop stops on ties there)
+    and penalties that wrap in the lane width, at 8, 16 and 32 bits, for the
+    score-only nw/sg kernels (src/nw_striped_avx2_256_16.c), the statistics
+    nw/sg kernels and the score-only SW kernels (util/templates/
+    sw_striped_bias.c, util/templates/sw_striped.c)."""
+    rng = random.Random(seed)
+    bad, total = [], 0
+    cases = (("sw", 3), ("nw", 0), ("sg", 0), ("sg_qx", 0), ("sg_de", 0), ("sg_qb_db", 0), ("nw", 1),
+             ("sg_qe_db", 1))
+    for it in range(6):
+        for bits in (8, 16, 32):
+            for name, kind in cases:
+                stats = kind == 1
+                if it % 2:
+                    key, a = "blosum62", AA
+                    op, gp = rng.choice([(1, 1), (3, 3), (0, 1), (1, 2), (2, 2), (200, 1), (5, 5)])
+                else:
+                    key, a = ("ACGT", 2, -3), DNA
+                    op, gp = rng.choice([(1, 1), (2, 2), (0, 1), (1, 3), (130, 2), (3, 3)])
+                hi = rng.randint(1, 250)
+                q = rand_seq(rng, rng.randint(1, hi), a)
+                t = mutate(rng, q, a, 0.2, 0.04) if it % 3 == 0 else rand_seq(rng, rng.randint(1, hi), a)
+                m = _matrix(key)
+                sg = [0, 0, 0, 0]
+                if name.startswith("sg"):
+                    f = O.SG_CASES[name]
+                    sg = [int(bool(f & O.S1_BEG)), int(bool(f & O.S1_END)), int(bool(f & O.S2_BEG)),
+                          int(bool(f & O.S2_END))]
+                exp = O.ref_vector(name, stats, "striped", str(bits), q, t, op, gp, key)
+                o = _emulate(lanelib, kind, bits, m, q, t, op, gp, sg)
+                got = {"score": int(o[0]), "end_query": int(o[1]), "end_ref": int(o[2])}
+                if stats:
+                    got.update(matches=int(o[3]), similar=int(o[4]), length=int(o[5]))
+                total += 1
+                e = dict(exp)
+                esat = int(bool(e.pop("flag") & 64))
+                if esat != int(o[6]) or any(got.get(k) != v for k, v in e.items()):
+                    bad.append((name, kind, bits, key, op, gp, q, t, exp, got))
+    assert total == 6 * 3 * len(cases)
+    assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])
