@@ -74,6 +74,20 @@ def dist_init(n):
     return rank, world
 
 
+def over_ranks(world, t_max, n_sum, device):
+    """Every rank's timings reduced by max and its work counts by sum: one
+    all-reduce of each, in the same order on every rank."""
+    if world <= 1:
+        return [float(x) for x in t_max], [float(x) for x in n_sum]
+    import torch
+    import torch.distributed as dist
+    a = torch.tensor([float(x) for x in t_max], dtype=torch.float64, device=device)
+    b = torch.tensor([float(x) for x in n_sum], dtype=torch.float64, device=device)
+    dist.all_reduce(a, op=dist.ReduceOp.MAX)
+    dist.all_reduce(b, op=dist.ReduceOp.SUM)
+    return a.tolist(), b.tolist()
+
+
 def workload(rank, n_targets=N_TARGETS):
     from parasail_b200 import synth
     return synth.protein_db_search(seed=2 + rank, n_targets=n_targets, query_lengths=QUERY_LENGTHS)
@@ -311,22 +325,16 @@ def main():
     stop.set()
     th.join(timeout=2)
 
-    # max over ranks
-    ms_step = total_ms / args.steps
-    e2e_step = e2e_ms / e2e_steps
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms_step, e2e_step], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step, e2e_step = float(t[0]), float(t[1])
+    # times: max over ranks; cells and pairs: sum over ranks (each rank has its own shard)
+    cells = float(sum(len(q) for q in queries)) * float(lens.sum())
+    (ms_step, e2e_step), (cells_all, pairs_all) = over_ranks(
+        world, [total_ms / args.steps, e2e_ms / e2e_steps], [cells, len(queries) * n], "cuda")
     if rank != 0:
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
         return
-    cells = float(sum(len(q) for q in queries)) * float(lens.sum())
-    pairs = len(queries) * n
-    gcups = cells * world / (ms_step * 1e-3) / 1e9
+    gcups = cells_all / (ms_step * 1e-3) / 1e9
     # the device and host paths must agree, and both with the reference
     dev_rec = d_rec.cpu().numpy()
     h_rec = h_rec.reshape(len(queries), n)
@@ -352,8 +360,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int16x2 (int32 rerun past the 16-bit range)", "data": "synthetic",
         "config": config_of(n, world, cells),
-        "pairs_per_s": pairs * world / (ms_step * 1e-3),
-        "e2e": {"value": cells * world / (e2e_step * 1e-3) / 1e9, "unit": "GCUPS",
+        "pairs_per_s": pairs_all / (ms_step * 1e-3),
+        "e2e": {"value": cells_all / (e2e_step * 1e-3) / 1e9, "unit": "GCUPS",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "roofline": {"bound": "int", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s",
