@@ -495,13 +495,13 @@ extern "C" int pb_cuda_band_gradients(const pb_band_model *m, int n, const float
                                       float tau, float *d_gw, float *d_gb, float *loss_out)
 {
     float *h1, *h2, *y, *dy, *d2, *d1, *loss;
-    cudaMalloc(&h1, sizeof(float) * n * pb::MLP_H);
-    cudaMalloc(&h2, sizeof(float) * n * pb::MLP_H);
-    cudaMalloc(&d1, sizeof(float) * n * pb::MLP_H);
-    cudaMalloc(&d2, sizeof(float) * n * pb::MLP_H);
-    cudaMalloc(&y, sizeof(float) * n * pb::MLP_OUT);
-    cudaMalloc(&dy, sizeof(float) * n * pb::MLP_OUT);
-    cudaMalloc(&loss, sizeof(float) * n);
+    cudaMallocAsync((void **)&h1, sizeof(float) * n * pb::MLP_H, 0);
+    cudaMallocAsync((void **)&h2, sizeof(float) * n * pb::MLP_H, 0);
+    cudaMallocAsync((void **)&d1, sizeof(float) * n * pb::MLP_H, 0);
+    cudaMallocAsync((void **)&d2, sizeof(float) * n * pb::MLP_H, 0);
+    cudaMallocAsync((void **)&y, sizeof(float) * n * pb::MLP_OUT, 0);
+    cudaMallocAsync((void **)&dy, sizeof(float) * n * pb::MLP_OUT, 0);
+    cudaMallocAsync((void **)&loss, sizeof(float) * n, 0);
     const pb::MlpWeights w = weights_of(m);
     pb::k_mlp_fwd<<<n, pb::MLP_H>>>(n, d_x, w, h1, h2, y);
     pb::k_mlp_delta<<<n, pb::MLP_H>>>(n, y, d_target, tau, w, h1, h2, dy, d2, d1, loss);
@@ -515,7 +515,7 @@ extern "C" int pb_cuda_band_gradients(const pb_band_model *m, int n, const float
     double tot = 0;
     for (int k = 0; k < n; ++k) tot += hl[k];
     if (loss_out) *loss_out = (float)(tot / n);
-    cudaFree(h1); cudaFree(h2); cudaFree(d1); cudaFree(d2); cudaFree(y); cudaFree(dy); cudaFree(loss);
+    cudaFreeAsync(h1, 0); cudaFreeAsync(h2, 0); cudaFreeAsync(d1, 0); cudaFreeAsync(d2, 0); cudaFreeAsync(y, 0); cudaFreeAsync(dy, 0); cudaFreeAsync(loss, 0);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -553,12 +553,12 @@ extern "C" int pb_cuda_band_certify(int npairs, int a, int open, int ext, const 
 {
     pb::CostModel c = {a, open, ext};
     int *d_fail = nullptr;
-    cudaMalloc(&d_fail, sizeof(int));
+    cudaMallocAsync((void **)&d_fail, sizeof(int), 0);
     cudaMemset(d_fail, 0, sizeof(int));
     pb::k_certify<<<(npairs + 255) / 256, 256>>>(npairs, c, d_qlen, d_tlen, d_lo, d_hi, d_score, d_cert, d_fail);
     pb_diag_count_launch(1);
     cudaMemcpy(h_failures, d_fail, sizeof(int), cudaMemcpyDeviceToHost);
-    cudaFree(d_fail);
+    cudaFreeAsync(d_fail, 0);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -587,17 +587,17 @@ extern "C" int pb_cuda_band_tune(pb_band_model *m, int n, const float *d_x, cons
     float *y = nullptr;
     int *lo = nullptr, *hi = nullptr;
     unsigned long long *cost = nullptr;
-    cudaMalloc(&y, sizeof(float) * n * pb::MLP_OUT);
-    cudaMalloc(&lo, sizeof(int) * n);
-    cudaMalloc(&hi, sizeof(int) * n);
-    cudaMalloc(&cost, sizeof(unsigned long long));
+    cudaMallocAsync((void **)&y, sizeof(float) * n * pb::MLP_OUT, 0);
+    cudaMallocAsync((void **)&lo, sizeof(int) * n, 0);
+    cudaMallocAsync((void **)&hi, sizeof(int) * n, 0);
+    cudaMallocAsync((void **)&cost, sizeof(unsigned long long), 0);
     int rc = pb_cuda_band_forward(m, n, d_x, nullptr, nullptr, y);
     unsigned long long best = ~0ull;
     float bw = m->widen;
     for (unsigned g = 0; rc == 0 && g < sizeof grid / sizeof grid[0]; ++g) {
         unsigned long long c = 0;
         rc = pb_cuda_band_from_pred(n, d_qlen, d_tlen, y, grid[g], m->slack, lo, hi);
-        cudaMemset(cost, 0, sizeof(unsigned long long));
+        cudaMemsetAsync(cost, 0, sizeof(unsigned long long), 0);
         pb::k_tune_cost<<<(n + 127) / 128, 128>>>(n, d_qlen, d_tlen, lo, hi, d_lab_lo, d_lab_hi, cost);
         pb_diag_count_launch(1);
         if (cudaMemcpy(&c, cost, sizeof c, cudaMemcpyDeviceToHost) != cudaSuccess) rc = -1;
@@ -605,7 +605,7 @@ extern "C" int pb_cuda_band_tune(pb_band_model *m, int n, const float *d_x, cons
     }
     if (rc == 0) m->widen = bw;
     if (chosen) *chosen = m->widen;
-    cudaFree(y); cudaFree(lo); cudaFree(hi); cudaFree(cost);
+    cudaFreeAsync(y, 0); cudaFreeAsync(lo, 0); cudaFreeAsync(hi, 0); cudaFreeAsync(cost, 0);
     return rc;
 }
 

@@ -73,14 +73,14 @@ extern "C" int pb_cuda_nw_banded(const pb_device_profile *dp, const uint8_t *h_s
     cudaStream_t st = nullptr;
     uint8_t *d_s2 = nullptr;
     int *d_h = nullptr, *d_e = nullptr, *d_out = nullptr;
-    if (cudaMalloc(&d_s2, s2Len) != cudaSuccess) return -1;
-    if (cudaMalloc(&d_h, sizeof(int) * (colLen + 2)) != cudaSuccess) { cudaFree(d_s2); return -1; }
-    if (cudaMalloc(&d_e, sizeof(int) * (colLen + 2)) != cudaSuccess) { cudaFree(d_s2); cudaFree(d_h); return -1; }
-    if (cudaMalloc(&d_out, sizeof(int)) != cudaSuccess) { cudaFree(d_s2); cudaFree(d_h); cudaFree(d_e); return -1; }
+    if (cudaMallocAsync((void **)&d_s2, s2Len, 0) != cudaSuccess) return -1;
+    if (cudaMallocAsync((void **)&d_h, sizeof(int) * (colLen + 2), 0) != cudaSuccess) { cudaFreeAsync(d_s2, 0); return -1; }
+    if (cudaMallocAsync((void **)&d_e, sizeof(int) * (colLen + 2), 0) != cudaSuccess) { cudaFreeAsync(d_s2, 0); cudaFreeAsync(d_h, 0); return -1; }
+    if (cudaMallocAsync((void **)&d_out, sizeof(int), 0) != cudaSuccess) { cudaFreeAsync(d_s2, 0); cudaFreeAsync(d_h, 0); cudaFreeAsync(d_e, 0); return -1; }
     cudaMemcpyAsync(d_s2, h_s2, s2Len, cudaMemcpyHostToDevice, st);
     k_nw_banded_one<<<1, 1, 0, st>>>(dp->d_prof32, dp->lp, d_s2, s1Len, s2Len, open, gap, k, d_h, d_e, d_out);
     cudaError_t e = cudaMemcpyAsync(score, d_out, sizeof(int), cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
-    cudaFree(d_s2); cudaFree(d_h); cudaFree(d_e); cudaFree(d_out);
+    cudaFreeAsync(d_s2, 0); cudaFreeAsync(d_h, 0); cudaFreeAsync(d_e, 0); cudaFreeAsync(d_out, 0);
     return (e == cudaSuccess && cudaGetLastError() == cudaSuccess) ? 0 : -1;
 }

@@ -39,15 +39,16 @@ namespace pb {
 
 static constexpr int NWL_RL = 8;          /* query rows per lane */
 static constexpr int NWL_WARPS = 8;       /* warps per CTA */
-static constexpr int NWL_CLUSTER = 8;     /* CTAs per cluster for the largest pairs, full DP */
-/* banded: consecutive passes start ~350 columns apart, so a team of T warps
- * only keeps busy on bands of ~350 T columns; smaller clusters suit the band
- * widths of long pairs better */
-static constexpr int NWL_CLUSTER_BANDED = 4;
-/* banded: a team only pays off for the pairs well above a fair share of
- * the work (it idles on bands narrower than ~350 columns per warp) */
-static constexpr int NWL_COOP_SHARE_BANDED = 1;
+/* team classes: class c runs each pair on a cluster of c + 1 CTAs (class 0:
+ * one CTA); one launch per class */
+static constexpr int NWL_CLASSES = 8;
 static constexpr int NWL_NEG = INT32_MIN / 4;
+
+/* How large a team a pair gets (k_team_class). `share`: a pair gets the
+ * smallest team whose warps hold its share of the work (its cells over the
+ * launch's cells per warp, divided by share); `max_class` caps it; `jump`:
+ * every pair above one CTA's share gets the largest team instead. */
+struct TeamPolicy { int max_class; float share; int jump; };
 
 struct NwWaveParams {
     int npairs, open, gap, msize, small_alpha;
@@ -380,7 +381,7 @@ __global__ void k_iota_nw(int *v, int n)
 }
 
 /* sort key: the pair's work (cells, or for a band its rows x the columns
- * its passes sweep); the total goes to *total for k_coop_flag */
+ * its passes sweep); the total goes to *total for k_team_class */
 __global__ void k_cells(const int *ql, const int *tl, const int *lo, const int *hi, int n,
                         unsigned long long *keys, unsigned long long *total)
 {
@@ -397,25 +398,38 @@ __global__ void k_cells(const int *ql, const int *tl, const int *lo, const int *
     if ((threadIdx.x & 31) == 0 && k) atomicAdd(total, k);
 }
 
-/* NWL_COOP_BIT for the pairs a whole cluster should run: those whose work
- * is above `share` fair shares of the total per CTA (left to one CTA, they
- * would finish last), that give every warp of the team a pass, and, banded, whose
- * band is at least 1024 diagonals wide. (A banded pass starts about 350
- * columns after the one above it, the band moving with the rows, so a team
- * of T warps is only fully busy on bands of about 350 T columns; below that
- * the team still finishes a large pair sooner than one CTA would.) */
-__global__ void k_coop_flag(const int *ql, const int *lo, const int *hi, int n, int nctas, int coop_pass,
-                            int share, const unsigned long long *total, unsigned long long *keys, int *ncoop)
+/*
+ * The team class of every pair, in the key's bits 59-61 (and NWL_COOP_BIT
+ * for classes >= 1), counted per class. A team of T warps is busy only
+ * while T passes are in flight: a pass takes (its columns + 31) iterations
+ * and the next one starts about (256 + 94) columns later when banded (the
+ * band moves 256 columns per pass), 94 otherwise, so a pair keeps at most
+ * kappa = (columns + 31) / lag warps busy. The team is the smallest number
+ * of CTAs that holds the pair's share of the warps, or kappa if that is
+ * smaller, and every warp of the team gets a pass.
+ */
+__global__ void k_team_class(const int *ql, const int *tl, const int *lo, const int *hi, int n, int nwarps,
+                             TeamPolicy pol, const unsigned long long *total, unsigned long long *keys,
+                             int *count)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const int npass = (ql[i] + 32 * NWL_RL - 1) / (32 * NWL_RL);
     const unsigned long long k = keys[i];
-    if (npass >= coop_pass && (!lo || hi[i] - lo[i] >= 1024) &&
-        k * (unsigned long long)nctas > (unsigned long long)share * *total) {
-        keys[i] = k | NWL_COOP_BIT;
-        atomicAdd(ncoop, 1);
+    const int npass = (ql[i] + 32 * NWL_RL - 1) / (32 * NWL_RL);
+    const long long m = tl[i];
+    const bool narrow = lo && (long long)hi[i] - lo[i] + 32 * NWL_RL < m;
+    const double cols = narrow ? (double)((long long)hi[i] - lo[i] + 32 * NWL_RL) : (double)m;
+    const double kappa = (cols + 31.0) / (narrow ? 32.0 * NWL_RL + 94.0 : 94.0);
+    const double share = (double)k * nwarps / ((double)*total * pol.share);
+    int c = 0;
+    if (pol.jump) {
+        if (share > NWL_WARPS && npass >= NWL_WARPS * (pol.max_class + 1)) c = pol.max_class;
+    } else {
+        const double want = share < kappa ? share : kappa;
+        while (c < pol.max_class && NWL_WARPS * (c + 1) < want && npass >= NWL_WARPS * (c + 2)) ++c;
     }
+    keys[i] = k | (c ? NWL_COOP_BIT | ((unsigned long long)c << 59) : 0ull);
+    atomicAdd(&count[c], 1);
 }
 
 }  // namespace pb
@@ -456,71 +470,92 @@ static int nw_long_impl(int npairs, int open, int gap, const int32_t *h_mat, int
              : (ge ? pb::k_nw_wave<false, true> : pb::k_nw_wave<false, false>);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, pb::NWL_WARPS * 32, 0);
     if (per_sm < 1) per_sm = 1;
-    /* clusters of NWL_CLUSTER CTAs run the largest pairs as one team */
-    int C = d_lo ? pb::NWL_CLUSTER_BANDED : pb::NWL_CLUSTER, nclusters = 0;
+    const int plain_max = per_sm * nsm;
+    /* the largest cluster class the device runs, and how many clusters of
+     * each class fit at once */
+    /* full DP: kappa is in the hundreds, the largest pairs take 8-CTA teams;
+     * banded: teams as large as the pair's share, bounded by what its band
+     * keeps busy */
+    pb::TeamPolicy pol = d_lo ? pb::TeamPolicy{7, 1.0f, 0} : pb::TeamPolicy{7, 1.0f, 1};
+    int maxclusters[pb::NWL_CLASSES] = {plain_max, 0, 0, 0, 0, 0, 0, 0};
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = C;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    cfg.gridDim = dim3(C * nsm);
     cfg.blockDim = dim3(pb::NWL_WARPS * 32);
     cfg.dynamicSmemBytes = 0;
-    cfg.stream = st;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (cudaOccupancyMaxActiveClusters(&nclusters, (const void *)kern, &cfg) != cudaSuccess || nclusters < 1) {
-        cudaGetLastError();
-        C = 1;
+    for (int c = 1; c <= pol.max_class; ++c) {
+        attr[0].val.clusterDim.x = c + 1;
+        cfg.gridDim = dim3((c + 1) * nsm);
+        if (cudaOccupancyMaxActiveClusters(&maxclusters[c], (const void *)kern, &cfg) != cudaSuccess ||
+            maxclusters[c] < 1) {
+            cudaGetLastError();
+            pol.max_class = c - 1;
+            break;
+        }
     }
-    const int plain_max = per_sm * nsm;
     cudaMallocAsync((void **)&d_mat, hm.size(), st);
     cudaMemcpyAsync(d_mat, hm.data(), hm.size(), cudaMemcpyHostToDevice, st);
     cudaMallocAsync((void **)&idx, sizeof(int) * npairs, st);
     cudaMallocAsync((void **)&order, sizeof(int) * npairs, st);
     cudaMallocAsync((void **)&keys, sizeof(unsigned long long) * npairs, st);
     cudaMallocAsync((void **)&keys_sorted, sizeof(unsigned long long) * npairs, st);
-    cudaMallocAsync((void **)&counter, sizeof(int) * 8, st);
-    cudaMemsetAsync(counter, 0, sizeof(int) * 8, st);
-    /* counter[0], [1]: pair counters of the two launches; [2..3]: total
-     * work; [4]: cooperative pairs */
-    unsigned long long *total = reinterpret_cast<unsigned long long *>(counter + 2);
+    cudaMallocAsync((void **)&counter, sizeof(int) * 32, st);
+    cudaMemsetAsync(counter, 0, sizeof(int) * 32, st);
+    /* counter[0..7]: pair counters of the class launches; [8..9]: total
+     * work; [16..23]: pairs per class */
+    unsigned long long *total = reinterpret_cast<unsigned long long *>(counter + 8);
     pb::k_iota_nw<<<(npairs + 255) / 256, 256, 0, st>>>(idx, npairs);
     pb::k_cells<<<(npairs + 255) / 256, 256, 0, st>>>(d_qlen, d_tlen, d_lo, d_hi, npairs, keys, total);
-    if (C > 1)
-        pb::k_coop_flag<<<(npairs + 255) / 256, 256, 0, st>>>(d_qlen, d_lo, d_hi, npairs, plain_max,
-                                                              C * pb::NWL_WARPS,
-                                                              d_lo ? pb::NWL_COOP_SHARE_BANDED : 1, total, keys,
-                                                              counter + 4);
+    pb::k_team_class<<<(npairs + 255) / 256, 256, 0, st>>>(d_qlen, d_tlen, d_lo, d_hi, npairs,
+                                                           plain_max * pb::NWL_WARPS, pol, total, keys,
+                                                           counter + 16);
+    pb_diag_count_launch(3);
     cub::DeviceRadixSort::SortPairsDescending(nullptr, tmpb, keys, keys_sorted, idx, order, npairs, 0, 64, st);
     cudaMallocAsync(&tmp, tmpb, st);
     cub::DeviceRadixSort::SortPairsDescending(tmp, tmpb, keys, keys_sorted, idx, order, npairs, 0, 64, st);
-    /* the cooperative pairs (sorted first) go to a cluster launch, the rest
-     * to a plain launch on a second stream; the two never wait on each other */
-    int ncoop = 0;
-    cudaMemcpyAsync(&ncoop, counter + 4, sizeof(int), cudaMemcpyDeviceToHost, st);
+    /* pairs sorted by class, largest first; one launch per class, each on
+     * its own stream, the largest teams first; they never wait on each other */
+    int ncls[pb::NWL_CLASSES] = {0, 0, 0, 0, 0, 0, 0, 0};
+    cudaMemcpyAsync(ncls, counter + 16, sizeof ncls, cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
-    const int cblocks = ncoop > 0 ? (ncoop < nclusters ? ncoop : nclusters) * C : 0;
-    const int pblocks = npairs - ncoop < plain_max ? npairs - ncoop : plain_max;
-    const int blocks = cblocks + pblocks;
+    /* CTAs beyond what is resident only wait for a slot: the launches
+     * together get at most twice the resident CTAs (each at least one
+     * team), which bounds the ring buffers */
+    int cblocks[pb::NWL_CLASSES], first[pb::NWL_CLASSES], blocks = 0, before = 0;
+    for (int c = pb::NWL_CLASSES - 1; c >= 0; --c) {
+        const int C = c + 1;
+        int nc = ncls[c] < maxclusters[c] ? ncls[c] : maxclusters[c];
+        const int room = (2 * plain_max - blocks) / C;
+        if (nc > room) nc = room > 1 ? room : 1;
+        cblocks[c] = ncls[c] > 0 ? nc * C : 0;
+        first[c] = before;
+        before += ncls[c];
+        blocks += cblocks[c];
+    }
     int2 *scratch = nullptr;
     long long *prog = nullptr;
     int *d_err = nullptr;
     int rc = 0, herr = 0;
-    cudaStream_t st2 = nullptr;
-    cudaEvent_t ev = nullptr;
+    cudaStream_t sc[pb::NWL_CLASSES] = {};
+    cudaEvent_t ev = nullptr, evc[pb::NWL_CLASSES] = {};
     cudaMallocAsync((void **)&d_err, sizeof(int), st);
     cudaMemsetAsync(d_err, 0, sizeof(int), st);
     if (cudaMallocAsync((void **)&scratch, sizeof(int2) * (size_t)(maxlen + 1) * blocks * pb::NWL_WARPS, st) != cudaSuccess ||
         cudaMallocAsync((void **)&prog, sizeof(long long) * (size_t)blocks * pb::NWL_WARPS, st) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
         rc = -1;
+    for (int c = 0; c < pb::NWL_CLASSES && rc == 0; ++c)
+        if (cblocks[c] > 0 &&
+            (cudaStreamCreateWithFlags(&sc[c], cudaStreamNonBlocking) != cudaSuccess ||
+             cudaEventCreateWithFlags(&evc[c], cudaEventDisableTiming) != cudaSuccess))
+            rc = -1;
     if (rc == 0) {
         cudaMemsetAsync(prog, 0, sizeof(long long) * (size_t)blocks * pb::NWL_WARPS, st);
         cudaEventRecord(ev, st);
-        cudaStreamWaitEvent(st2, ev, 0);
         pb::NwWaveParams p;
         p.open = open; p.gap = gap; p.msize = msize; p.small_alpha = small;
         p.mat = d_mat; p.q = d_q; p.qoff = d_qoff; p.qlen = d_qlen;
@@ -529,26 +564,30 @@ static int nw_long_impl(int npairs, int open, int gap, const int32_t *h_mat, int
         p.cert = d_lo && d_rounds ? 1 : 0;
         p.cm.a = cert_a; p.cm.open = open; p.cm.ext = gap;
         p.lo_out = d_lo_out; p.hi_out = d_hi_out; p.rounds = d_rounds;
-        if (cblocks > 0) {
+        size_t slot = 0;
+        int nlaunch = 0;
+        for (int c = pb::NWL_CLASSES - 1; c >= 0; --c) {
+            if (cblocks[c] <= 0) continue;
+            cudaStreamWaitEvent(sc[c], ev, 0);
             pb::NwWaveParams pc = p;
-            pc.npairs = ncoop; pc.order = order; pc.keys = keys_sorted;
-            pc.scratch = scratch; pc.prog = prog;
-            cfg.gridDim = dim3(cblocks);
-            if (cudaLaunchKernelEx(&cfg, kern, pc, counter, d_err) != cudaSuccess) rc = -1;
-            pb_diag_count_launch(1);
+            pc.npairs = ncls[c]; pc.order = order + first[c]; pc.keys = keys_sorted + first[c];
+            pc.scratch = scratch + slot * p.maxlen;
+            pc.prog = prog + slot;
+            slot += (size_t)cblocks[c] * pb::NWL_WARPS;
+            if (c > 0) {
+                attr[0].val.clusterDim.x = c + 1;
+                cfg.gridDim = dim3(cblocks[c]);
+                cfg.stream = sc[c];
+                if (cudaLaunchKernelEx(&cfg, kern, pc, counter + c, d_err) != cudaSuccess) rc = -1;
+            } else {
+                kern<<<cblocks[c], pb::NWL_WARPS * 32, 0, sc[c]>>>(pc, counter + c, d_err);
+            }
+            ++nlaunch;
+            cudaEventRecord(evc[c], sc[c]);
+            cudaStreamWaitEvent(st, evc[c], 0);
         }
-        if (pblocks > 0) {
-            pb::NwWaveParams pp = p;
-            pp.npairs = npairs - ncoop; pp.order = order + ncoop; pp.keys = keys_sorted + ncoop;
-            pp.scratch = scratch + (size_t)cblocks * pb::NWL_WARPS * p.maxlen;
-            pp.prog = prog + (size_t)cblocks * pb::NWL_WARPS;
-            kern<<<pblocks, pb::NWL_WARPS * 32, 0, st2>>>(pp, counter + 1, d_err);
-            pb_diag_count_launch(1);
-        }
+        pb_diag_count_launch(nlaunch);
         if (cudaGetLastError() != cudaSuccess) rc = -1;
-        pb_diag_count_launch(C > 1 ? 3 : 2);   /* k_iota_nw, k_cells, k_coop_flag */
-        cudaEventRecord(ev, st2);
-        cudaStreamWaitEvent(st, ev, 0);
         cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
     }
     cudaFreeAsync(d_mat, st); cudaFreeAsync(idx, st); cudaFreeAsync(order, st);
@@ -558,7 +597,10 @@ static int nw_long_impl(int npairs, int open, int gap, const int32_t *h_mat, int
     if (prog) cudaFreeAsync(prog, st);
     cudaFreeAsync(d_err, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
-    if (st2) cudaStreamDestroy(st2);
+    for (int c = 0; c < pb::NWL_CLASSES; ++c) {
+        if (sc[c]) cudaStreamDestroy(sc[c]);
+        if (evc[c]) cudaEventDestroy(evc[c]);
+    }
     if (ev) cudaEventDestroy(ev);
     if (herr) {
         fprintf(stderr, "pb_cuda_nw_long: a pipeline wait exceeded its bound; pair abandoned\n");
