@@ -85,6 +85,35 @@ def test_banded_vs_oracle_and_certificate_soundness():
     assert 0 < ncert < len(qs)
 
 
+def test_banded_pass_edges_vs_oracle():
+    """Banded pairs whose lengths sit at the 256-row pass and 8-row lane
+    boundaries, with narrow and wide bands, for open > gap, open < gap (the
+    kernel's general F recurrence) and a protein matrix (scores from the
+    shared-memory table rather than the byte permute)."""
+    rng = random.Random(5)
+    dna = pb.matrix_create("ACGT", 1, -2)
+    om = O.Matrix.simple("ACGT", 1, -2)
+    b62 = pb.matrix_lookup("blosum62")
+    ob = O.Matrix.from_struct(b62)
+    lens = [255, 256, 257, 263, 264, 511, 512, 513, 520, 767, 768, 769]
+    for mat, omat, alpha, op, gp in ((dna, om, DNA, OPEN, GAP), (dna, om, DNA, 1, 3), (b62, ob, AA, 11, 1)):
+        qs, ts, lo, hi = [], [], [], []
+        for L in lens:
+            for w in (0, 5, 40, 400):
+                q = rand_seq(rng, L, alpha)
+                t = mutate(rng, q, alpha, 0.06, 0.02) if rng.random() < 0.7 else \
+                    rand_seq(rng, L + rng.randint(-30, 30), alpha)
+                d_end = len(q) - len(t)
+                c = d_end // 2 + rng.randint(-5, 5)
+                qs.append(q)
+                ts.append(t)
+                lo.append(min(c - w, min(0, d_end)))
+                hi.append(max(c + w, max(0, d_end)))
+        sc, _ = pb.nw_banded_certified(mat, *_pack(qs), *_pack(ts), op, gp, lo, hi)
+        for k, (q, t) in enumerate(zip(qs, ts)):
+            assert sc[k] == O.nw_band(q, t, op, gp, lo[k], hi[k], omat), (k, len(q), len(t), lo[k], hi[k], op, gp)
+
+
 def _bf16(x):
     u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
     u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
