@@ -228,25 +228,29 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
             int tc_n1 = res_at(jlo - lane), tc_n2 = res_at(jlo - lane + 1);
             /* the previous pass's bottom row, one 32-column chunk per
              * register (lane l holds column chunk start + l; lane 0 takes its
-             * column by shuffle), loaded one chunk ahead so that the L2
-             * latency is off the column loop. A chunk is read only after the
-             * previous pass has published the next one. */
+             * column by shuffle), loaded when the chunk starts, as soon as the
+             * previous pass has published it. Loading a chunk ahead would hide
+             * one L2 latency per 32 columns, but it makes each pass wait for
+             * its predecessor to be 32 columns further along; a banded pair's
+             * passes then start about 350 instead of 318 columns apart, and
+             * the largest pairs, which keep only (band + 287) / lag warps
+             * busy, take longer: 0.089 vs 0.080 s for the 300-pair
+             * learned-band call. */
             auto ring_at = [&](int c) -> int2 {
                 return (pass > 0 && c >= prev_jlo && c <= prev_jhi) ? __ldcg(&in_buf[c])
                                                                       : make_int2(NWL_NEG, NWL_NEG);
             };
-            int2 cur_v = make_int2(NWL_NEG, NWL_NEG), nxt_v = cur_v;
+            int2 cur_v = make_int2(NWL_NEG, NWL_NEG);
             bool aborted = false;
             for (int it = jlo; it <= tend; ++it) {
                 const int j = it - lane;
                 const int cpos = (it - jlo) & 31;
                 if (cpos == 0) {
                     bool ok = true;
-                    if (lane == 0) ok = wait_for(it + 63);
+                    if (lane == 0) ok = wait_for(it + 31);
                     ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0);
                     if (!ok) { aborted = true; break; }
-                    cur_v = it == jlo ? ring_at(it + lane) : nxt_v;
-                    nxt_v = ring_at(it + 32 + lane);
+                    cur_v = ring_at(it + lane);
                 }
                 const int vh = __shfl_sync(0xffffffffu, cur_v.x, cpos);
                 const int vf = __shfl_sync(0xffffffffu, cur_v.y, cpos);
@@ -402,8 +406,9 @@ __global__ void k_cells(const int *ql, const int *tl, const int *lo, const int *
  * The team class of every pair, in the key's bits 59-61 (and NWL_COOP_BIT
  * for classes >= 1), counted per class. A team of T warps is busy only
  * while T passes are in flight: a pass takes (its columns + 31) iterations
- * and the next one starts about (256 + 94) columns later when banded (the
- * band moves 256 columns per pass), 94 otherwise, so a pair keeps at most
+ * and the next one starts at most (256 + 94) columns later when banded (the
+ * band moves 256 columns per pass; 31 of lane skew and up to 63 of the
+ * 32-column hand-off), 94 otherwise, so a pair keeps at least
  * kappa = (columns + 31) / lag warps busy. The team is the smallest number
  * of CTAs that holds the pair's share of the warps, or kappa if that is
  * smaller, and every warp of the team gets a pass.
@@ -475,8 +480,10 @@ static int nw_long_impl(int npairs, int open, int gap, const int32_t *h_mat, int
      * each class fit at once */
     /* full DP: kappa is in the hundreds, the largest pairs take 8-CTA teams;
      * banded: teams as large as the pair's share, bounded by what its band
-     * keeps busy */
-    pb::TeamPolicy pol = d_lo ? pb::TeamPolicy{7, 1.0f, 0} : pb::TeamPolicy{7, 1.0f, 1};
+     * keeps busy, and by 4 CTAs (larger teams leave fewer slots to the other
+     * pairs than they gain: 0.064 vs 0.073 s for 300 long pairs on their
+     * certified bands) */
+    pb::TeamPolicy pol = d_lo ? pb::TeamPolicy{3, 1.0f, 0} : pb::TeamPolicy{7, 1.0f, 1};
     int maxclusters[pb::NWL_CLASSES] = {plain_max, 0, 0, 0, 0, 0, 0, 0};
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
