@@ -132,7 +132,9 @@ extern int parasail_b200_nw_long(
 
 /** The learned-band model: a 258 -> 128 -> 128 -> 2 MLP (ReLU, BF16 weights,
  * FP32 accumulation) mapping a pair's k = 8 diagonal-offset histogram (256
- * bins) and both lengths to a band centre and half-width. */
+ * bins) and both lengths to a band centre and half-width. Bands are placed
+ * at the certificate's own centre, (n - m) / 2 diagonals, with the predicted
+ * half-width; the centre output is trained but not used for them. */
 typedef struct parasail_b200_band_model parasail_b200_band_model_t;
 
 typedef struct parasail_b200_band_stats {
