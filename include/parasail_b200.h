@@ -167,8 +167,10 @@ extern int parasail_b200_band_model_gradients(
  * each pair's optimal score from the full-DP kernel. The last tenth of the
  * pairs (when n >= 20) is held out of the gradient steps and then chooses
  * the band scaling: the widen factor (of 1.0 ... 3.0) with the least
- * expected DP work, band cells plus a full DP for every pair whose band
- * would fail the certificate. */
+ * expected DP work, the band cells of every held-out pair plus, for each
+ * pair whose band would fail the certificate, six times the cells of the
+ * rerun band (its band joined with its label band; a rerun lengthens its
+ * pair's latency, which bounds the launch). */
 extern int parasail_b200_band_model_train(
         parasail_b200_band_model_t *model, const parasail_matrix_t *matrix,
         const char *queries, const int64_t *qoffsets, const int *qlengths,
@@ -177,7 +179,8 @@ extern int parasail_b200_band_model_train(
 /** The band scaling chosen at training (widen factor, slack diagonals). */
 extern void parasail_b200_band_model_scaling(const parasail_b200_band_model_t *model, float *widen, int *slack);
 /** Global alignment scores through the learned band: predicted band
- * (half-width scaled by `widen`, plus `slack` diagonals; widen <= 0 and
+ * (centred on (n - m) / 2 diagonals, predicted half-width scaled by
+ * `widen`, plus `slack` diagonals; widen <= 0 and
  * slack < 0 take the scaling chosen at training), banded DP with the
  * exactness certificate checked inside the launch. A pair whose band fails
  * it reruns at once, in the same launch, on its band widened by the label
