@@ -529,15 +529,28 @@ static int nw_long_impl(int npairs, int open, int gap, const int32_t *h_mat, int
     int ncls[pb::NWL_CLASSES] = {0, 0, 0, 0, 0, 0, 0, 0};
     cudaMemcpyAsync(ncls, counter + 16, sizeof ncls, cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
-    /* CTAs beyond what is resident only wait for a slot: the launches
-     * together get at most twice the resident CTAs (each at least one
-     * team), which bounds the ring buffers */
+    /* Each launch gets as many teams as fit at once (or as it has pairs);
+     * CTAs beyond what is resident only wait for a slot. If the launches
+     * together exceed four times the resident CTAs, all are scaled down by
+     * the same factor (each keeps at least one team), which bounds the ring
+     * buffers without leaving any launch a handful of teams for many pairs
+     * (a budget taken largest team first did that: one launch of many
+     * pairs then ran on a single cluster). */
     int cblocks[pb::NWL_CLASSES], first[pb::NWL_CLASSES], blocks = 0, before = 0;
+    long long want = 0;
+    for (int c = pb::NWL_CLASSES - 1; c >= 0; --c) {
+        const int nc = ncls[c] < maxclusters[c] ? ncls[c] : maxclusters[c];
+        cblocks[c] = nc * (c + 1);
+        want += cblocks[c];
+    }
+    const long long cap = 4LL * plain_max;
     for (int c = pb::NWL_CLASSES - 1; c >= 0; --c) {
         const int C = c + 1;
-        int nc = ncls[c] < maxclusters[c] ? ncls[c] : maxclusters[c];
-        const int room = (2 * plain_max - blocks) / C;
-        if (nc > room) nc = room > 1 ? room : 1;
+        int nc = cblocks[c] / C;
+        if (want > cap && nc > 0) {
+            nc = (int)((long long)nc * cap / want);
+            if (nc < 1) nc = 1;
+        }
         cblocks[c] = ncls[c] > 0 ? nc * C : 0;
         first[c] = before;
         before += ncls[c];
