@@ -5,6 +5,7 @@
  * stats, striped/scan, width or the _sat chain), validates the arguments with
  * the reference's checks, and runs the device pipeline of pb_batch.cu.
  */
+#include <stddef.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -71,17 +72,18 @@ static void mapper_bytes(const parasail_matrix_t *m, uint8_t *out)
     for (c = 0; c < 256; ++c) out[c] = (uint8_t)m->mapper[c];
 }
 
-static void copy_records(const pb_record *in, parasail_b200_record_t *out, int n)
-{
-    int i;
-    for (i = 0; i < n; ++i) {
-        out[i].score = in[i].score; out[i].end_query = in[i].end_query;
-        out[i].end_ref = in[i].end_ref; out[i].flag = in[i].flag;
-        out[i].matches = in[i].matches; out[i].similar = in[i].similar;
-        out[i].length = in[i].length; out[i].reserved = 0;
-        if (in[i].ambig) pb_ambiguous_count += in[i].ambig;
-    }
-}
+/* The device writes records in the public layout (the resolution leaves
+ * the last field, reserved, at 0), so results are copied straight into the
+ * caller's array. */
+_Static_assert(sizeof(pb_record) == sizeof(parasail_b200_record_t), "record layout");
+_Static_assert(offsetof(pb_record, score) == offsetof(parasail_b200_record_t, score), "record layout");
+_Static_assert(offsetof(pb_record, end_query) == offsetof(parasail_b200_record_t, end_query), "record layout");
+_Static_assert(offsetof(pb_record, end_ref) == offsetof(parasail_b200_record_t, end_ref), "record layout");
+_Static_assert(offsetof(pb_record, flag) == offsetof(parasail_b200_record_t, flag), "record layout");
+_Static_assert(offsetof(pb_record, matches) == offsetof(parasail_b200_record_t, matches), "record layout");
+_Static_assert(offsetof(pb_record, similar) == offsetof(parasail_b200_record_t, similar), "record layout");
+_Static_assert(offsetof(pb_record, length) == offsetof(parasail_b200_record_t, length), "record layout");
+_Static_assert(offsetof(pb_record, ambig) == offsetof(parasail_b200_record_t, reserved), "record layout");
 
 static int check_common(const char *func, const parasail_profile_t *profile, int n, int open, int gap)
 {
@@ -102,7 +104,6 @@ int parasail_b200_batch_profile(const char *funcname, const parasail_profile_t *
     pb_batch b;
     const pb_device_profile *profs[1];
     uint8_t map[256];
-    pb_record *tmp;
     int i, rc;
     if (check_common(__func__, profile, n, open, gap) != 0) return -1;
     if (n == 0) return 0;
@@ -119,12 +120,8 @@ int parasail_b200_batch_profile(const char *funcname, const parasail_profile_t *
     b.alg = job.mode.alg; b.sgflags = job.mode.sgflags; b.stats = job.mode.stats;
     b.open = open; b.gap = gap; b.profs = profs; b.nprofs = 1; b.npairs = n;
     mapper_bytes(profile->matrix, map);
-    tmp = (pb_record *)malloc(sizeof(pb_record) * (size_t)n);
-    if (!tmp) return -1;
-    rc = pb_cuda_batch_host(&job, &b, map, targets, offsets, lengths, NULL, NULL, NULL, n, tmp);
-    if (rc == 0) copy_records(tmp, records, n);
-    else fprintf(stderr, "%s: GPU alignment failed: %s\n", __func__, pb_cuda_last_error());
-    free(tmp);
+    rc = pb_cuda_batch_host(&job, &b, map, targets, offsets, lengths, NULL, NULL, NULL, n, (pb_record *)records);
+    if (rc != 0) fprintf(stderr, "%s: GPU alignment failed: %s\n", __func__, pb_cuda_last_error());
     return rc;
 }
 
@@ -204,7 +201,6 @@ int parasail_b200_batch_pairs(const char *funcname, const parasail_matrix_t *mat
     pb_job job;
     pb_batch b;
     uint8_t map[256];
-    pb_record *tmp;
     int32_t *d_mat = NULL;
     int i, rc;
     if (!matrix) { fprintf(stderr, "%s: missing %s\n", __func__, "matrix"); return -1; }
@@ -238,12 +234,9 @@ int parasail_b200_batch_pairs(const char *funcname, const parasail_matrix_t *mat
     b.open = open; b.gap = gap; b.nprofs = 0; b.npairs = n;
     b.d_mat = d_mat; b.msize = matrix->size; b.mmax = matrix->max; b.mmin = matrix->min;
     mapper_bytes(matrix, map);
-    tmp = (pb_record *)malloc(sizeof(pb_record) * (size_t)n);
-    if (!tmp) { pb_cuda_free(d_mat); return -1; }
-    rc = pb_cuda_batch_host(&job, &b, map, targets, toffsets, tlengths, queries, qoffsets, qlengths, n, tmp);
-    if (rc == 0) copy_records(tmp, records, n);
-    else fprintf(stderr, "%s: GPU alignment failed: %s\n", __func__, pb_cuda_last_error());
-    free(tmp);
+    rc = pb_cuda_batch_host(&job, &b, map, targets, toffsets, tlengths, queries, qoffsets, qlengths, n,
+                            (pb_record *)records);
+    if (rc != 0) fprintf(stderr, "%s: GPU alignment failed: %s\n", __func__, pb_cuda_last_error());
     pb_cuda_free(d_mat);
     pb_cuda_sync();
     return rc;
@@ -279,7 +272,6 @@ int parasail_b200_batch_db(const char *funcname, const parasail_profile_t *const
     pb_batch b;
     const pb_device_profile **profs;
     uint8_t map[256];
-    pb_record *tmp;
     int i, rc;
     if (n == 0) return 0;
     if (!targets || !offsets || !lengths || !records) { fprintf(stderr, "%s: missing arrays\n", __func__); return -1; }
@@ -292,12 +284,8 @@ int parasail_b200_batch_db(const char *funcname, const parasail_profile_t *const
     b.alg = job.mode.alg; b.sgflags = job.mode.sgflags; b.stats = job.mode.stats;
     b.open = open; b.gap = gap; b.profs = profs; b.nprofs = nq; b.npairs = n;
     mapper_bytes(profiles[0]->matrix, map);
-    tmp = (pb_record *)malloc(sizeof(pb_record) * (size_t)n * nq);
-    if (!tmp) { free(profs); return -1; }
-    rc = pb_cuda_batch_host(&job, &b, map, targets, offsets, lengths, NULL, NULL, NULL, n, tmp);
-    if (rc == 0) copy_records(tmp, records, n * nq);
-    else fprintf(stderr, "%s: GPU alignment failed: %s\n", __func__, pb_cuda_last_error());
-    free(tmp);
+    rc = pb_cuda_batch_host(&job, &b, map, targets, offsets, lengths, NULL, NULL, NULL, n, (pb_record *)records);
+    if (rc != 0) fprintf(stderr, "%s: GPU alignment failed: %s\n", __func__, pb_cuda_last_error());
     free(profs);
     return rc;
 }

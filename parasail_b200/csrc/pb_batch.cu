@@ -47,10 +47,13 @@ __global__ void k_resolve(pb_job job, const pb_pair_out *__restrict__ o1,
     if (o2) b = o2[i];
     pb_lane_res x[3];
     lane_views(e, i, x);
-    const pb_record r = pb_chain_resolve(&job, &a, o2 ? &b : nullptr, qlen ? qlen[i] : qlen_all, tlen[i],
-                                         &x[0], &x[1], &x[2]);
-    rec[i] = r;
+    pb_record r = pb_chain_resolve(&job, &a, o2 ? &b : nullptr, qlen ? qlen[i] : qlen_all, tlen[i],
+                                   &x[0], &x[1], &x[2]);
     const int t = r.ambig == 8 ? 0 : r.ambig == 16 ? 1 : r.ambig == 32 ? 2 : -1;
+    /* a finished record goes out as the public record, whose last field
+     * (here the fallback note) is reserved and 0 */
+    if (t < 0) r.ambig = 0;
+    rec[i] = r;
     if (t >= 0) need[(size_t)t * n_all + atomicAdd(&counts[t], 1)] = i;
 }
 

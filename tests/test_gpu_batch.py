@@ -136,3 +136,24 @@ def test_db_batch_matches_single_query_batches():
         assert [(int(r["score"]), int(r["end_query"]), int(r["end_ref"])) for r in one] == [e[:3] for e in exp]
     for p in profs:
         p.close()
+
+
+def test_records_reserved_field_is_zero_and_host_equals_single_calls():
+    """The host batch calls copy the device's records straight into the
+    caller's array: the reserved field is 0, and every other field equals
+    the single-call result, across the 8 -> 16 -> 32 chain with statistics
+    and pairs near the saturation bounds."""
+    rng = random.Random(41)
+    dna = pb.matrix_create("ACGT", 2, -3)
+    for name, creator, st in (("nw_stats_striped_profile_sat", "parasail_profile_create_stats_sat", 1),
+                              ("sg_qx_striped_profile_sat", "parasail_profile_create_sat", 0),
+                              ("sw_striped_profile_sat", "parasail_profile_create_sat", 0)):
+        q = rand_seq(rng, 180, DNA)
+        targets = [mutate(rng, q, DNA, 0.02, 0.01) if k % 2 else rand_seq(rng, rng.randint(20, 400), DNA)
+                   for k in range(120)]
+        prof = pb.ProfileHandle(creator, q, dna)
+        recs = pb.batch_profile(name, prof, targets, 5, 2)
+        assert (recs["reserved"] == 0).all()
+        for t, r in zip(targets, pb.records_to_dicts(recs, st)):
+            assert r == pb.align_profile("parasail_" + name, prof, t, 5, 2), (name, t)
+        prof.close()
