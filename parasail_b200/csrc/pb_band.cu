@@ -11,9 +11,12 @@
  *                    (where the certificate centres every label band), of
  *                    the predicted half-width; it always contains the start
  *                    and end diagonals
- *   4. banded global DP (pb_nwlong.cu)
- *   5. k_certify     exactness certificate; pairs that fail rerun on the
- *                    full DP, which is the fallback and the judge
+ *   4. banded global DP (pb_nwlong.cu) with the exactness certificate
+ *                    checked in the launch: a pair that fails it reruns at
+ *                    once on its band joined with the label band of its own
+ *                    banded cost, which always passes
+ *   5. k_certify     the certificate on its own, for caller-given bands
+ *                    (parasail_b200_nw_banded_certified)
  *
  * Certificate. With a = the matrix's largest score, any global alignment
  * of lengths n (query) and m (target) has cost C = a(n+m)/2 - score, a sum
