@@ -204,18 +204,25 @@ extern "C" int pb_cuda_batch_run(const pb_job *job, const pb_batch *tmpl, pb_rec
         b.d_qlim = nullptr;
         b.d_tlim = nullptr;
         rc = pb_cuda_align_sw16_multi(&b, o1);
+    } else if (tmpl->nprofs >= 1) {
+        /* every query against every target in one launch */
+        pb_batch b = *tmpl;
+        b.d_out = o1;
+        b.d_qlim = nullptr;
+        b.d_tlim = nullptr;
+        b.stats = sw_score ? 0 : m->stats;
+        b.pad_rows = (job->bits < 0 || (m->alg == PB_SW && !m->stats)) ? 0
+                   : (job->bits == 0 || job->bits == 8) ? 32 : job->bits == 16 ? 16 : 8;
+        rc = pb_cuda_align_exact_db(&b);
     } else {
-        for (int q = 0; q < nq && rc == 0; ++q) {
-            pb_batch b = *tmpl;
-            if (tmpl->nprofs > 0) { b.profs = &tmpl->profs[q]; b.nprofs = 1; }
-            b.d_out = o1 + (size_t)q * n;
-            b.d_qlim = nullptr;
-            b.d_tlim = nullptr;
-            b.stats = sw_score ? 0 : m->stats;
-            b.pad_rows = (job->bits < 0 || (m->alg == PB_SW && !m->stats)) ? 0
-                       : (job->bits == 0 || job->bits == 8) ? 32 : job->bits == 16 ? 16 : 8;
-            rc = pb_cuda_align_exact(&b);
-        }
+        pb_batch b = *tmpl;
+        b.d_out = o1;
+        b.d_qlim = nullptr;
+        b.d_tlim = nullptr;
+        b.stats = sw_score ? 0 : m->stats;
+        b.pad_rows = (job->bits < 0 || (m->alg == PB_SW && !m->stats)) ? 0
+                   : (job->bits == 0 || job->bits == 8) ? 32 : job->bits == 16 ? 16 : 8;
+        rc = pb_cuda_align_exact(&b);
     }
     if (rc == 0 && pb_job_is_faststats(job)) {
         cudaMallocAsync((void **)&o2, sizeof(pb_pair_out) * n * (size_t)nq, st);

@@ -115,6 +115,8 @@ int pb_cuda_sync(void);
 /* --- alignment ------------------------------------------------------------- */
 /* Exact int32 kernel: any mode, stats, padded-row predicate statistics. */
 int pb_cuda_align_exact(const pb_batch *b);
+/* every profile of b against every target, one launch, outputs query-major */
+int pb_cuda_align_exact_db(const pb_batch *b);
 /* Fast Smith-Waterman score-only kernel: two pairs per thread in packed
  * int16x2 lanes. Pairs whose values leave the 16-bit range come back with
  * PB_ST_OVERFLOW16 and must be rerun with pb_cuda_align_exact. Only

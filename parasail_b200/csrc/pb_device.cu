@@ -14,6 +14,7 @@
 
 #include <cuda_runtime.h>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_radix_sort.cuh>
 
 #include "pb_cuda.h"
 #include "pb_kernels.cuh"
@@ -95,6 +96,20 @@ __global__ void k_scratch_sizes(const int *__restrict__ tlen, const int *__restr
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p < n) sizes[p] = (int64_t)(tlim ? tlim[p] : tlen[p]) * nv;
+}
+
+/* every query against every target: scratch per (query, target) item,
+ * query-major, and the item's work (query length x target length) */
+__global__ void k_exact_db_items(const int *__restrict__ tlen, const int *__restrict__ qlens, int n, int nq, int nv,
+                                 int64_t *__restrict__ sizes, unsigned long long *__restrict__ keys,
+                                 int *__restrict__ idx)
+{
+    const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k >= (long long)n * nq) return;
+    const int t = (int)(k % n), q = (int)(k / n);
+    sizes[k] = (int64_t)tlen[t] * nv;
+    keys[k] = (unsigned long long)qlens[q] * (unsigned long long)tlen[t];
+    idx[k] = (int)k;
 }
 
 /* Copies the host descriptors of the batch's profiles to the device. */
@@ -298,6 +313,75 @@ int pb_cuda_align_exact(const pb_batch *b)
     cudaFreeAsync(sizes, st);
     cudaFreeAsync(soff, st);
     if (d_profs) cudaFreeAsync(d_profs, st);
+    CK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+/*
+ * Every profile of the batch against every target in one exact-kernel
+ * launch (outputs query-major: d_out[q * npairs + t]). One thread aligns
+ * one pair, so a warp runs as long as its longest pair: the items go to
+ * the threads in order of work, largest first, which gives each warp pairs
+ * of like size and starts the longest ones first.
+ */
+int pb_cuda_align_exact_db(const pb_batch *b)
+{
+    if (pb_cuda_init() != 0) return -1;
+    const int n = b->npairs, nq = b->nprofs;
+    if (n <= 0 || nq <= 0) return 0;
+    if ((long long)n * nq > INT32_MAX) { snprintf(g_err, sizeof g_err, "batch too large"); return -1; }
+    const int N = n * nq;
+    cudaStream_t st = stream();
+    const int nv = b->stats ? 8 : 2;
+    int64_t *sizes = nullptr, *soff = nullptr;
+    unsigned long long *keys = nullptr, *keys_sorted = nullptr;
+    int *idx = nullptr, *order = nullptr, *d_qlens = nullptr;
+    void *tmp = nullptr, *stmp = nullptr;
+    size_t tmp_bytes = 0, stmp_bytes = 0;
+    std::vector<int> hq(nq);
+    for (int q = 0; q < nq; ++q) hq[q] = b->profs[q]->qlen;
+    CK(cudaMallocAsync((void **)&sizes, sizeof(int64_t) * N, st));
+    CK(cudaMallocAsync((void **)&soff, sizeof(int64_t) * N, st));
+    CK(cudaMallocAsync((void **)&keys, sizeof(unsigned long long) * N, st));
+    CK(cudaMallocAsync((void **)&keys_sorted, sizeof(unsigned long long) * N, st));
+    CK(cudaMallocAsync((void **)&idx, sizeof(int) * N, st));
+    CK(cudaMallocAsync((void **)&order, sizeof(int) * N, st));
+    CK(cudaMallocAsync((void **)&d_qlens, sizeof(int) * nq, st));
+    CK(cudaMemcpyAsync(d_qlens, hq.data(), sizeof(int) * nq, cudaMemcpyHostToDevice, st));
+    k_exact_db_items<<<(N + 255) / 256, 256, 0, st>>>(b->d_tlen, d_qlens, n, nq, nv, sizes, keys, idx);
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, sizes, soff, N, st);
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, stmp_bytes, keys, keys_sorted, idx, order, N, 0, 64, st);
+    CK(cudaMallocAsync(&tmp, tmp_bytes, st));
+    CK(cudaMallocAsync(&stmp, stmp_bytes, st));
+    cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, sizes, soff, N, st);
+    cub::DeviceRadixSort::SortPairsDescending(stmp, stmp_bytes, keys, keys_sorted, idx, order, N, 0, 64, st);
+    int64_t last_off = 0, last_size = 0;
+    CK(cudaMemcpyAsync(&last_off, soff + N - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last_size, sizes + N - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    int *scratch = nullptr;
+    CK(cudaMallocAsync((void **)&scratch, sizeof(int) * (size_t)(last_off + last_size + 1), st));
+    pb::ProfDesc *d_profs = upload_profs(b, st);
+    if (!d_profs) { snprintf(g_err, sizeof g_err, "profile descriptor upload failed"); return -1; }
+
+    pb::ExactParams p;
+    p.alg = b->alg; p.sgflags = b->sgflags; p.open = b->open; p.gap = b->gap;
+    p.pad_rows = b->pad_rows; p.npairs = N;
+    p.profs = d_profs; p.prof_index = nullptr;
+    p.targets = b->d_targets; p.toff = b->d_toff; p.tlen = b->d_tlen;
+    p.qlim = nullptr; p.tlim = nullptr;
+    p.scratch = scratch; p.soff = soff; p.out = b->d_out;
+    p.mat = nullptr; p.msize = 0; p.qall = nullptr; p.qoff = nullptr; p.qlen = nullptr;
+    p.order = order; p.nt = n;
+    pb::launch_exact(p, b->alg, b->stats != 0, st);
+    pb_diag_count_launch(2);   /* k_exact_db_items, k_exact (plus the library scan and sort) */
+    CK(cudaGetLastError());
+    cudaFreeAsync(scratch, st);
+    cudaFreeAsync(tmp, st); cudaFreeAsync(stmp, st);
+    cudaFreeAsync(sizes, st); cudaFreeAsync(soff, st);
+    cudaFreeAsync(keys, st); cudaFreeAsync(keys_sorted, st);
+    cudaFreeAsync(idx, st); cudaFreeAsync(order, st); cudaFreeAsync(d_qlens, st);
+    cudaFreeAsync(d_profs, st);
     CK(cudaStreamSynchronize(st));
     return 0;
 }

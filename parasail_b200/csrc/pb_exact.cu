@@ -31,7 +31,9 @@ k_exact(ExactParams p)
 template <int ALG, bool STATS>
 static void launch_alg(const ExactParams &p, cudaStream_t st)
 {
-    constexpr int R = STATS ? 8 : 16;
+    /* score-only: 32-row strips (34 vs 29 GCUPS for NW against 16 rows,
+     * 128 registers); statistics: 8 (the row loop stays rolled there) */
+    constexpr int R = STATS ? 8 : 32;
     const int threads = 128;
     const int blocks = (p.npairs + threads - 1) / threads;
     k_exact<ALG, STATS, R><<<blocks, threads, 0, st>>>(p);

@@ -49,20 +49,22 @@ __host__ __device__ __forceinline__ int left_h(int i, int open, int gap, int sgf
 }
 
 template <int ALG, bool STATS, int R>
-__host__ __device__ __forceinline__ void exact_pair(const ExactParams &p, const int pid)
+__host__ __device__ __forceinline__ void exact_pair(const ExactParams &p, const int k)
 {
+    const int pid = p.order ? p.order[k] : k;          /* output slot */
+    const int ti = p.nt ? pid % p.nt : pid;            /* target (and per-pair query) index */
 
     const bool matmode = p.mat != nullptr;
     ProfDesc pd;
     if (matmode) {
-        pd.prof = nullptr; pd.prof8 = nullptr; pd.qcodes = p.qall + p.qoff[pid];
-        pd.qlen = p.qlen[pid]; pd.lp = 0; pd.size = p.msize; pd.pad_ = 0;
+        pd.prof = nullptr; pd.prof8 = nullptr; pd.qcodes = p.qall + p.qoff[ti];
+        pd.qlen = p.qlen[ti]; pd.lp = 0; pd.size = p.msize; pd.pad_ = 0;
     } else {
-        pd = p.profs[p.prof_index ? p.prof_index[pid] : 0];
+        pd = p.profs[p.nt ? pid / p.nt : (p.prof_index ? p.prof_index[pid] : 0)];
     }
-    const uint8_t *PB_RESTRICT tseq = p.targets + p.toff[pid];
+    const uint8_t *PB_RESTRICT tseq = p.targets + p.toff[ti];
     const int ql = p.qlim ? p.qlim[pid] : pd.qlen;
-    const int tl = p.tlim ? p.tlim[pid] : p.tlen[pid];
+    const int tl = p.tlim ? p.tlim[pid] : p.tlen[ti];
     const int open = p.open, gap = p.gap, sgf = p.sgflags;
     const int c8 = (ql + 7) & ~7, c16 = (ql + 15) & ~15, c32 = (ql + 31) & ~31;
     const int nrows = p.pad_rows == 0 ? ql

@@ -39,6 +39,11 @@ struct ExactParams {
     const uint8_t *qall;
     const int64_t *qoff;
     const int *qlen;
+    /* work item k aligns pair order[k] (nullptr: pair k) */
+    const int *order = nullptr;
+    /* > 0: pair index = query * nt + target, every query of profs against
+     * the same nt targets (outputs query-major); 0: one pair per target */
+    int nt = 0;
 };
 
 struct Sw16Query {
