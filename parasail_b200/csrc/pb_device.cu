@@ -101,15 +101,21 @@ __global__ void k_scratch_sizes(const int *__restrict__ tlen, const int *__restr
 /* every query against every target: scratch per (query, target) item,
  * query-major, and the item's work (query length x target length) */
 __global__ void k_exact_db_items(const int *__restrict__ tlen, const int *__restrict__ qlens, int n, int nq, int nv,
-                                 int64_t *__restrict__ sizes, unsigned long long *__restrict__ keys,
-                                 int *__restrict__ idx)
+                                 int warp_min_qlen, int64_t *__restrict__ sizes,
+                                 unsigned long long *__restrict__ keys, int *__restrict__ idx, int *nwarp)
 {
     const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (k >= (long long)n * nq) return;
     const int t = (int)(k % n), q = (int)(k / n);
     sizes[k] = (int64_t)tlen[t] * nv;
-    keys[k] = (unsigned long long)qlens[q] * (unsigned long long)tlen[t];
+    /* items for the warp-per-pair kernel sort first (bit 62): queries that
+     * fill a 512-row pass, and any pair of 2^18 cells or more (on one
+     * thread, at about 11 M cells/s, it would last past the launch) */
+    const long long cells = (long long)qlens[q] * tlen[t];
+    const bool w = warp_min_qlen > 0 && (qlens[q] >= warp_min_qlen || (qlens[q] >= 64 && cells >= (1LL << 18)));
+    keys[k] = (unsigned long long)qlens[q] * (unsigned long long)tlen[t] | (w ? 1ull << 62 : 0ull);
     idx[k] = (int)k;
+    if (w) atomicAdd(nwarp, 1);
 }
 
 /* Copies the host descriptors of the batch's profiles to the device. */
@@ -335,7 +341,7 @@ int pb_cuda_align_exact_db(const pb_batch *b)
     const int nv = b->stats ? 8 : 2;
     int64_t *sizes = nullptr, *soff = nullptr;
     unsigned long long *keys = nullptr, *keys_sorted = nullptr;
-    int *idx = nullptr, *order = nullptr, *d_qlens = nullptr;
+    int *idx = nullptr, *order = nullptr, *d_qlens = nullptr, *d_nwarp = nullptr;
     void *tmp = nullptr, *stmp = nullptr;
     size_t tmp_bytes = 0, stmp_bytes = 0;
     std::vector<int> hq(nq);
@@ -347,8 +353,13 @@ int pb_cuda_align_exact_db(const pb_batch *b)
     CK(cudaMallocAsync((void **)&idx, sizeof(int) * N, st));
     CK(cudaMallocAsync((void **)&order, sizeof(int) * N, st));
     CK(cudaMallocAsync((void **)&d_qlens, sizeof(int) * nq, st));
+    CK(cudaMallocAsync((void **)&d_nwarp, sizeof(int), st));
     CK(cudaMemcpyAsync(d_qlens, hq.data(), sizeof(int) * nq, cudaMemcpyHostToDevice, st));
-    k_exact_db_items<<<(N + 255) / 256, 256, 0, st>>>(b->d_tlen, d_qlens, n, nq, nv, sizes, keys, idx);
+    CK(cudaMemsetAsync(d_nwarp, 0, sizeof(int), st));
+    /* score-only: long pairs go one per warp */
+    const int warp_min_qlen = b->stats ? 0 : 512;
+    k_exact_db_items<<<(N + 255) / 256, 256, 0, st>>>(b->d_tlen, d_qlens, n, nq, nv, warp_min_qlen, sizes, keys,
+                                                      idx, d_nwarp);
     cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, sizes, soff, N, st);
     cub::DeviceRadixSort::SortPairsDescending(nullptr, stmp_bytes, keys, keys_sorted, idx, order, N, 0, 64, st);
     CK(cudaMallocAsync(&tmp, tmp_bytes, st));
@@ -356,8 +367,10 @@ int pb_cuda_align_exact_db(const pb_batch *b)
     cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, sizes, soff, N, st);
     cub::DeviceRadixSort::SortPairsDescending(stmp, stmp_bytes, keys, keys_sorted, idx, order, N, 0, 64, st);
     int64_t last_off = 0, last_size = 0;
+    int nwarp = 0;
     CK(cudaMemcpyAsync(&last_off, soff + N - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(&last_size, sizes + N - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&nwarp, d_nwarp, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     int *scratch = nullptr;
     CK(cudaMallocAsync((void **)&scratch, sizeof(int) * (size_t)(last_off + last_size + 1), st));
@@ -373,16 +386,40 @@ int pb_cuda_align_exact_db(const pb_batch *b)
     p.scratch = scratch; p.soff = soff; p.out = b->d_out;
     p.mat = nullptr; p.msize = 0; p.qall = nullptr; p.qoff = nullptr; p.qlen = nullptr;
     p.order = order; p.nt = n;
-    pb::launch_exact(p, b->alg, b->stats != 0, st);
-    pb_diag_count_launch(2);   /* k_exact_db_items, k_exact (plus the library scan and sort) */
+    /* the warp-per-pair items (sorted first) on a second stream, the rest
+     * one per thread beside them */
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev = nullptr;
+    if (nwarp > 0) {
+        CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        CK(cudaEventRecord(ev, st));
+        CK(cudaStreamWaitEvent(st2, ev, 0));
+        pb::launch_exact_warp(p, b->alg, nwarp, st2);
+        pb_diag_count_launch(1);
+    }
+    if (N - nwarp > 0) {
+        pb::ExactParams pt = p;
+        pt.order = order + nwarp;
+        pt.npairs = N - nwarp;
+        pb::launch_exact(pt, b->alg, b->stats != 0, st);
+        pb_diag_count_launch(1);
+    }
+    if (st2) {
+        CK(cudaEventRecord(ev, st2));
+        CK(cudaStreamWaitEvent(st, ev, 0));
+    }
+    pb_diag_count_launch(1);   /* k_exact_db_items (plus the library scan and sort) */
     CK(cudaGetLastError());
     cudaFreeAsync(scratch, st);
     cudaFreeAsync(tmp, st); cudaFreeAsync(stmp, st);
     cudaFreeAsync(sizes, st); cudaFreeAsync(soff, st);
     cudaFreeAsync(keys, st); cudaFreeAsync(keys_sorted, st);
-    cudaFreeAsync(idx, st); cudaFreeAsync(order, st); cudaFreeAsync(d_qlens, st);
+    cudaFreeAsync(idx, st); cudaFreeAsync(order, st); cudaFreeAsync(d_qlens, st); cudaFreeAsync(d_nwarp, st);
     cudaFreeAsync(d_profs, st);
     CK(cudaStreamSynchronize(st));
+    if (st2) cudaStreamDestroy(st2);
+    if (ev) cudaEventDestroy(ev);
     return 0;
 }
 

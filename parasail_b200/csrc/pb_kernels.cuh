@@ -46,6 +46,10 @@ struct ExactParams {
     int nt = 0;
 };
 
+/* the exact kernel with one warp per pair (pb_exact_warp.cu), score only:
+ * items order[0..nitems) of p, which uses p.nt query-major pairs */
+void launch_exact_warp(const ExactParams &p, int alg, int nitems, cudaStream_t st);
+
 struct Sw16Query {
     int prof_off;            /* byte offset of the query's int8 profile in shared memory */
     int qlen, lp, posmax;

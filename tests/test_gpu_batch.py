@@ -157,3 +157,34 @@ def test_records_reserved_field_is_zero_and_host_equals_single_calls():
         for t, r in zip(targets, pb.records_to_dicts(recs, st)):
             assert r == pb.align_profile("parasail_" + name, prof, t, 5, 2), (name, t)
         prof.close()
+
+
+@pytest.mark.parametrize("width", ["16", "32", "sat"])
+def test_long_query_batches_nw_sg_vs_oracle(width):
+    """Queries of 512 rows and more, and pairs of 2^18 cells and more, run
+    one warp per pair (lanes on 16-row slices of 512-row passes): NW and the
+    SG end variants against the oracle, query lengths at the pass and lane
+    boundaries and below a pass, and targets from short to several times the
+    query; flags from the width chain."""
+    rng = random.Random({"16": 16, "32": 32, "sat": 3}[width])
+    b62 = pb.matrix_lookup("blosum62")
+    om = _b62()
+    for alg_name in ("nw", "sg", "sg_qx", "sg_db", "sg_qe_de", "sg_qb_de"):
+        alg, sgf = O.alg_of(alg_name)
+        for ql in (100, 300, 512, 513, 1023, 1024, 1300):
+            q = rand_seq(rng, ql, AA)
+            # short queries reach the warp kernel through long targets (2^18 cells and more)
+            targets = [mutate(rng, q, AA, 0.2, 0.03) if k % 4 == 0 else
+                       rand_seq(rng, rng.randint(2700, 3000) if k % 3 == 1 else rng.randint(1, 900), AA)
+                       for k in range(10)]
+            prof = pb.ProfileHandle("parasail_profile_create_%s" % width, q, b62)
+            recs = pb.records_to_dicts(pb.batch_profile("%s_striped_profile_%s" % (alg_name, width), prof,
+                                                        targets, 11, 1), 0)
+            for t, r in zip(targets, recs):
+                e = O.align(alg, sgf, 0, q, t, 11, 1, om)
+                one = pb.align_profile("parasail_%s_striped_profile_%s" % (alg_name, width), prof, t, 11, 1)
+                assert r == one, (alg_name, width, ql, len(t))
+                if not (r["flag"] & pb.FLAG_SATURATED):
+                    assert (r["score"], r["end_query"], r["end_ref"]) == (e["score"], e["end_query"], e["end_ref"]), \
+                        (alg_name, width, ql, len(t), r, e)
+            prof.close()
