@@ -109,7 +109,7 @@ __global__ void k_exact_db_items(const int *__restrict__ tlen, const int *__rest
     const int t = (int)(k % n), q = (int)(k / n);
     sizes[k] = (int64_t)tlen[t] * nv;
     /* items for the warp-per-pair kernel sort first (bit 62): queries that
-     * fill a 512-row pass, and any pair of 2^18 cells or more (on one
+     * fill one of its passes, and any pair of 2^18 cells or more (on one
      * thread, at about 11 M cells/s, it would last past the launch) */
     const long long cells = (long long)qlens[q] * tlen[t];
     const bool w = warp_min_qlen > 0 && (qlens[q] >= warp_min_qlen || (qlens[q] >= 64 && cells >= (1LL << 18)));
@@ -356,8 +356,8 @@ int pb_cuda_align_exact_db(const pb_batch *b)
     CK(cudaMallocAsync((void **)&d_nwarp, sizeof(int), st));
     CK(cudaMemcpyAsync(d_qlens, hq.data(), sizeof(int) * nq, cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(d_nwarp, 0, sizeof(int), st));
-    /* score-only: long pairs go one per warp */
-    const int warp_min_qlen = b->stats ? 0 : 512;
+    /* long pairs go one per warp */
+    const int warp_min_qlen = pb::exact_warp_pass_rows(b->stats != 0);
     k_exact_db_items<<<(N + 255) / 256, 256, 0, st>>>(b->d_tlen, d_qlens, n, nq, nv, warp_min_qlen, sizes, keys,
                                                       idx, d_nwarp);
     cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, sizes, soff, N, st);
@@ -395,7 +395,7 @@ int pb_cuda_align_exact_db(const pb_batch *b)
         CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         CK(cudaEventRecord(ev, st));
         CK(cudaStreamWaitEvent(st2, ev, 0));
-        pb::launch_exact_warp(p, b->alg, nwarp, st2);
+        pb::launch_exact_warp(p, b->alg, b->stats != 0, nwarp, st2);
         pb_diag_count_launch(1);
     }
     if (N - nwarp > 0) {

@@ -46,9 +46,11 @@ struct ExactParams {
     int nt = 0;
 };
 
-/* the exact kernel with one warp per pair (pb_exact_warp.cu), score only:
- * items order[0..nitems) of p, which uses p.nt query-major pairs */
-void launch_exact_warp(const ExactParams &p, int alg, int nitems, cudaStream_t st);
+/* the exact kernel with one warp per pair (pb_exact_warp.cu): items
+ * order[0..nitems) of p, which uses p.nt query-major pairs */
+void launch_exact_warp(const ExactParams &p, int alg, bool stats, int nitems, cudaStream_t st);
+/* query rows of one of its passes */
+int exact_warp_pass_rows(bool stats);
 
 struct Sw16Query {
     int prof_off;            /* byte offset of the query's int8 profile in shared memory */

@@ -188,3 +188,31 @@ def test_long_query_batches_nw_sg_vs_oracle(width):
                     assert (r["score"], r["end_query"], r["end_ref"]) == (e["score"], e["end_query"], e["end_ref"]), \
                         (alg_name, width, ql, len(t), r, e)
             prof.close()
+
+
+@pytest.mark.parametrize("width", ["16", "32", "sat"])
+def test_long_query_batches_with_statistics_vs_oracle(width):
+    """Long pairs with statistics run one warp per pair (lanes on 8-row
+    slices of 256-row passes): NW and SG statistics (striped) and SW
+    statistics (scan) against the oracle, query lengths at the pass and
+    lane boundaries; the single calls (one thread per pair) must agree."""
+    rng = random.Random({"16": 61, "32": 62, "sat": 63}[width])
+    b62 = pb.matrix_lookup("blosum62")
+    om = _b62()
+    for alg_name, scheme in (("nw", "striped"), ("sg_qe_db", "striped"), ("sg_qx", "scan"), ("sw", "scan")):
+        alg, sgf = O.alg_of(alg_name)
+        for ql in (100, 256, 257, 300, 513, 800):
+            q = rand_seq(rng, ql, AA)
+            targets = [mutate(rng, q, AA, 0.2, 0.03) if k % 4 == 0 else
+                       rand_seq(rng, rng.randint(2700, 3000) if k % 3 == 1 else rng.randint(1, 700), AA)
+                       for k in range(8)]
+            prof = pb.ProfileHandle("parasail_profile_create_stats_%s" % width, q, b62)
+            name = "%s_stats_%s_profile_%s" % (alg_name, scheme, width)
+            recs = pb.records_to_dicts(pb.batch_profile(name, prof, targets, 11, 1), 1)
+            for t, r in zip(targets, recs):
+                assert r == pb.align_profile("parasail_" + name, prof, t, 11, 1), (name, ql, len(t))
+                if not (r["flag"] & pb.FLAG_SATURATED):
+                    e = O.align(alg, sgf, 1, q, t, 11, 1, om)
+                    for k in ("score", "end_query", "end_ref", "matches", "similar", "length"):
+                        assert r[k] == e[k], (name, ql, len(t), r, e)
+            prof.close()
