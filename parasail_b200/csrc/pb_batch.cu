@@ -224,7 +224,23 @@ extern "C" int pb_cuda_batch_run(const pb_job *job, const pb_batch *tmpl, pb_rec
                    : (job->bits == 0 || job->bits == 8) ? 32 : job->bits == 16 ? 16 : 8;
         rc = pb_cuda_align_exact(&b);
     }
-    if (rc == 0 && pb_job_is_faststats(job)) {
+    if (rc == 0 && pb_job_is_faststats(job) && tmpl->nprofs >= 1) {
+        /* the prefix statistics pass of every query in one launch: limits
+         * per (query, target) item, query-major like o1 */
+        cudaMallocAsync((void **)&o2, sizeof(pb_pair_out) * n * (size_t)nq, st);
+        cudaMallocAsync((void **)&qlim, sizeof(int) * n * (size_t)nq, st);
+        cudaMallocAsync((void **)&tlim, sizeof(int) * n * (size_t)nq, st);
+        pb::k_prefix_limits<<<(int)(((size_t)n * nq + 255) / 256), 256, 0, st>>>(*job, o1, n * nq, qlim, tlim);
+        pb_diag_count_launch(1);
+        cudaStreamSynchronize(st);
+        pb_batch b2 = *tmpl;
+        b2.stats = 1;
+        b2.pad_rows = 32;
+        b2.d_qlim = qlim;
+        b2.d_tlim = tlim;
+        b2.d_out = o2;
+        rc = pb_cuda_align_exact_db(&b2);
+    } else if (rc == 0 && pb_job_is_faststats(job)) {
         cudaMallocAsync((void **)&o2, sizeof(pb_pair_out) * n * (size_t)nq, st);
         cudaMallocAsync((void **)&qlim, sizeof(int) * n, st);
         cudaMallocAsync((void **)&tlim, sizeof(int) * n, st);

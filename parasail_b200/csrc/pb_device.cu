@@ -100,20 +100,23 @@ __global__ void k_scratch_sizes(const int *__restrict__ tlen, const int *__restr
 
 /* every query against every target: scratch per (query, target) item,
  * query-major, and the item's work (query length x target length) */
-__global__ void k_exact_db_items(const int *__restrict__ tlen, const int *__restrict__ qlens, int n, int nq, int nv,
+__global__ void k_exact_db_items(const int *__restrict__ tlen, const int *__restrict__ qlens,
+                                 const int *__restrict__ qlim, const int *__restrict__ tlim, int n, int nq, int nv,
                                  int warp_min_qlen, int64_t *__restrict__ sizes,
                                  unsigned long long *__restrict__ keys, int *__restrict__ idx, int *nwarp)
 {
     const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (k >= (long long)n * nq) return;
     const int t = (int)(k % n), q = (int)(k / n);
-    sizes[k] = (int64_t)tlen[t] * nv;
+    /* per-item limits (a prefix of the pair) when given */
+    const int ql = qlim ? qlim[k] : qlens[q], tl = tlim ? tlim[k] : tlen[t];
+    sizes[k] = (int64_t)tl * nv;
     /* items for the warp-per-pair kernel sort first (bit 62): queries that
      * fill one of its passes, and any pair of 2^18 cells or more (on one
      * thread, at about 11 M cells/s, it would last past the launch) */
-    const long long cells = (long long)qlens[q] * tlen[t];
-    const bool w = warp_min_qlen > 0 && (qlens[q] >= warp_min_qlen || (qlens[q] >= 64 && cells >= (1LL << 18)));
-    keys[k] = (unsigned long long)qlens[q] * (unsigned long long)tlen[t] | (w ? 1ull << 62 : 0ull);
+    const long long cells = (long long)ql * tl;
+    const bool w = warp_min_qlen > 0 && (ql >= warp_min_qlen || (ql >= 64 && cells >= (1LL << 18)));
+    keys[k] = (unsigned long long)cells | (w ? 1ull << 62 : 0ull);
     idx[k] = (int)k;
     if (w) atomicAdd(nwarp, 1);
 }
@@ -358,8 +361,8 @@ int pb_cuda_align_exact_db(const pb_batch *b)
     CK(cudaMemsetAsync(d_nwarp, 0, sizeof(int), st));
     /* long pairs go one per warp */
     const int warp_min_qlen = pb::exact_warp_pass_rows(b->stats != 0);
-    k_exact_db_items<<<(N + 255) / 256, 256, 0, st>>>(b->d_tlen, d_qlens, n, nq, nv, warp_min_qlen, sizes, keys,
-                                                      idx, d_nwarp);
+    k_exact_db_items<<<(N + 255) / 256, 256, 0, st>>>(b->d_tlen, d_qlens, b->d_qlim, b->d_tlim, n, nq, nv,
+                                                      warp_min_qlen, sizes, keys, idx, d_nwarp);
     cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, sizes, soff, N, st);
     cub::DeviceRadixSort::SortPairsDescending(nullptr, stmp_bytes, keys, keys_sorted, idx, order, N, 0, 64, st);
     CK(cudaMallocAsync(&tmp, tmp_bytes, st));
@@ -382,7 +385,7 @@ int pb_cuda_align_exact_db(const pb_batch *b)
     p.pad_rows = b->pad_rows; p.npairs = N;
     p.profs = d_profs; p.prof_index = nullptr;
     p.targets = b->d_targets; p.toff = b->d_toff; p.tlen = b->d_tlen;
-    p.qlim = nullptr; p.tlim = nullptr;
+    p.qlim = b->d_qlim; p.tlim = b->d_tlim;      /* per item (query-major), or none */
     p.scratch = scratch; p.soff = soff; p.out = b->d_out;
     p.mat = nullptr; p.msize = 0; p.qall = nullptr; p.qoff = nullptr; p.qlen = nullptr;
     p.order = order; p.nt = n;

@@ -62,8 +62,8 @@ k_exact_warp(ExactParams p, int nitems)
     const int ti = pid % p.nt;
     const ProfDesc pd = p.profs[pid / p.nt];
     const uint8_t *tseq = p.targets + p.toff[ti];
-    const int ql = pd.qlen;
-    const int tl = p.tlen[ti];
+    const int ql = p.qlim ? p.qlim[pid] : pd.qlen;       /* a prefix of the pair when limited */
+    const int tl = p.tlim ? p.tlim[pid] : p.tlen[ti];
     const int open = p.open, gap = p.gap, sgf = p.sgflags;
     const int c8 = (ql + 7) & ~7, c16 = (ql + 15) & ~15, c32 = (ql + 31) & ~31;
     const int nrows = p.pad_rows == 0 ? ql : (p.pad_rows == 8 ? c8 : (p.pad_rows == 16 ? c16 : c32));

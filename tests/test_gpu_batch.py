@@ -193,13 +193,15 @@ def test_long_query_batches_nw_sg_vs_oracle(width):
 @pytest.mark.parametrize("width", ["16", "32", "sat"])
 def test_long_query_batches_with_statistics_vs_oracle(width):
     """Long pairs with statistics run one warp per pair (lanes on 8-row
-    slices of 256-row passes): NW and SG statistics (striped) and SW
-    statistics (scan) against the oracle, query lengths at the pass and
-    lane boundaries; the single calls (one thread per pair) must agree."""
+    slices of 256-row passes): NW and SG statistics (striped), SW statistics
+    (scan) and the prefix pass of SW statistics striped (FASTSTATS) against
+    the oracle, query lengths at the pass and lane boundaries; the single
+    calls (one thread per pair) must agree."""
     rng = random.Random({"16": 61, "32": 62, "sat": 63}[width])
     b62 = pb.matrix_lookup("blosum62")
     om = _b62()
-    for alg_name, scheme in (("nw", "striped"), ("sg_qe_db", "striped"), ("sg_qx", "scan"), ("sw", "scan")):
+    for alg_name, scheme in (("nw", "striped"), ("sg_qe_db", "striped"), ("sg_qx", "scan"), ("sw", "scan"),
+                             ("sw", "striped")):
         alg, sgf = O.alg_of(alg_name)
         for ql in (100, 256, 257, 300, 513, 800):
             q = rand_seq(rng, ql, AA)
