@@ -111,11 +111,14 @@ __global__ void k_exact_db_items(const int *__restrict__ tlen, const int *__rest
     /* per-item limits (a prefix of the pair) when given */
     const int ql = qlim ? qlim[k] : qlens[q], tl = tlim ? tlim[k] : tlen[t];
     sizes[k] = (int64_t)tl * nv;
-    /* items for the warp-per-pair kernel sort first (bit 62): queries that
-     * fill one of its passes, and any pair of 2^18 cells or more (on one
-     * thread, at about 11 M cells/s, it would last past the launch) */
+    /* items for the warp-per-pair kernel sort first (bit 62): every query of
+     * 32 rows or more, and shorter ones (8 or more) whose pair has 2^14
+     * cells or more. On 5 queries (100-2000) x 20,000 targets this beat
+     * one thread per pair at every size: NW 455 GCUPS against 288 with the
+     * warp kernel only for pairs of 2^18 cells and queries that fill a
+     * pass, and NW statistics 227 against 74 */
     const long long cells = (long long)ql * tl;
-    const bool w = warp_min_qlen > 0 && (ql >= warp_min_qlen || (ql >= 64 && cells >= (1LL << 18)));
+    const bool w = warp_min_qlen > 0 && (ql >= 32 || (ql >= 8 && cells >= (1LL << 14)));
     keys[k] = (unsigned long long)cells | (w ? 1ull << 62 : 0ull);
     idx[k] = (int)k;
     if (w) atomicAdd(nwarp, 1);
@@ -359,7 +362,7 @@ int pb_cuda_align_exact_db(const pb_batch *b)
     CK(cudaMallocAsync((void **)&d_nwarp, sizeof(int), st));
     CK(cudaMemcpyAsync(d_qlens, hq.data(), sizeof(int) * nq, cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(d_nwarp, 0, sizeof(int), st));
-    /* long pairs go one per warp */
+    /* pairs go one per warp (k_exact_db_items) */
     const int warp_min_qlen = pb::exact_warp_pass_rows(b->stats != 0);
     k_exact_db_items<<<(N + 255) / 256, 256, 0, st>>>(b->d_tlen, d_qlens, b->d_qlim, b->d_tlim, n, nq, nv,
                                                       warp_min_qlen, sizes, keys, idx, d_nwarp);
