@@ -161,11 +161,12 @@ def test_records_reserved_field_is_zero_and_host_equals_single_calls():
 
 @pytest.mark.parametrize("width", ["16", "32", "sat"])
 def test_long_query_batches_nw_sg_vs_oracle(width):
-    """Queries of 512 rows and more, and pairs of 2^18 cells and more, run
-    one warp per pair (lanes on 16-row slices of 512-row passes): NW and the
-    SG end variants against the oracle, query lengths at the pass and lane
-    boundaries and below a pass, and targets from short to several times the
-    query; flags from the width chain."""
+    """Batches run one warp per pair (lanes on 16-row slices of 512-row
+    passes) for every query of 32 rows and more: NW and the SG end variants
+    against the oracle and against the single calls (one thread per pair),
+    query lengths at the pass and lane boundaries and below a pass, and
+    targets from short to several times the query; flags from the width
+    chain."""
     rng = random.Random({"16": 16, "32": 32, "sat": 3}[width])
     b62 = pb.matrix_lookup("blosum62")
     om = _b62()
@@ -173,7 +174,7 @@ def test_long_query_batches_nw_sg_vs_oracle(width):
         alg, sgf = O.alg_of(alg_name)
         for ql in (100, 300, 512, 513, 1023, 1024, 1300):
             q = rand_seq(rng, ql, AA)
-            # short queries reach the warp kernel through long targets (2^18 cells and more)
+            # targets from a few residues to several times the query
             targets = [mutate(rng, q, AA, 0.2, 0.03) if k % 4 == 0 else
                        rand_seq(rng, rng.randint(2700, 3000) if k % 3 == 1 else rng.randint(1, 900), AA)
                        for k in range(10)]
