@@ -118,6 +118,39 @@ extern int parasail_b200_batch_pairs(
         const char *targets, const int64_t *toffsets, const int *tlengths, int n,
         int open, int gap, parasail_b200_record_t *records);
 
+/** parasail_b200_batch_pairs with device-resident, already mapped queries
+ * and targets (codes through matrix->mapper, one byte per residue) and
+ * device-resident records; query i is d_qcodes[d_qoffsets[i] ..
+ * d_qoffsets[i] + d_qlengths[i]). Replaces n calls of the reference's
+ * direct function (parasail.h:184-188) with inputs already on the GPU. */
+extern int parasail_b200_batch_pairs_device(
+        const char *funcname, const parasail_matrix_t *matrix,
+        const uint8_t *d_qcodes, const int64_t *d_qoffsets, const int *d_qlengths,
+        const uint8_t *d_tcodes, const int64_t *d_toffsets, const int *d_tlengths,
+        int n, int open, int gap, parasail_b200_record_t *d_records);
+
+/** All-vs-all: every pair (i, j), i < j, of n sequences (host memory;
+ * sequence i is seqs[offsets[i] .. offsets[i] + lengths[i])), sequence i as
+ * the query (the profile side) and j as the target, scored with `matrix`
+ * by `funcname` (profile or direct form, e.g. "sw_stats_striped_profile_32";
+ * both forms return the same results). records[p] receives pair p of the
+ * upper triangle in row-major order: p = i*n - i*(i+1)/2 + (j - i - 1), n(n-1)/2
+ * records in all. Replaces the reference aligner's all-against-all mode,
+ * which enumerates these pairs (apps/parasail_aligner.cpp:1441-1447), builds
+ * one profile per query sequence (:1543-1567) and calls the pfunction per
+ * pair under OpenMP (:1714-1740). */
+extern int parasail_b200_batch_all(
+        const char *funcname, const parasail_matrix_t *matrix,
+        const char *seqs, const int64_t *offsets, const int *lengths, int n,
+        int open, int gap, parasail_b200_record_t *records);
+
+/** parasail_b200_batch_all with device-resident, already mapped sequences
+ * and device-resident records. */
+extern int parasail_b200_batch_all_device(
+        const char *funcname, const parasail_matrix_t *matrix,
+        const uint8_t *d_codes, const int64_t *d_offsets, const int *d_lengths, int n,
+        int open, int gap, parasail_b200_record_t *d_records);
+
 /* ---- long global alignments and the learned band ---------------------- */
 
 /** Global alignment score of each long pair (query i against target i),

@@ -1,0 +1,456 @@
+"""ctypes mirror of the C API of libparasail_b200.so (parasail.h and the
+batch extensions of parasail_b200.h).
+
+The product is the C library `libparasail_b200.so` (C host code + sm_100a
+CUDA kernels) built in this directory; this module is a thin ctypes mirror of
+its C API, used by the tests and the benchmark. It is loaded on first use of
+an attribute of the `parasail_b200` package. Every call goes through the
+C ABI. There is no Python or CPU implementation of any alignment here: if the
+library is missing the import fails, and on a machine without a usable GPU
+the alignment calls return NULL, which this module raises as RuntimeError.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libparasail_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError("parasail_b200: %s is not built (run __graft_entry__.build())" % LIB_PATH)
+
+lib = ctypes.CDLL(LIB_PATH)
+
+FLAG_NW = 1 << 0
+FLAG_SG = 1 << 1
+FLAG_SW = 1 << 2
+FLAG_SG_S1_BEG = 1 << 3
+FLAG_SG_S1_END = 1 << 4
+FLAG_SATURATED = 1 << 6
+FLAG_BANDED = 1 << 7
+FLAG_NOVEC = 1 << 8
+FLAG_NOVEC_SCAN = 1 << 9
+FLAG_SCAN = 1 << 10
+FLAG_STRIPED = 1 << 11
+FLAG_SG_S2_BEG = 1 << 14
+FLAG_SG_S2_END = 1 << 15
+FLAG_STATS = 1 << 16
+FLAG_BITS_8 = 1 << 20
+FLAG_BITS_16 = 1 << 21
+FLAG_BITS_32 = 1 << 22
+
+
+class ResultStats(ctypes.Structure):
+    _fields_ = [("matches", ctypes.c_int), ("similar", ctypes.c_int),
+                ("length", ctypes.c_int), ("extra", ctypes.c_void_p)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("score", ctypes.c_int), ("end_query", ctypes.c_int),
+                ("end_ref", ctypes.c_int), ("flag", ctypes.c_int),
+                ("extra", ctypes.c_void_p)]
+
+
+class Matrix(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char_p), ("matrix", ctypes.POINTER(ctypes.c_int)),
+                ("mapper", ctypes.POINTER(ctypes.c_int)), ("size", ctypes.c_int),
+                ("max", ctypes.c_int), ("min", ctypes.c_int),
+                ("user_matrix", ctypes.POINTER(ctypes.c_int)), ("type", ctypes.c_int),
+                ("length", ctypes.c_int), ("alphabet", ctypes.c_char_p),
+                ("query", ctypes.c_char_p)]
+
+
+class ProfileData(ctypes.Structure):
+    _fields_ = [("score", ctypes.c_void_p), ("matches", ctypes.c_void_p),
+                ("similar", ctypes.c_void_p)]
+
+
+class Profile(ctypes.Structure):
+    _fields_ = [("s1", ctypes.c_char_p), ("s1Len", ctypes.c_int),
+                ("matrix", ctypes.POINTER(Matrix)),
+                ("profile8", ProfileData), ("profile16", ProfileData),
+                ("profile32", ProfileData), ("profile64", ProfileData),
+                ("free", ctypes.c_void_p), ("stop", ctypes.c_int)]
+
+
+_RP = ctypes.POINTER(Result)
+_MP = ctypes.POINTER(Matrix)
+_PP = ctypes.POINTER(Profile)
+
+lib.parasail_matrix_lookup.restype = _MP
+lib.parasail_matrix_lookup.argtypes = [ctypes.c_char_p]
+lib.parasail_matrix_create.restype = _MP
+lib.parasail_matrix_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+lib.parasail_matrix_free.argtypes = [_MP]
+lib.parasail_result_free.argtypes = [_RP]
+lib.parasail_profile_free.argtypes = [_PP]
+lib.parasail_nw_banded.restype = _RP
+lib.parasail_nw_banded.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, _MP]
+for _n in ("get_matches", "get_similar", "get_length"):
+    getattr(lib, "parasail_result_" + _n).argtypes = [_RP]
+
+
+def matrix_lookup(name):
+    m = lib.parasail_matrix_lookup(name.encode())
+    if not m:
+        raise KeyError(name)
+    return m
+
+
+def matrix_create(alphabet, match, mismatch):
+    return lib.parasail_matrix_create(alphabet.encode(), match, mismatch)
+
+
+def _fn(name, profile_form):
+    f = getattr(lib, name)
+    f.restype = _RP
+    if profile_form:
+        f.argtypes = [_PP, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    else:
+        f.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                      ctypes.c_int, ctypes.c_int, _MP]
+    return f
+
+
+def _unpack(r, name):
+    if not r:
+        raise RuntimeError("%s returned NULL" % name)
+    c = r.contents
+    out = {"score": c.score, "end_query": c.end_query, "end_ref": c.end_ref, "flag": c.flag}
+    if c.flag & FLAG_STATS:
+        st = ctypes.cast(c.extra, ctypes.POINTER(ResultStats)).contents
+        out.update(matches=st.matches, similar=st.similar, length=st.length)
+    lib.parasail_result_free(r)
+    return out
+
+
+def align(name, s1, s2, open_, gap, matrix):
+    """Calls a direct-form entry point, e.g. align('parasail_sw_striped_16', ...)."""
+    b1, b2 = s1.encode() if isinstance(s1, str) else s1, s2.encode() if isinstance(s2, str) else s2
+    return _unpack(_fn(name, False)(b1, len(b1), b2, len(b2), open_, gap, matrix), name)
+
+
+class ProfileHandle:
+    """Owns a parasail_profile_t and the query bytes it borrows."""
+
+    def __init__(self, creator, s1, matrix):
+        self.s1 = s1.encode() if isinstance(s1, str) else s1
+        self.matrix = matrix
+        f = getattr(lib, creator)
+        f.restype = _PP
+        f.argtypes = [ctypes.c_char_p, ctypes.c_int, _MP]
+        self.ptr = f(self.s1, len(self.s1), matrix)
+        if not self.ptr:
+            raise RuntimeError("%s returned NULL" % creator)
+
+    def close(self):
+        if self.ptr:
+            lib.parasail_profile_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        self.close()
+
+
+def align_profile(name, profile, s2, open_, gap):
+    b2 = s2.encode() if isinstance(s2, str) else s2
+    return _unpack(_fn(name, True)(profile.ptr, b2, len(b2), open_, gap), name)
+
+
+def nw_banded(s1, s2, open_, gap, k, matrix):
+    b1, b2 = s1.encode(), s2.encode()
+    return _unpack(lib.parasail_nw_banded(b1, len(b1), b2, len(b2), open_, gap, k, matrix),
+                   "parasail_nw_banded")
+
+
+# ---------------------------------------------------------------------------
+# Batch API (include/parasail_b200.h)
+
+class Record(ctypes.Structure):
+    _fields_ = [("score", ctypes.c_int), ("end_query", ctypes.c_int), ("end_ref", ctypes.c_int),
+                ("flag", ctypes.c_int), ("matches", ctypes.c_int), ("similar", ctypes.c_int),
+                ("length", ctypes.c_int), ("reserved", ctypes.c_int)]
+
+
+lib.parasail_b200_batch_profile.restype = ctypes.c_int
+lib.parasail_b200_batch_profile.argtypes = [ctypes.c_char_p, _PP, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_void_p]
+lib.parasail_b200_batch_profile_device.restype = ctypes.c_int
+lib.parasail_b200_batch_profile_device.argtypes = [ctypes.c_char_p, _PP, ctypes.c_void_p, ctypes.c_void_p,
+                                                   ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                                   ctypes.c_int, ctypes.c_void_p]
+lib.parasail_b200_batch_profile_device_noalloc.restype = ctypes.c_int
+lib.parasail_b200_batch_profile_device_noalloc.argtypes = lib.parasail_b200_batch_profile_device.argtypes
+lib.parasail_b200_noalloc_scratch_bytes.restype = ctypes.c_size_t
+lib.parasail_b200_noalloc_scratch_bytes.argtypes = []
+lib.parasail_b200_batch_pairs.restype = ctypes.c_int
+lib.parasail_b200_batch_pairs.argtypes = [ctypes.c_char_p, _MP] + [ctypes.c_void_p] * 6 + \
+    [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+lib.parasail_b200_kernel_launches.restype = ctypes.c_long
+lib.parasail_b200_sw16_kernel_ms.restype = ctypes.c_double
+lib.parasail_b200_sw16_kernel_ms.argtypes = [ctypes.POINTER(ctypes.c_long)]
+lib.parasail_b200_dpx_peak.restype = ctypes.c_double
+
+
+def _np():
+    import numpy
+    return numpy
+
+
+def pack(seqs):
+    """list of str/bytes -> (uint8 buffer, int64 offsets, int32 lengths)."""
+    np = _np()
+    bs = [s.encode() if isinstance(s, str) else s for s in seqs]
+    lens = np.array([len(b) for b in bs], dtype=np.int32)
+    offs = np.zeros(len(bs), dtype=np.int64)
+    if len(bs):
+        offs[1:] = np.cumsum(lens, dtype=np.int64)[:-1]
+    buf = np.frombuffer(b"".join(bs), dtype=np.uint8).copy() if bs else np.zeros(0, np.uint8)
+    return buf, offs, lens
+
+
+def records_to_dicts(recs, stats):
+    out = []
+    for r in recs:
+        d = {"score": int(r["score"]), "end_query": int(r["end_query"]), "end_ref": int(r["end_ref"]),
+             "flag": int(r["flag"])}
+        if stats and (d["flag"] & FLAG_STATS):
+            d.update(matches=int(r["matches"]), similar=int(r["similar"]), length=int(r["length"]))
+        out.append(d)
+    return out
+
+
+RECORD_DTYPE = None
+
+
+def record_dtype():
+    global RECORD_DTYPE
+    if RECORD_DTYPE is None:
+        np = _np()
+        RECORD_DTYPE = np.dtype([(n, np.int32) for n, _ in Record._fields_])
+    return RECORD_DTYPE
+
+
+def batch_profile(name, profile, targets, open_, gap, packed=None):
+    """Aligns many targets against profile with one batch call. Returns a
+    numpy structured array of records."""
+    np = _np()
+    buf, offs, lens = packed if packed is not None else pack(targets)
+    n = len(lens)
+    recs = np.zeros(n, dtype=record_dtype())
+    rc = lib.parasail_b200_batch_profile(name.encode(), profile.ptr, buf.ctypes.data, offs.ctypes.data,
+                                         lens.ctypes.data, n, open_, gap, recs.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("parasail_b200_batch_profile failed")
+    return recs
+
+
+def batch_pairs(name, matrix, queries, targets, open_, gap):
+    np = _np()
+    qb, qo, ql = pack(queries)
+    tb, to, tl = pack(targets)
+    n = len(tl)
+    recs = np.zeros(n, dtype=record_dtype())
+    rc = lib.parasail_b200_batch_pairs(name.encode(), matrix, qb.ctypes.data, qo.ctypes.data, ql.ctypes.data,
+                                       tb.ctypes.data, to.ctypes.data, tl.ctypes.data, n, open_, gap,
+                                       recs.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("parasail_b200_batch_pairs failed")
+    return recs
+
+lib.parasail_b200_batch_db.restype = ctypes.c_int
+lib.parasail_b200_batch_db.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_void_p]
+lib.parasail_b200_batch_db_device.restype = ctypes.c_int
+lib.parasail_b200_batch_db_device.argtypes = lib.parasail_b200_batch_db.argtypes
+
+
+lib.parasail_b200_batch_pairs_device.restype = ctypes.c_int
+lib.parasail_b200_batch_pairs_device.argtypes = [ctypes.c_char_p, _MP] + [ctypes.c_void_p] * 6 + \
+    [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+lib.parasail_b200_batch_all.restype = ctypes.c_int
+lib.parasail_b200_batch_all.argtypes = [ctypes.c_char_p, _MP, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+lib.parasail_b200_batch_all_device.restype = ctypes.c_int
+lib.parasail_b200_batch_all_device.argtypes = lib.parasail_b200_batch_all.argtypes
+
+
+def batch_all(name, matrix, seqs, open_, gap, packed=None):
+    """Every pair (i, j), i < j, of seqs; returns the n(n-1)/2 records in
+    row-major upper-triangle order."""
+    np = _np()
+    buf, offs, lens = packed if packed is not None else pack(seqs)
+    n = len(lens)
+    recs = np.zeros(max(0, n * (n - 1) // 2), dtype=record_dtype())
+    rc = lib.parasail_b200_batch_all(name.encode(), matrix, buf.ctypes.data, offs.ctypes.data, lens.ctypes.data,
+                                     n, open_, gap, recs.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("parasail_b200_batch_all failed")
+    return recs
+
+
+def profile_array(profiles):
+    arr = (_PP * len(profiles))(*[p.ptr for p in profiles])
+    return arr
+
+
+def batch_db(name, profiles, targets, open_, gap, packed=None):
+    """Every profile against every target in one call; returns records
+    shaped [len(profiles), n]."""
+    np = _np()
+    buf, offs, lens = packed if packed is not None else pack(targets)
+    n = len(lens)
+    recs = np.zeros(len(profiles) * n, dtype=record_dtype())
+    arr = profile_array(profiles)
+    rc = lib.parasail_b200_batch_db(name.encode(), ctypes.cast(arr, ctypes.c_void_p), len(profiles),
+                                    buf.ctypes.data, offs.ctypes.data, lens.ctypes.data, n, open_, gap,
+                                    recs.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("parasail_b200_batch_db failed")
+    return recs.reshape(len(profiles), n)
+
+
+# ---------------------------------------------------------------------------
+# Long global alignments and the learned band
+
+class BandStats(ctypes.Structure):
+    _fields_ = [("pairs", ctypes.c_longlong), ("certified", ctypes.c_longlong),
+                ("fallback", ctypes.c_longlong), ("band_cells", ctypes.c_double)]
+
+
+_V = ctypes.c_void_p
+lib.parasail_b200_nw_long.restype = ctypes.c_int
+lib.parasail_b200_nw_long.argtypes = [_MP, _V, _V, _V, _V, _V, _V, ctypes.c_int, ctypes.c_int, ctypes.c_int, _V]
+lib.parasail_b200_band_model_new.restype = _V
+lib.parasail_b200_band_model_new.argtypes = [ctypes.c_uint]
+lib.parasail_b200_band_model_free.argtypes = [_V]
+lib.parasail_b200_band_model_sizes.argtypes = [ctypes.POINTER(ctypes.c_int)] * 5
+lib.parasail_b200_band_model_get.argtypes = [_V, _V, _V]
+lib.parasail_b200_band_model_scaling.restype = None
+lib.parasail_b200_band_model_scaling.argtypes = [_V, _V, _V]
+lib.parasail_b200_band_model_set.argtypes = [_V, _V, _V]
+lib.parasail_b200_band_features.argtypes = [_MP, _V, _V, _V, _V, _V, _V, ctypes.c_int, _V]
+lib.parasail_b200_band_model_gradients.argtypes = [_V, _V, _V, ctypes.c_int, ctypes.c_float, _V, _V,
+                                                   ctypes.POINTER(ctypes.c_float)]
+lib.parasail_b200_band_model_train.argtypes = [_V, _MP, _V, _V, _V, _V, _V, _V, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                               ctypes.POINTER(ctypes.c_float)]
+lib.parasail_b200_nw_learned_band.argtypes = [_V, _MP, _V, _V, _V, _V, _V, _V, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_float, ctypes.c_int, _V, _V, _V,
+                                              ctypes.POINTER(BandStats)]
+lib.parasail_b200_nw_banded_certified.argtypes = [_MP, _V, _V, _V, _V, _V, _V, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_int, _V, _V, _V, _V]
+
+
+def _pairs_args(qbuf, qoff, qlen, tbuf, toff, tlen):
+    return (qbuf.ctypes.data, qoff.ctypes.data, qlen.ctypes.data, tbuf.ctypes.data, toff.ctypes.data,
+            tlen.ctypes.data)
+
+
+def nw_long(matrix, qbuf, qoff, qlen, tbuf, toff, tlen, open_, gap):
+    np = _np()
+    n = len(qlen)
+    out = np.zeros(n, dtype=np.int32)
+    rc = lib.parasail_b200_nw_long(matrix, *_pairs_args(qbuf, qoff, qlen, tbuf, toff, tlen), n, open_, gap,
+                                   out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("parasail_b200_nw_long failed")
+    return out
+
+
+class BandModel:
+    def __init__(self, seed=1):
+        self.ptr = lib.parasail_b200_band_model_new(seed)
+        if not self.ptr:
+            raise RuntimeError("parasail_b200_band_model_new failed")
+        v = [ctypes.c_int() for _ in range(5)]
+        lib.parasail_b200_band_model_sizes(*[ctypes.byref(x) for x in v])
+        self.n_in, self.n_hidden, self.n_out, self.n_weights, self.n_biases = [x.value for x in v]
+
+    def close(self):
+        if self.ptr:
+            lib.parasail_b200_band_model_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        self.close()
+
+    def get(self):
+        np = _np()
+        w = np.zeros(self.n_weights, np.float32)
+        b = np.zeros(self.n_biases, np.float32)
+        if lib.parasail_b200_band_model_get(self.ptr, w.ctypes.data, b.ctypes.data) != 0:
+            raise RuntimeError("get failed")
+        return w, b
+
+    def set(self, w, b):
+        np = _np()
+        w = np.ascontiguousarray(w, np.float32)
+        b = np.ascontiguousarray(b, np.float32)
+        if lib.parasail_b200_band_model_set(self.ptr, w.ctypes.data, b.ctypes.data) != 0:
+            raise RuntimeError("set failed")
+
+    def scaling(self):
+        """(widen, slack) chosen at training on held-out pairs."""
+        w, sl = ctypes.c_float(), ctypes.c_int()
+        lib.parasail_b200_band_model_scaling(self.ptr, ctypes.byref(w), ctypes.byref(sl))
+        return float(w.value), int(sl.value)
+
+    def gradients(self, x, target, tau):
+        np = _np()
+        x = np.ascontiguousarray(x, np.float32)
+        target = np.ascontiguousarray(target, np.float32)
+        gw = np.zeros(self.n_weights, np.float32)
+        gb = np.zeros(self.n_biases, np.float32)
+        loss = ctypes.c_float()
+        rc = lib.parasail_b200_band_model_gradients(self.ptr, x.ctypes.data, target.ctypes.data, len(x), tau,
+                                                    gw.ctypes.data, gb.ctypes.data, ctypes.byref(loss))
+        if rc != 0:
+            raise RuntimeError("gradients failed")
+        return gw, gb, loss.value
+
+    def train(self, matrix, qbuf, qoff, qlen, tbuf, toff, tlen, open_, gap, epochs=30, batch=256, lr=1e-3):
+        loss = ctypes.c_float()
+        rc = lib.parasail_b200_band_model_train(self.ptr, matrix, *_pairs_args(qbuf, qoff, qlen, tbuf, toff, tlen),
+                                                len(qlen), open_, gap, epochs, batch, lr, ctypes.byref(loss))
+        if rc != 0:
+            raise RuntimeError("train failed")
+        return loss.value
+
+    def align(self, matrix, qbuf, qoff, qlen, tbuf, toff, tlen, open_, gap, widen=1.0, slack=32):
+        np = _np()
+        n = len(qlen)
+        sc, lo, hi = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.int32)
+        st = BandStats()
+        rc = lib.parasail_b200_nw_learned_band(self.ptr, matrix, *_pairs_args(qbuf, qoff, qlen, tbuf, toff, tlen),
+                                               n, open_, gap, widen, slack, sc.ctypes.data, lo.ctypes.data,
+                                               hi.ctypes.data, ctypes.byref(st))
+        if rc != 0:
+            raise RuntimeError("learned band failed")
+        return sc, lo, hi, st
+
+
+def band_features(matrix, qbuf, qoff, qlen, tbuf, toff, tlen, n_in=258):
+    np = _np()
+    n = len(qlen)
+    f = np.zeros((n, n_in), np.float32)
+    if lib.parasail_b200_band_features(matrix, *_pairs_args(qbuf, qoff, qlen, tbuf, toff, tlen), n,
+                                       f.ctypes.data) != 0:
+        raise RuntimeError("features failed")
+    return f
+
+
+def nw_banded_certified(matrix, qbuf, qoff, qlen, tbuf, toff, tlen, open_, gap, lo, hi):
+    np = _np()
+    n = len(qlen)
+    lo = np.ascontiguousarray(lo, np.int32)
+    hi = np.ascontiguousarray(hi, np.int32)
+    sc, cert = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    rc = lib.parasail_b200_nw_banded_certified(matrix, *_pairs_args(qbuf, qoff, qlen, tbuf, toff, tlen), n,
+                                               open_, gap, lo.ctypes.data, hi.ctypes.data, sc.ctypes.data,
+                                               cert.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("banded certified failed")
+    return sc, cert

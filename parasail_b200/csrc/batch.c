@@ -23,7 +23,8 @@ static const struct { const char *name; int alg, sgflags; } g_algs[] = {
 };
 
 /* "[parasail_]ALG[_stats]_{striped,scan}[_profile]_{8,16,32,sat}" -> job.
- * want_profile: 1 profile form required, 0 direct form required. */
+ * want_profile: 1 profile form required, 0 direct form required, -1 either
+ * (both forms of one function return the same results). */
 static int parse_job(const char *funcname, int want_profile, int open, int gap,
                      const parasail_matrix_t *matrix, pb_job *job)
 {
@@ -49,7 +50,7 @@ static int parse_job(const char *funcname, int want_profile, int open, int gap,
     else if (0 == strcmp(s, "_32")) bits = 32;
     else if (0 == strcmp(s, "_sat")) bits = 0;
     else return -1;
-    if (prof != want_profile) return -1;
+    if (want_profile >= 0 && prof != want_profile) return -1;
     memset(job, 0, sizeof *job);
     job->mode.alg = alg; job->mode.sgflags = sgf; job->mode.stats = stats;
     job->mode.striped = striped; job->mode.open = open; job->mode.gap = gap;
@@ -309,5 +310,127 @@ int parasail_b200_batch_db_device(const char *funcname, const parasail_profile_t
     b.d_targets = d_codes; b.d_toff = d_offsets; b.d_tlen = d_lengths;
     rc = pb_cuda_batch_run(&job, &b, (pb_record *)d_records);
     free(profs);
+    return rc;
+}
+
+/* Matrix table on the device for the pairs and all-vs-all batches: vector
+ * orientation, row = target letter (src/memory_avx2.c:113-116). */
+static int32_t *matrix_to_device(const parasail_matrix_t *matrix)
+{
+    int32_t *d_mat = (int32_t *)pb_cuda_malloc(sizeof(int32_t) * (size_t)matrix->size * matrix->size);
+    if (!d_mat) return NULL;
+    if (pb_cuda_h2d(d_mat, matrix->matrix, sizeof(int32_t) * (size_t)matrix->size * matrix->size) != 0) {
+        pb_cuda_free(d_mat);
+        return NULL;
+    }
+    pb_cuda_sync();
+    return d_mat;
+}
+
+static int check_square(const char *func, const parasail_matrix_t *matrix, int n, int open, int gap)
+{
+    if (!matrix) { fprintf(stderr, "%s: missing %s\n", func, "matrix"); return -1; }
+    if (matrix->type != PARASAIL_MATRIX_TYPE_SQUARE) {
+        fprintf(stderr, "%s: this batch needs a square matrix\n", func);
+        return -1;
+    }
+    if (n < 0 || open < 0 || gap < 0) { fprintf(stderr, "%s: invalid n/open/gap\n", func); return -1; }
+    return 0;
+}
+
+int parasail_b200_batch_pairs_device(const char *funcname, const parasail_matrix_t *matrix,
+                                     const uint8_t *d_qcodes, const int64_t *d_qoffsets, const int *d_qlengths,
+                                     const uint8_t *d_tcodes, const int64_t *d_toffsets, const int *d_tlengths,
+                                     int n, int open, int gap, parasail_b200_record_t *d_records)
+{
+    pb_job job;
+    pb_batch b;
+    int32_t *d_mat;
+    int rc;
+    if (check_square(__func__, matrix, n, open, gap) != 0) return -1;
+    if (n == 0) return 0;
+    if (!d_qcodes || !d_qoffsets || !d_qlengths || !d_tcodes || !d_toffsets || !d_tlengths || !d_records) {
+        fprintf(stderr, "%s: missing arrays\n", __func__);
+        return -1;
+    }
+    if (parse_job(funcname, 0, open, gap, matrix, &job) != 0) {
+        fprintf(stderr, "%s: unknown function '%s'\n", __func__, funcname ? funcname : "(null)");
+        return -1;
+    }
+    if (!pb_gpu_ready(__func__)) return -1;
+    if (!(d_mat = matrix_to_device(matrix))) return -1;
+    memset(&b, 0, sizeof b);
+    b.alg = job.mode.alg; b.sgflags = job.mode.sgflags; b.stats = job.mode.stats;
+    b.open = open; b.gap = gap; b.nprofs = 0; b.npairs = n;
+    b.d_mat = d_mat; b.msize = matrix->size; b.mmax = matrix->max; b.mmin = matrix->min;
+    b.d_qall = d_qcodes; b.d_qoff = d_qoffsets; b.d_qlen = d_qlengths;
+    b.d_targets = d_tcodes; b.d_toff = d_toffsets; b.d_tlen = d_tlengths;
+    rc = pb_cuda_batch_run(&job, &b, (pb_record *)d_records);
+    if (rc != 0) fprintf(stderr, "%s: GPU alignment failed: %s\n", __func__, pb_cuda_last_error());
+    pb_cuda_free(d_mat);
+    pb_cuda_sync();
+    return rc;
+}
+
+/* All-vs-all: the upper triangle of n sequences, pair p = (i, j), i < j,
+ * in row-major order, query i (the profile side) against target j. */
+static int all_common(const char *func, const char *funcname, const parasail_matrix_t *matrix, int n,
+                      int open, int gap, pb_job *job, pb_batch *b, int32_t **d_mat)
+{
+    if (check_square(func, matrix, n, open, gap) != 0) return -1;
+    if ((long long)n * (n - 1) / 2 > 0x7fffffffLL) {
+        fprintf(stderr, "%s: %d sequences give more than 2^31 - 1 pairs\n", func, n);
+        return -1;
+    }
+    if (parse_job(funcname, -1, open, gap, matrix, job) != 0) {
+        fprintf(stderr, "%s: unknown function '%s'\n", func, funcname ? funcname : "(null)");
+        return -1;
+    }
+    if (!pb_gpu_ready(func)) return -1;
+    if (!(*d_mat = matrix_to_device(matrix))) return -1;
+    memset(b, 0, sizeof *b);
+    b->alg = job->mode.alg; b->sgflags = job->mode.sgflags; b->stats = job->mode.stats;
+    b->open = open; b->gap = gap; b->nprofs = 0;
+    b->d_mat = *d_mat; b->msize = matrix->size; b->mmax = matrix->max; b->mmin = matrix->min;
+    return 0;
+}
+
+int parasail_b200_batch_all(const char *funcname, const parasail_matrix_t *matrix,
+                            const char *seqs, const int64_t *offsets, const int *lengths, int n,
+                            int open, int gap, parasail_b200_record_t *records)
+{
+    pb_job job;
+    pb_batch b;
+    int32_t *d_mat = NULL;
+    uint8_t map[256];
+    int i, rc;
+    if (n < 2) return 0;
+    if (!seqs || !offsets || !lengths || !records) { fprintf(stderr, "%s: missing arrays\n", __func__); return -1; }
+    for (i = 0; i < n; ++i)
+        if (lengths[i] <= 0) { fprintf(stderr, "%s: lengths[%d] must be > 0\n", __func__, i); return -1; }
+    if (all_common(__func__, funcname, matrix, n, open, gap, &job, &b, &d_mat) != 0) return -1;
+    mapper_bytes(matrix, map);
+    rc = pb_cuda_batch_all_host(&job, &b, map, seqs, offsets, lengths, n, (pb_record *)records);
+    if (rc != 0) fprintf(stderr, "%s: GPU alignment failed: %s\n", __func__, pb_cuda_last_error());
+    pb_cuda_free(d_mat);
+    pb_cuda_sync();
+    return rc;
+}
+
+int parasail_b200_batch_all_device(const char *funcname, const parasail_matrix_t *matrix,
+                                   const uint8_t *d_codes, const int64_t *d_offsets, const int *d_lengths,
+                                   int n, int open, int gap, parasail_b200_record_t *d_records)
+{
+    pb_job job;
+    pb_batch b;
+    int32_t *d_mat = NULL;
+    int rc;
+    if (n < 2) return 0;
+    if (!d_codes || !d_offsets || !d_lengths || !d_records) { fprintf(stderr, "%s: missing arrays\n", __func__); return -1; }
+    if (all_common(__func__, funcname, matrix, n, open, gap, &job, &b, &d_mat) != 0) return -1;
+    rc = pb_cuda_batch_all(&job, &b, d_codes, d_offsets, d_lengths, n, (pb_record *)d_records);
+    if (rc != 0) fprintf(stderr, "%s: GPU alignment failed: %s\n", __func__, pb_cuda_last_error());
+    pb_cuda_free(d_mat);
+    pb_cuda_sync();
     return rc;
 }

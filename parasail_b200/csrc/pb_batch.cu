@@ -85,7 +85,9 @@ __global__ void k_prefix_limits(pb_job job, const pb_pair_out *__restrict__ o1, 
  * width). `la` describes the query side (profile or matrix mode) and the
  * targets. Work memory: from `work` (work_bytes, 256-byte aligned) when
  * given, otherwise from the stream's pool. Synchronises the stream once per
- * round.
+ * round. Returns 0; -1 on a device error; -2 when `work` is smaller than
+ * the lists and results; -3 when what `work` has left after them does not
+ * hold one warp's lane-exact arrays.
  */
 int resolve_rounds(const pb_job &job, const pb_lane_args &la, const pb_pair_out *o1, const pb_pair_out *o2,
                    const int *qlen, int qlen_all, const int *tlen, int n, pb_record *rec, cudaStream_t st,
@@ -142,9 +144,11 @@ int resolve_rounds(const pb_job &job, const pb_lane_args &la, const pb_pair_out 
         a.sgflags = job.mode.sgflags;
         a.open = job.mode.open; a.gap = job.mode.gap;
         for (int t = 0; t < 3 && rc == 0; ++t)
-            if (hc[t] && pb_cuda_lane_run(w3[t], &a, lists[cur] + (size_t)t * n, hc[t], res, lane_scratch,
-                                          lane_bytes, st) != 0)
-                rc = -1;
+            if (hc[t]) {
+                const int lr = pb_cuda_lane_run(w3[t], &a, lists[cur] + (size_t)t * n, hc[t], res, lane_scratch,
+                                                lane_bytes, st);
+                if (lr != 0) rc = lr == -3 ? -3 : -1;
+            }
         if (rc) break;
         const int nxt = cur ^ 1;
         cudaMemsetAsync(counts, 0, 3 * sizeof(int), st);
@@ -189,23 +193,31 @@ extern "C" int pb_cuda_batch_run(const pb_job *job, const pb_batch *tmpl, pb_rec
     if (n <= 0) return 0;
     const pb_mode *m = &job->mode;
     const int nq = tmpl->nprofs > 0 ? tmpl->nprofs : 1;   /* pairs mode: one "query set" */
+    const size_t nitems = (size_t)n * nq;
     cudaStream_t st = nullptr;
-    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return -1;
     pb_pair_out *o1 = nullptr, *o2 = nullptr;
     int *qlim = nullptr, *tlim = nullptr;
     int rc = 0;
-    cudaMallocAsync((void **)&o1, sizeof(pb_pair_out) * n * (size_t)nq, st);
-    cudaStreamSynchronize(st);
-    const bool sw_score = m->alg == PB_SW && (!m->stats || pb_job_is_faststats(job)) && job->bits >= 0;
-    if (sw_score && tmpl->nprofs >= 1) {
+    /* every buffer is checked before any launch that would write through it */
+    if (cudaMallocAsync((void **)&o1, sizeof(pb_pair_out) * nitems, st) != cudaSuccess) rc = -1;
+    const bool faststats = pb_job_is_faststats(job);
+    if (rc == 0 && faststats &&
+        (cudaMallocAsync((void **)&o2, sizeof(pb_pair_out) * nitems, st) != cudaSuccess ||
+         cudaMallocAsync((void **)&qlim, sizeof(int) * nitems, st) != cudaSuccess ||
+         cudaMallocAsync((void **)&tlim, sizeof(int) * nitems, st) != cudaSuccess))
+        rc = -1;
+    if (rc == 0 && cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
+    const bool sw_score = m->alg == PB_SW && (!m->stats || faststats) && job->bits >= 0;
+    if (rc == 0 && sw_score && tmpl->nprofs >= 1) {
         pb_batch b = *tmpl;
         b.stats = 0;
         b.pad_rows = 0;
         b.d_qlim = nullptr;
         b.d_tlim = nullptr;
         rc = pb_cuda_align_sw16_multi(&b, o1);
-    } else if (tmpl->nprofs >= 1) {
-        /* every query against every target in one launch */
+    } else if (rc == 0) {
+        /* every query against every target (or every pair) in one launch */
         pb_batch b = *tmpl;
         b.d_out = o1;
         b.d_qlim = nullptr;
@@ -213,50 +225,21 @@ extern "C" int pb_cuda_batch_run(const pb_job *job, const pb_batch *tmpl, pb_rec
         b.stats = sw_score ? 0 : m->stats;
         b.pad_rows = (job->bits < 0 || (m->alg == PB_SW && !m->stats)) ? 0
                    : (job->bits == 0 || job->bits == 8) ? 32 : job->bits == 16 ? 16 : 8;
-        rc = pb_cuda_align_exact_db(&b);
-    } else {
-        pb_batch b = *tmpl;
-        b.d_out = o1;
-        b.d_qlim = nullptr;
-        b.d_tlim = nullptr;
-        b.stats = sw_score ? 0 : m->stats;
-        b.pad_rows = (job->bits < 0 || (m->alg == PB_SW && !m->stats)) ? 0
-                   : (job->bits == 0 || job->bits == 8) ? 32 : job->bits == 16 ? 16 : 8;
-        rc = pb_cuda_align_exact(&b);
+        rc = tmpl->nprofs >= 1 ? pb_cuda_align_exact_db(&b) : pb_cuda_align_exact(&b);
     }
-    if (rc == 0 && pb_job_is_faststats(job) && tmpl->nprofs >= 1) {
-        /* the prefix statistics pass of every query in one launch: limits
+    if (rc == 0 && faststats) {
+        /* the prefix statistics pass of every item in one launch: limits
          * per (query, target) item, query-major like o1 */
-        cudaMallocAsync((void **)&o2, sizeof(pb_pair_out) * n * (size_t)nq, st);
-        cudaMallocAsync((void **)&qlim, sizeof(int) * n * (size_t)nq, st);
-        cudaMallocAsync((void **)&tlim, sizeof(int) * n * (size_t)nq, st);
-        pb::k_prefix_limits<<<(int)(((size_t)n * nq + 255) / 256), 256, 0, st>>>(*job, o1, n * nq, qlim, tlim);
+        pb::k_prefix_limits<<<(int)((nitems + 255) / 256), 256, 0, st>>>(*job, o1, (int)nitems, qlim, tlim);
         pb_diag_count_launch(1);
-        cudaStreamSynchronize(st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
         pb_batch b2 = *tmpl;
         b2.stats = 1;
         b2.pad_rows = 32;
         b2.d_qlim = qlim;
         b2.d_tlim = tlim;
         b2.d_out = o2;
-        rc = pb_cuda_align_exact_db(&b2);
-    } else if (rc == 0 && pb_job_is_faststats(job)) {
-        cudaMallocAsync((void **)&o2, sizeof(pb_pair_out) * n * (size_t)nq, st);
-        cudaMallocAsync((void **)&qlim, sizeof(int) * n, st);
-        cudaMallocAsync((void **)&tlim, sizeof(int) * n, st);
-        for (int q = 0; q < nq && rc == 0; ++q) {
-            pb::k_prefix_limits<<<(n + 255) / 256, 256, 0, st>>>(*job, o1 + (size_t)q * n, n, qlim, tlim);
-            pb_diag_count_launch(1);
-            cudaStreamSynchronize(st);
-            pb_batch b2 = *tmpl;
-            if (tmpl->nprofs > 0) { b2.profs = &tmpl->profs[q]; b2.nprofs = 1; }
-            b2.stats = 1;
-            b2.pad_rows = 32;
-            b2.d_qlim = qlim;
-            b2.d_tlim = tlim;
-            b2.d_out = o2 + (size_t)q * n;
-            rc = pb_cuda_align_exact(&b2);
-        }
+        if (rc == 0) rc = tmpl->nprofs >= 1 ? pb_cuda_align_exact_db(&b2) : pb_cuda_align_exact(&b2);
     }
     for (int q = 0; q < nq && rc == 0; ++q) {
         const int qall = tmpl->nprofs > 0 ? tmpl->profs[q]->qlen : 0;
@@ -265,7 +248,7 @@ extern "C" int pb_cuda_batch_run(const pb_job *job, const pb_batch *tmpl, pb_rec
                                 tmpl->nprofs > 0 ? nullptr : tmpl->d_qlen, qall, tmpl->d_tlen, n,
                                 d_rec + (size_t)q * n, st, nullptr, 0);
     }
-    cudaFreeAsync(o1, st);
+    if (o1) cudaFreeAsync(o1, st);
     if (o2) cudaFreeAsync(o2, st);
     if (qlim) cudaFreeAsync(qlim, st);
     if (tlim) cudaFreeAsync(tlim, st);
@@ -299,7 +282,7 @@ extern "C" int pb_cuda_batch_host(const pb_job *job, const pb_batch *tmpl, const
     if (pb_cuda_init() != 0) return -1;
     if (n <= 0) return 0;
     cudaStream_t st = nullptr;
-    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return -1;
     int64_t tbytes = 0, qbytes = 0;
     for (int i = 0; i < n; ++i) {
         const int64_t e = h_toff[i] + h_tlen[i];
@@ -315,28 +298,33 @@ extern "C" int pb_cuda_batch_host(const pb_job *job, const pb_batch *tmpl, const
     pb_record *d_rec = nullptr;
     int rc = 0;
     const int nq = tmpl->nprofs > 0 ? tmpl->nprofs : 1;
-    cudaMallocAsync((void **)&d_t, tbytes + 16, st);
-    cudaMallocAsync((void **)&d_toff, sizeof(int64_t) * n, st);
-    cudaMallocAsync((void **)&d_tlen, sizeof(int) * n, st);
-    cudaMallocAsync((void **)&d_map, 256, st);
-    cudaMallocAsync((void **)&d_rec, sizeof(pb_record) * n * (size_t)nq, st);
-    cudaMemcpyAsync(d_t, h_targets, tbytes, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(d_toff, h_toff, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(d_tlen, h_tlen, sizeof(int) * n, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(d_map, mapper256, 256, cudaMemcpyHostToDevice, st);
-    k_map_codes<<<296, 256, 0, st>>>(d_t, tbytes, d_map);
-    pb_diag_count_launch(1);
-    if (h_queries) {
-        cudaMallocAsync((void **)&d_q, qbytes + 16, st);
-        cudaMallocAsync((void **)&d_qoff, sizeof(int64_t) * n, st);
-        cudaMallocAsync((void **)&d_qlen, sizeof(int) * n, st);
-        cudaMemcpyAsync(d_q, h_queries, qbytes, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(d_qoff, h_qoff, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(d_qlen, h_qlen, sizeof(int) * n, cudaMemcpyHostToDevice, st);
-        k_map_codes<<<296, 256, 0, st>>>(d_q, qbytes, d_map);
+    if (cudaMallocAsync((void **)&d_t, tbytes + 16, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_toff, sizeof(int64_t) * n, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_tlen, sizeof(int) * n, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_map, 256, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_rec, sizeof(pb_record) * n * (size_t)nq, st) != cudaSuccess)
+        rc = -1;
+    if (rc == 0 && h_queries &&
+        (cudaMallocAsync((void **)&d_q, qbytes + 16, st) != cudaSuccess ||
+         cudaMallocAsync((void **)&d_qoff, sizeof(int64_t) * n, st) != cudaSuccess ||
+         cudaMallocAsync((void **)&d_qlen, sizeof(int) * n, st) != cudaSuccess))
+        rc = -1;
+    if (rc == 0) {
+        cudaMemcpyAsync(d_t, h_targets, tbytes, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_toff, h_toff, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_tlen, h_tlen, sizeof(int) * n, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_map, mapper256, 256, cudaMemcpyHostToDevice, st);
+        k_map_codes<<<296, 256, 0, st>>>(d_t, tbytes, d_map);
         pb_diag_count_launch(1);
+        if (h_queries) {
+            cudaMemcpyAsync(d_q, h_queries, qbytes, cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(d_qoff, h_qoff, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(d_qlen, h_qlen, sizeof(int) * n, cudaMemcpyHostToDevice, st);
+            k_map_codes<<<296, 256, 0, st>>>(d_q, qbytes, d_map);
+            pb_diag_count_launch(1);
+        }
+        if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
     }
-    if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
     if (rc == 0) {
         pb_batch b = *tmpl;
         b.npairs = n;
@@ -346,9 +334,120 @@ extern "C" int pb_cuda_batch_host(const pb_job *job, const pb_batch *tmpl, const
     }
     if (rc == 0 && cudaMemcpyAsync(h_rec, d_rec, sizeof(pb_record) * n * (size_t)nq, cudaMemcpyDeviceToHost, st) != cudaSuccess)
         rc = -1;
-    cudaFreeAsync(d_t, st); cudaFreeAsync(d_toff, st); cudaFreeAsync(d_tlen, st);
-    cudaFreeAsync(d_map, st); cudaFreeAsync(d_rec, st);
-    if (d_q) { cudaFreeAsync(d_q, st); cudaFreeAsync(d_qoff, st); cudaFreeAsync(d_qlen, st); }
+    if (d_t) cudaFreeAsync(d_t, st);
+    if (d_toff) cudaFreeAsync(d_toff, st);
+    if (d_tlen) cudaFreeAsync(d_tlen, st);
+    if (d_map) cudaFreeAsync(d_map, st);
+    if (d_rec) cudaFreeAsync(d_rec, st);
+    if (d_q) cudaFreeAsync(d_q, st);
+    if (d_qoff) cudaFreeAsync(d_qoff, st);
+    if (d_qlen) cudaFreeAsync(d_qlen, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
+    cudaStreamDestroy(st);
+    return rc;
+}
+
+namespace {
+
+/* pair p of the upper triangle of n sequences -> (i, j), i < j, row-major:
+ * row i starts at i*n - i*(i+1)/2 */
+__global__ void k_all_pairs(const int64_t *__restrict__ off, const int *__restrict__ len, int n, int npairs,
+                            int64_t *__restrict__ qoff, int *__restrict__ qlen, int64_t *__restrict__ toff,
+                            int *__restrict__ tlen)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const int64_t N = n;
+    int lo = 0, hi = n - 2;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((int64_t)mid * N - (int64_t)mid * (mid + 1) / 2 <= p) lo = mid; else hi = mid - 1;
+    }
+    const int i = lo;
+    const int j = i + 1 + (int)(p - ((int64_t)i * N - (int64_t)i * (i + 1) / 2));
+    qoff[p] = off[i]; qlen[p] = len[i];
+    toff[p] = off[j]; tlen[p] = len[j];
+}
+
+}  // namespace
+
+extern "C" int pb_cuda_batch_all(const pb_job *job, const pb_batch *tmpl, const uint8_t *d_codes,
+                                 const int64_t *d_off, const int *d_len, int n, pb_record *d_rec)
+{
+    if (pb_cuda_init() != 0) return -1;
+    if (n < 2) return 0;
+    const int npairs = (int)((int64_t)n * (n - 1) / 2);
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    int64_t *qoff = nullptr, *toff = nullptr;
+    int *qlen = nullptr, *tlen = nullptr;
+    int rc = 0;
+    if (cudaMallocAsync((void **)&qoff, sizeof(int64_t) * npairs, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&toff, sizeof(int64_t) * npairs, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&qlen, sizeof(int) * npairs, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&tlen, sizeof(int) * npairs, st) != cudaSuccess)
+        rc = -1;
+    if (rc == 0) {
+        k_all_pairs<<<(npairs + 255) / 256, 256, 0, st>>>(d_off, d_len, n, npairs, qoff, qlen, toff, tlen);
+        pb_diag_count_launch(1);
+        if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
+    }
+    if (rc == 0) {
+        pb_batch b = *tmpl;
+        b.nprofs = 0;
+        b.npairs = npairs;
+        b.d_qall = d_codes; b.d_qoff = qoff; b.d_qlen = qlen;
+        b.d_targets = d_codes; b.d_toff = toff; b.d_tlen = tlen;
+        rc = pb_cuda_batch_run(job, &b, d_rec);
+    }
+    if (qoff) cudaFreeAsync(qoff, st);
+    if (toff) cudaFreeAsync(toff, st);
+    if (qlen) cudaFreeAsync(qlen, st);
+    if (tlen) cudaFreeAsync(tlen, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
+    cudaStreamDestroy(st);
+    return rc;
+}
+
+extern "C" int pb_cuda_batch_all_host(const pb_job *job, const pb_batch *tmpl, const uint8_t *mapper256,
+                                      const char *h_seqs, const int64_t *h_off, const int *h_len, int n,
+                                      pb_record *h_rec)
+{
+    if (pb_cuda_init() != 0) return -1;
+    if (n < 2) return 0;
+    const size_t npairs = (size_t)n * (n - 1) / 2;
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    int64_t bytes = 0;
+    for (int i = 0; i < n; ++i) bytes = h_off[i] + h_len[i] > bytes ? h_off[i] + h_len[i] : bytes;
+    uint8_t *d_s = nullptr, *d_map = nullptr;
+    int64_t *d_off = nullptr;
+    int *d_len = nullptr;
+    pb_record *d_rec = nullptr;
+    int rc = 0;
+    if (cudaMallocAsync((void **)&d_s, bytes + 16, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_off, sizeof(int64_t) * n, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_len, sizeof(int) * n, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_map, 256, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_rec, sizeof(pb_record) * npairs, st) != cudaSuccess)
+        rc = -1;
+    if (rc == 0) {
+        cudaMemcpyAsync(d_s, h_seqs, bytes, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_off, h_off, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_len, h_len, sizeof(int) * n, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_map, mapper256, 256, cudaMemcpyHostToDevice, st);
+        k_map_codes<<<296, 256, 0, st>>>(d_s, bytes, d_map);
+        pb_diag_count_launch(1);
+        if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
+    }
+    if (rc == 0) rc = pb_cuda_batch_all(job, tmpl, d_s, d_off, d_len, n, d_rec);
+    if (rc == 0 && cudaMemcpyAsync(h_rec, d_rec, sizeof(pb_record) * npairs, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        rc = -1;
+    if (d_s) cudaFreeAsync(d_s, st);
+    if (d_off) cudaFreeAsync(d_off, st);
+    if (d_len) cudaFreeAsync(d_len, st);
+    if (d_map) cudaFreeAsync(d_map, st);
+    if (d_rec) cudaFreeAsync(d_rec, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
     cudaStreamDestroy(st);
     return rc;

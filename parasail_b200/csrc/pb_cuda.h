@@ -146,6 +146,17 @@ int pb_cuda_batch_host(const struct pb_job *job, const pb_batch *tmpl, const uin
                        const char *h_queries, const int64_t *h_qoff, const int *h_qlen,
                        int n, struct pb_record *h_rec);
 
+/* All-vs-all: the upper triangle of n device-resident sequences (codes),
+ * pair p = (i, j), i < j, row-major, query i against target j, run as a
+ * pairs batch (tmpl in pairs mode: matrix table set, queries unset);
+ * d_rec receives n(n-1)/2 records. The host form copies and maps the
+ * characters first and copies the records back. */
+int pb_cuda_batch_all(const struct pb_job *job, const pb_batch *tmpl, const uint8_t *d_codes,
+                      const int64_t *d_off, const int *d_len, int n, struct pb_record *d_rec);
+int pb_cuda_batch_all_host(const struct pb_job *job, const pb_batch *tmpl, const uint8_t *mapper256,
+                           const char *h_seqs, const int64_t *h_off, const int *h_len, int n,
+                           struct pb_record *h_rec);
+
 /* Lane-exact emulation of the reference's 8/16-bit striped kernels
  * (pb_lane.cu) for the pairs listed in d_list. kind: 0 nw/sg score-only,
  * 1 nw/sg with statistics, 2 the SW statistics kernel on the FASTSTATS prefix
@@ -167,7 +178,9 @@ typedef struct pb_lane_args {
 
 /* scratch: NULL to allocate from the stream's pool, else at least
  * pb_cuda_lane_scratch_per_warp bytes (fewer warps run when it is small).
- * stream: a cudaStream_t. Asynchronous. */
+ * stream: a cudaStream_t. Asynchronous. Returns 0, -1 on a device error or
+ * invalid arguments, -3 when the given scratch is smaller than one warp's
+ * arrays. */
 int pb_cuda_lane_run(int bits, const pb_lane_args *a, const int *d_list, int nlist, pb_lane_res *d_res,
                      void *scratch, size_t scratch_bytes, void *stream);
 size_t pb_cuda_lane_scratch_per_warp(int bits, int kind, int max_qlen);

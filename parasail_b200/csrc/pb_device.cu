@@ -46,6 +46,37 @@ cudaStream_t stream()
     return g_stream;
 }
 
+/* A second stream and an event per host thread, for work that runs beside
+ * the thread's main stream; created once and kept. */
+thread_local cudaStream_t g_stream2 = nullptr;
+thread_local cudaEvent_t g_event2 = nullptr;
+
+int side_stream(cudaStream_t *st2, cudaEvent_t *ev)
+{
+    if (!g_stream2 && cudaStreamCreateWithFlags(&g_stream2, cudaStreamNonBlocking) != cudaSuccess) {
+        g_stream2 = nullptr;
+        return -1;
+    }
+    if (!g_event2 && cudaEventCreateWithFlags(&g_event2, cudaEventDisableTiming) != cudaSuccess) {
+        g_event2 = nullptr;
+        return -1;
+    }
+    *st2 = g_stream2;
+    *ev = g_event2;
+    return 0;
+}
+
+/* Stream-ordered frees of a call's pool allocations, on every return path
+ * (an early error return included). */
+struct PoolFrees {
+    cudaStream_t st;
+    void *p[16];
+    int n = 0;
+    explicit PoolFrees(cudaStream_t s) : st(s) {}
+    template <typename T> T *add(T *q) { if (q && n < 16) p[n++] = (void *)q; return q; }
+    ~PoolFrees() { for (int k = 0; k < n; ++k) cudaFreeAsync(p[k], st); }
+};
+
 void do_init()
 {
     int n = 0;
@@ -287,15 +318,19 @@ int pb_cuda_align_exact(const pb_batch *b)
     if (pb_cuda_init() != 0) return -1;
     if (b->npairs <= 0) return 0;
     cudaStream_t st = stream();
+    PoolFrees frees(st);
     const int nv = b->stats ? 8 : 2;
     int64_t *sizes = nullptr, *soff = nullptr;
     void *tmp = nullptr;
     size_t tmp_bytes = 0;
     CK(cudaMallocAsync((void **)&sizes, sizeof(int64_t) * b->npairs, st));
+    frees.add(sizes);
     CK(cudaMallocAsync((void **)&soff, sizeof(int64_t) * b->npairs, st));
+    frees.add(soff);
     k_scratch_sizes<<<(b->npairs + 255) / 256, 256, 0, st>>>(b->d_tlen, b->d_tlim, b->npairs, nv, sizes);
     cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, sizes, soff, b->npairs, st);
     CK(cudaMallocAsync(&tmp, tmp_bytes, st));
+    frees.add(tmp);
     cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, sizes, soff, b->npairs, st);
     int64_t last_off = 0, last_size = 0;
     CK(cudaMemcpyAsync(&last_off, soff + b->npairs - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
@@ -303,9 +338,10 @@ int pb_cuda_align_exact(const pb_batch *b)
     CK(cudaStreamSynchronize(st));
     int *scratch = nullptr;
     CK(cudaMallocAsync((void **)&scratch, sizeof(int) * (size_t)(last_off + last_size + 1), st));
+    frees.add(scratch);
     pb::ProfDesc *d_profs = nullptr;
     if (b->nprofs > 0) {
-        d_profs = upload_profs(b, st);
+        d_profs = frees.add(upload_profs(b, st));
         if (!d_profs) { snprintf(g_err, sizeof g_err, "profile descriptor upload failed"); return -1; }
     }
 
@@ -320,11 +356,6 @@ int pb_cuda_align_exact(const pb_batch *b)
     pb::launch_exact(p, b->alg, b->stats != 0, st);
     pb_diag_count_launch(2);   /* k_scratch_sizes, k_exact */
     CK(cudaGetLastError());
-    cudaFreeAsync(scratch, st);
-    cudaFreeAsync(tmp, st);
-    cudaFreeAsync(sizes, st);
-    cudaFreeAsync(soff, st);
-    if (d_profs) cudaFreeAsync(d_profs, st);
     CK(cudaStreamSynchronize(st));
     return 0;
 }
@@ -352,14 +383,23 @@ int pb_cuda_align_exact_db(const pb_batch *b)
     size_t tmp_bytes = 0, stmp_bytes = 0;
     std::vector<int> hq(nq);
     for (int q = 0; q < nq; ++q) hq[q] = b->profs[q]->qlen;
+    PoolFrees frees(st);
     CK(cudaMallocAsync((void **)&sizes, sizeof(int64_t) * N, st));
+    frees.add(sizes);
     CK(cudaMallocAsync((void **)&soff, sizeof(int64_t) * N, st));
+    frees.add(soff);
     CK(cudaMallocAsync((void **)&keys, sizeof(unsigned long long) * N, st));
+    frees.add(keys);
     CK(cudaMallocAsync((void **)&keys_sorted, sizeof(unsigned long long) * N, st));
+    frees.add(keys_sorted);
     CK(cudaMallocAsync((void **)&idx, sizeof(int) * N, st));
+    frees.add(idx);
     CK(cudaMallocAsync((void **)&order, sizeof(int) * N, st));
+    frees.add(order);
     CK(cudaMallocAsync((void **)&d_qlens, sizeof(int) * nq, st));
+    frees.add(d_qlens);
     CK(cudaMallocAsync((void **)&d_nwarp, sizeof(int), st));
+    frees.add(d_nwarp);
     CK(cudaMemcpyAsync(d_qlens, hq.data(), sizeof(int) * nq, cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(d_nwarp, 0, sizeof(int), st));
     /* pairs go one per warp (k_exact_db_items) */
@@ -369,7 +409,9 @@ int pb_cuda_align_exact_db(const pb_batch *b)
     cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, sizes, soff, N, st);
     cub::DeviceRadixSort::SortPairsDescending(nullptr, stmp_bytes, keys, keys_sorted, idx, order, N, 0, 64, st);
     CK(cudaMallocAsync(&tmp, tmp_bytes, st));
+    frees.add(tmp);
     CK(cudaMallocAsync(&stmp, stmp_bytes, st));
+    frees.add(stmp);
     cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, sizes, soff, N, st);
     cub::DeviceRadixSort::SortPairsDescending(stmp, stmp_bytes, keys, keys_sorted, idx, order, N, 0, 64, st);
     int64_t last_off = 0, last_size = 0;
@@ -380,7 +422,8 @@ int pb_cuda_align_exact_db(const pb_batch *b)
     CK(cudaStreamSynchronize(st));
     int *scratch = nullptr;
     CK(cudaMallocAsync((void **)&scratch, sizeof(int) * (size_t)(last_off + last_size + 1), st));
-    pb::ProfDesc *d_profs = upload_profs(b, st);
+    frees.add(scratch);
+    pb::ProfDesc *d_profs = frees.add(upload_profs(b, st));
     if (!d_profs) { snprintf(g_err, sizeof g_err, "profile descriptor upload failed"); return -1; }
 
     pb::ExactParams p;
@@ -392,13 +435,12 @@ int pb_cuda_align_exact_db(const pb_batch *b)
     p.scratch = scratch; p.soff = soff; p.out = b->d_out;
     p.mat = nullptr; p.msize = 0; p.qall = nullptr; p.qoff = nullptr; p.qlen = nullptr;
     p.order = order; p.nt = n;
-    /* the warp-per-pair items (sorted first) on a second stream, the rest
-     * one per thread beside them */
+    /* the warp-per-pair items (sorted first) on the thread's side stream,
+     * the rest one per thread beside them */
     cudaStream_t st2 = nullptr;
     cudaEvent_t ev = nullptr;
     if (nwarp > 0) {
-        CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
-        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        if (side_stream(&st2, &ev) != 0) { snprintf(g_err, sizeof g_err, "side stream creation failed"); return -1; }
         CK(cudaEventRecord(ev, st));
         CK(cudaStreamWaitEvent(st2, ev, 0));
         pb::launch_exact_warp(p, b->alg, b->stats != 0, nwarp, st2);
@@ -417,15 +459,7 @@ int pb_cuda_align_exact_db(const pb_batch *b)
     }
     pb_diag_count_launch(1);   /* k_exact_db_items (plus the library scan and sort) */
     CK(cudaGetLastError());
-    cudaFreeAsync(scratch, st);
-    cudaFreeAsync(tmp, st); cudaFreeAsync(stmp, st);
-    cudaFreeAsync(sizes, st); cudaFreeAsync(soff, st);
-    cudaFreeAsync(keys, st); cudaFreeAsync(keys_sorted, st);
-    cudaFreeAsync(idx, st); cudaFreeAsync(order, st); cudaFreeAsync(d_qlens, st); cudaFreeAsync(d_nwarp, st);
-    cudaFreeAsync(d_profs, st);
     CK(cudaStreamSynchronize(st));
-    if (st2) cudaStreamDestroy(st2);
-    if (ev) cudaEventDestroy(ev);
     return 0;
 }
 

@@ -201,7 +201,7 @@ int pb_cuda_lane_run(int bits, const pb_lane_args *a, const int *d_list, int nli
     bool own = false;
     if (scratch) {
         const long long fit = (long long)(scratch_bytes / per_warp);
-        if (fit < 1) return -1;
+        if (fit < 1) return -3;   /* the given scratch does not hold one warp's arrays */
         if (warps > fit) warps = fit;
     }
     if (warps >= wpb) {

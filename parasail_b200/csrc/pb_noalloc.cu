@@ -184,6 +184,18 @@ int pb_cuda_noalloc_run(const pb_job *job, const pb_batch *b, pb_record *d_rec)
                      "%d pairs need more resolution work space than the static scratch has left", n);
             return -1;
         }
+        if (rr == -3) {
+            size_t need = 0;
+            for (int w = 8; w <= 32; w *= 2) {
+                const size_t x = pb_cuda_lane_scratch_per_warp(w, pb_lane_kind(&job->mode), prof->qlen);
+                need = x > need ? x : need;
+            }
+            snprintf(g_noalloc_err, sizeof g_noalloc_err,
+                     "the lane-exact kernel needs up to %zu bytes per warp for this query (%d rows), more than the "
+                     "%zu bytes of static scratch left after the batch's other regions",
+                     need, prof->qlen, (size_t)PB_NOALLOC_SCRATCH_BYTES - off_strip);
+            return -1;
+        }
         if (rr != 0) goto fail;
     }
     if (cudaGetLastError() != cudaSuccess) goto fail;
