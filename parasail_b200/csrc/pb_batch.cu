@@ -202,13 +202,16 @@ extern "C" int pb_cuda_batch_run(const pb_job *job, const pb_batch *tmpl, pb_rec
     /* every buffer is checked before any launch that would write through it */
     if (cudaMallocAsync((void **)&o1, sizeof(pb_pair_out) * nitems, st) != cudaSuccess) rc = -1;
     const bool faststats = pb_job_is_faststats(job);
+    int *rest = nullptr;      /* items the 16-bit pair kernels leave to the exact kernel */
     if (rc == 0 && faststats &&
         (cudaMallocAsync((void **)&o2, sizeof(pb_pair_out) * nitems, st) != cudaSuccess ||
          cudaMallocAsync((void **)&qlim, sizeof(int) * nitems, st) != cudaSuccess ||
          cudaMallocAsync((void **)&tlim, sizeof(int) * nitems, st) != cudaSuccess))
         rc = -1;
+    if (rc == 0 && cudaMallocAsync((void **)&rest, sizeof(int) * nitems, st) != cudaSuccess) rc = -1;
     if (rc == 0 && cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
     const bool sw_score = m->alg == PB_SW && (!m->stats || faststats) && job->bits >= 0;
+    const int *group = tmpl->nprofs > 0 ? nullptr : tmpl->d_qgroup;
     if (rc == 0 && sw_score && tmpl->nprofs >= 1) {
         pb_batch b = *tmpl;
         b.stats = 0;
@@ -217,7 +220,9 @@ extern "C" int pb_cuda_batch_run(const pb_job *job, const pb_batch *tmpl, pb_rec
         b.d_tlim = nullptr;
         rc = pb_cuda_align_sw16_multi(&b, o1);
     } else if (rc == 0) {
-        /* every query against every target (or every pair) in one launch */
+        /* every item on the int16x2 pair kernels where the 16-bit bounds
+         * hold, the rest (and items whose width verdicts need exact
+         * extremes) on the exact kernel */
         pb_batch b = *tmpl;
         b.d_out = o1;
         b.d_qlim = nullptr;
@@ -225,11 +230,14 @@ extern "C" int pb_cuda_batch_run(const pb_job *job, const pb_batch *tmpl, pb_rec
         b.stats = sw_score ? 0 : m->stats;
         b.pad_rows = (job->bits < 0 || (m->alg == PB_SW && !m->stats)) ? 0
                    : (job->bits == 0 || job->bits == 8) ? 32 : job->bits == 16 ? 16 : 8;
-        rc = tmpl->nprofs >= 1 ? pb_cuda_align_exact_db(&b) : pb_cuda_align_exact(&b);
+        int nrest = 0;
+        rc = pb::p16_pass(*job, &b, 0, nullptr, o1, group, rest, &nrest, st);
+        if (rc == 0 && nrest > 0) rc = pb::exact_subset(&b, rest, nrest, b.stats, b.pad_rows, o1, st);
     }
     if (rc == 0 && faststats) {
-        /* the prefix statistics pass of every item in one launch: limits
-         * per (query, target) item, query-major like o1 */
+        /* the prefix statistics pass of every item: limits per (query,
+         * target) item, query-major like o1; statistics by the direction-bit
+         * walk from the score pass's ends */
         pb::k_prefix_limits<<<(int)((nitems + 255) / 256), 256, 0, st>>>(*job, o1, (int)nitems, qlim, tlim);
         pb_diag_count_launch(1);
         if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
@@ -239,7 +247,9 @@ extern "C" int pb_cuda_batch_run(const pb_job *job, const pb_batch *tmpl, pb_rec
         b2.d_qlim = qlim;
         b2.d_tlim = tlim;
         b2.d_out = o2;
-        if (rc == 0) rc = tmpl->nprofs >= 1 ? pb_cuda_align_exact_db(&b2) : pb_cuda_align_exact(&b2);
+        int nrest = 0;
+        if (rc == 0) rc = pb::p16_pass(*job, &b2, 1, o1, o2, group, rest, &nrest, st);
+        if (rc == 0 && nrest > 0) rc = pb::exact_subset(&b2, rest, nrest, 1, 32, o2, st);
     }
     for (int q = 0; q < nq && rc == 0; ++q) {
         const int qall = tmpl->nprofs > 0 ? tmpl->profs[q]->qlen : 0;
@@ -250,6 +260,7 @@ extern "C" int pb_cuda_batch_run(const pb_job *job, const pb_batch *tmpl, pb_rec
     }
     if (o1) cudaFreeAsync(o1, st);
     if (o2) cudaFreeAsync(o2, st);
+    if (rest) cudaFreeAsync(rest, st);
     if (qlim) cudaFreeAsync(qlim, st);
     if (tlim) cudaFreeAsync(tlim, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
@@ -353,7 +364,7 @@ namespace {
  * row i starts at i*n - i*(i+1)/2 */
 __global__ void k_all_pairs(const int64_t *__restrict__ off, const int *__restrict__ len, int n, int npairs,
                             int64_t *__restrict__ qoff, int *__restrict__ qlen, int64_t *__restrict__ toff,
-                            int *__restrict__ tlen)
+                            int *__restrict__ tlen, int *__restrict__ grp)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npairs) return;
@@ -367,6 +378,7 @@ __global__ void k_all_pairs(const int64_t *__restrict__ off, const int *__restri
     const int j = i + 1 + (int)(p - ((int64_t)i * N - (int64_t)i * (i + 1) / 2));
     qoff[p] = off[i]; qlen[p] = len[i];
     toff[p] = off[j]; tlen[p] = len[j];
+    grp[p] = i;
 }
 
 }  // namespace
@@ -380,15 +392,16 @@ extern "C" int pb_cuda_batch_all(const pb_job *job, const pb_batch *tmpl, const 
     cudaStream_t st = nullptr;
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return -1;
     int64_t *qoff = nullptr, *toff = nullptr;
-    int *qlen = nullptr, *tlen = nullptr;
+    int *qlen = nullptr, *tlen = nullptr, *grp = nullptr;
     int rc = 0;
     if (cudaMallocAsync((void **)&qoff, sizeof(int64_t) * npairs, st) != cudaSuccess ||
         cudaMallocAsync((void **)&toff, sizeof(int64_t) * npairs, st) != cudaSuccess ||
         cudaMallocAsync((void **)&qlen, sizeof(int) * npairs, st) != cudaSuccess ||
-        cudaMallocAsync((void **)&tlen, sizeof(int) * npairs, st) != cudaSuccess)
+        cudaMallocAsync((void **)&tlen, sizeof(int) * npairs, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&grp, sizeof(int) * npairs, st) != cudaSuccess)
         rc = -1;
     if (rc == 0) {
-        k_all_pairs<<<(npairs + 255) / 256, 256, 0, st>>>(d_off, d_len, n, npairs, qoff, qlen, toff, tlen);
+        k_all_pairs<<<(npairs + 255) / 256, 256, 0, st>>>(d_off, d_len, n, npairs, qoff, qlen, toff, tlen, grp);
         pb_diag_count_launch(1);
         if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
     }
@@ -398,8 +411,10 @@ extern "C" int pb_cuda_batch_all(const pb_job *job, const pb_batch *tmpl, const 
         b.npairs = npairs;
         b.d_qall = d_codes; b.d_qoff = qoff; b.d_qlen = qlen;
         b.d_targets = d_codes; b.d_toff = toff; b.d_tlen = tlen;
+        b.d_qgroup = grp;
         rc = pb_cuda_batch_run(job, &b, d_rec);
     }
+    if (grp) cudaFreeAsync(grp, st);
     if (qoff) cudaFreeAsync(qoff, st);
     if (toff) cudaFreeAsync(toff, st);
     if (qlen) cudaFreeAsync(qlen, st);

@@ -58,7 +58,8 @@ typedef struct pb_pair_out {
 
 enum {
     PB_ST_OVERFLOW16 = 1,   /* a 16-bit lane left its exact range: rerun in 32 bits */
-    PB_ST_BADCODE = 2       /* a residue code outside the profile alphabet */
+    PB_ST_BADCODE = 2,      /* a residue code outside the profile alphabet */
+    PB_ST_BOUNDED = 4       /* the extremes fields are sound bounds, not exact values */
 };
 
 /* A batch of pairs sharing one alignment mode. Every pointer is DEVICE
@@ -85,6 +86,9 @@ typedef struct pb_batch {
     const uint8_t *d_qall;
     const int64_t *d_qoff;
     const int *d_qlen;
+    /* pairs mode, optional: per-pair query id; pairs with one id share the
+     * query (e.g. the rows of an all-vs-all batch) */
+    const int *d_qgroup;
 } pb_batch;
 
 /* --- device management ------------------------------------------------- */

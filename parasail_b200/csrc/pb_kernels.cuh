@@ -77,6 +77,55 @@ struct Sw16Params {
     pb_pair_out *out;        /* [nq][npairs] */
 };
 
+/* The int16x2 pair kernels (pb_pair16.cu). Items are pairs (pairs mode:
+ * query codes per item scored through an int8 matrix) or query x target
+ * products (db mode: item = query * nt + target, int8 profiles). */
+struct P16Params {
+    int alg, sgflags, open, gap, mmax, mmin;
+    int nletters;                 /* alphabet size, <= 32 */
+    int nitems;                   /* eligible items: sorted positions [0, nitems) */
+    const int *order;             /* sorted position -> item */
+    const int *rows, *cols;       /* per item: query rows (or prefix limit) and target columns */
+    const int *task_wmax, *task_npass;
+    const long long *task_bits;   /* per task: first uint4 of its direction bits in `bits` */
+    uint4 *bits;
+    const int8_t *mat8;           /* pairs mode: [target letter][query letter] int8, else nullptr */
+    const int32_t *mat32;         /* pairs mode: the same in int32 (the statistics walk) */
+    const uint8_t *qall;
+    const int64_t *qoff;
+    const ProfDesc *profs;        /* db mode */
+    int nt;                       /* db mode: targets per query; 0 in pairs mode */
+    const uint8_t *targets;
+    const int64_t *toff;
+    uint2 *scratch;               /* per resident warp [maxlen + 1][32] pass boundaries */
+    int maxlen;
+    pb_pair_out *out;
+};
+
+struct P16Setup {
+    int alg, open, gap, mmax, mmin, nitems, nt, max_cols;
+    const int *qlen;              /* pairs mode, per item */
+    const int *prof_qlen;         /* db mode, per query */
+    const int *tlen;              /* per target */
+    const int *qlim, *tlim;       /* per item limits, or nullptr */
+    const int *group;             /* per item query group (pairs mode), or nullptr */
+};
+
+/* Runs the items of batch b that fit 16-bit lanes on the pair kernels:
+ * scores and ends (prefix = 0), with statistics by the direction-bit walk
+ * when the job has them; or (prefix = 1, the FASTSTATS prefix pass, b
+ * carrying qlim/tlim) statistics only, walked from the ends in `ends`.
+ * Items outside the 16-bit bounds, and items whose width verdicts need
+ * exact extremes, are listed in d_rest (*n_rest of them, device memory of
+ * at least one int per item) for the exact kernel. group: optional per-item
+ * query group (pairs that share a query). Synchronises st. */
+int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out *ends, pb_pair_out *out,
+             const int *group, int *d_rest, int *n_rest, cudaStream_t st);
+/* The exact kernel on the listed items of batch b (pairs or db mode),
+ * outputs scattered to out[item]. stats / pad_rows as for the exact kernel. */
+int exact_subset(const pb_batch *b, const int *d_list, int n, int stats, int pad_rows, pb_pair_out *out,
+                 cudaStream_t st);
+
 void launch_exact(const ExactParams &p, int alg, bool stats, cudaStream_t st);
 /* resolution with the lane-exact rounds (pb_batch.cu) */
 int resolve_rounds(const pb_job &job, const pb_lane_args &la, const pb_pair_out *o1, const pb_pair_out *o2,
