@@ -450,6 +450,12 @@ def leg_config5(pb, args, td):
     full, t_full = runs_full[-1][0], sorted(r[1] for r in runs_full)[reps // 2]
     (sc, lo, hi, st), t_band = runs_band[-1][0], sorted(r[1] for r in runs_band)[reps // 2]
     model.close()
+    # the non-learned baseline: the same certificate, bands doubling from a
+    # half-width of w0 diagonals until they pass
+    w0 = 64
+    pb.nw_doubling_band(dna, *te[:6], 4, 1, w0)
+    runs_dbl = [timed(lambda: pb.nw_doubling_band(dna, *te[:6], 4, 1, w0)) for _ in range(reps)]
+    (dsc, dst), t_dbl = runs_dbl[-1][0], sorted(r[1] for r in runs_dbl)[reps // 2]
     # the reference's full DP on the first pairs of the test set
     k = min(args.band_cpu_pairs, n_test)
     qf, tf = os.path.join(td, "c5q.txt"), os.path.join(td, "c5t.txt")
@@ -466,7 +472,12 @@ def leg_config5(pb, args, td):
                              "certified": int(st.certified), "rebanded": int(st.fallback),
                              "band_scaling": {"widen": widen, "slack": slack},
                              "band_cells_frac": st.band_cells / cells},
+            "doubling_band": {"pairs_per_s": n_test / t_dbl, "seconds": t_dbl, "start_half_width": w0,
+                              "certified_first_band": int(dst.certified), "rebanded": int(dst.fallback),
+                              "band_cells_frac": dst.band_cells / cells,
+                              "scores_identical_to_full_dp": bool((dsc == full).all())},
             "speedup_pairs_per_s": t_full / t_band,
+            "speedup_over_doubling_band": t_dbl / t_band,
             "scores_identical_to_full_dp": bool((sc == full).all()),
             "train": {"pairs": len(tr[2]), "epochs": 120, "final_loss": loss, "seconds": train_s},
             "cpu_baseline": cpu_block(r, "reference nw_scan_profile_32 on the first %d test pairs" % k),

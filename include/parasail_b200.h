@@ -227,6 +227,17 @@ extern int parasail_b200_nw_learned_band(
         const char *targets, const int64_t *toffsets, const int *tlengths, int n,
         int open, int gap, float widen, int slack,
         int *scores, int *band_lo, int *band_hi, parasail_b200_band_stats_t *stats);
+/** The same scores without a model: every pair starts on the band of
+ * half-width w0 around (n - m) / 2 diagonals, and a pair whose banded score
+ * fails the exactness certificate reruns on a band twice as wide, until it
+ * passes or the band covers the whole matrix. The non-learned baseline of
+ * parasail_b200_nw_learned_band; stats as there (fallback = pairs that
+ * needed more than one band, band_cells = cells of every round). */
+extern int parasail_b200_nw_doubling_band(
+        const parasail_matrix_t *matrix,
+        const char *queries, const int64_t *qoffsets, const int *qlengths,
+        const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+        int open, int gap, int w0, int *scores, parasail_b200_band_stats_t *stats);
 /** Banded DP with caller-given bands and the certificate, no fallback:
  * certified[i] = 1 when scores[i] is provably the full optimum. */
 extern int parasail_b200_nw_banded_certified(
@@ -234,6 +245,19 @@ extern int parasail_b200_nw_banded_certified(
         const char *queries, const int64_t *qoffsets, const int *qlengths,
         const char *targets, const int64_t *toffsets, const int *tlengths, int n,
         int open, int gap, const int *band_lo, const int *band_hi, int *scores, int *certified);
+
+/** parasail_nw_banded (parasail.h:293-296) for n independent pairs in one
+ * launch: scores[i] is the value parasail_nw_banded(query i, target i,
+ * open, gap, k, matrix) returns. The band of src/nw_banded.c:92-97 -- query
+ * positions [j + s1Len - s2Len - k, j + k] of target column j when s1Len <=
+ * s2Len, [j - k, j + s1Len - s2Len + k] otherwise -- runs as a band of
+ * diagonals on the wavefront kernel. Square matrix of at most 32 letters
+ * with |scores| <= 127; k > 0. */
+extern int parasail_b200_nw_banded_batch(
+        const parasail_matrix_t *matrix,
+        const char *queries, const int64_t *qoffsets, const int *qlengths,
+        const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+        int open, int gap, int k, int *scores);
 
 /** Diagnostics: number of this library's kernel launches so far. */
 extern long parasail_b200_kernel_launches(void);

@@ -344,6 +344,11 @@ lib.parasail_b200_nw_banded_certified.argtypes = [_MP, _V, _V, _V, _V, _V, _V, c
                                                   ctypes.c_int, _V, _V, _V, _V]
 
 
+lib.parasail_b200_nw_banded_batch.restype = ctypes.c_int
+lib.parasail_b200_nw_banded_batch.argtypes = [_MP, _V, _V, _V, _V, _V, _V, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, _V]
+
+
 def _pairs_args(qbuf, qoff, qlen, tbuf, toff, tlen):
     return (qbuf.ctypes.data, qoff.ctypes.data, qlen.ctypes.data, tbuf.ctypes.data, toff.ctypes.data,
             tlen.ctypes.data)
@@ -454,3 +459,34 @@ def nw_banded_certified(matrix, qbuf, qoff, qlen, tbuf, toff, tlen, open_, gap, 
     if rc != 0:
         raise RuntimeError("banded certified failed")
     return sc, cert
+
+
+def nw_banded_batch(matrix, queries, targets, open_, gap, k):
+    """parasail_nw_banded scores of many pairs in one call."""
+    np = _np()
+    qb, qo, ql = pack(queries)
+    tb, to, tl = pack(targets)
+    sc = np.zeros(len(ql), np.int32)
+    rc = lib.parasail_b200_nw_banded_batch(matrix, qb.ctypes.data, qo.ctypes.data, ql.ctypes.data, tb.ctypes.data,
+                                           to.ctypes.data, tl.ctypes.data, len(ql), open_, gap, k, sc.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("parasail_b200_nw_banded_batch failed")
+    return sc
+
+
+lib.parasail_b200_nw_doubling_band.restype = ctypes.c_int
+lib.parasail_b200_nw_doubling_band.argtypes = [_MP, _V, _V, _V, _V, _V, _V, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, _V, ctypes.POINTER(BandStats)]
+
+
+def nw_doubling_band(matrix, qbuf, qoff, qlen, tbuf, toff, tlen, open_, gap, w0=64):
+    """Certified banded global scores without a model (band doubling)."""
+    np = _np()
+    n = len(qlen)
+    sc = np.zeros(n, np.int32)
+    st = BandStats()
+    rc = lib.parasail_b200_nw_doubling_band(matrix, *_pairs_args(qbuf, qoff, qlen, tbuf, toff, tlen), n, open_,
+                                            gap, w0, sc.ctypes.data, ctypes.byref(st))
+    if rc != 0:
+        raise RuntimeError("parasail_b200_nw_doubling_band failed")
+    return sc, st

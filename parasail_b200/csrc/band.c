@@ -418,3 +418,163 @@ int parasail_b200_nw_banded_certified(const parasail_matrix_t *matrix,
     dev_pairs_free(&d);
     return rc;
 }
+
+/* parasail_nw_banded's band (src/nw_banded.c:92-97): query positions
+ * [j + low, j + k] of target column j when s1Len <= s2Len (low = s1Len -
+ * s2Len - k), [j - k, j + s1Len - s2Len + k] otherwise; as diagonals i - j. */
+static void banded_k_band(int s1Len, int s2Len, int k, int *lo, int *hi)
+{
+    if (s1Len <= s2Len) { *lo = s1Len - s2Len - k; *hi = k; }
+    else { *lo = -k; *hi = s1Len - s2Len + k; }
+}
+
+int pb_nw_banded_fits_wave(const parasail_matrix_t *matrix)
+{
+    return matrix && matrix->type == PARASAIL_MATRIX_TYPE_SQUARE && matrix->size <= 32 &&
+           matrix->max <= 127 && matrix->min >= -127;
+}
+
+int parasail_b200_nw_banded_batch(const parasail_matrix_t *matrix,
+                                  const char *queries, const int64_t *qoffsets, const int *qlengths,
+                                  const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+                                  int open, int gap, int k, int *scores)
+{
+    dev_pairs d;
+    int *d_score, *d_lo, *d_hi, *h_lo, *h_hi, rc, i;
+    if (!long_ok(__func__, matrix, open, gap)) return -1;
+    if (!pb_nw_banded_fits_wave(matrix)) {
+        fprintf(stderr, "%s: needs a square matrix of at most 32 letters with |scores| <= 127\n", __func__);
+        return -1;
+    }
+    if (k <= 0) { fprintf(stderr, "%s: %s must be > 0\n", __func__, "k"); return -1; }
+    if (n <= 0) return n == 0 ? 0 : -1;
+    if (!scores) { fprintf(stderr, "%s: missing %s\n", __func__, "scores"); return -1; }
+    if (dev_pairs_upload(matrix, queries, qoffsets, qlengths, targets, toffsets, tlengths, n, &d) != 0) {
+        fprintf(stderr, "%s: invalid pairs\n", __func__);
+        return -1;
+    }
+    h_lo = (int *)malloc(sizeof(int) * (size_t)n);
+    h_hi = (int *)malloc(sizeof(int) * (size_t)n);
+    if (!h_lo || !h_hi) { free(h_lo); free(h_hi); dev_pairs_free(&d); return -1; }
+    for (i = 0; i < n; ++i) banded_k_band(qlengths[i], tlengths[i], k, &h_lo[i], &h_hi[i]);
+    d_score = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    d_lo = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    d_hi = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    rc = (!d_score || !d_lo || !d_hi) ? -1 : 0;
+    if (rc == 0) rc = pb_cuda_h2d(d_lo, h_lo, sizeof(int) * n);
+    if (rc == 0) rc = pb_cuda_h2d(d_hi, h_hi, sizeof(int) * n);
+    pb_cuda_sync();
+    if (rc == 0)
+        rc = pb_cuda_nw_long(n, open, gap, matrix->matrix, matrix->size, d.q, d.qoff, d.qlen, d.t, d.toff, d.tlen,
+                             d_lo, d_hi, d.maxlen, d_score);
+    if (rc == 0) rc = pb_cuda_d2h(scores, d_score, sizeof(int) * n);
+    pb_cuda_free(d_score); pb_cuda_free(d_lo); pb_cuda_free(d_hi);
+    free(h_lo); free(h_hi);
+    dev_pairs_free(&d);
+    return rc;
+}
+
+/* Certified banded global alignment without a model: every pair starts on
+ * the band of half-width w0 around the certificate's centre (n - m) / 2
+ * diagonals (always holding the diagonals between 0 and n - m); a pair whose
+ * banded score fails the exactness certificate reruns on a band twice as
+ * wide, until the band covers the whole matrix, where the score is the
+ * full DP's. Returns the scores of parasail_b200_nw_long. */
+int parasail_b200_nw_doubling_band(const parasail_matrix_t *matrix,
+                                   const char *queries, const int64_t *qoffsets, const int *qlengths,
+                                   const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+                                   int open, int gap, int w0, int *scores, parasail_b200_band_stats_t *stats)
+{
+    dev_pairs d;
+    int *act = NULL, *h_lo = NULL, *h_hi = NULL, *h_sc = NULL, *h_cert = NULL, *h_ql = NULL, *h_tl = NULL;
+    int64_t *h_qo = NULL, *h_to = NULL;
+    int64_t *d_qo = NULL, *d_to = NULL;
+    int *d_ql = NULL, *d_tl = NULL, *d_lo = NULL, *d_hi = NULL, *d_sc = NULL, *d_cert = NULL;
+    int na = n, i, rc = 0, round = 0, nfail = 0;
+    long long w = w0 > 0 ? w0 : 64;
+    parasail_b200_band_stats_t st;
+    memset(&st, 0, sizeof st);
+    if (!long_ok(__func__, matrix, open, gap)) return -1;
+    if (n <= 0) return n == 0 ? 0 : -1;
+    if (!scores) { fprintf(stderr, "%s: missing %s\n", __func__, "scores"); return -1; }
+    if (dev_pairs_upload(matrix, queries, qoffsets, qlengths, targets, toffsets, tlengths, n, &d) != 0) {
+        fprintf(stderr, "%s: invalid pairs\n", __func__);
+        return -1;
+    }
+    act = (int *)malloc(sizeof(int) * (size_t)n);
+    h_lo = (int *)malloc(sizeof(int) * (size_t)n);
+    h_hi = (int *)malloc(sizeof(int) * (size_t)n);
+    h_sc = (int *)malloc(sizeof(int) * (size_t)n);
+    h_cert = (int *)malloc(sizeof(int) * (size_t)n);
+    h_ql = (int *)malloc(sizeof(int) * (size_t)n);
+    h_tl = (int *)malloc(sizeof(int) * (size_t)n);
+    h_qo = (int64_t *)malloc(sizeof(int64_t) * (size_t)n);
+    h_to = (int64_t *)malloc(sizeof(int64_t) * (size_t)n);
+    d_qo = (int64_t *)pb_cuda_malloc(sizeof(int64_t) * (size_t)n);
+    d_to = (int64_t *)pb_cuda_malloc(sizeof(int64_t) * (size_t)n);
+    d_ql = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    d_tl = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    d_lo = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    d_hi = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    d_sc = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    d_cert = (int *)pb_cuda_malloc(sizeof(int) * (size_t)n);
+    if (!act || !h_lo || !h_hi || !h_sc || !h_cert || !h_ql || !h_tl || !h_qo || !h_to || !d_qo || !d_to ||
+        !d_ql || !d_tl || !d_lo || !d_hi || !d_sc || !d_cert)
+        rc = -1;
+    for (i = 0; i < n; ++i) act[i] = i;
+    st.pairs = n;
+    while (rc == 0 && na > 0) {
+        int k, full = 1;
+        unsigned long long cells = 0;
+        for (k = 0; k < na; ++k) {
+            const int p = act[k], qn = qlengths[p], tm = tlengths[p], de = qn - tm;
+            long long lo = (de >= 0 ? de / 2 : -((-de + 1) / 2)) - w, hi = (de >= 0 ? (de + 1) / 2 : -((-de) / 2)) + w;
+            if (lo > 0) lo = 0;
+            if (lo > de) lo = de;
+            if (hi < 0) hi = 0;
+            if (hi < de) hi = de;
+            /* a band past the matrix's corners is the whole matrix */
+            if (lo < -(long long)tm) lo = -tm;
+            if (hi > qn) hi = qn;
+            if (lo > -(long long)tm || hi < qn) full = 0;
+            h_lo[k] = (int)lo; h_hi[k] = (int)hi;
+            h_qo[k] = qoffsets[p]; h_to[k] = toffsets[p]; h_ql[k] = qn; h_tl[k] = tm;
+        }
+        (void)full;
+        if (pb_cuda_h2d(d_qo, h_qo, sizeof(int64_t) * na) || pb_cuda_h2d(d_to, h_to, sizeof(int64_t) * na) ||
+            pb_cuda_h2d(d_ql, h_ql, sizeof(int) * na) || pb_cuda_h2d(d_tl, h_tl, sizeof(int) * na) ||
+            pb_cuda_h2d(d_lo, h_lo, sizeof(int) * na) || pb_cuda_h2d(d_hi, h_hi, sizeof(int) * na)) { rc = -1; break; }
+        pb_cuda_sync();
+        rc = pb_cuda_nw_long(na, open, gap, matrix->matrix, matrix->size, d.q, d_qo, d_ql, d.t, d_to, d_tl,
+                             d_lo, d_hi, d.maxlen, d_sc);
+        if (rc == 0) rc = pb_cuda_band_certify(na, matrix->max, open, gap, d_ql, d_tl, d_lo, d_hi, d_sc, d_cert, &nfail);
+        if (rc == 0) rc = pb_cuda_band_cells(na, d_ql, d_tl, d_lo, d_hi, &cells);
+        if (rc == 0) rc = pb_cuda_d2h(h_sc, d_sc, sizeof(int) * na);
+        if (rc == 0) rc = pb_cuda_d2h(h_cert, d_cert, sizeof(int) * na);
+        if (rc != 0) break;
+        st.band_cells += (double)cells;
+        {
+            int nn = 0;
+            for (k = 0; k < na; ++k) {
+                /* a band holding the whole matrix is the full DP */
+                const int whole = h_lo[k] <= -h_tl[k] && h_hi[k] >= h_ql[k];
+                if (h_cert[k] || whole) {
+                    scores[act[k]] = h_sc[k];
+                    if (round == 0) st.certified += 1;
+                } else {
+                    act[nn++] = act[k];
+                }
+            }
+            if (round == 0) st.fallback = nn;
+            na = nn;
+        }
+        w *= 2;
+        ++round;
+    }
+    pb_cuda_free(d_qo); pb_cuda_free(d_to); pb_cuda_free(d_ql); pb_cuda_free(d_tl);
+    pb_cuda_free(d_lo); pb_cuda_free(d_hi); pb_cuda_free(d_sc); pb_cuda_free(d_cert);
+    free(act); free(h_lo); free(h_hi); free(h_sc); free(h_cert); free(h_ql); free(h_tl); free(h_qo); free(h_to);
+    dev_pairs_free(&d);
+    if (stats) *stats = st;
+    return rc;
+}

@@ -4,6 +4,9 @@
 #include <stdlib.h>
 
 #include "pb_internal.h"
+#include "parasail_b200.h"
+
+int pb_nw_banded_fits_wave(const parasail_matrix_t *matrix);
 
 parasail_result_t *parasail_nw_banded(const char *const restrict s1, const int s1Len,
                                       const char *const restrict s2, const int s2Len,
@@ -23,6 +26,24 @@ parasail_result_t *parasail_nw_banded(const char *const restrict s1, const int s
     PB_CHECK_GT0(k);
     PB_CHECK_NULL(matrix);
     if (!pb_gpu_ready(__func__)) return NULL;
+    if (pb_nw_banded_fits_wave(matrix)) {
+        /* the band as diagonals on the wavefront kernel (pb_nwlong.cu) */
+        const int64_t zero = 0;
+        if (parasail_b200_nw_banded_batch(matrix, s1, &zero, &s1Len, s2, &zero, &s2Len, 1, open, gap, k, &score) != 0) {
+            fprintf(stderr, "%s: GPU alignment failed\n", __func__);
+            return NULL;
+        }
+        r = pb_result_new(0);
+        if (!r) return NULL;
+        r->score = score;
+        r->end_query = s1Len - 1;
+        r->end_ref = s2Len - 1;
+        r->flag = PARASAIL_FLAG_NW | PARASAIL_FLAG_NOVEC | PARASAIL_FLAG_BANDED
+                | PARASAIL_FLAG_BITS_32 | PARASAIL_FLAG_LANES_1;
+        return r;
+    }
+    /* other matrices (PSSM, wider alphabets or scores): one pair on the
+     * column recurrence of src/nw_banded.c */
     profile = pb_profile_create(s1, s1Len, matrix, 4, 0, 1);
     if (!profile) return NULL;
     codes = (uint8_t *)malloc((size_t)s2Len);

@@ -243,3 +243,18 @@ def test_learned_band_trains_certifies_and_beats_fixed_band():
     fixed_cells = cells(flo, fhi) + float(full_cells[fcert == 0].sum())
     assert learned_cells < fixed_cells
     m.close()
+
+
+def test_doubling_band_equals_full_dp():
+    """The model-free certified band (doubling on certificate failure)
+    returns the full-DP score of every pair, including pairs whose first
+    band is far too narrow and short pairs whose band covers the matrix."""
+    a, ao, al, b, bo, bl, _ = synth.dna_long_pairs(seed=31, n_pairs=40, lo=200, hi=4000)
+    dna = pb.matrix_create("ACGT", 1, -2)
+    full = pb.nw_long(dna, a, ao, al, b, bo, bl, 4, 1)
+    for w0 in (1, 16, 5000):
+        sc, st = pb.nw_doubling_band(dna, a, ao, al, b, bo, bl, 4, 1, w0)
+        assert (sc == full).all(), w0
+        assert st.pairs == 40
+    _, st1 = pb.nw_doubling_band(dna, a, ao, al, b, bo, bl, 4, 1, 1)
+    assert st1.fallback > 0        # a one-diagonal start fails the certificate somewhere

@@ -215,6 +215,38 @@ def test_nw_banded_vs_oracle():
         assert got["flag"] & pb.FLAG_BANDED
 
 
+def test_nw_banded_batch_and_wide_matrices_vs_oracle():
+    """parasail_nw_banded on the wavefront kernel (band as diagonals) in a
+    batch and per call, against the oracle's restatement of
+    src/nw_banded.c, for both length orders, bands narrower and wider than
+    the length difference, a protein matrix, and (per call) a matrix whose
+    scores exceed int8, which runs the column recurrence instead."""
+    rng = random.Random(23)
+    for alpha, key, m_args, op, gp in ((DNA, "dna", ("ACGT", 2, -3), 5, 2), (AA, "b62", None, 11, 1)):
+        m = pb.matrix_create(*m_args) if m_args else pb.matrix_lookup("blosum62")
+        om = O.Matrix.simple(*m_args) if m_args else O.Matrix.from_struct(m)
+        qs, ts = [], []
+        for _ in range(60):
+            q = rand_seq(rng, rng.randint(1, 700), alpha)
+            t = mutate(rng, q, alpha, 0.1, 0.05) if rng.random() < 0.6 else rand_seq(rng, rng.randint(1, 700), alpha)
+            qs.append(q)
+            ts.append(t)
+        for k in (1, 7, 40, 300):
+            got = pb.nw_banded_batch(m, qs, ts, op, gp, k)
+            for q, t, g in zip(qs, ts, got):
+                assert g == O.nw_banded(q, t, op, gp, k, om)["score"], (key, k, len(q), len(t))
+        for q, t in list(zip(qs, ts))[:10]:
+            one = pb.nw_banded(q, t, op, gp, 9, m)
+            assert one["score"] == O.nw_banded(q, t, op, gp, 9, om)["score"]
+    wide = pb.matrix_create("ACGT", 200, -300)
+    owide = O.Matrix.simple("ACGT", 200, -300)
+    for _ in range(10):
+        q = rand_seq(rng, rng.randint(1, 150), DNA)
+        t = mutate(rng, q, DNA)
+        got = pb.nw_banded(q, t, 400, 100, 12, wide)
+        assert got["score"] == O.nw_banded(q, t, 400, 100, 12, owide)["score"]
+
+
 @pytest.mark.skipif(O.ref() is None, reason="reference library not built")
 @pytest.mark.parametrize("width", ["8", "16", "sat"])
 def test_batch_striped_narrow_vs_live_reference(width):
