@@ -287,7 +287,6 @@ k_p16(P16Params p, const int *__restrict__ tlist, int ntl, int *counter)
             int top = p16_top(ALG, sgf, 0, open, gap);
             const int top_step = (ALG == PB_SW || (ALG == PB_SG && (sgf & PB_S2_BEG))) ? 0 : gap;
             P16Best sa = {0, -1, -1}, sb = {0, -1, -1};
-            uint32_t sbest = 0u;
             int cb = 0;
             const bool more = pass + 1 < npass;
             const bool lastpass = ENDS && ALG != PB_SW && pass == p_last;
@@ -381,26 +380,20 @@ k_p16(P16Params p, const int *__restrict__ tlist, int ntl, int *counter)
                     }
                 }
                 if (ENDS && ALG == PB_SW) {
-                    bool ge_lo, ge_hi;
-                    (void)__vibmax_s16x2(sbest, cmax, &ge_hi, &ge_lo);
-                    const bool up_a = !ge_lo && j < cols;
-                    const bool up_b = !ge_hi && j >= 1 && j <= cols;
-                    if (up_a || up_b) {
-                        if (up_a) {
-                            const int c = p16_lo(cmax);
-                            int rr = 0;
+                    /* a strictly higher column maximum than the strip's best
+                     * so far: the first column reaching it, smallest row */
+                    const int c_lo = p16_lo(cmax), c_hi = p16_hi(cmax);
+                    if (c_lo > sa.score && j < cols) {
+                        int rr = 0;
 #pragma unroll
-                            for (int r = P16_R - 1; r >= 0; --r) if (p16_lo(H[r]) == c) rr = r;
-                            sa.score = c; sa.j = j; sa.i = r0 + rr;
-                        }
-                        if (up_b) {
-                            const int c = p16_hi(cmax);
-                            int rr = 0;
+                        for (int r = P16_R - 1; r >= 0; --r) if (p16_lo(H[r]) == c_lo) rr = r;
+                        sa.score = c_lo; sa.j = j; sa.i = r0 + rr;
+                    }
+                    if (c_hi > sb.score && j >= 1 && j <= cols) {
+                        int rr = 0;
 #pragma unroll
-                            for (int r = P16_R - 1; r >= 0; --r) if (p16_hi(H[r]) == c) rr = r;
-                            sb.score = c; sb.j = j - 1; sb.i = r0 + P16_R + rr;
-                        }
-                        sbest = (uint32_t)(uint16_t)sa.score | ((uint32_t)(uint16_t)sb.score << 16);
+                        for (int r = P16_R - 1; r >= 0; --r) if (p16_hi(H[r]) == c_hi) rr = r;
+                        sb.score = c_hi; sb.j = j - 1; sb.i = r0 + P16_R + rr;
                     }
                 }
                 if (ENDS && ALG != PB_SW) {
