@@ -7,8 +7,11 @@ and the same function names and signatures for the in-scope entry points
 (score-only and stats SW / NW / 11 semi-global variants, striped and scan,
 8/16/32-bit and the `_sat` 8->16->32 chains, profile and non-profile forms,
 profile creators, parasail_nw_banded, result accessors, matrix functions and
-the name lookups). Out-of-scope families (diag, blocked, table, rowcol, trace,
-64-bit lanes, ISA-specific names) are not declared.
+the name lookups), plus the traceback entry points of the exact widths (the
+serial trace forms and the 32-bit striped/scan trace forms, profile and
+direct) and the CIGAR functions. Out-of-scope families (diag, blocked, table,
+rowcol, 8/16-bit and _sat trace, 64-bit lanes, ISA-specific names) are not
+declared.
 
 Run:  python include/gen_parasail_h.py > include/parasail.h
 """
@@ -268,6 +271,37 @@ extern int parasail_result_get_matches(const parasail_result_t * const restrict 
 extern int parasail_result_get_similar(const parasail_result_t * const restrict result);
 extern int parasail_result_get_length(const parasail_result_t * const restrict result);
 
+/* CIGAR of a trace result: reference parasail.h:375-449; src/cigar.c,
+ * src/cigar_template.c. Each element is length << 4 | op, op indexing
+ * "MIDNSHP=XB" (the BAM encoding). */
+extern const uint8_t parasail_cigar_encoded_ops[];
+
+typedef struct parasail_cigar_ {
+    uint32_t *seq;
+    int len;
+    int beg_query;
+    int beg_ref;
+} parasail_cigar_t;
+
+extern uint32_t parasail_cigar_encode(uint32_t length, char op_letter);
+extern parasail_cigar_t* parasail_cigar_encode_string(const char *cigar);
+extern char parasail_cigar_decode_op(uint32_t cigar_int);
+extern uint32_t parasail_cigar_decode_len(uint32_t cigar_int);
+extern char* parasail_cigar_decode(parasail_cigar_t *cigar);
+extern parasail_cigar_t* parasail_result_get_cigar(
+        parasail_result_t *result,
+        const char *seqA, int lena,
+        const char *seqB, int lenb,
+        const parasail_matrix_t *matrix);
+extern parasail_cigar_t* parasail_result_get_cigar_extra(
+        parasail_result_t *result,
+        const char *seqA, int lena,
+        const char *seqB, int lenb,
+        const parasail_matrix_t *matrix,
+        int case_sensitive,
+        const char *alphabet_aliases);
+extern void parasail_cigar_free(parasail_cigar_t *cigar);
+
 /* query profiles: reference parasail.h:85201-85317; src/memory_avx2.c:28-528,
  * src/dispatch_profile.c. The 8/16/32 creators build one device profile; the
  * _sat creators build the bundle used by the 8->16->32 chains. */
@@ -309,6 +343,25 @@ def main():
                        "        const char * const restrict s2, const int s2Len,\n"
                        "        const int open, const int gap,\n"
                        "        const parasail_matrix_t* matrix);\n" % name)
+    out.append("\n/* traceback entry points (the exact widths): serial forms, reference\n"
+               " * src/{sw,nw,sg}_trace{,_scan}.c; 32-bit striped/scan forms, reference\n"
+               " * src/{sw,nw,sg}_trace_{striped,scan}_*_32.c. Paths from the GPU. */\n")
+    for alg in ALGS:
+        for suffix, is_prof in (("trace", False), ("trace_scan", False), ("trace_striped_32", False),
+                                ("trace_scan_32", False), ("trace_striped_profile_32", True),
+                                ("trace_scan_profile_32", True)):
+            name = "parasail_%s_%s" % (alg, suffix)
+            if is_prof:
+                out.append("extern parasail_result_t* %s(\n"
+                           "        const parasail_profile_t * const restrict profile,\n"
+                           "        const char * const restrict s2, const int s2Len,\n"
+                           "        const int open, const int gap);\n" % name)
+            else:
+                out.append("extern parasail_result_t* %s(\n"
+                           "        const char * const restrict s1, const int s1Len,\n"
+                           "        const char * const restrict s2, const int s2Len,\n"
+                           "        const int open, const int gap,\n"
+                           "        const parasail_matrix_t* matrix);\n" % name)
     out.append(TAIL)
     print("".join(out), end="")
 

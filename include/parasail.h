@@ -234,6 +234,37 @@ extern int parasail_result_get_matches(const parasail_result_t * const restrict 
 extern int parasail_result_get_similar(const parasail_result_t * const restrict result);
 extern int parasail_result_get_length(const parasail_result_t * const restrict result);
 
+/* CIGAR of a trace result: reference parasail.h:375-449; src/cigar.c,
+ * src/cigar_template.c. Each element is length << 4 | op, op indexing
+ * "MIDNSHP=XB" (the BAM encoding). */
+extern const uint8_t parasail_cigar_encoded_ops[];
+
+typedef struct parasail_cigar_ {
+    uint32_t *seq;
+    int len;
+    int beg_query;
+    int beg_ref;
+} parasail_cigar_t;
+
+extern uint32_t parasail_cigar_encode(uint32_t length, char op_letter);
+extern parasail_cigar_t* parasail_cigar_encode_string(const char *cigar);
+extern char parasail_cigar_decode_op(uint32_t cigar_int);
+extern uint32_t parasail_cigar_decode_len(uint32_t cigar_int);
+extern char* parasail_cigar_decode(parasail_cigar_t *cigar);
+extern parasail_cigar_t* parasail_result_get_cigar(
+        parasail_result_t *result,
+        const char *seqA, int lena,
+        const char *seqB, int lenb,
+        const parasail_matrix_t *matrix);
+extern parasail_cigar_t* parasail_result_get_cigar_extra(
+        parasail_result_t *result,
+        const char *seqA, int lena,
+        const char *seqB, int lenb,
+        const parasail_matrix_t *matrix,
+        int case_sensitive,
+        const char *alphabet_aliases);
+extern void parasail_cigar_free(parasail_cigar_t *cigar);
+
 /* query profiles: reference parasail.h:85201-85317; src/memory_avx2.c:28-528,
  * src/dispatch_profile.c. The 8/16/32 creators build one device profile; the
  * _sat creators build the bundle used by the 8->16->32 chains. */
@@ -2394,6 +2425,374 @@ extern parasail_result_t* parasail_sg_qe_de_stats_scan_sat(
         const int open, const int gap,
         const parasail_matrix_t* matrix);
 extern parasail_result_t* parasail_sg_qe_de_stats_scan_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+
+/* traceback entry points (the exact widths): serial forms, reference
+ * src/{sw,nw,sg}_trace{,_scan}.c; 32-bit striped/scan forms, reference
+ * src/{sw,nw,sg}_trace_{striped,scan}_*_32.c. Paths from the GPU. */
+extern parasail_result_t* parasail_sw_trace(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_trace_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_trace_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_trace_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_trace(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_trace_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_trace_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_trace_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_trace(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_trace_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_trace_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_trace_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_trace(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_trace_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_trace_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_trace_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_trace(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_trace_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_trace_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_trace_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_trace(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_trace_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_trace_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_trace_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_trace(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_trace_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_trace_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_trace_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_trace(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_trace_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_trace_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_trace_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_trace(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_trace_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_trace_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_trace_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_trace(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_trace_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_trace_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_trace_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_trace(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_trace_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_trace_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_trace_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_trace(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_trace_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_trace_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_trace_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_trace(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_trace_scan(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_trace_striped_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_trace_striped_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_trace_scan_profile_32(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);

@@ -151,6 +151,25 @@ extern int parasail_b200_batch_all_device(
         const uint8_t *d_codes, const int64_t *d_offsets, const int *d_lengths, int n,
         int open, int gap, parasail_b200_record_t *d_records);
 
+/** CIGARs of n independent pairs (host memory) with a trace function of
+ * parasail.h: "sw_trace", "nw_trace_scan", "sg_qx_trace_striped_32",
+ * "sg_de_trace_scan_32", ... (serial and 32-bit forms; with or without the
+ * "parasail_" prefix). For pair i: records[i] holds the score, ends and
+ * flags the trace function returns; its CIGAR -- the one
+ * parasail_result_get_cigar gives for that result (src/cigar.c), BAM
+ * encoding -- goes to cigars[o_i ..] with o_i = sum over k < i of
+ * qlengths[k] + tlengths[k] (the buffer holds sum over all pairs), its
+ * element count to cigar_lengths[i] (-1 when the pair's scores leave the
+ * int16 range of the traceback kernel), and the first aligned positions
+ * to beg_query[i], beg_ref[i]. Replaces n calls of a trace function
+ * followed by parasail_result_get_cigar. */
+extern int parasail_b200_batch_pairs_cigar(
+        const char *funcname, const parasail_matrix_t *matrix,
+        const char *queries, const int64_t *qoffsets, const int *qlengths,
+        const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+        int open, int gap, parasail_b200_record_t *records, uint32_t *cigars,
+        int *cigar_lengths, int *beg_query, int *beg_ref);
+
 /* ---- long global alignments and the learned band ---------------------- */
 
 /** Global alignment score of each long pair (query i against target i),

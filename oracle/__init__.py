@@ -336,3 +336,43 @@ def ref_nw_banded(q, t, open_, gap, k, matrix_key):
                    ctypes.c_int, ctypes.c_int, ctypes.POINTER(PMatrix)]
     qb, tb = q.encode(), t.encode()
     return _ref_result(r, fn(qb, len(qb), tb, len(tb), open_, gap, k, mp))
+
+
+class PCigar(ctypes.Structure):
+    _fields_ = [("seq", ctypes.POINTER(ctypes.c_uint32)), ("len", ctypes.c_int),
+                ("beg_query", ctypes.c_int), ("beg_ref", ctypes.c_int)]
+
+
+def ref_trace(alg_name, form, q, t, open_, gap, matrix_key):
+    """The reference's trace function `parasail_{alg}_trace{form}` on one pair
+    (form "", "_scan", "_striped_32" or "_scan_32"; the vector forms call
+    the AVX2 kernels), followed by its parasail_result_get_cigar
+    (src/cigar.c). Returns {score, end_query, end_ref, flag, cigar,
+    beg_query, beg_ref} (cigar None when the reference returns none)."""
+    r = ref()
+    if r is None:
+        return None
+    mp = ref_matrix_ptr(matrix_key)
+    fname = "parasail_%s_trace%s" % (alg_name, form.replace("_32", "_avx2_256_32"))
+    fn = getattr(r, fname)
+    fn.restype = ctypes.POINTER(PResult)
+    fn.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                   ctypes.c_int, ctypes.POINTER(PMatrix)]
+    r.parasail_result_get_cigar.restype = ctypes.POINTER(PCigar)
+    r.parasail_result_get_cigar.argtypes = [ctypes.POINTER(PResult), ctypes.c_char_p, ctypes.c_int,
+                                            ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(PMatrix)]
+    r.parasail_cigar_decode.restype = ctypes.c_void_p
+    r.parasail_cigar_decode.argtypes = [ctypes.POINTER(PCigar)]
+    r.parasail_cigar_free.argtypes = [ctypes.POINTER(PCigar)]
+    qb, tb = q.encode(), t.encode()
+    rp = fn(qb, len(qb), tb, len(tb), open_, gap, mp)
+    c = rp.contents
+    out = {"score": c.score, "end_query": c.end_query, "end_ref": c.end_ref, "flag": c.flag,
+           "cigar": None, "beg_query": None, "beg_ref": None}
+    cg = r.parasail_result_get_cigar(rp, qb, len(qb), tb, len(tb), mp)
+    if cg:
+        s = ctypes.cast(r.parasail_cigar_decode(cg), ctypes.c_char_p).value.decode()
+        out.update(cigar=s, beg_query=cg.contents.beg_query, beg_ref=cg.contents.beg_ref)
+        r.parasail_cigar_free(cg)
+    r.parasail_result_free(rp)
+    return out

@@ -490,3 +490,90 @@ def nw_doubling_band(matrix, qbuf, qoff, qlen, tbuf, toff, tlen, open_, gap, w0=
     if rc != 0:
         raise RuntimeError("parasail_b200_nw_doubling_band failed")
     return sc, st
+
+
+# ---------------------------------------------------------------------------
+# Traceback and CIGAR (parasail.h trace functions, parasail_b200_batch_pairs_cigar)
+
+class Cigar(ctypes.Structure):
+    _fields_ = [("seq", ctypes.POINTER(ctypes.c_uint32)), ("len", ctypes.c_int),
+                ("beg_query", ctypes.c_int), ("beg_ref", ctypes.c_int)]
+
+
+_CP = ctypes.POINTER(Cigar)
+lib.parasail_result_get_cigar.restype = _CP
+lib.parasail_result_get_cigar.argtypes = [_RP, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, _MP]
+lib.parasail_cigar_decode.restype = ctypes.c_void_p
+lib.parasail_cigar_decode.argtypes = [_CP]
+lib.parasail_cigar_free.argtypes = [_CP]
+lib.parasail_cigar_encode_string.restype = _CP
+lib.parasail_cigar_encode_string.argtypes = [ctypes.c_char_p]
+lib.parasail_cigar_encode.restype = ctypes.c_uint32
+lib.parasail_cigar_encode.argtypes = [ctypes.c_uint32, ctypes.c_char]
+lib.parasail_cigar_decode_op.restype = ctypes.c_char
+lib.parasail_cigar_decode_op.argtypes = [ctypes.c_uint32]
+lib.parasail_cigar_decode_len.restype = ctypes.c_uint32
+lib.parasail_cigar_decode_len.argtypes = [ctypes.c_uint32]
+lib.parasail_b200_batch_pairs_cigar.restype = ctypes.c_int
+lib.parasail_b200_batch_pairs_cigar.argtypes = [ctypes.c_char_p, _MP] + [ctypes.c_void_p] * 6 + \
+    [ctypes.c_int, ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 5
+_libc = ctypes.CDLL(None)
+_libc.free.argtypes = [ctypes.c_void_p]
+
+
+def cigar_string(c):
+    """Decoded CIGAR of a parasail_cigar_t pointer (freed here)."""
+    p = lib.parasail_cigar_decode(c)
+    s = ctypes.cast(p, ctypes.c_char_p).value.decode()
+    _libc.free(p)
+    out = (s, c.contents.beg_query, c.contents.beg_ref)
+    lib.parasail_cigar_free(c)
+    return out
+
+
+def trace(name, s1, s2, open_, gap, matrix, profile=None):
+    """A trace function ('parasail_sw_trace', 'parasail_nw_trace_scan_32',
+    ...) on one pair, then parasail_result_get_cigar."""
+    b1, b2 = s1.encode(), s2.encode()
+    if profile is not None:
+        r = _fn(name, True)(profile.ptr, b2, len(b2), open_, gap)
+    else:
+        r = _fn(name, False)(b1, len(b1), b2, len(b2), open_, gap, matrix)
+    if not r:
+        raise RuntimeError("%s returned NULL" % name)
+    c = r.contents
+    out = {"score": c.score, "end_query": c.end_query, "end_ref": c.end_ref, "flag": c.flag,
+           "cigar": None, "beg_query": None, "beg_ref": None}
+    cg = lib.parasail_result_get_cigar(r, b1, len(b1), b2, len(b2), matrix)
+    if cg:
+        out["cigar"], out["beg_query"], out["beg_ref"] = cigar_string(cg)
+    lib.parasail_result_free(r)
+    return out
+
+
+def batch_pairs_cigar(name, matrix, queries, targets, open_, gap):
+    """CIGARs of many pairs with one call: list of dicts like trace()."""
+    np = _np()
+    qb, qo, ql = pack(queries)
+    tb, to, tl = pack(targets)
+    n = len(ql)
+    recs = np.zeros(n, dtype=record_dtype())
+    cig = np.zeros(int(ql.sum() + tl.sum()) + 1, np.uint32)
+    clen, bq, br = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.int32)
+    rc = lib.parasail_b200_batch_pairs_cigar(name.encode(), matrix, qb.ctypes.data, qo.ctypes.data, ql.ctypes.data,
+                                             tb.ctypes.data, to.ctypes.data, tl.ctypes.data, n, open_, gap,
+                                             recs.ctypes.data, cig.ctypes.data, clen.ctypes.data, bq.ctypes.data,
+                                             br.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("parasail_b200_batch_pairs_cigar failed")
+    out, off = [], 0
+    for k in range(n):
+        s = None
+        if clen[k] >= 0:
+            s = "".join("%d%s" % (int(x) >> 4, "MIDNSHP=XB"[int(x) & 15]) for x in cig[off:off + clen[k]])
+        out.append({"score": int(recs[k]["score"]), "end_query": int(recs[k]["end_query"]),
+                    "end_ref": int(recs[k]["end_ref"]), "flag": int(recs[k]["flag"]), "cigar": s,
+                    "beg_query": int(bq[k]) if s is not None else None,
+                    "beg_ref": int(br[k]) if s is not None else None})
+        off += int(ql[k] + tl[k])
+    return out

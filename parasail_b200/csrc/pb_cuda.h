@@ -161,6 +161,13 @@ int pb_cuda_batch_all_host(const struct pb_job *job, const pb_batch *tmpl, const
                            const char *h_seqs, const int64_t *h_off, const int *h_len, int n,
                            struct pb_record *h_rec);
 
+/* Traceback paths of independent pairs from host memory on the int16x2
+ * pair kernels (pb_pair16.cu); see the definition for the outputs. */
+int pb_cuda_trace_pairs_host(const struct pb_job *job, const pb_batch *tmpl, const uint8_t *mapper256,
+                             const char *h_q, const int64_t *h_qoff, const int *h_qlen,
+                             const char *h_t, const int64_t *h_toff, const int *h_tlen, int n,
+                             int *h_ends, uint8_t *h_ops, const int64_t *h_ops_off, int *h_info);
+
 /* Lane-exact emulation of the reference's 8/16-bit striped kernels
  * (pb_lane.cu) for the pairs listed in d_list. kind: 0 nw/sg score-only,
  * 1 nw/sg with statistics, 2 the SW statistics kernel on the FASTSTATS prefix

@@ -45,6 +45,9 @@ typedef struct pb_host_profile {
 /* result.c */
 parasail_result_t *pb_result_new(int with_stats);
 
+/* trace.c: releases the path of a trace result */
+void pb_trace_free(parasail_result_t *r);
+
 /* profile.c */
 parasail_profile_t *pb_profile_create(const char *s1, int s1Len,
                                       const parasail_matrix_t *matrix,

@@ -100,6 +100,12 @@ struct P16Params {
     uint2 *scratch;               /* per resident warp [maxlen + 1][32] pass boundaries */
     int maxlen;
     pb_pair_out *out;
+    /* traceback paths (optional): per item, steps written backwards into
+     * ops[ops_off[item] .. + rows + cols), and path_info[3 * item] = steps,
+     * the row and the column where the walk stopped */
+    uint8_t *ops;
+    const int64_t *ops_off;
+    int *path_info;
 };
 
 struct P16Setup {
@@ -120,7 +126,8 @@ struct P16Setup {
  * at least one int per item) for the exact kernel. group: optional per-item
  * query group (pairs that share a query). Synchronises st. */
 int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out *ends, pb_pair_out *out,
-             const int *group, int *d_rest, int *n_rest, cudaStream_t st);
+             const int *group, int *d_rest, int *n_rest, cudaStream_t st,
+             uint8_t *d_ops = nullptr, const int64_t *d_ops_off = nullptr, int *d_path_info = nullptr);
 /* The exact kernel on the listed items of batch b (pairs or db mode),
  * outputs scattered to out[item]. stats / pad_rows as for the exact kernel. */
 int exact_subset(const pb_batch *b, const int *d_list, int n, int stats, int pad_rows, pb_pair_out *out,

@@ -553,6 +553,85 @@ __global__ void k_p16_walk(P16Params p, const int *__restrict__ tlist, int ntl, 
     o->length = Ln;
 }
 
+/*
+ * The traceback path of one item: the walk of k_p16_walk, recording its
+ * steps instead of counting them -- 0 a diagonal step (query and target
+ * residue aligned), 1 a step up a vertical gap (a query residue against a
+ * gap), 2 a step left along a horizontal gap (a target residue against a
+ * gap) -- written backwards from the end of the item's op buffer, with
+ * the cell where the walk stopped. These are the decisions the reference's
+ * trace tables hold (src/sw_trace.c:138-147: DIAG when H == H_diag, else
+ * DEL when H == F, else INS; DIAG_F / DIAG_E when the gap opened by strict
+ * >), followed as its CIGAR builder does (src/cigar_template.c:143-243).
+ */
+template <int ALG>
+__global__ void k_p16_path(P16Params p, const int *__restrict__ tlist, int ntl, const pb_pair_out *__restrict__ ends,
+                           int open, int gap)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ntl * 32) return;
+    const int task = tlist[g >> 5], lane = g & 31;
+    const int s = task * 32 + lane;
+    if (s >= p.nitems) return;
+    const int item = p.order[s];
+    const int wmax = p.task_wmax[task];
+    const uint4 *tb = p.bits + p.task_bits[task];
+    const pb_pair_out e = ends[item];
+    const int rows = p.rows[item], cols = p.cols[item];
+    const int cap = rows + cols;
+    uint8_t *ops = p.ops + p.ops_off[item];
+    int *info = p.path_info + 3 * (size_t)item;
+    int i = e.end_query, j = e.end_ref;
+    int v = e.score;
+    if (i >= rows || j >= cols || i < 0 || j < 0) {
+        info[0] = -1; info[1] = i; info[2] = j;
+        return;
+    }
+    const int ti = p.nt ? item % p.nt : item;
+    const uint8_t *tseq = p.targets + p.toff[ti];
+    const uint8_t *qseq;
+    const int32_t *prof32 = nullptr;
+    int lp = 0;
+    if (p.mat8) {
+        qseq = p.qall + p.qoff[item];
+    } else {
+        const ProfDesc pd = p.profs[p.nt ? item / p.nt : 0];
+        qseq = pd.qcodes;
+        prof32 = pd.prof;
+        lp = pd.lp;
+    }
+    const int L = p.nletters;
+    int n = 0, state = 0;                       /* 0 H, 1 F, 2 E */
+    for (int step = 0; step <= 2 * cap + 2 && n < cap; ++step) {
+        if (i < 0 || j < 0) break;
+        if (ALG == PB_SW && state == 0 && v <= 0) break;
+        const int half = (i >> 4) & 1, bit = half * 16 + (i & 15);
+        const uint4 w = tb[((size_t)(i >> 5) * (wmax + 1) + j + half) * 32 + lane];
+        if (state == 0) {
+            if (!((w.x >> bit) & 1u)) {
+                int qc = qseq[i], tc = tseq[j];
+                if (qc >= L) qc = 0;
+                if (tc >= L) tc = 0;
+                v -= p.mat32 ? p.mat32[tc * L + qc] : prof32[(size_t)tc * lp + i];
+                ops[cap - 1 - n++] = 0;
+                --i;
+                --j;
+            } else {
+                state = ((w.y >> bit) & 1u) ? 2 : 1;
+            }
+        } else if (state == 1) {
+            ops[cap - 1 - n++] = 1;
+            if ((w.w >> bit) & 1u) { v += open; state = 0; } else { v += gap; }
+            --i;
+        } else {
+            ops[cap - 1 - n++] = 2;
+            if ((w.z >> bit) & 1u) { v += open; state = 0; } else { v += gap; }
+            --j;
+        }
+    }
+    info[0] = n; info[1] = i; info[2] = j;
+}
+
 /* per item: rows, columns, eligibility and the sort key (eligible first,
  * then by query group, passes and columns, all descending) */
 __global__ void k_p16_setup(P16Setup q, int *__restrict__ rows, int *__restrict__ cols,
@@ -683,8 +762,6 @@ __global__ void k_copy_int(const int *__restrict__ src, int n, int *__restrict__
     if (k < n) dst[k] = src[k];
 }
 
-namespace {
-
 struct P16Frees {
     cudaStream_t st;
     std::vector<void *> v;
@@ -692,6 +769,8 @@ struct P16Frees {
     template <typename T> T *add(T *q) { if (q) v.push_back((void *)q); return q; }
     ~P16Frees() { for (void *q : v) cudaFreeAsync(q, st); }
 };
+
+namespace {
 
 #define P16_CK(call)                                           \
     do {                                                       \
@@ -732,7 +811,8 @@ p16_kernel_t pick(int alg, bool bits, bool ends, bool shared, int warps)
 }  // namespace
 
 int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out *ends, pb_pair_out *out,
-             const int *group, int *d_rest, int *n_rest, cudaStream_t st)
+             const int *group, int *d_rest, int *n_rest, cudaStream_t st,
+             uint8_t *d_ops, const int64_t *d_ops_off, int *d_path_info)
 {
     const pb_mode *m = &job.mode;
     const bool dbmode = b->nprofs > 0;
@@ -740,7 +820,9 @@ int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out
     *n_rest = 0;
     if (N <= 0) return 0;
     if ((long long)(dbmode ? (long long)b->npairs * b->nprofs : b->npairs) > INT32_MAX) return -1;
-    const bool bits = prefix || (m->stats && !pb_job_is_faststats(&job));
+    const bool paths = d_ops != nullptr;
+    const bool bits = prefix || (m->stats && !pb_job_is_faststats(&job)) || paths;
+    const bool walk = prefix || (m->stats && !pb_job_is_faststats(&job));
     const bool ends_on = !prefix;
     P16Frees frees(st);
     /* alphabet and score source; anything the kernels cannot take goes to the exact kernel */
@@ -839,6 +921,7 @@ int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out
         p.qall = b->d_qall; p.qoff = b->d_qoff; p.profs = d_profs; p.nt = dbmode ? b->npairs : 0;
         p.targets = b->d_targets; p.toff = b->d_toff;
         p.out = out;
+        p.ops = d_ops; p.ops_off = d_ops_off; p.path_info = d_path_info;
         int *twmax = nullptr, *tnpass = nullptr, *tshared = nullptr;
         long long *tbits = nullptr;
         P16_CK(cudaMallocAsync((void **)&twmax, sizeof(int) * ntasks, st)); frees.add(twmax);
@@ -932,7 +1015,15 @@ int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out
                 pb_diag_count_launch(1);
                 P16_CK(cudaGetLastError());
             }
-            if (bits) {
+            if (paths) {
+                const int nw = (int)all.size() * 32;
+                if (m->alg == PB_SW) k_p16_path<PB_SW><<<(nw + 127) / 128, 128, 0, st>>>(p, d_tlist, (int)all.size(), out, m->open, m->gap);
+                else if (m->alg == PB_NW) k_p16_path<PB_NW><<<(nw + 127) / 128, 128, 0, st>>>(p, d_tlist, (int)all.size(), out, m->open, m->gap);
+                else k_p16_path<PB_SG><<<(nw + 127) / 128, 128, 0, st>>>(p, d_tlist, (int)all.size(), out, m->open, m->gap);
+                pb_diag_count_launch(1);
+                P16_CK(cudaGetLastError());
+            }
+            if (walk) {
                 const int nw = (int)all.size() * 32;
                 const pb_pair_out *e = prefix ? ends : out;
                 if (m->alg == PB_SW) k_p16_walk<PB_SW><<<(nw + 127) / 128, 128, 0, st>>>(p, d_tlist, (int)all.size(), e, m->open, m->gap);
@@ -1036,3 +1127,111 @@ int exact_subset(const pb_batch *b, const int *d_list, int n, int stats, int pad
 }
 
 }  // namespace pb
+
+namespace {
+
+__global__ void k_p16_map(uint8_t *__restrict__ buf, int64_t n, const uint8_t *__restrict__ map)
+{
+    __shared__ uint8_t smap[256];
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) smap[k] = map[k];
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        buf[i] = smap[buf[i]];
+}
+
+__global__ void k_p16_ends(const pb_pair_out *__restrict__ o, int n, int *__restrict__ se)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    se[3 * k] = o[k].score;
+    se[3 * k + 1] = o[k].end_query;
+    se[3 * k + 2] = o[k].end_ref;
+}
+
+}  // namespace
+
+/* Traceback paths of n pairs from host memory (pairs mode: tmpl carries the
+ * matrix table on the device): characters copied and mapped on the device,
+ * the pair kernels with direction bits and the path walk, then per pair
+ * h_ends[3k..] = score, end_query, end_ref, the steps in
+ * h_ops[h_ops_off[k] ..] (written backwards from the end of the pair's
+ * qlen + tlen bytes) and h_info[3k..] = steps (-1: the pair is outside the
+ * 16-bit bounds of the pair kernels and has no path), stop row, stop
+ * column. */
+extern "C" int pb_cuda_trace_pairs_host(const pb_job *job, const pb_batch *tmpl, const uint8_t *mapper256,
+                                        const char *h_q, const int64_t *h_qoff, const int *h_qlen,
+                                        const char *h_t, const int64_t *h_toff, const int *h_tlen, int n,
+                                        int *h_ends, uint8_t *h_ops, const int64_t *h_ops_off, int *h_info)
+{
+    if (pb_cuda_init() != 0) return -1;
+    if (n <= 0) return 0;
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    int rc = 0;
+    {
+        pb::P16Frees frees(st);
+        int64_t qb = 0, tb = 0, ob = 0;
+        for (int i = 0; i < n; ++i) {
+            qb = std::max(qb, h_qoff[i] + h_qlen[i]);
+            tb = std::max(tb, h_toff[i] + h_tlen[i]);
+            ob = std::max(ob, h_ops_off[i] + h_qlen[i] + h_tlen[i]);
+        }
+        uint8_t *d_q = nullptr, *d_t = nullptr, *d_map = nullptr, *d_ops = nullptr;
+        int64_t *d_qoff = nullptr, *d_toff = nullptr, *d_ooff = nullptr;
+        int *d_qlen = nullptr, *d_tlen = nullptr, *d_info = nullptr, *d_rest = nullptr, *d_se = nullptr;
+        pb_pair_out *d_o = nullptr;
+        if (cudaMallocAsync((void **)&d_q, qb + 16, st) || cudaMallocAsync((void **)&d_t, tb + 16, st) ||
+            cudaMallocAsync((void **)&d_map, 256, st) || cudaMallocAsync((void **)&d_ops, ob + 16, st) ||
+            cudaMallocAsync((void **)&d_qoff, sizeof(int64_t) * n, st) ||
+            cudaMallocAsync((void **)&d_toff, sizeof(int64_t) * n, st) ||
+            cudaMallocAsync((void **)&d_ooff, sizeof(int64_t) * n, st) ||
+            cudaMallocAsync((void **)&d_qlen, sizeof(int) * n, st) || cudaMallocAsync((void **)&d_tlen, sizeof(int) * n, st) ||
+            cudaMallocAsync((void **)&d_info, sizeof(int) * 3 * (size_t)n, st) ||
+            cudaMallocAsync((void **)&d_se, sizeof(int) * 3 * (size_t)n, st) ||
+            cudaMallocAsync((void **)&d_rest, sizeof(int) * n, st) ||
+            cudaMallocAsync((void **)&d_o, sizeof(pb_pair_out) * n, st))
+            rc = -1;
+        void *ptrs[] = {d_q, d_t, d_map, d_ops, d_qoff, d_toff, d_ooff, d_qlen, d_tlen, d_info, d_se, d_rest, d_o};
+        for (void *x : ptrs) frees.add(x);
+        if (rc == 0) {
+            cudaMemcpyAsync(d_q, h_q, qb, cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(d_t, h_t, tb, cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(d_map, mapper256, 256, cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(d_qoff, h_qoff, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(d_toff, h_toff, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(d_ooff, h_ops_off, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(d_qlen, h_qlen, sizeof(int) * n, cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(d_tlen, h_tlen, sizeof(int) * n, cudaMemcpyHostToDevice, st);
+            cudaMemsetAsync(d_info, 0xff, sizeof(int) * 3 * (size_t)n, st);
+            cudaMemsetAsync(d_o, 0, sizeof(pb_pair_out) * n, st);
+            k_p16_map<<<148, 256, 0, st>>>(d_q, qb, d_map);
+            k_p16_map<<<148, 256, 0, st>>>(d_t, tb, d_map);
+            pb_diag_count_launch(2);
+            if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
+        }
+        if (rc == 0) {
+            pb_batch b = *tmpl;
+            b.nprofs = 0;
+            b.npairs = n;
+            b.stats = 0;
+            b.d_qall = d_q; b.d_qoff = d_qoff; b.d_qlen = d_qlen;
+            b.d_targets = d_t; b.d_toff = d_toff; b.d_tlen = d_tlen;
+            b.d_qlim = nullptr; b.d_tlim = nullptr;
+            b.d_out = d_o;
+            int nrest = 0;
+            rc = pb::p16_pass(*job, &b, 0, nullptr, d_o, nullptr, d_rest, &nrest, st, d_ops, d_ooff, d_info);
+        }
+        if (rc == 0) {
+            k_p16_ends<<<(n + 255) / 256, 256, 0, st>>>(d_o, n, d_se);
+            pb_diag_count_launch(1);
+            if (cudaMemcpyAsync(h_ends, d_se, sizeof(int) * 3 * (size_t)n, cudaMemcpyDeviceToHost, st) ||
+                cudaMemcpyAsync(h_info, d_info, sizeof(int) * 3 * (size_t)n, cudaMemcpyDeviceToHost, st) ||
+                cudaMemcpyAsync(h_ops, d_ops, ob, cudaMemcpyDeviceToHost, st))
+                rc = -1;
+        }
+        if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
+    }
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    return rc;
+}

@@ -35,6 +35,7 @@ void parasail_result_free(parasail_result_t *result)
         return;
     }
     if ((result->flag & PARASAIL_FLAG_STATS) && result->stats) free(result->stats);
+    if (result->flag & PARASAIL_FLAG_TRACE) pb_trace_free(result);
     free(result);
 }
 

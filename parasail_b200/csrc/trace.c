@@ -1,0 +1,526 @@
+/*
+ * trace.c -- traceback entry points and CIGAR strings of parasail-b200.
+ *
+ * A trace result carries the alignment path the reference's trace tables
+ * encode, computed on the GPU (pb_pair16.cu: direction bits per cell and a
+ * walk from the end cell): the trace functions of the exact widths --
+ *   parasail_{alg}_trace, parasail_{alg}_trace_scan        (serial forms,
+ *       src/sw_trace.c etc.: flags NOVEC / NOVEC_SCAN, 32 bits, 1 lane)
+ *   parasail_{alg}_trace_{striped,scan}[_profile]_32       (the 32-bit
+ *       trace kernels, e.g. src/sw_trace_striped_avx2_256_32.c: flags
+ *       STRIPED / SCAN, 32 bits, 8 lanes)
+ * -- return the score and ends of the alignment with PARASAIL_FLAG_TRACE,
+ * and parasail_result_get_cigar builds the CIGAR from the path with the
+ * rules of src/cigar_template.c: steps walked back from the end cell
+ * (diagonal, vertical gap, horizontal gap, as the trace table's DIAG / DEL /
+ * INS and DIAG_E / DIAG_F bits select: src/sw_trace.c:138-147), '=' or 'X'
+ * by comparing the characters (upper-cased unless case sensitive, with
+ * optional alias pairs), a query residue against a gap written 'I' and a
+ * target residue against a gap 'D', the gaps to the matrix edge when the
+ * walk reaches row or column -1, and for semi-global alignments the end
+ * gaps past the end cell. The CIGAR encoding (length << 4 | op index into
+ * "MIDNSHP=XB") is the BAM one the reference uses (src/cigar.c).
+ */
+#include <ctype.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "pb_internal.h"
+#include "parasail_b200.h"
+
+/* the path behind a trace result's `extra` pointer */
+typedef struct pb_trace_path {
+    uint8_t *ops;     /* steps in forward order: 0 diagonal, 1 vertical gap (query residue), 2 horizontal gap */
+    int n;
+    int stop_i, stop_j;   /* the cell where the walk stopped (row/column; -1 = boundary) */
+} pb_trace_path;
+
+void pb_trace_free(parasail_result_t *r)
+{
+    pb_trace_path *t = (pb_trace_path *)r->extra;
+    if (t) {
+        free(t->ops);
+        free(t);
+    }
+    r->extra = NULL;
+}
+
+/* ---- CIGAR encoding (src/cigar.c) ---------------------------------------- */
+
+static const char cigar_ops[] = "MIDNSHP=XB";
+
+const uint8_t parasail_cigar_encoded_ops[256] = {
+    ['M'] = 0, ['I'] = 1, ['D'] = 2, ['N'] = 3, ['S'] = 4, ['H'] = 5, ['P'] = 6, ['='] = 7, ['X'] = 8, ['B'] = 9,
+};
+
+uint32_t parasail_cigar_encode(uint32_t length, char op_letter)
+{
+    return (length << 4) | parasail_cigar_encoded_ops[(unsigned char)op_letter];
+}
+
+char parasail_cigar_decode_op(uint32_t cigar_int)
+{
+    const uint32_t op = cigar_int & 0xfu;
+    return op < 10 ? cigar_ops[op] : 'M';
+}
+
+uint32_t parasail_cigar_decode_len(uint32_t cigar_int)
+{
+    return cigar_int >> 4;
+}
+
+char *parasail_cigar_decode(parasail_cigar_t *cigar)
+{
+    size_t cap, used = 0;
+    int k;
+    char *s;
+    if (!cigar) { fprintf(stderr, "%s: missing %s\n", __func__, "cigar"); return NULL; }
+    cap = (size_t)cigar->len * 12 + 1;
+    s = (char *)malloc(cap);
+    if (!s) return NULL;
+    s[0] = 0;
+    for (k = 0; k < cigar->len; ++k)
+        used += (size_t)snprintf(s + used, cap - used, "%u%c", parasail_cigar_decode_len(cigar->seq[k]),
+                                 parasail_cigar_decode_op(cigar->seq[k]));
+    return s;
+}
+
+parasail_cigar_t *parasail_cigar_encode_string(const char *cigar)
+{
+    parasail_cigar_t *c;
+    size_t cap = 16;
+    const char *p = cigar;
+    if (!cigar) { fprintf(stderr, "%s: missing %s\n", __func__, "cigar"); return NULL; }
+    c = (parasail_cigar_t *)calloc(1, sizeof *c);
+    if (!c) return NULL;
+    c->seq = (uint32_t *)malloc(sizeof(uint32_t) * cap);
+    if (!c->seq) { free(c); return NULL; }
+    while (*p) {
+        char *end;
+        const unsigned long len = strtoul(p, &end, 10);
+        if (end == p || !*end || !strchr(cigar_ops, *end)) {
+            fprintf(stderr, "%s: invalid CIGAR string '%s'\n", __func__, cigar);
+            free(c->seq);
+            free(c);
+            return NULL;
+        }
+        if ((size_t)c->len == cap) {
+            uint32_t *x = (uint32_t *)realloc(c->seq, sizeof(uint32_t) * cap * 2);
+            if (!x) { free(c->seq); free(c); return NULL; }
+            c->seq = x;
+            cap *= 2;
+        }
+        c->seq[c->len++] = parasail_cigar_encode((uint32_t)len, *end);
+        p = end + 1;
+    }
+    return c;
+}
+
+void parasail_cigar_free(parasail_cigar_t *cigar)
+{
+    if (!cigar) return;
+    free(cigar->seq);
+    free(cigar);
+}
+
+/* ---- CIGAR of a trace result ------------------------------------------------ */
+
+typedef struct cigar_builder {
+    parasail_cigar_t *c;
+    size_t cap;
+    char op;          /* pending run */
+    uint32_t run;
+} cigar_builder;
+
+static int cb_flush(cigar_builder *b)
+{
+    if (!b->run) return 0;
+    if ((size_t)b->c->len == b->cap) {
+        uint32_t *x = (uint32_t *)realloc(b->c->seq, sizeof(uint32_t) * b->cap * 2);
+        if (!x) return -1;
+        b->c->seq = x;
+        b->cap *= 2;
+    }
+    b->c->seq[b->c->len++] = parasail_cigar_encode(b->run, b->op);
+    b->run = 0;
+    return 0;
+}
+
+static int cb_add(cigar_builder *b, char op, uint32_t n)
+{
+    if (!n) return 0;
+    if (b->run && b->op != op && cb_flush(b) != 0) return -1;
+    b->op = op;
+    b->run += n;
+    return 0;
+}
+
+static int same_residue(char a, char b, int case_sensitive, const char *aliases)
+{
+    size_t k, n;
+    if (!case_sensitive) { a = (char)toupper((unsigned char)a); b = (char)toupper((unsigned char)b); }
+    if (a == b) return 1;
+    if (!aliases) return 0;
+    n = strlen(aliases);
+    for (k = 0; k + 1 < n; k += 2) {
+        char x = aliases[k], y = aliases[k + 1];
+        if (!case_sensitive) { x = (char)toupper((unsigned char)x); y = (char)toupper((unsigned char)y); }
+        if ((x == a && y == b) || (y == a && x == b)) return 1;
+    }
+    return 0;
+}
+
+parasail_cigar_t *parasail_result_get_cigar_extra(parasail_result_t *result, const char *seqA, int lena,
+                                                  const char *seqB, int lenb, const parasail_matrix_t *matrix,
+                                                  int case_sensitive, const char *alphabet_aliases)
+{
+    const pb_trace_path *t;
+    cigar_builder b;
+    int i, j, k;
+    (void)matrix;
+    PB_CHECK_NULL(result);
+    PB_CHECK_NULL(seqA);
+    PB_CHECK_NULL(seqB);
+    if (!(result->flag & PARASAIL_FLAG_TRACE) || !result->extra) {
+        fprintf(stderr, "%s: assert(%s) failed\n", __func__, "parasail_result_is_trace(result)");
+        return NULL;
+    }
+    if (alphabet_aliases && strlen(alphabet_aliases) % 2 != 0) {
+        fprintf(stderr, "%s: alphabet aliases must come in pairs\n", __func__);
+        return NULL;
+    }
+    t = (const pb_trace_path *)result->extra;
+    memset(&b, 0, sizeof b);
+    b.c = (parasail_cigar_t *)calloc(1, sizeof *b.c);
+    b.cap = (size_t)(t->n + 4);
+    if (!b.c || !(b.c->seq = (uint32_t *)malloc(sizeof(uint32_t) * b.cap))) { free(b.c); return NULL; }
+    i = t->stop_i;
+    j = t->stop_j;
+    b.c->beg_query = i + 1;
+    b.c->beg_ref = j + 1;
+    /* the walk reached the matrix edge: the rest of the other sequence
+     * aligns against gaps and the alignment begins at 0, 0
+     * (src/cigar_template.c:145-163) */
+    if (i < 0 && j >= 0) { cb_add(&b, 'D', (uint32_t)(j + 1)); b.c->beg_ref = 0; }
+    else if (j < 0 && i >= 0) { cb_add(&b, 'I', (uint32_t)(i + 1)); b.c->beg_query = 0; }
+    /* the path's first step starts at (stop_i + 1, stop_j + 1) */
+    i += 1;
+    j += 1;
+    for (k = 0; k < t->n; ++k) {
+        const uint8_t op = t->ops[k];
+        int rc;
+        if (op == 0) {
+            if (i >= lena || j >= lenb) break;
+            rc = cb_add(&b, same_residue(seqA[i], seqB[j], case_sensitive, alphabet_aliases) ? '=' : 'X', 1);
+            ++i;
+            ++j;
+        } else if (op == 1) {
+            rc = cb_add(&b, 'I', 1);
+            ++i;
+        } else {
+            rc = cb_add(&b, 'D', 1);
+            ++j;
+        }
+        if (rc != 0) { parasail_cigar_free(b.c); return NULL; }
+    }
+    /* semi-global: the end gaps past the end cell (src/cigar_template.c:124-142) */
+    if (result->flag & PARASAIL_FLAG_SG) {
+        if (result->end_query + 1 == lena) cb_add(&b, 'D', (uint32_t)(lenb - 1 - result->end_ref));
+        else if (result->end_ref + 1 == lenb) cb_add(&b, 'I', (uint32_t)(lena - 1 - result->end_query));
+        else { parasail_cigar_free(b.c); return NULL; }
+    }
+    if (cb_flush(&b) != 0) { parasail_cigar_free(b.c); return NULL; }
+    return b.c;
+}
+
+parasail_cigar_t *parasail_result_get_cigar(parasail_result_t *result, const char *seqA, int lena,
+                                            const char *seqB, int lenb, const parasail_matrix_t *matrix)
+{
+    return parasail_result_get_cigar_extra(result, seqA, lena, seqB, lenb, matrix, 0, NULL);
+}
+
+/* ---- paths on the GPU ------------------------------------------------------- */
+
+static int trace_job(int alg, int sgflags, const parasail_matrix_t *matrix, int open, int gap, pb_job *job)
+{
+    memset(job, 0, sizeof *job);
+    job->mode.alg = alg; job->mode.sgflags = sgflags; job->mode.stats = 0; job->mode.striped = 0;
+    job->mode.open = open; job->mode.gap = gap; job->mode.mmax = matrix->max; job->mode.mmin = matrix->min;
+    job->bits = -1;     /* exact values, no width verdicts */
+    return 0;
+}
+
+static void mapper_of(const parasail_matrix_t *m, uint8_t *out)
+{
+    int c;
+    for (c = 0; c < 256; ++c) out[c] = (uint8_t)m->mapper[c];
+}
+
+/* Paths of n pairs (host characters). ends[3k..] score, end_query,
+ * end_ref; paths[k] allocated here (NULL when the pair has no path: it is
+ * outside the 16-bit bounds of the pair kernels). */
+static int trace_pairs(int alg, int sgflags, const parasail_matrix_t *matrix, int open, int gap,
+                       const char *q, const int64_t *qoff, const int *qlen,
+                       const char *t, const int64_t *toff, const int *tlen, int n,
+                       int *ends, pb_trace_path **paths)
+{
+    pb_job job;
+    pb_batch b;
+    uint8_t map[256];
+    int32_t *d_mat;
+    int64_t *ooff;
+    uint8_t *ops;
+    int *info;
+    int64_t total = 0;
+    int k, rc;
+    if (matrix->type != PARASAIL_MATRIX_TYPE_SQUARE) return -2;
+    trace_job(alg, sgflags, matrix, open, gap, &job);
+    ooff = (int64_t *)malloc(sizeof(int64_t) * (size_t)n);
+    info = (int *)malloc(sizeof(int) * 3 * (size_t)n);
+    if (!ooff || !info) { free(ooff); free(info); return -1; }
+    for (k = 0; k < n; ++k) { ooff[k] = total; total += (int64_t)qlen[k] + tlen[k]; }
+    ops = (uint8_t *)malloc((size_t)total + 16);
+    d_mat = (int32_t *)pb_cuda_malloc(sizeof(int32_t) * (size_t)matrix->size * matrix->size);
+    if (!ops || !d_mat) { free(ooff); free(info); free(ops); pb_cuda_free(d_mat); return -1; }
+    rc = pb_cuda_h2d(d_mat, matrix->matrix, sizeof(int32_t) * (size_t)matrix->size * matrix->size);
+    pb_cuda_sync();
+    memset(&b, 0, sizeof b);
+    b.alg = alg; b.sgflags = sgflags; b.open = open; b.gap = gap;
+    b.d_mat = d_mat; b.msize = matrix->size; b.mmax = matrix->max; b.mmin = matrix->min;
+    mapper_of(matrix, map);
+    if (rc == 0)
+        rc = pb_cuda_trace_pairs_host(&job, &b, map, q, qoff, qlen, t, toff, tlen, n, ends, ops, ooff, info);
+    pb_cuda_free(d_mat);
+    pb_cuda_sync();
+    for (k = 0; k < n; ++k) paths[k] = NULL;
+    for (k = 0; rc == 0 && k < n; ++k) {
+        const int steps = info[3 * k];
+        const int64_t cap = (int64_t)qlen[k] + tlen[k];
+        pb_trace_path *p;
+        if (steps < 0) continue;
+        p = (pb_trace_path *)calloc(1, sizeof *p);
+        if (!p || !(p->ops = (uint8_t *)malloc((size_t)steps + 1))) { free(p); rc = -1; break; }
+        memcpy(p->ops, ops + ooff[k] + cap - steps, (size_t)steps);
+        p->n = steps;
+        p->stop_i = info[3 * k + 1];
+        p->stop_j = info[3 * k + 2];
+        paths[k] = p;
+    }
+    free(ooff);
+    free(info);
+    free(ops);
+    return rc;
+}
+
+static parasail_result_t *trace_one(const char *func, int alg, int sgflags, int flags, const char *s1, int s1Len,
+                                    const char *s2, int s2Len, int open, int gap, const parasail_matrix_t *matrix)
+{
+    int ends[3];
+    pb_trace_path *path = NULL;
+    const int64_t zero = 0;
+    parasail_result_t *r;
+    int rc;
+    if (!pb_gpu_ready(func)) return NULL;
+    rc = trace_pairs(alg, sgflags, matrix, open, gap, s1, &zero, &s1Len, s2, &zero, &s2Len, 1, ends, &path);
+    if (rc == -2) {
+        fprintf(stderr, "%s: traceback needs a square matrix\n", func);
+        return NULL;
+    }
+    if (rc != 0) {
+        fprintf(stderr, "%s: GPU alignment failed: %s\n", func, pb_cuda_last_error());
+        return NULL;
+    }
+    if (!path) {
+        fprintf(stderr, "%s: the pair's scores leave the range of the traceback kernel (int16)\n", func);
+        return NULL;
+    }
+    r = pb_result_new(0);
+    if (!r) { free(path->ops); free(path); return NULL; }
+    r->score = ends[0];
+    r->end_query = ends[1];
+    r->end_ref = ends[2];
+    r->flag = flags | PARASAIL_FLAG_TRACE | PARASAIL_FLAG_BITS_32;
+    r->extra = path;
+    return r;
+}
+
+static int alg_flags(int alg, int sgflags)
+{
+    int f = alg == PB_SW ? PARASAIL_FLAG_SW : alg == PB_NW ? PARASAIL_FLAG_NW : PARASAIL_FLAG_SG;
+    if (alg == PB_SG) {
+        if (sgflags & PB_S1_BEG) f |= PARASAIL_FLAG_SG_S1_BEG;
+        if (sgflags & PB_S1_END) f |= PARASAIL_FLAG_SG_S1_END;
+        if (sgflags & PB_S2_BEG) f |= PARASAIL_FLAG_SG_S2_BEG;
+        if (sgflags & PB_S2_END) f |= PARASAIL_FLAG_SG_S2_END;
+    }
+    return f;
+}
+
+/* the reference's checks and messages (parasail/memory.h:46-80) */
+#define TRACE_CHECKS()            \
+    PB_CHECK_NULL(s1);            \
+    PB_CHECK_GT0(s1Len);          \
+    PB_CHECK_NULL(s2);            \
+    PB_CHECK_GT0(s2Len);          \
+    PB_CHECK_GE0(open);           \
+    PB_CHECK_GE0(gap);            \
+    PB_CHECK_NULL(matrix)
+
+#define PCHECKS()                                                         \
+    PB_CHECK_NULL(profile);                                               \
+    PB_CHECK_NULL(profile->matrix);                                       \
+    PB_CHECK_NULL(s2);                                                    \
+    PB_CHECK_GT0(s2Len);                                                  \
+    PB_CHECK_GE0(open);                                                   \
+    PB_CHECK_GE0(gap)
+
+#define TRACE_FAMILY(name, ALG, SGF)                                                                           \
+    parasail_result_t *parasail_##name##_trace(const char *const restrict s1, const int s1Len,                  \
+                                               const char *const restrict s2, const int s2Len, const int open,   \
+                                               const int gap, const parasail_matrix_t *matrix)                  \
+    {                                                                                                           \
+        TRACE_CHECKS();                                                                                         \
+        return trace_one(__func__, ALG, SGF, alg_flags(ALG, SGF) | PARASAIL_FLAG_NOVEC | PARASAIL_FLAG_LANES_1,  \
+                         s1, s1Len, s2, s2Len, open, gap, matrix);                                              \
+    }                                                                                                           \
+    parasail_result_t *parasail_##name##_trace_scan(const char *const restrict s1, const int s1Len,             \
+                                                    const char *const restrict s2, const int s2Len,              \
+                                                    const int open, const int gap,                              \
+                                                    const parasail_matrix_t *matrix)                            \
+    {                                                                                                           \
+        TRACE_CHECKS();                                                                                         \
+        return trace_one(__func__, ALG, SGF,                                                                    \
+                         alg_flags(ALG, SGF) | PARASAIL_FLAG_NOVEC_SCAN | PARASAIL_FLAG_LANES_1, s1, s1Len, s2,  \
+                         s2Len, open, gap, matrix);                                                             \
+    }                                                                                                           \
+    parasail_result_t *parasail_##name##_trace_striped_32(const char *const restrict s1, const int s1Len,       \
+                                                          const char *const restrict s2, const int s2Len,        \
+                                                          const int open, const int gap,                        \
+                                                          const parasail_matrix_t *matrix)                      \
+    {                                                                                                           \
+        TRACE_CHECKS();                                                                                         \
+        return trace_one(__func__, ALG, SGF, alg_flags(ALG, SGF) | PARASAIL_FLAG_STRIPED | PARASAIL_FLAG_LANES_8, \
+                         s1, s1Len, s2, s2Len, open, gap, matrix);                                              \
+    }                                                                                                           \
+    parasail_result_t *parasail_##name##_trace_scan_32(const char *const restrict s1, const int s1Len,          \
+                                                       const char *const restrict s2, const int s2Len,           \
+                                                       const int open, const int gap,                           \
+                                                       const parasail_matrix_t *matrix)                         \
+    {                                                                                                           \
+        TRACE_CHECKS();                                                                                         \
+        return trace_one(__func__, ALG, SGF, alg_flags(ALG, SGF) | PARASAIL_FLAG_SCAN | PARASAIL_FLAG_LANES_8,   \
+                         s1, s1Len, s2, s2Len, open, gap, matrix);                                              \
+    }                                                                                                           \
+    parasail_result_t *parasail_##name##_trace_striped_profile_32(const parasail_profile_t *const restrict profile, \
+                                                                  const char *const restrict s2, const int s2Len, \
+                                                                  const int open, const int gap)                \
+    {                                                                                                           \
+        PCHECKS();                                                                                              \
+        return trace_one(__func__, ALG, SGF, alg_flags(ALG, SGF) | PARASAIL_FLAG_STRIPED | PARASAIL_FLAG_LANES_8, \
+                         profile->s1, profile->s1Len, s2, s2Len, open, gap, profile->matrix);                   \
+    }                                                                                                           \
+    parasail_result_t *parasail_##name##_trace_scan_profile_32(const parasail_profile_t *const restrict profile,   \
+                                                               const char *const restrict s2, const int s2Len,    \
+                                                               const int open, const int gap)                   \
+    {                                                                                                           \
+        PCHECKS();                                                                                              \
+        return trace_one(__func__, ALG, SGF, alg_flags(ALG, SGF) | PARASAIL_FLAG_SCAN | PARASAIL_FLAG_LANES_8,   \
+                         profile->s1, profile->s1Len, s2, s2Len, open, gap, profile->matrix);                   \
+    }
+
+TRACE_FAMILY(sw, PB_SW, 0)
+TRACE_FAMILY(nw, PB_NW, 0)
+TRACE_FAMILY(sg, PB_SG, PB_S1_BEG | PB_S1_END | PB_S2_BEG | PB_S2_END)
+TRACE_FAMILY(sg_qb, PB_SG, PB_S1_BEG)
+TRACE_FAMILY(sg_qe, PB_SG, PB_S1_END)
+TRACE_FAMILY(sg_qx, PB_SG, PB_S1_BEG | PB_S1_END)
+TRACE_FAMILY(sg_db, PB_SG, PB_S2_BEG)
+TRACE_FAMILY(sg_de, PB_SG, PB_S2_END)
+TRACE_FAMILY(sg_dx, PB_SG, PB_S2_BEG | PB_S2_END)
+TRACE_FAMILY(sg_qb_de, PB_SG, PB_S1_BEG | PB_S2_END)
+TRACE_FAMILY(sg_qe_db, PB_SG, PB_S1_END | PB_S2_BEG)
+TRACE_FAMILY(sg_qb_db, PB_SG, PB_S1_BEG | PB_S2_BEG)
+TRACE_FAMILY(sg_qe_de, PB_SG, PB_S1_END | PB_S2_END)
+
+/* ---- batch CIGARs (include/parasail_b200.h) ------------------------------- */
+
+int parasail_b200_batch_pairs_cigar(const char *funcname, const parasail_matrix_t *matrix,
+                                    const char *queries, const int64_t *qoffsets, const int *qlengths,
+                                    const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+                                    int open, int gap, parasail_b200_record_t *records, uint32_t *cigars,
+                                    int *cigar_lengths, int *beg_query, int *beg_ref)
+{
+    static const struct { const char *name; int alg, sgf; } algs[] = {
+        {"sw", PB_SW, 0}, {"nw", PB_NW, 0},
+        {"sg_qb_de", PB_SG, PB_S1_BEG | PB_S2_END}, {"sg_qe_db", PB_SG, PB_S1_END | PB_S2_BEG},
+        {"sg_qb_db", PB_SG, PB_S1_BEG | PB_S2_BEG}, {"sg_qe_de", PB_SG, PB_S1_END | PB_S2_END},
+        {"sg_qb", PB_SG, PB_S1_BEG}, {"sg_qe", PB_SG, PB_S1_END}, {"sg_qx", PB_SG, PB_S1_BEG | PB_S1_END},
+        {"sg_db", PB_SG, PB_S2_BEG}, {"sg_de", PB_SG, PB_S2_END}, {"sg_dx", PB_SG, PB_S2_BEG | PB_S2_END},
+        {"sg", PB_SG, PB_S1_BEG | PB_S1_END | PB_S2_BEG | PB_S2_END},
+    };
+    const char *s = funcname;
+    int alg = -1, sgf = 0, flags = 0, k, rc;
+    int64_t off = 0;
+    int *ends;
+    pb_trace_path **paths;
+    size_t a;
+    if (!matrix || !queries || !qoffsets || !qlengths || !targets || !toffsets || !tlengths || !records || !cigars ||
+        !cigar_lengths || !beg_query || !beg_ref || !funcname) {
+        fprintf(stderr, "%s: missing arguments\n", __func__);
+        return -1;
+    }
+    if (n < 0 || open < 0 || gap < 0) { fprintf(stderr, "%s: invalid n/open/gap\n", __func__); return -1; }
+    if (n == 0) return 0;
+    if (0 == strncmp(s, "parasail_", 9)) s += 9;
+    for (a = 0; a < sizeof algs / sizeof algs[0]; ++a) {
+        const size_t l = strlen(algs[a].name);
+        if (0 == strncmp(s, algs[a].name, l) && 0 == strncmp(s + l, "_trace", 6)) {
+            alg = algs[a].alg; sgf = algs[a].sgf; s += l + 6; break;
+        }
+    }
+    if (alg >= 0) {
+        if (!*s) flags = PARASAIL_FLAG_NOVEC | PARASAIL_FLAG_LANES_1;
+        else if (!strcmp(s, "_scan")) flags = PARASAIL_FLAG_NOVEC_SCAN | PARASAIL_FLAG_LANES_1;
+        else if (!strcmp(s, "_striped_32")) flags = PARASAIL_FLAG_STRIPED | PARASAIL_FLAG_LANES_8;
+        else if (!strcmp(s, "_scan_32")) flags = PARASAIL_FLAG_SCAN | PARASAIL_FLAG_LANES_8;
+        else alg = -1;
+    }
+    if (alg < 0) { fprintf(stderr, "%s: unknown trace function '%s'\n", __func__, funcname); return -1; }
+    for (k = 0; k < n; ++k)
+        if (qlengths[k] <= 0 || tlengths[k] <= 0) { fprintf(stderr, "%s: pair %d has an empty sequence\n", __func__, k); return -1; }
+    if (!pb_gpu_ready(__func__)) return -1;
+    ends = (int *)malloc(sizeof(int) * 3 * (size_t)n);
+    paths = (pb_trace_path **)calloc((size_t)n, sizeof *paths);
+    if (!ends || !paths) { free(ends); free(paths); return -1; }
+    rc = trace_pairs(alg, sgf, matrix, open, gap, queries, qoffsets, qlengths, targets, toffsets, tlengths, n, ends,
+                     paths);
+    if (rc == -2) fprintf(stderr, "%s: traceback needs a square matrix\n", __func__);
+    for (k = 0; rc == 0 && k < n; off += (int64_t)qlengths[k] + tlengths[k], ++k) {
+        parasail_result_t r;
+        parasail_cigar_t *c;
+        parasail_b200_record_t *rec = &records[k];
+        memset(rec, 0, sizeof *rec);
+        cigar_lengths[k] = -1;
+        beg_query[k] = beg_ref[k] = 0;
+        rec->score = ends[3 * k]; rec->end_query = ends[3 * k + 1]; rec->end_ref = ends[3 * k + 2];
+        rec->flag = alg_flags(alg, sgf) | flags | PARASAIL_FLAG_TRACE | PARASAIL_FLAG_BITS_32;
+        if (!paths[k]) continue;
+        memset(&r, 0, sizeof r);
+        r.score = rec->score; r.end_query = rec->end_query; r.end_ref = rec->end_ref; r.flag = rec->flag;
+        r.extra = paths[k];
+        c = parasail_result_get_cigar(&r, queries + qoffsets[k], qlengths[k], targets + toffsets[k], tlengths[k],
+                                      matrix);
+        if (c) {
+            memcpy(cigars + off, c->seq, sizeof(uint32_t) * (size_t)c->len);
+            cigar_lengths[k] = c->len;
+            beg_query[k] = c->beg_query;
+            beg_ref[k] = c->beg_ref;
+            parasail_cigar_free(c);
+        }
+    }
+    for (k = 0; k < n; ++k) if (paths[k]) { free(paths[k]->ops); free(paths[k]); }
+    free(paths);
+    free(ends);
+    if (rc != 0) fprintf(stderr, "%s: GPU alignment failed\n", __func__);
+    return rc;
+}

@@ -1,0 +1,85 @@
+"""Traceback and CIGAR: the trace entry points of parasail.h (serial and
+32-bit striped/scan forms, direct and profile) and the batch CIGAR call,
+against the reference's own trace functions and parasail_result_get_cigar
+(src/cigar.c) compiled into oracle/_ref; and the CIGAR string helpers on
+CPU."""
+import random
+
+import pytest
+
+import oracle as O
+from conftest import AA, DNA, rand_seq, mutate
+
+pb = pytest.importorskip("parasail_b200")
+
+ALGS = ["sw", "nw", "sg", "sg_qb", "sg_qe", "sg_qx", "sg_db", "sg_de", "sg_dx", "sg_qb_de", "sg_qe_db",
+        "sg_qb_db", "sg_qe_de"]
+FORMS = ["", "_scan", "_striped_32", "_scan_32"]
+
+
+def test_cigar_string_round_trip():
+    for s in ("3=2I2=1X4D14=", "1=", "120M", "7S3=1X"):
+        c = pb.lib.parasail_cigar_encode_string(s.encode())
+        assert c
+        assert pb.cigar_string(c)[0] == s
+    x = pb.lib.parasail_cigar_encode(17, b"X")
+    assert x == (17 << 4) | 8
+    assert pb.lib.parasail_cigar_decode_op(x) == b"X" and pb.lib.parasail_cigar_decode_len(x) == 17
+
+
+def _pairs(rng, n, alpha):
+    out = []
+    for _ in range(n):
+        q = rand_seq(rng, rng.randint(2, 160), alpha)
+        r = rng.random()
+        t = mutate(rng, q, alpha, 0.15, 0.06) if r < 0.6 else \
+            (rand_seq(rng, 20, alpha) + q[5:] + rand_seq(rng, 7, alpha) if r < 0.8 else
+             rand_seq(rng, rng.randint(2, 160), alpha))
+        out.append((q, t))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(O.ref() is None, reason="reference library not built")
+def test_trace_cigar_vs_reference():
+    """Every algorithm and trace form on protein and DNA pairs (open > gap
+    and open == gap): score, ends, flags, CIGAR and begin positions equal
+    the reference's."""
+    rng = random.Random(123)
+    b62 = pb.matrix_lookup("blosum62")
+    dna = pb.matrix_create("ACGT", 2, -3)
+    bad, total = [], 0
+    for key, m, alpha, pens in (("blosum62", b62, AA, ((11, 1), (3, 3))), (("ACGT", 2, -3), dna, DNA, ((5, 2),))):
+        for q, t in _pairs(rng, 12, alpha):
+            for op, gp in pens:
+                for alg in ALGS:
+                    for form in FORMS:
+                        exp = O.ref_trace(alg, form, q, t, op, gp, key)
+                        if alg == "sw" and exp["score"] < 0:
+                            continue     # a reference quirk, see the test below
+                        got = pb.trace("parasail_%s_trace%s" % (alg, form), q, t, op, gp, m)
+                        total += 1
+                        if got != exp:
+                            bad.append((alg, form, op, gp, q, t, got, exp))
+    assert total > 2000
+    assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])
+
+
+@pytest.mark.gpu
+def test_trace_profile_forms_and_batch_equal_direct():
+    rng = random.Random(7)
+    b62 = pb.matrix_lookup("blosum62")
+    pairs = _pairs(rng, 40, AA)
+    for alg in ("sw", "nw", "sg_qx", "sg_de"):
+        for form in ("_striped", "_scan"):
+            for q, t in pairs[:8]:
+                prof = pb.ProfileHandle("parasail_profile_create_32", q, b62)
+                a = pb.trace("parasail_%s_trace%s_profile_32" % (alg, form), q, t, 11, 1, b62, profile=prof)
+                b = pb.trace("parasail_%s_trace%s_32" % (alg, form), q, t, 11, 1, b62)
+                prof.close()
+                assert a == b, (alg, form)
+        qs, ts = [p[0] for p in pairs], [p[1] for p in pairs]
+        for form in ("", "_scan_32"):
+            got = pb.batch_pairs_cigar("%s_trace%s" % (alg, form), b62, qs, ts, 11, 1)
+            for q, t, g in zip(qs, ts, got):
+                assert g == pb.trace("parasail_%s_trace%s" % (alg, form), q, t, 11, 1, b62), (alg, form)
