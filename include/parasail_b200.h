@@ -108,6 +108,30 @@ extern int parasail_b200_batch_db_device(
         const uint8_t *d_codes, const int64_t *d_offsets, const int *d_lengths, int n,
         int open, int gap, parasail_b200_record_t *d_records);
 
+/** A database-search plan: parasail_b200_batch_db_device prepared once
+ * and recorded as a CUDA graph. Creation does the host-side work that
+ * depends only on the profiles and the target lengths (the length order of
+ * the targets, the task list, the concatenated profiles, every device
+ * buffer) and captures the device work of one search -- the int16x2
+ * score kernel, the count of pairs past its 16-bit range and the width
+ * resolution of the 8 -> 16 -> 32 chain writing d_records -- in one graph.
+ * Each parasail_b200_db_plan_run replays it on the current contents of
+ * d_codes (same offsets and lengths) and gives the records
+ * parasail_b200_batch_db_device would give; a search with a pair past the
+ * 16-bit range runs once through the full pipeline instead. Plans hold the
+ * Smith-Waterman score-only functions (sw_{striped,scan}_profile_{8,16,32,sat})
+ * with open > gap and profiles whose scores fit int8; creation returns NULL
+ * for anything else. The buffers must outlive the plan. Replaces the
+ * reference aligner's repeated searches of one database
+ * (apps/parasail_aligner.cpp:1694-1740) without per-call host work. */
+typedef struct parasail_b200_db_plan parasail_b200_db_plan_t;
+extern parasail_b200_db_plan_t *parasail_b200_db_plan_create(
+        const char *funcname, const parasail_profile_t *const *profiles, int nq,
+        const uint8_t *d_codes, const int64_t *d_offsets, const int *d_lengths, int n,
+        int open, int gap, parasail_b200_record_t *d_records);
+extern int parasail_b200_db_plan_run(parasail_b200_db_plan_t *plan);
+extern void parasail_b200_db_plan_free(parasail_b200_db_plan_t *plan);
+
 /** Independent pairs: query i against target i, both from host memory,
  * scored with `matrix` by the direct-form function `funcname`
  * ("nw_stats_scan_16", "sg_qx_stats_striped_16", ...). Replaces n calls of

@@ -577,3 +577,11 @@ def batch_pairs_cigar(name, matrix, queries, targets, open_, gap):
                     "beg_ref": int(br[k]) if s is not None else None})
         off += int(ql[k] + tl[k])
     return out
+
+
+lib.parasail_b200_db_plan_create.restype = ctypes.c_void_p
+lib.parasail_b200_db_plan_create.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int] + \
+    [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+lib.parasail_b200_db_plan_run.restype = ctypes.c_int
+lib.parasail_b200_db_plan_run.argtypes = [ctypes.c_void_p]
+lib.parasail_b200_db_plan_free.argtypes = [ctypes.c_void_p]

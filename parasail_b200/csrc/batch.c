@@ -434,3 +434,54 @@ int parasail_b200_batch_all_device(const char *funcname, const parasail_matrix_t
     pb_cuda_sync();
     return rc;
 }
+
+/* ---- database-search plans ---------------------------------------------- */
+
+struct parasail_b200_db_plan {
+    void *plan;
+};
+
+parasail_b200_db_plan_t *parasail_b200_db_plan_create(const char *funcname, const parasail_profile_t *const *profiles,
+                                                      int nq, const uint8_t *d_codes, const int64_t *d_offsets,
+                                                      const int *d_lengths, int n, int open, int gap,
+                                                      parasail_b200_record_t *d_records)
+{
+    pb_job job;
+    pb_batch b;
+    const pb_device_profile **profs;
+    parasail_b200_db_plan_t *pl;
+    if (n <= 0 || !d_codes || !d_offsets || !d_lengths || !d_records) {
+        fprintf(stderr, "%s: missing arrays or n <= 0\n", __func__);
+        return NULL;
+    }
+    profs = (const pb_device_profile **)malloc(sizeof(*profs) * (size_t)(nq > 0 ? nq : 1));
+    pl = (parasail_b200_db_plan_t *)calloc(1, sizeof *pl);
+    if (!profs || !pl) { free(profs); free(pl); return NULL; }
+    if (db_common(__func__, funcname, profiles, nq, n, open, gap, &job, profs) != 0) {
+        free(profs); free(pl); return NULL;
+    }
+    memset(&b, 0, sizeof b);
+    b.alg = job.mode.alg; b.sgflags = job.mode.sgflags; b.stats = job.mode.stats;
+    b.open = open; b.gap = gap; b.profs = profs; b.nprofs = nq; b.npairs = n;
+    b.d_targets = d_codes; b.d_toff = d_offsets; b.d_tlen = d_lengths;
+    if (pb_cuda_db_plan_create(&job, &b, (pb_record *)d_records, &pl->plan) != 0) {
+        fprintf(stderr, "%s: '%s' cannot be planned (plans hold Smith-Waterman score-only searches with "
+                "open > gap and int8 profiles)\n", __func__, funcname ? funcname : "(null)");
+        free(profs); free(pl); return NULL;
+    }
+    free(profs);
+    return pl;
+}
+
+int parasail_b200_db_plan_run(parasail_b200_db_plan_t *plan)
+{
+    if (!plan) { fprintf(stderr, "%s: missing %s\n", __func__, "plan"); return -1; }
+    return pb_cuda_db_plan_run(plan->plan);
+}
+
+void parasail_b200_db_plan_free(parasail_b200_db_plan_t *plan)
+{
+    if (!plan) return;
+    pb_cuda_db_plan_free(plan->plan);
+    free(plan);
+}

@@ -166,6 +166,15 @@ int resolve_rounds(const pb_job &job, const pb_lane_args &la, const pb_pair_out 
     return rc;
 }
 
+/* One resolution pass of n pairs of one query (no lane-exact rounds): the
+ * width verdicts of jobs whose every width the exact values settle. */
+void launch_resolve_plain(const pb_job &job, const pb_pair_out *o1, int qlen_all, const int *tlen, int n,
+                          pb_record *rec, int *need, int *counts, cudaStream_t st)
+{
+    k_resolve<<<(n + 255) / 256, 256, 0, st>>>(job, o1, nullptr, nullptr, qlen_all, tlen, n, n, nullptr, nullptr,
+                                               rec, need, counts);
+}
+
 /* the lane arguments of query q of a batch */
 pb_lane_args lane_args_of(const pb_batch *b, int q, const pb_pair_out *o1)
 {

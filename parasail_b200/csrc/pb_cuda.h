@@ -150,6 +150,12 @@ int pb_cuda_batch_host(const struct pb_job *job, const pb_batch *tmpl, const uin
                        const char *h_queries, const int64_t *h_qoff, const int *h_qlen,
                        int n, struct pb_record *h_rec);
 
+/* Database-search plans (pb_sw16.cu): SW score-only searches recorded
+ * once as a CUDA graph and replayed. */
+int pb_cuda_db_plan_create(const struct pb_job *job, const pb_batch *b, struct pb_record *d_rec, void **plan);
+int pb_cuda_db_plan_run(void *plan);
+void pb_cuda_db_plan_free(void *plan);
+
 /* All-vs-all: the upper triangle of n device-resident sequences (codes),
  * pair p = (i, j), i < j, row-major, query i against target j, run as a
  * pairs batch (tmpl in pairs mode: matrix table set, queries unset);

@@ -139,6 +139,8 @@ int resolve_rounds(const pb_job &job, const pb_lane_args &la, const pb_pair_out 
                    const int *qlen, int qlen_all, const int *tlen, int n, pb_record *rec, cudaStream_t st,
                    void *work, size_t work_bytes);
 pb_lane_args lane_args_of(const pb_batch *b, int q, const pb_pair_out *o1);
+void launch_resolve_plain(const pb_job &job, const pb_pair_out *o1, int qlen_all, const int *tlen, int n,
+                          pb_record *rec, int *need, int *counts, cudaStream_t st);
 void launch_sw16(const Sw16Params &p, cudaStream_t st);
 
 }  // namespace pb

@@ -366,33 +366,31 @@ __global__ void k_scatter(const pb_pair_out *src, const int *list, int n, pb_pai
 
 }  // namespace
 
-/* nq profiles against the same targets; out[q * npairs + i]. */
-extern "C" int pb_cuda_align_sw16_multi(const pb_batch *b, pb_pair_out *d_out_all)
+/* Everything the score kernel needs for a batch that depends only on the
+ * profiles and the target lengths: the length order of the targets, the
+ * task list (most cells first, team tasks at the front), the concatenated
+ * int8 profiles and the per-warp pass buffers. Buffers come from st's pool
+ * and are released by sw16_release. */
+struct Sw16Prep {
+    pb::Sw16Params p;
+    int blocks;
+    size_t prof_bytes;
+    int *counter;                 /* [warp tasks, team tasks, error, spare] */
+    void *bufs[9];
+};
+
+static void sw16_release(Sw16Prep *pr, cudaStream_t st)
 {
-    if (pb_cuda_init() != 0) return -1;
+    for (void *x : pr->bufs) if (x) cudaFreeAsync(x, st);
+    memset(pr->bufs, 0, sizeof pr->bufs);
+}
+
+static int sw16_prepare(const pb_batch *b, pb_pair_out *d_out_all, size_t prof_bytes, cudaStream_t st,
+                        Sw16Prep *pr)
+{
     const int n = b->npairs, nq = b->nprofs;
-    if (n <= 0 || nq <= 0) return 0;
-    bool ok = b->alg == PB_SW && !b->stats && !b->d_qlim && !b->d_tlim && b->open + b->gap <= 30000;
-    size_t prof_bytes = 0;
-    for (int q = 0; q < nq && ok; ++q) {
-        const pb_device_profile *dp = b->profs[q];
-        ok = dp->fits8 && dp->size == b->profs[0]->size;
-        prof_bytes += (size_t)dp->size * dp->lp;
-    }
-    if (!ok || prof_bytes > 200 * 1024) {
-        /* outside this kernel's domain: the exact kernel, one profile at a time */
-        for (int q = 0; q < nq; ++q) {
-            pb_batch one = *b;
-            one.profs = &b->profs[q];
-            one.nprofs = 1;
-            one.d_out = d_out_all + (size_t)q * n;
-            if (pb_cuda_align_exact(&one) != 0) return -1;
-        }
-        return 0;
-    }
-    cudaStream_t st = 0;
-    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-    int rc = 0;
+    memset(pr, 0, sizeof *pr);
+    pr->prof_bytes = prof_bytes;
     /* targets sorted by length, descending */
     int *keys_sorted = nullptr, *idx = nullptr, *order = nullptr, *counter = nullptr;
     void *tmp = nullptr;
@@ -459,17 +457,21 @@ extern "C" int pb_cuda_align_sw16_multi(const pb_batch *b, pb_pair_out *d_out_al
     if (per_sm < 1) per_sm = 1;
     int blocks = per_sm * nsm;
     const int need = (int)((sorted_tasks.size() + pb::SW16_WARPS - 1) / pb::SW16_WARPS);
-    if (blocks > need) blocks = need;
+    /* few tasks (a small database, e.g. one query against 1,000 targets):
+     * every task gets a block of its own and is run as a team task, its
+     * passes spread over the block's warps, instead of leaving most SMs
+     * idle with one warp per task */
+    const bool few = (int)sorted_tasks.size() <= blocks;
+    if (few) blocks = (int)sorted_tasks.size();
+    else if (blocks > need) blocks = need;
     const int maxlen = hlen[0] + 1;
     uint32_t *scratch = nullptr;
-    if (cudaMallocAsync((void **)&scratch, sizeof(uint2) * (size_t)maxlen * 32 * blocks * pb::SW16_WARPS, st) != cudaSuccess) {
-        cudaStreamDestroy(st);
-        return -1;
-    }
+    if (cudaMallocAsync((void **)&scratch, sizeof(uint2) * (size_t)maxlen * 32 * blocks * pb::SW16_WARPS, st) != cudaSuccess)
+        scratch = nullptr;
     /* team tasks: those above a fair share of the work per warp, which one
      * warp alone would finish last */
-    int nteam = 0;
-    {
+    int nteam = few ? (int)sorted_tasks.size() : 0;
+    if (!few) {
         double total = 0.0;
         for (const auto &t : sorted_tasks) total += (double)hq[t.q].qlen * hlen[t.first];
         const double fair = total / ((double)blocks * pb::SW16_WARPS);
@@ -477,18 +479,71 @@ extern "C" int pb_cuda_align_sw16_multi(const pb_batch *b, pb_pair_out *d_out_al
                (double)hq[sorted_tasks[nteam].q].qlen * hlen[sorted_tasks[nteam].first] > fair)
             ++nteam;
     }
-    pb::Sw16Params p;
+    pb::Sw16Params &p = pr->p;
     p.open = b->open; p.gap = b->gap; p.npairs = n; p.nq = nq;
     p.ntasks = (int)sorted_tasks.size(); p.maxlen = maxlen; p.nteam = nteam;
     p.queries = d_q; p.prof_all = prof_all; p.prof_bytes = (int)prof_bytes;
     p.order = order; p.tasks = d_tasks;
     p.targets = b->d_targets; p.toff = b->d_toff; p.tlen = b->d_tlen;
     p.scratch = scratch; p.out = d_out_all;
+    pr->blocks = blocks;
+    pr->counter = counter;
+    void *owned[9] = {keys_sorted, idx, order, counter, tmp, prof_all, d_tasks, d_q, scratch};
+    memcpy(pr->bufs, owned, sizeof owned);
+    if (!keys_sorted || !idx || !order || !counter || !tmp || !prof_all || !d_tasks || !d_q || !scratch ||
+        cudaGetLastError() != cudaSuccess) {
+        sw16_release(pr, st);
+        return -1;
+    }
+    return 0;
+}
+
+/* the kernel on a prepared batch (its counters zeroed first) */
+static void sw16_launch(const Sw16Prep &pr, cudaStream_t st)
+{
+    cudaMemsetAsync(pr.counter, 0, sizeof(int) * 4, st);
+    pb::k_sw16<<<pr.blocks, pb::SW16_WARPS * 32, pr.prof_bytes, st>>>(pr.p, pr.counter);
+}
+
+/* nq profiles against the same targets; out[q * npairs + i]. */
+extern "C" int pb_cuda_align_sw16_multi(const pb_batch *b, pb_pair_out *d_out_all)
+{
+    if (pb_cuda_init() != 0) return -1;
+    const int n = b->npairs, nq = b->nprofs;
+    if (n <= 0 || nq <= 0) return 0;
+    bool ok = b->alg == PB_SW && !b->stats && !b->d_qlim && !b->d_tlim && b->open + b->gap <= 30000;
+    size_t prof_bytes = 0;
+    for (int q = 0; q < nq && ok; ++q) {
+        const pb_device_profile *dp = b->profs[q];
+        ok = dp->fits8 && dp->size == b->profs[0]->size;
+        prof_bytes += (size_t)dp->size * dp->lp;
+    }
+    if (!ok || prof_bytes > 200 * 1024) {
+        /* outside this kernel's domain: the exact kernel, one profile at a time */
+        for (int q = 0; q < nq; ++q) {
+            pb_batch one = *b;
+            one.profs = &b->profs[q];
+            one.nprofs = 1;
+            one.d_out = d_out_all + (size_t)q * n;
+            if (pb_cuda_align_exact(&one) != 0) return -1;
+        }
+        return 0;
+    }
+    cudaStream_t st = 0;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    int rc = 0;
+    Sw16Prep prep;
+    if (sw16_prepare(b, d_out_all, prof_bytes, st, &prep) != 0) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+        return -1;
+    }
+    int *counter = prep.counter;
     cudaEvent_t ev0, ev1;
     cudaEventCreate(&ev0);
     cudaEventCreate(&ev1);
     cudaEventRecord(ev0, st);
-    pb::k_sw16<<<blocks, pb::SW16_WARPS * 32, prof_bytes, st>>>(p, counter);
+    sw16_launch(prep, st);
     cudaEventRecord(ev1, st);
     if (cudaGetLastError() != cudaSuccess) rc = -1;
     pb_diag_count_launch(2);   /* k_iota, k_sw16 */
@@ -542,9 +597,7 @@ extern "C" int pb_cuda_align_sw16_multi(const pb_batch *b, pb_pair_out *d_out_al
         }
     }
     cudaFreeAsync(list, st); cudaFreeAsync(otlen, st); cudaFreeAsync(otoff, st);
-    cudaFreeAsync(scratch, st); cudaFreeAsync(prof_all, st); cudaFreeAsync(tmp, st);
-    cudaFreeAsync(keys_sorted, st); cudaFreeAsync(idx, st); cudaFreeAsync(order, st);
-    cudaFreeAsync(counter, st); cudaFreeAsync(d_tasks, st); cudaFreeAsync(d_q, st);
+    sw16_release(&prep, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
     cudaStreamDestroy(st);
     return rc;
@@ -554,4 +607,141 @@ extern "C" int pb_cuda_align_sw16(const pb_batch *b)
 {
     if (b->nprofs != 1 || b->d_prof_index) return pb_cuda_align_exact(b);
     return pb_cuda_align_sw16_multi(b, b->d_out);
+}
+
+/* ---- database-search plans: the search as one CUDA graph ------------------ */
+
+namespace {
+
+__global__ void k_count_overflow(const pb_pair_out *__restrict__ out, int n, int *__restrict__ count)
+{
+    int c = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        c += (out[i].status & PB_ST_OVERFLOW16) != 0;
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
+struct DbPlan {
+    cudaStream_t st = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    Sw16Prep prep;
+    bool prepared = false;
+    pb_pair_out *o1 = nullptr;
+    int *need = nullptr, *counts = nullptr;   /* counts[0..2] lane lists (unused), [4] overflow */
+    pb_job job;
+    pb_batch b;
+    std::vector<const pb_device_profile *> profs;
+    pb_record *rec = nullptr;
+};
+
+void plan_destroy(DbPlan *pl)
+{
+    if (pl->exec) cudaGraphExecDestroy(pl->exec);
+    if (pl->graph) cudaGraphDestroy(pl->graph);
+    if (pl->st) {
+        if (pl->prepared) sw16_release(&pl->prep, pl->st);
+        if (pl->o1) cudaFreeAsync(pl->o1, pl->st);
+        if (pl->need) cudaFreeAsync(pl->need, pl->st);
+        if (pl->counts) cudaFreeAsync(pl->counts, pl->st);
+        cudaStreamSynchronize(pl->st);
+        cudaStreamDestroy(pl->st);
+    }
+    delete pl;
+}
+
+}  // namespace
+
+/* A Smith-Waterman score-only database search (every profile of b against
+ * every target) whose host-side preparation -- the length order of the
+ * targets, the task list, the concatenated profiles, every buffer -- is done
+ * once, and whose device work -- the int16x2 score kernel, the count of
+ * pairs past the 16-bit range and the width resolution writing d_rec -- is
+ * recorded once as a CUDA graph. Running the plan replays the graph on the
+ * current contents of b's target buffers (same lengths). Returns -1 when
+ * the job is outside what the graph holds (statistics, lane-exact widths,
+ * the score kernel's domain). */
+extern "C" int pb_cuda_db_plan_create(const pb_job *job, const pb_batch *b, pb_record *d_rec, void **out)
+{
+    *out = nullptr;
+    if (pb_cuda_init() != 0) return -1;
+    const int n = b->npairs, nq = b->nprofs;
+    const pb_mode *m = &job->mode;
+    if (n <= 0 || nq <= 0 || m->alg != PB_SW || m->stats || job->bits < 0) return -1;
+    for (int w = 8; w <= 32; w *= 2) if (pb_lane_forced(m, w)) return -1;
+    if (b->open + b->gap > 30000 || (long long)n * nq > INT32_MAX) return -1;
+    size_t prof_bytes = 0;
+    for (int q = 0; q < nq; ++q) {
+        const pb_device_profile *dp = b->profs[q];
+        if (!dp->fits8 || dp->size != b->profs[0]->size) return -1;
+        prof_bytes += (size_t)dp->size * dp->lp;
+    }
+    if (prof_bytes > 200 * 1024) return -1;
+    DbPlan *pl = new DbPlan();
+    pl->job = *job;
+    pl->profs.assign(b->profs, b->profs + nq);
+    pl->b = *b;
+    pl->b.profs = pl->profs.data();
+    pl->rec = d_rec;
+    int rc = 0;
+    if (cudaStreamCreateWithFlags(&pl->st, cudaStreamNonBlocking) != cudaSuccess) { pl->st = nullptr; rc = -1; }
+    const size_t N = (size_t)n * nq;
+    if (rc == 0 && (cudaMallocAsync((void **)&pl->o1, sizeof(pb_pair_out) * N, pl->st) != cudaSuccess ||
+                    cudaMallocAsync((void **)&pl->need, sizeof(int) * 3 * (size_t)n, pl->st) != cudaSuccess ||
+                    cudaMallocAsync((void **)&pl->counts, sizeof(int) * 8, pl->st) != cudaSuccess))
+        rc = -1;
+    if (rc == 0) {
+        pb_batch bb = pl->b;
+        bb.stats = 0; bb.pad_rows = 0; bb.d_qlim = nullptr; bb.d_tlim = nullptr;
+        rc = sw16_prepare(&bb, pl->o1, prof_bytes, pl->st, &pl->prep);
+        pl->prepared = rc == 0;
+    }
+    if (rc == 0 && cudaStreamSynchronize(pl->st) != cudaSuccess) rc = -1;
+    if (rc == 0 && cudaStreamBeginCapture(pl->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = -1;
+    if (rc == 0) {
+        sw16_launch(pl->prep, pl->st);
+        cudaMemsetAsync(pl->counts, 0, sizeof(int) * 8, pl->st);
+        k_count_overflow<<<148, 256, 0, pl->st>>>(pl->o1, (int)N, pl->counts + 4);
+        for (int q = 0; q < nq; ++q)
+            pb::launch_resolve_plain(pl->job, pl->o1 + (size_t)q * n, pl->profs[q]->qlen, b->d_tlen, n,
+                                     d_rec + (size_t)q * n, pl->need, pl->counts, pl->st);
+        if (cudaStreamEndCapture(pl->st, &pl->graph) != cudaSuccess) rc = -1;
+    }
+    if (rc == 0 && cudaGraphInstantiate(&pl->exec, pl->graph, 0) != cudaSuccess) rc = -1;
+    if (rc != 0) {
+        cudaGetLastError();
+        plan_destroy(pl);
+        return -1;
+    }
+    *out = pl;
+    return 0;
+}
+
+/* Replays the plan's graph; pairs past the 16-bit range (rare: a score
+ * above 32767 - max(matrix) - 1) send the whole search once through the
+ * batch pipeline, which reruns them in 32 bits. */
+extern "C" int pb_cuda_db_plan_run(void *plan)
+{
+    DbPlan *pl = (DbPlan *)plan;
+    if (!pl) return -1;
+    int h[8] = {0};
+    if (cudaGraphLaunch(pl->exec, pl->st) != cudaSuccess) return -1;
+    pb_diag_count_launch(2 + (long)pl->profs.size());   /* k_sw16, overflow count, resolution */
+    if (cudaMemcpyAsync(h, pl->counts, sizeof h, cudaMemcpyDeviceToHost, pl->st) != cudaSuccess) return -1;
+    int herr = 0;
+    if (cudaMemcpyAsync(&herr, pl->prep.counter + 2, sizeof(int), cudaMemcpyDeviceToHost, pl->st) != cudaSuccess)
+        return -1;
+    if (cudaStreamSynchronize(pl->st) != cudaSuccess) return -1;
+    if (herr) {
+        fprintf(stderr, "pb_cuda_db_plan_run: a pass wait exceeded its bound\n");
+        return -1;
+    }
+    if (h[4] > 0) return pb_cuda_batch_run(&pl->job, &pl->b, pl->rec);
+    return 0;
+}
+
+extern "C" void pb_cuda_db_plan_free(void *plan)
+{
+    if (plan) plan_destroy((DbPlan *)plan);
 }
