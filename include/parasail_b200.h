@@ -302,6 +302,18 @@ extern int parasail_b200_nw_banded_batch(
         const char *targets, const int64_t *toffsets, const int *tlengths, int n,
         int open, int gap, int k, int *scores);
 
+/** The schedule table of global score-only pair batches: bit b set sends
+ * the pairs of length bucket b (the longer sequence at most 64 << b
+ * residues) to the intra-task wavefront kernel (a team of warps per pair)
+ * instead of the inter-task pair kernel (one thread per pair). Read on
+ * first use from $PARASAIL_B200_SCHEDULE or from schedule.txt beside the
+ * library, which the tuner (parasail_b200/tune.py) writes from measured
+ * rates per bucket; the reference has no counterpart (its one-time ISA
+ * dispatch, src/sw_dispatch.c:4082-4121, picks kernels by CPU features,
+ * not by size). */
+extern unsigned parasail_b200_schedule_get(void);
+extern void parasail_b200_schedule_set(unsigned intra_mask);
+
 /** Diagnostics: number of this library's kernel launches so far. */
 extern long parasail_b200_kernel_launches(void);
 /** Diagnostics: summed device time (ms) of the int16x2 Smith-Waterman score

@@ -9,7 +9,7 @@ library.
 """
 import importlib
 
-_SUBMODULES = ("api", "synth")
+_SUBMODULES = ("api", "synth", "tune")
 
 
 def __getattr__(name):

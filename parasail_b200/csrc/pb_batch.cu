@@ -240,7 +240,20 @@ extern "C" int pb_cuda_batch_run(const pb_job *job, const pb_batch *tmpl, pb_rec
         b.pad_rows = (job->bits < 0 || (m->alg == PB_SW && !m->stats)) ? 0
                    : (job->bits == 0 || job->bits == 8) ? 32 : job->bits == 16 ? 16 : 8;
         int nrest = 0;
-        rc = pb::p16_pass(*job, &b, 0, nullptr, o1, group, rest, &nrest, st);
+        /* global score-only pairs: the length buckets the schedule table
+         * gives the intra-task wavefront kernel go there, with every pair
+         * the pair kernels cannot take */
+        const bool wave = pb::wave_ok(*job, &b);
+        rc = pb::p16_pass(*job, &b, 0, nullptr, o1, group, rest, &nrest, st, nullptr, nullptr, nullptr,
+                          wave ? pb::pb_schedule_nw_mask() : 0u);
+        if (rc == 0 && wave && nrest > 0) {
+            int *rest2 = nullptr, nrest2 = 0;
+            if (cudaMallocAsync((void **)&rest2, sizeof(int) * (size_t)nrest, st) != cudaSuccess) rc = -1;
+            if (rc == 0) rc = pb::wave_subset(*job, &b, rest, nrest, o1, rest2, &nrest2, st);
+            if (rc == 0 && nrest2 > 0) rc = pb::exact_subset(&b, rest2, nrest2, b.stats, b.pad_rows, o1, st);
+            if (rest2) cudaFreeAsync(rest2, st);
+            nrest = 0;
+        }
         if (rc == 0 && nrest > 0) rc = pb::exact_subset(&b, rest, nrest, b.stats, b.pad_rows, o1, st);
     }
     if (rc == 0 && faststats) {

@@ -115,7 +115,18 @@ struct P16Setup {
     const int *tlen;              /* per target */
     const int *qlim, *tlim;       /* per item limits, or nullptr */
     const int *group;             /* per item query group (pairs mode), or nullptr */
+    /* length buckets (bucket b: max(rows, cols) <= 64 << b) whose items go
+     * to the intra-task kernel instead (bit b set); 0: none */
+    unsigned intra_mask;
 };
+
+/* length bucket of a pair for the schedule table */
+__host__ __device__ inline int p16_bucket(int rows, int cols)
+{
+    int m = rows > cols ? rows : cols, b = 0;
+    while (b < 31 && (64 << b) < m) ++b;
+    return b;
+}
 
 /* Runs the items of batch b that fit 16-bit lanes on the pair kernels:
  * scores and ends (prefix = 0), with statistics by the direction-bit walk
@@ -127,7 +138,18 @@ struct P16Setup {
  * query group (pairs that share a query). Synchronises st. */
 int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out *ends, pb_pair_out *out,
              const int *group, int *d_rest, int *n_rest, cudaStream_t st,
-             uint8_t *d_ops = nullptr, const int64_t *d_ops_off = nullptr, int *d_path_info = nullptr);
+             uint8_t *d_ops = nullptr, const int64_t *d_ops_off = nullptr, int *d_path_info = nullptr,
+             unsigned intra_mask = 0);
+/* Global score-only pairs (pairs mode) on the intra-task wavefront kernel
+ * (pb_nwlong.cu): the listed items of b, scores and ends into out with
+ * sound bounds for the width verdicts; items whose verdicts need exact
+ * extremes, or that the kernel cannot take, are listed in d_rest2. */
+int wave_subset(const pb_job &job, const pb_batch *b, const int *d_list, int n, pb_pair_out *out, int *d_rest2,
+                int *n_rest2, cudaStream_t st);
+/* can wave_subset take this job? */
+bool wave_ok(const pb_job &job, const pb_batch *b);
+/* the schedule table's intra-task buckets of global score-only pairs */
+unsigned pb_schedule_nw_mask();
 /* The exact kernel on the listed items of batch b (pairs or db mode),
  * outputs scattered to out[item]. stats / pad_rows as for the exact kernel. */
 int exact_subset(const pb_batch *b, const int *d_list, int n, int stats, int pad_rows, pb_pair_out *out,

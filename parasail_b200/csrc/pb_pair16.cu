@@ -61,6 +61,9 @@
 
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
+#include <dlfcn.h>
+#include <mutex>
+#include <string>
 
 #include "pb_cuda.h"
 #include "pb_kernels.cuh"
@@ -646,7 +649,7 @@ __global__ void k_p16_setup(P16Setup q, int *__restrict__ rows, int *__restrict_
     rows[item] = r;
     cols[item] = c;
     idx[item] = item;
-    bool ok = r >= 1 && c >= 1 && c <= q.max_cols && r <= 65535;
+    bool ok = r >= 1 && c >= 1 && c <= q.max_cols && r <= 65535 && !((q.intra_mask >> p16_bucket(r, c)) & 1u);
     if (ok) {
         const P16Bounds b = p16_bounds(q.alg, r, c, q.open, q.gap, q.mmax, q.mmin);
         ok = p16_fits(b, q.open, q.gap);
@@ -812,7 +815,7 @@ p16_kernel_t pick(int alg, bool bits, bool ends, bool shared, int warps)
 
 int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out *ends, pb_pair_out *out,
              const int *group, int *d_rest, int *n_rest, cudaStream_t st,
-             uint8_t *d_ops, const int64_t *d_ops_off, int *d_path_info)
+             uint8_t *d_ops, const int64_t *d_ops_off, int *d_path_info, unsigned intra_mask)
 {
     const pb_mode *m = &job.mode;
     const bool dbmode = b->nprofs > 0;
@@ -894,6 +897,7 @@ int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out
     q.tlen = b->d_tlen;
     q.qlim = b->d_qlim; q.tlim = b->d_tlim;
     q.group = dbmode ? nullptr : group;
+    q.intra_mask = intra_mask;
     k_p16_setup<<<(N + 255) / 256, 256, 0, st>>>(q, rows, cols, keys, idx, counts);
     pb_diag_count_launch(1);
     size_t sort_bytes = 0;
@@ -1049,6 +1053,85 @@ int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out
         }
     }
     *n_rest = nrest;
+    P16_CK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+/* --- the intra-task wavefront kernel on a subset (global score-only) -------- */
+
+namespace {
+
+__global__ void k_wave_fill(pb_job job, const int *__restrict__ list, int n, const int *__restrict__ score,
+                            const int *__restrict__ qlen, const int *__restrict__ tlen, pb_pair_out *__restrict__ out,
+                            int *__restrict__ rest, int *__restrict__ nrest)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int item = list[k];
+    const int rows = qlen[k], cols = tlen[k];
+    const P16Bounds bd = p16_bounds(PB_NW, rows, cols, job.mode.open, job.mode.gap, job.mode.mmax, job.mode.mmin);
+    pb_pair_out o;
+    o.score = score[k]; o.end_query = rows - 1; o.end_ref = cols - 1;
+    o.matches = o.similar = o.length = 0;
+    o.max_h = bd.ub;
+    o.min_h_real = bd.lb; o.min_f_real = bd.lb - job.mode.open; o.max_stat_real = ((rows + 31) & ~31) + cols;
+    for (int x = 0; x < 3; ++x) { o.min_h_pad[x] = bd.lb; o.max_stat_pad[x] = o.max_stat_real; o.min_f_pad[x] = bd.lb - job.mode.open; }
+    o.status = PB_ST_BOUNDED;
+    out[item] = o;
+    if (!p16_definite(job, o, rows, cols)) rest[atomicAdd(nrest, 1)] = item;
+}
+
+__global__ void k_gather_pairs(const int *__restrict__ list, int n, const int64_t *__restrict__ qoff,
+                               const int *__restrict__ qlen, const int64_t *__restrict__ toff,
+                               const int *__restrict__ tlen, int64_t *__restrict__ gqoff, int *__restrict__ gqlen,
+                               int64_t *__restrict__ gtoff, int *__restrict__ gtlen)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int item = list[k];
+    gqoff[k] = qoff[item]; gqlen[k] = qlen[item];
+    gtoff[k] = toff[item]; gtlen[k] = tlen[item];
+}
+
+}  // namespace
+
+bool wave_ok(const pb_job &job, const pb_batch *b)
+{
+    return job.mode.alg == PB_NW && !job.mode.stats && b->nprofs == 0 && b->d_mat && !b->d_qlim && !b->d_tlim &&
+           b->msize <= 32 && b->mmax <= 127 && b->mmin >= -127;
+}
+
+int wave_subset(const pb_job &job, const pb_batch *b, const int *d_list, int n, pb_pair_out *out, int *d_rest2,
+                int *n_rest2, cudaStream_t st)
+{
+    *n_rest2 = 0;
+    if (n <= 0) return 0;
+    P16Frees frees(st);
+    int64_t *gq = nullptr, *gt = nullptr;
+    int *gql = nullptr, *gtl = nullptr, *sc = nullptr, *cnt = nullptr;
+    P16_CK(cudaMallocAsync((void **)&gq, sizeof(int64_t) * n, st)); frees.add(gq);
+    P16_CK(cudaMallocAsync((void **)&gt, sizeof(int64_t) * n, st)); frees.add(gt);
+    P16_CK(cudaMallocAsync((void **)&gql, sizeof(int) * n, st)); frees.add(gql);
+    P16_CK(cudaMallocAsync((void **)&gtl, sizeof(int) * n, st)); frees.add(gtl);
+    P16_CK(cudaMallocAsync((void **)&sc, sizeof(int) * n, st)); frees.add(sc);
+    P16_CK(cudaMallocAsync((void **)&cnt, sizeof(int), st)); frees.add(cnt);
+    k_gather_pairs<<<(n + 255) / 256, 256, 0, st>>>(d_list, n, b->d_qoff, b->d_qlen, b->d_toff, b->d_tlen, gq, gql,
+                                                    gt, gtl);
+    pb_diag_count_launch(1);
+    std::vector<int> hl(n), hm((size_t)b->msize * b->msize);
+    P16_CK(cudaMemcpyAsync(hl.data(), gtl, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+    P16_CK(cudaMemcpyAsync(hm.data(), b->d_mat, sizeof(int) * hm.size(), cudaMemcpyDeviceToHost, st));
+    P16_CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
+    P16_CK(cudaStreamSynchronize(st));
+    int maxlen = 0;
+    for (int x : hl) maxlen = x > maxlen ? x : maxlen;
+    if (pb_cuda_nw_long(n, job.mode.open, job.mode.gap, hm.data(), b->msize, b->d_qall, gq, gql, b->d_targets, gt,
+                        gtl, nullptr, nullptr, maxlen, sc) != 0)
+        return -1;
+    P16_CK(cudaDeviceSynchronize());
+    k_wave_fill<<<(n + 255) / 256, 256, 0, st>>>(job, d_list, n, sc, gql, gtl, out, d_rest2, cnt);
+    pb_diag_count_launch(1);
+    P16_CK(cudaMemcpyAsync(n_rest2, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
     P16_CK(cudaStreamSynchronize(st));
     return 0;
 }
@@ -1234,4 +1317,79 @@ extern "C" int pb_cuda_trace_pairs_host(const pb_job *job, const pb_batch *tmpl,
     cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
     return rc;
+}
+
+/* ---- the schedule table -------------------------------------------------------
+ * Which length buckets of global score-only pairs run on the intra-task
+ * wavefront kernel (one team of warps per pair) rather than the inter-task
+ * pair kernel (one thread per pair). Written by the tuner
+ * (parasail_b200/tune.py) as lines "mode bucket max_len inter_gcups
+ * intra_gcups winner"; read from $PARASAIL_B200_SCHEDULE, else from
+ * schedule.txt beside the library, on first use. */
+
+namespace {
+
+std::once_flag g_sched_once;
+std::mutex g_sched_mu;
+unsigned g_sched_nw = 0;
+
+int sched_load_file(const char *path, unsigned *mask)
+{
+    FILE *f = fopen(path, "r");
+    if (!f) return -1;
+    char line[256], mode[32], win[32];
+    unsigned m = 0;
+    int bucket, maxlen;
+    double a, b;
+    while (fgets(line, sizeof line, f)) {
+        if (line[0] == '#') continue;
+        if (sscanf(line, "%31s %d %d %lf %lf %31s", mode, &bucket, &maxlen, &a, &b, win) == 6 &&
+            !strcmp(mode, "nw") && bucket >= 0 && bucket < 32 && !strcmp(win, "intra"))
+            m |= 1u << bucket;
+    }
+    fclose(f);
+    *mask = m;
+    return 0;
+}
+
+void sched_init()
+{
+    unsigned m = 0;
+    const char *env = getenv("PARASAIL_B200_SCHEDULE");
+    if (env && *env) {
+        if (sched_load_file(env, &m) == 0) g_sched_nw = m;
+        return;
+    }
+    Dl_info info;
+    if (dladdr((void *)&sched_init, &info) && info.dli_fname) {
+        std::string dir(info.dli_fname);
+        const size_t slash = dir.rfind('/');
+        dir = slash == std::string::npos ? std::string(".") : dir.substr(0, slash);
+        if (sched_load_file((dir + "/schedule.txt").c_str(), &m) == 0) g_sched_nw = m;
+    }
+}
+
+}  // namespace
+
+namespace pb {
+
+unsigned pb_schedule_nw_mask()
+{
+    std::call_once(g_sched_once, sched_init);
+    std::lock_guard<std::mutex> lk(g_sched_mu);
+    return g_sched_nw;
+}
+
+}  // namespace pb
+
+extern "C" unsigned parasail_b200_schedule_get(void)
+{
+    return pb::pb_schedule_nw_mask();
+}
+
+extern "C" void parasail_b200_schedule_set(unsigned intra_mask)
+{
+    std::call_once(g_sched_once, sched_init);
+    std::lock_guard<std::mutex> lk(g_sched_mu);
+    g_sched_nw = intra_mask;
 }

@@ -121,3 +121,38 @@ def test_short_queries_long_targets(ql):
                 keys = ("score", "end_query", "end_ref") + (("matches", "similar", "length") if stats else ())
                 assert all(r[k] == e[k] for k in keys), (name, len(t), r, e)
         prof.close()
+
+
+def test_schedule_table_routes_global_pairs_and_keeps_results():
+    """Global score-only pairs give the same records whichever schedule the
+    table names for their length bucket: the inter-task pair kernel, or the
+    intra-task wavefront kernel (also the route of pairs past the pair
+    kernel's 16-bit bounds); both equal the oracle."""
+    rng = random.Random(91)
+    dna = pb.matrix_create("ACGT", 1, -2)
+    om = O.Matrix.simple("ACGT", 1, -2)
+    qs, ts = [], []
+    for L in (20, 70, 150, 300, 700, 1500, 3000, 9000, 20000):
+        for _ in range(3):
+            q = rand_seq(rng, rng.randint(L // 2, L), DNA)
+            qs.append(q)
+            ts.append(mutate(rng, q, DNA, 0.1, 0.02))
+    saved = pb.lib.parasail_b200_schedule_get()
+    try:
+        out = {}
+        for mask in (0, 0xFFFFFFFF, 0b1010101010):
+            pb.lib.parasail_b200_schedule_set(mask)
+            out[mask] = [_rec_tuple(r) for r in pb.batch_pairs("nw_scan_32", dna, qs, ts, 4, 1)]
+        assert out[0] == out[0xFFFFFFFF] == out[0b1010101010]
+        for q, t, r in zip(qs, ts, out[0]):
+            e = O.align(O.NW, 0, 0, q, t, 4, 1, om)
+            assert r[:3] == (e["score"], e["end_query"], e["end_ref"]), (len(q), len(t))
+        # the 8 -> 16 -> 32 chain on the same pairs
+        pb.lib.parasail_b200_schedule_set(0xFFFFFFFF)
+        a = [_rec_tuple(r) for r in pb.batch_pairs("nw_striped_sat", dna, qs, ts, 4, 1)]
+        pb.lib.parasail_b200_schedule_set(0)
+        b = [_rec_tuple(r) for r in pb.batch_pairs("nw_striped_sat", dna, qs, ts, 4, 1)]
+        assert a == b
+    finally:
+        pb.lib.parasail_b200_schedule_set(saved)
+    pb.lib.parasail_matrix_free(dna)
