@@ -9,7 +9,8 @@ and the same function names and signatures for the in-scope entry points
 profile creators, parasail_nw_banded, result accessors, matrix functions and
 the name lookups), plus the traceback entry points of the exact widths (the
 serial trace forms and the 32-bit striped/scan trace forms, profile and
-direct) and the CIGAR functions. Out-of-scope families (diag, blocked, table,
+direct), the CIGAR and traceback-string functions and matrices read from
+files. Out-of-scope families (diag, blocked, table,
 rowcol, 8/16-bit and _sat trace, 64-bit lanes, ISA-specific names) are not
 declared.
 
@@ -241,6 +242,11 @@ extern parasail_matrix_t* parasail_matrix_convert_square_to_pssm(
         const parasail_matrix_t *original, const char *seq, int len);
 extern void parasail_matrix_set_value(parasail_matrix_t *matrix, int row, int col, int value);
 
+/* matrices read from a text file (square, or PSSM rows): reference
+ * parasail.h:276-279; src/io.c:960-1179 */
+extern parasail_matrix_t* parasail_matrix_from_file(const char *filename);
+extern parasail_matrix_t* parasail_matrix_from_file_case_sensitive(const char *filename);
+
 /* banded global alignment: reference parasail.h:293-296; src/nw_banded.c:29-189 */
 extern parasail_result_t* parasail_nw_banded(
         const char * const restrict s1, const int s1Len,
@@ -301,6 +307,58 @@ extern parasail_cigar_t* parasail_result_get_cigar_extra(
         int case_sensitive,
         const char *alphabet_aliases);
 extern void parasail_cigar_free(parasail_cigar_t *cigar);
+
+/* traceback strings and the printed alignment of a trace result: reference
+ * parasail.h:298-373; src/traceback.c, src/traceback_template.c */
+typedef struct parasail_traceback_{
+    char *query;
+    char *comp;
+    char *ref;
+} parasail_traceback_t;
+
+extern parasail_traceback_t* parasail_result_get_traceback(
+        parasail_result_t *result,
+        const char *seqA, int lena,
+        const char *seqB, int lenb,
+        const parasail_matrix_t *matrix,
+        char match, char pos, char neg);
+extern parasail_traceback_t* parasail_result_get_traceback_extra(
+        parasail_result_t *result,
+        const char *seqA, int lena,
+        const char *seqB, int lenb,
+        const parasail_matrix_t *matrix,
+        char match, char pos, char neg,
+        int case_sensitive,
+        const char *alphabet_aliases);
+extern void parasail_traceback_free(parasail_traceback_t *traceback);
+extern void parasail_traceback_generic(
+        const char *seqA, int lena,
+        const char *seqB, int lenb,
+        const char *nameA, const char *nameB,
+        const parasail_matrix_t *matrix,
+        parasail_result_t *result,
+        char match, char pos, char neg,
+        int width, int name_width, int use_stats);
+extern void parasail_traceback_generic_extra(
+        const char *seqA, int lena,
+        const char *seqB, int lenb,
+        const char *nameA, const char *nameB,
+        const parasail_matrix_t *matrix,
+        parasail_result_t *result,
+        char match, char pos, char neg,
+        int width, int name_width, int use_stats, int int_width,
+        FILE *stream);
+extern void parasail_traceback_generic_extra2(
+        const char *seqA, int lena,
+        const char *seqB, int lenb,
+        const char *nameA, const char *nameB,
+        const parasail_matrix_t *matrix,
+        parasail_result_t *result,
+        char match, char pos, char neg,
+        int width, int name_width, int use_stats, int int_width,
+        FILE *stream,
+        int case_sensitive,
+        const char *alphabet_aliases);
 
 /* query profiles: reference parasail.h:85201-85317; src/memory_avx2.c:28-528,
  * src/dispatch_profile.c. The 8/16/32 creators build one device profile; the

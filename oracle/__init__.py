@@ -343,7 +343,53 @@ class PCigar(ctypes.Structure):
                 ("beg_query", ctypes.c_int), ("beg_ref", ctypes.c_int)]
 
 
-def ref_trace(alg_name, form, q, t, open_, gap, matrix_key):
+class PTraceback(ctypes.Structure):
+    _fields_ = [("query", ctypes.c_void_p), ("comp", ctypes.c_void_p), ("ref", ctypes.c_void_p)]
+
+
+def ref_traceback_text(r, rp, q, t, mp, aliases=None, case_sensitive=0):
+    """The reference's traceback strings and printed alignments of its trace
+    result rp (src/traceback.c: parasail_result_get_traceback_extra and
+    parasail_traceback_generic_extra2, in the two layouts of the reference
+    aligner's EMBOSS and SSW outputs, apps/parasail_aligner.cpp:2240-2350)."""
+    import tempfile
+    libc = ctypes.CDLL(None)
+    libc.fopen.restype = ctypes.c_void_p
+    libc.fopen.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+    libc.fclose.argtypes = [ctypes.c_void_p]
+    RP = ctypes.POINTER(PResult)
+    MP = ctypes.POINTER(PMatrix)
+    r.parasail_result_get_traceback_extra.restype = ctypes.POINTER(PTraceback)
+    r.parasail_result_get_traceback_extra.argtypes = [RP, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p,
+                                                      ctypes.c_int, MP, ctypes.c_char, ctypes.c_char,
+                                                      ctypes.c_char, ctypes.c_int, ctypes.c_char_p]
+    r.parasail_traceback_free.argtypes = [ctypes.POINTER(PTraceback)]
+    r.parasail_traceback_generic_extra2.restype = None
+    r.parasail_traceback_generic_extra2.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                                                    ctypes.c_char_p, ctypes.c_char_p, MP, RP, ctypes.c_char,
+                                                    ctypes.c_char, ctypes.c_char, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                                    ctypes.c_char_p]
+    b1, b2 = q.encode(), t.encode()
+    al = aliases.encode() if aliases else None
+    tb = r.parasail_result_get_traceback_extra(rp, b1, len(b1), b2, len(b2), mp, b"|", b":", b".",
+                                               case_sensitive, al)
+    rows = (None, None, None)
+    if tb:
+        rows = tuple(ctypes.string_at(getattr(tb.contents, f)).decode() for f in ("query", "comp", "ref"))
+        r.parasail_traceback_free(tb)
+    with tempfile.NamedTemporaryFile(suffix=".txt") as f:
+        fp = libc.fopen(f.name.encode(), b"w")
+        r.parasail_traceback_generic_extra2(b1, len(b1), b2, len(b2), b"query_name", b"a_long_target_name", mp,
+                                            rp, b"|", b":", b".", 50, 14, 1, 7, fp, case_sensitive, al)
+        r.parasail_traceback_generic_extra2(b1, len(b1), b2, len(b2), b"Query:", b"Target:", mp, rp,
+                                            b"|", b"*", b"*", 60, 10, 0, 7, fp, case_sensitive, al)
+        libc.fclose(fp)
+        text = open(f.name).read()
+    return rows + (text,)
+
+
+def ref_trace(alg_name, form, q, t, open_, gap, matrix_key, strings=False):
     """The reference's trace function `parasail_{alg}_trace{form}` on one pair
     (form "", "_scan", "_striped_32" or "_scan_32"; the vector forms call
     the AVX2 kernels), followed by its parasail_result_get_cigar
@@ -374,5 +420,7 @@ def ref_trace(alg_name, form, q, t, open_, gap, matrix_key):
         s = ctypes.cast(r.parasail_cigar_decode(cg), ctypes.c_char_p).value.decode()
         out.update(cigar=s, beg_query=cg.contents.beg_query, beg_ref=cg.contents.beg_ref)
         r.parasail_cigar_free(cg)
+    if strings:
+        out["traceback"] = ref_traceback_text(r, rp, q, t, mp, **(strings if isinstance(strings, dict) else {}))
     r.parasail_result_free(rp)
     return out

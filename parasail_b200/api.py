@@ -531,9 +531,57 @@ def cigar_string(c):
     return out
 
 
-def trace(name, s1, s2, open_, gap, matrix, profile=None):
+class Traceback(ctypes.Structure):
+    _fields_ = [("query", ctypes.c_void_p), ("comp", ctypes.c_void_p), ("ref", ctypes.c_void_p)]
+
+
+_TBP = ctypes.POINTER(Traceback)
+lib.parasail_result_get_traceback_extra.restype = _TBP
+lib.parasail_result_get_traceback_extra.argtypes = [_RP, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p,
+                                                    ctypes.c_int, _MP, ctypes.c_char, ctypes.c_char,
+                                                    ctypes.c_char, ctypes.c_int, ctypes.c_char_p]
+lib.parasail_traceback_free.argtypes = [_TBP]
+lib.parasail_traceback_generic_extra2.restype = None
+lib.parasail_traceback_generic_extra2.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                                                  ctypes.c_char_p, ctypes.c_char_p, _MP, _RP, ctypes.c_char,
+                                                  ctypes.c_char, ctypes.c_char, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                                  ctypes.c_char_p]
+_libc.fopen.restype = ctypes.c_void_p
+_libc.fopen.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+_libc.fclose.argtypes = [ctypes.c_void_p]
+
+
+def traceback_text(tlib, r, s1, s2, matrix, aliases=None, case_sensitive=0):
+    """The traceback strings (parasail_result_get_traceback_extra with '|',
+    ':', '.') and the printed alignments of a trace result r in the two
+    layouts the reference aligner writes (EMBOSS-like: width 50, names 14,
+    statistics; SSW-like: width 60, names 10, '|', '*', '*'), produced by
+    library `tlib`. Returns (query, comp, ref, printed_text)."""
+    import tempfile
+    b1, b2 = s1.encode(), s2.encode()
+    al = aliases.encode() if aliases else None
+    tb = tlib.parasail_result_get_traceback_extra(r, b1, len(b1), b2, len(b2), matrix, b"|", b":", b".",
+                                                  case_sensitive, al)
+    rows = (None, None, None)
+    if tb:
+        rows = tuple(ctypes.string_at(getattr(tb.contents, f)).decode() for f in ("query", "comp", "ref"))
+        tlib.parasail_traceback_free(tb)
+    with tempfile.NamedTemporaryFile(suffix=".txt") as f:
+        fp = _libc.fopen(f.name.encode(), b"w")
+        tlib.parasail_traceback_generic_extra2(b1, len(b1), b2, len(b2), b"query_name", b"a_long_target_name",
+                                               matrix, r, b"|", b":", b".", 50, 14, 1, 7, fp, case_sensitive, al)
+        tlib.parasail_traceback_generic_extra2(b1, len(b1), b2, len(b2), b"Query:", b"Target:", matrix, r,
+                                               b"|", b"*", b"*", 60, 10, 0, 7, fp, case_sensitive, al)
+        _libc.fclose(fp)
+        text = open(f.name).read()
+    return rows + (text,)
+
+
+def trace(name, s1, s2, open_, gap, matrix, profile=None, strings=False):
     """A trace function ('parasail_sw_trace', 'parasail_nw_trace_scan_32',
-    ...) on one pair, then parasail_result_get_cigar."""
+    ...) on one pair, then parasail_result_get_cigar; with strings=True also
+    the traceback strings and printed alignment (traceback_text)."""
     b1, b2 = s1.encode(), s2.encode()
     if profile is not None:
         r = _fn(name, True)(profile.ptr, b2, len(b2), open_, gap)
@@ -547,6 +595,8 @@ def trace(name, s1, s2, open_, gap, matrix, profile=None):
     cg = lib.parasail_result_get_cigar(r, b1, len(b1), b2, len(b2), matrix)
     if cg:
         out["cigar"], out["beg_query"], out["beg_ref"] = cigar_string(cg)
+    if strings:
+        out["traceback"] = traceback_text(lib, r, s1, s2, matrix, **(strings if isinstance(strings, dict) else {}))
     lib.parasail_result_free(r)
     return out
 

@@ -239,6 +239,263 @@ parasail_cigar_t *parasail_result_get_cigar(parasail_result_t *result, const cha
     return parasail_result_get_cigar_extra(result, seqA, lena, seqB, lenb, matrix, 0, NULL);
 }
 
+/* ---- traceback strings and the printed alignment (src/traceback.c,
+ *      src/traceback_template.c) ---------------------------------------------- */
+
+/* the three rows of an alignment in forward order: query residues or '-',
+ * the comparison characters (match / pos / neg, ' ' against a gap), target
+ * residues or '-'; c_ins and c_del count the target and query residues
+ * aligned against gaps */
+typedef struct {
+    char *q, *a, *d;
+    int64_t len, c_ins, c_del;
+} tb_rows;
+
+/* the comparison character of a query and a target residue
+ * (src/traceback.c:19-70): equal (upper-cased unless case sensitive), or
+ * equal through an alias -- the alias table is upper-cased and scanned at
+ * every offset, pairing each character with the next, against the residues
+ * as they are -- gives match; otherwise the substitution score (the PSSM row
+ * of the query position for a PSSM) > 0 gives pos, else neg */
+static char tb_match_char(const char *seqA, int ai, const char *seqB, int bi, const parasail_matrix_t *m,
+                          char match, char pos, char neg, int cs, const char *al, size_t nal)
+{
+    const char a = seqA ? seqA[ai] : '*';
+    const char b = seqB[bi];
+    int same = cs ? a == b : toupper((unsigned char)a) == toupper((unsigned char)b);
+    size_t k;
+    int sub;
+    for (k = 0; al && k < nal; ++k) {
+        const char next = k + 1 < nal ? al[k + 1] : '\0';
+        if (al[k] == a) same |= next == b;
+        else if (next == a) same |= al[k] == b;
+    }
+    if (same) return match;
+    if (m->type == PARASAIL_MATRIX_TYPE_SQUARE)
+        sub = m->matrix[m->mapper[(unsigned char)a] * m->size + m->mapper[(unsigned char)b]];
+    else
+        sub = m->matrix[ai * m->size + m->mapper[(unsigned char)b]];
+    return sub > 0 ? pos : neg;
+}
+
+static void tb_rows_free(tb_rows *r)
+{
+    free(r->q);
+    free(r->a);
+    free(r->d);
+}
+
+/* The rows of a trace result: the walk of src/traceback_template.c:57-174
+ * read from the result's path -- gaps to the matrix edge first (not for SW),
+ * then the path's steps, then a semi-global alignment's end gaps past the
+ * end cell. Returns 0, or -1 (message printed) for an unusable result. */
+static int tb_build(const char *who, parasail_result_t *result, const char *seqA, int lena, const char *seqB,
+                    int lenb, const parasail_matrix_t *matrix, char match, char pos, char neg, int cs,
+                    const char *aliases_in, tb_rows *out)
+{
+    const pb_trace_path *t;
+    char al[256];
+    size_t nal = 0, k;
+    int64_t n = 0, cap, i, j, s;
+    memset(out, 0, sizeof *out);
+    if (!result || !(result->flag & PARASAIL_FLAG_TRACE) || !result->extra) {
+        fprintf(stderr, "%s: assert(%s) failed\n", who, "parasail_result_is_trace(result)");
+        return -1;
+    }
+    if (aliases_in) {
+        nal = strlen(aliases_in);
+        if (!(nal % 2 == 0 && nal < 256)) {
+            fprintf(stderr, "%s: assert(%s) failed\n", who, "aliases_size % 2 == 0 && aliases_size < 256");
+            return -1;
+        }
+        for (k = 0; k < nal; ++k) al[k] = cs ? aliases_in[k] : (char)toupper((unsigned char)aliases_in[k]);
+    }
+    t = (const pb_trace_path *)result->extra;
+    cap = (int64_t)lena + lenb + 1;
+    out->q = (char *)malloc((size_t)cap);
+    out->a = (char *)malloc((size_t)cap);
+    out->d = (char *)malloc((size_t)cap);
+    if (!out->q || !out->a || !out->d) { tb_rows_free(out); return -1; }
+#define TB_PUT(qc, ac, dc) do { if (n + 1 >= cap) goto overflow; out->q[n] = (qc); out->a[n] = (ac); out->d[n] = (dc); ++n; } while (0)
+    if (!(result->flag & PARASAIL_FLAG_SW)) {
+        if (t->stop_i < 0 && t->stop_j >= 0)
+            for (j = 0; j <= t->stop_j; ++j) { TB_PUT('-', ' ', seqB[j]); ++out->c_ins; }
+        else if (t->stop_j < 0 && t->stop_i >= 0)
+            for (i = 0; i <= t->stop_i; ++i) { TB_PUT(seqA ? seqA[i] : '*', ' ', '-'); ++out->c_del; }
+    }
+    i = t->stop_i + 1;
+    j = t->stop_j + 1;
+    for (s = 0; s < t->n; ++s) {
+        const uint8_t op = t->ops[s];
+        if (op == 0) {
+            if (i >= lena || j >= lenb) break;
+            TB_PUT(seqA ? seqA[i] : '*', tb_match_char(seqA, (int)i, seqB, (int)j, matrix, match, pos, neg, cs,
+                                                         aliases_in ? al : NULL, nal), seqB[j]);
+            ++i;
+            ++j;
+        } else if (op == 1) {
+            TB_PUT(seqA ? seqA[i] : '*', ' ', '-');
+            ++out->c_del;
+            ++i;
+        } else {
+            TB_PUT('-', ' ', seqB[j]);
+            ++out->c_ins;
+            ++j;
+        }
+    }
+    if (result->flag & PARASAIL_FLAG_SG) {
+        if (result->end_query + 1 == lena) {
+            for (j = result->end_ref + 1; j < lenb; ++j) { TB_PUT('-', ' ', seqB[j]); ++out->c_ins; }
+        } else if (result->end_ref + 1 == lenb) {
+            for (i = result->end_query + 1; i < lena; ++i) { TB_PUT(seqA ? seqA[i] : '*', ' ', '-'); ++out->c_del; }
+        } else {
+            fprintf(stderr, "%s: assert(%s) failed\n", who, "0 && \"internal error\"");
+            tb_rows_free(out);
+            return -1;
+        }
+    }
+#undef TB_PUT
+    out->q[n] = out->a[n] = out->d[n] = '\0';
+    out->len = n;
+    return 0;
+overflow:
+    fprintf(stderr, "%s: path longer than the sequences\n", who);
+    tb_rows_free(out);
+    return -1;
+}
+
+parasail_traceback_t *parasail_result_get_traceback_extra(parasail_result_t *result, const char *seqA, int lena,
+                                                          const char *seqB, int lenb,
+                                                          const parasail_matrix_t *matrix, char match, char pos,
+                                                          char neg, int case_sensitive,
+                                                          const char *alphabet_aliases)
+{
+    tb_rows r;
+    parasail_traceback_t *tb;
+    if (tb_build(__func__, result, seqA, lena, seqB, lenb, matrix, match, pos, neg, case_sensitive,
+                 alphabet_aliases, &r) != 0)
+        return NULL;
+    tb = (parasail_traceback_t *)malloc(sizeof *tb);
+    if (!tb) { tb_rows_free(&r); return NULL; }
+    tb->query = r.q;
+    tb->comp = r.a;
+    tb->ref = r.d;
+    return tb;
+}
+
+parasail_traceback_t *parasail_result_get_traceback(parasail_result_t *result, const char *seqA, int lena,
+                                                    const char *seqB, int lenb, const parasail_matrix_t *matrix,
+                                                    char match, char pos, char neg)
+{
+    return parasail_result_get_traceback_extra(result, seqA, lena, seqB, lenb, matrix, match, pos, neg, 0, NULL);
+}
+
+void parasail_traceback_free(parasail_traceback_t *traceback)
+{
+    if (!traceback) return;
+    free(traceback->query);
+    free(traceback->comp);
+    free(traceback->ref);
+    free(traceback);
+}
+
+/* a name cut or padded to w characters */
+static void tb_name(FILE *f, const char *name, int w)
+{
+    const int64_t nl = name ? (int64_t)strlen(name) : 0;
+    int64_t k;
+    for (k = 0; k < w; ++k) fputc(k < nl ? name[k] : ' ', f);
+}
+
+/* The printed alignment (src/traceback_template.c:188-489): blocks of
+ * `width` columns, each a target line (name, first and last residue
+ * positions), the comparison line and a query line; positions count from 1,
+ * offset by where a local alignment begins; then, with use_stats, length,
+ * identity, similarity, gaps and score. */
+void parasail_traceback_generic_extra2(const char *seqA, int lena, const char *seqB, int lenb, const char *nameA,
+                                       const char *nameB, const parasail_matrix_t *matrix,
+                                       parasail_result_t *result, char match, char pos, char neg, int width,
+                                       int name_width, int use_stats, int int_width, FILE *stream,
+                                       int case_sensitive, const char *alphabet_aliases)
+{
+    tb_rows r;
+    char tmp[32];
+    int64_t qp, dp, mch = 0, sim = 0, gap = 0, c, col;
+    int need;
+    if (tb_build(__func__, result, seqA, lena, seqB, lenb, matrix, match, pos, neg, case_sensitive,
+                 alphabet_aliases, &r) != 0)
+        return;
+    need = snprintf(tmp, sizeof tmp, "%llu", (unsigned long long)lena + (unsigned long long)lenb);
+    if (int_width < need) int_width = need;
+    if (result->flag & PARASAIL_FLAG_SW) {
+        qp = result->end_query + 1 - r.len + r.c_ins;
+        dp = result->end_ref + 1 - r.len + r.c_del;
+    } else {
+        qp = dp = 0;
+    }
+    for (col = 0; col < r.len; col += width) {
+        const int64_t stop = col + width < r.len ? col + width : r.len;
+        fprintf(stream, "\n");
+        tb_name(stream, nameB, name_width);
+        fprintf(stream, " %*lld ", int_width, (long long)dp + 1);
+        for (c = col; c < stop; ++c) {
+            if (r.d[c] != '-') ++dp;
+            fputc(r.d[c], stream);
+        }
+        fprintf(stream, " %*lld\n", int_width, (long long)dp);
+        for (c = 0; c < name_width + 1 + int_width + 1; ++c) fputc(' ', stream);
+        for (c = col; c < stop; ++c) {
+            const char x = r.a[c];
+            if (x == match) { ++mch; ++sim; }
+            else if (x == pos) ++sim;
+            else if (x == neg) { }
+            else if (x == ' ') ++gap;
+            else {
+                fprintf(stderr, "bad char in traceback '%c'\n", x);
+                fprintf(stderr, "%s: assert(%s) failed\n", __func__, "0 && \"internal error\"");
+                tb_rows_free(&r);
+                return;
+            }
+            fputc(x, stream);
+        }
+        fprintf(stream, "\n");
+        tb_name(stream, nameA, name_width);
+        fprintf(stream, " %*lld ", int_width, (long long)qp + 1);
+        for (c = col; c < stop; ++c) {
+            if (r.q[c] != '-') ++qp;
+            fputc(r.q[c], stream);
+        }
+        fprintf(stream, " %*lld\n", int_width, (long long)qp);
+    }
+    if (use_stats) {
+        const long long L = (long long)r.len;
+        fprintf(stream, "\n");
+        fprintf(stream, "Length: %lld\n", L);
+        fprintf(stream, "Identity:   %*lld/%lld (%4.1f%%)\n", int_width, (long long)mch, L, 100.0 * mch / L);
+        fprintf(stream, "Similarity: %*lld/%lld (%4.1f%%)\n", int_width, (long long)sim, L, 100.0 * sim / L);
+        fprintf(stream, "Gaps:       %*lld/%lld (%4.1f%%)\n", int_width, (long long)gap, L, 100.0 * gap / L);
+        fprintf(stream, "Score: %d\n", result->score);
+    }
+    tb_rows_free(&r);
+}
+
+void parasail_traceback_generic_extra(const char *seqA, int lena, const char *seqB, int lenb, const char *nameA,
+                                      const char *nameB, const parasail_matrix_t *matrix,
+                                      parasail_result_t *result, char match, char pos, char neg, int width,
+                                      int name_width, int use_stats, int int_width, FILE *stream)
+{
+    parasail_traceback_generic_extra2(seqA, lena, seqB, lenb, nameA, nameB, matrix, result, match, pos, neg,
+                                      width, name_width, use_stats, int_width, stream, 0, NULL);
+}
+
+void parasail_traceback_generic(const char *seqA, int lena, const char *seqB, int lenb, const char *nameA,
+                                const char *nameB, const parasail_matrix_t *matrix, parasail_result_t *result,
+                                char match, char pos, char neg, int width, int name_width, int use_stats)
+{
+    parasail_traceback_generic_extra2(seqA, lena, seqB, lenb, nameA, nameB, matrix, result, match, pos, neg,
+                                      width, name_width, use_stats, 7, stdout, 0, NULL);
+}
+
 /* ---- paths on the GPU ------------------------------------------------------- */
 
 static int trace_job(int alg, int sgflags, const parasail_matrix_t *matrix, int open, int gap, pb_job *job)
