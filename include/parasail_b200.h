@@ -314,6 +314,56 @@ extern int parasail_b200_nw_banded_batch(
 extern unsigned parasail_b200_schedule_get(void);
 extern void parasail_b200_schedule_set(unsigned intra_mask);
 
+/** A packed sequence set resident on the device: the '$'-separated text of
+ * parasail_sequences_pack (every sequence followed by `sentinel`), mapped
+ * through `matrix`'s mapper and stored at 2 bits a residue when every code
+ * is below 4, 5 bits below 32, else 8 (parasail_b200_seqdb_bits). Sequence
+ * k is text[offsets[k] .. offsets[k] + lengths[k]) (host arrays of the
+ * set). NULL with a message on failure. The reference keeps the packed
+ * text in host memory (apps/parasail_aligner.cpp:1077-1178). */
+typedef struct parasail_b200_seqdb parasail_b200_seqdb_t;
+extern parasail_b200_seqdb_t *parasail_b200_seqdb_create(
+        const char *text, size_t size, char sentinel, const parasail_matrix_t *matrix);
+extern void parasail_b200_seqdb_free(parasail_b200_seqdb_t *db);
+extern int parasail_b200_seqdb_count(const parasail_b200_seqdb_t *db);
+extern int parasail_b200_seqdb_bits(const parasail_b200_seqdb_t *db);
+/** text characters of the set, sentinels included */
+extern size_t parasail_b200_seqdb_size(const parasail_b200_seqdb_t *db);
+/** device bytes of the packed residues */
+extern size_t parasail_b200_seqdb_device_bytes(const parasail_b200_seqdb_t *db);
+extern const int64_t *parasail_b200_seqdb_offsets(const parasail_b200_seqdb_t *db);
+extern const int *parasail_b200_seqdb_lengths(const parasail_b200_seqdb_t *db);
+/** One-byte codes of the whole text (parasail_b200_seqdb_size bytes, 16-byte
+ * aligned device buffer; sentinels as code 0). */
+extern int parasail_b200_seqdb_unpack(const parasail_b200_seqdb_t *db, uint8_t *d_codes);
+/** Pairs of a set's sequences: query first[k] against target second[k]
+ * with the direct or profile function `funcname` (score-only or stats,
+ * any algorithm and width). The pair list is cut into batches whose device
+ * footprint (about 512 bytes a pair plus the set's unpacked codes) fits
+ * `budget` bytes (0: 4 GiB); records[k] as parasail_b200_batch_pairs gives
+ * them. The batch loop of the reference aligner
+ * (apps/parasail_aligner.cpp:414-573, :1585-1760). */
+extern int parasail_b200_batch_pairs_seqdb(
+        const char *funcname, const parasail_matrix_t *matrix, const parasail_b200_seqdb_t *db,
+        const int *first, const int *second, size_t npairs, int open, int gap, size_t budget,
+        parasail_b200_record_t *records);
+
+/** Candidate pairs of the reference aligner's exact-match filter
+ * (apps/parasail_aligner.cpp:1316-1420, :1816-1904, its enhanced suffix
+ * array walked for maximal pairs of at least `cutoff` characters): the
+ * pairs of sequences of `text` -- every sequence followed by `sentinel`,
+ * the text ending with one (parasail_sequences_pack) -- that share a
+ * substring of `cutoff` characters, computed on the GPU by sorting every
+ * cutoff-window of the text. db_chars < 0: all against all, each pair
+ * (smaller id, larger id); db_chars >= 0: the first db_chars characters are
+ * the database file and only (query id, database id) pairs are kept, ids
+ * counting all sequences of the text. *pairs (malloc'd, freed by the
+ * caller) holds 2 * *count ints, the pairs in ascending order: the
+ * reference's std::set. Returns 0, or -1 with a message. */
+extern int parasail_b200_candidate_pairs(
+        const char *text, size_t size, char sentinel, int cutoff, long db_chars,
+        int **pairs, size_t *count);
+
 /** Diagnostics: number of this library's kernel launches so far. */
 extern long parasail_b200_kernel_launches(void);
 /** Diagnostics: summed device time (ms) of the int16x2 Smith-Waterman score

@@ -424,3 +424,59 @@ def ref_trace(alg_name, form, q, t, open_, gap, matrix_key, strings=False):
         out["traceback"] = ref_traceback_text(r, rp, q, t, mp, **(strings if isinstance(strings, dict) else {}))
     r.parasail_result_free(rp)
     return out
+
+
+# ---------------------------------------------------------------------------
+# Candidate pairs of the aligner's suffix-array filter
+
+ESA_SO = os.path.join(REF_DIR, "libesa_ref.so")
+_esa = None
+
+
+def esa_pairs(text, cutoff, db_chars=-1, sentinel=b"$"):
+    """Pairs the reference aligner's enhanced-suffix-array filter keeps for
+    the '$'-separated text (bytes): the reference's own sais builds SA/LCP,
+    oracle/esa_pairs.cpp restates the traversal
+    (apps/parasail_aligner.cpp:1316-1420, :1816-1904). db_chars >= 0: the
+    first db_chars characters are the database file, the rest queries.
+    Returns a sorted list of (first, second), or None without the library."""
+    global _esa
+    if _esa is None:
+        if not os.path.exists(ESA_SO):
+            return None
+        _esa = ctypes.CDLL(ESA_SO)
+        _esa.esa_pairs.restype = ctypes.c_long
+        _esa.esa_pairs.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_ubyte, ctypes.c_int, ctypes.c_long,
+                                   ctypes.c_void_p, ctypes.c_long]
+    import numpy as np
+    cap = 1 << 16
+    while True:
+        out = np.zeros(2 * cap, np.int32)
+        k = _esa.esa_pairs(text, len(text), sentinel[0], cutoff, db_chars, out.ctypes.data, cap)
+        if k < 0:
+            raise RuntimeError("esa_pairs failed")
+        if k <= cap:
+            return [(int(out[2 * i]), int(out[2 * i + 1])) for i in range(k)]
+        cap = k
+
+
+def kmer_pairs(seqs, cutoff, n_db=None):
+    """The same pair set stated directly (pure Python, small inputs): two
+    sequences pair when they share a substring of `cutoff` characters. With
+    n_db, only (query, database) pairs, queries numbered after the database
+    sequences."""
+    seen = {}
+    for sid, s in enumerate(seqs):
+        for p in range(len(s) - cutoff + 1):
+            seen.setdefault(s[p:p + cutoff], set()).add(sid)
+    out = set()
+    for ids in seen.values():
+        ids = sorted(ids)
+        for x in range(len(ids)):
+            for y in range(x + 1, len(ids)):
+                a, b = ids[x], ids[y]
+                if n_db is None:
+                    out.add((a, b))
+                elif (a < n_db) != (b < n_db):
+                    out.add((b, a))
+    return sorted(out)

@@ -638,3 +638,111 @@ lib.parasail_b200_db_plan_free.argtypes = [ctypes.c_void_p]
 
 lib.parasail_b200_schedule_get.restype = ctypes.c_uint
 lib.parasail_b200_schedule_set.argtypes = [ctypes.c_uint]
+
+
+# ---------------------------------------------------------------------------
+# Candidate pairs of the aligner's exact-match filter
+
+lib.parasail_b200_candidate_pairs.restype = ctypes.c_int
+lib.parasail_b200_candidate_pairs.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char, ctypes.c_int,
+                                              ctypes.c_long, ctypes.POINTER(ctypes.POINTER(ctypes.c_int)),
+                                              ctypes.POINTER(ctypes.c_size_t)]
+
+
+def candidate_pairs(text, cutoff, db_chars=-1, sentinel=b"$"):
+    """parasail_b200_candidate_pairs on a '$'-separated text (bytes): the
+    sorted list of (first, second) sequence-id pairs sharing a substring of
+    `cutoff` characters."""
+    p = ctypes.POINTER(ctypes.c_int)()
+    n = ctypes.c_size_t(0)
+    rc = lib.parasail_b200_candidate_pairs(text, len(text), sentinel, cutoff, db_chars, ctypes.byref(p),
+                                           ctypes.byref(n))
+    if rc != 0:
+        raise RuntimeError("parasail_b200_candidate_pairs failed")
+    flat = p[:2 * n.value]
+    _libc.free(ctypes.cast(p, ctypes.c_void_p))
+    return list(zip(flat[0::2], flat[1::2]))
+
+
+# ---------------------------------------------------------------------------
+# Device-resident packed sequence sets
+
+lib.parasail_b200_seqdb_create.restype = ctypes.c_void_p
+lib.parasail_b200_seqdb_create.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char, _MP]
+lib.parasail_b200_seqdb_free.argtypes = [ctypes.c_void_p]
+for _f in ("parasail_b200_seqdb_count", "parasail_b200_seqdb_bits"):
+    getattr(lib, _f).restype = ctypes.c_int
+    getattr(lib, _f).argtypes = [ctypes.c_void_p]
+for _f in ("parasail_b200_seqdb_size", "parasail_b200_seqdb_device_bytes"):
+    getattr(lib, _f).restype = ctypes.c_size_t
+    getattr(lib, _f).argtypes = [ctypes.c_void_p]
+lib.parasail_b200_seqdb_offsets.restype = ctypes.POINTER(ctypes.c_int64)
+lib.parasail_b200_seqdb_offsets.argtypes = [ctypes.c_void_p]
+lib.parasail_b200_seqdb_lengths.restype = ctypes.POINTER(ctypes.c_int)
+lib.parasail_b200_seqdb_lengths.argtypes = [ctypes.c_void_p]
+lib.parasail_b200_seqdb_unpack.restype = ctypes.c_int
+lib.parasail_b200_seqdb_unpack.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+lib.parasail_b200_batch_pairs_seqdb.restype = ctypes.c_int
+lib.parasail_b200_batch_pairs_seqdb.argtypes = [ctypes.c_char_p, _MP, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_size_t, ctypes.c_void_p]
+
+
+class SeqDB:
+    """parasail_b200_seqdb_t over a '$'-separated text (bytes)."""
+
+    def __init__(self, text, matrix, sentinel=b"$"):
+        self.ptr = lib.parasail_b200_seqdb_create(text, len(text), sentinel, matrix)
+        if not self.ptr:
+            raise RuntimeError("parasail_b200_seqdb_create failed")
+        self.matrix = matrix
+
+    @property
+    def count(self):
+        return lib.parasail_b200_seqdb_count(self.ptr)
+
+    @property
+    def bits(self):
+        return lib.parasail_b200_seqdb_bits(self.ptr)
+
+    @property
+    def size(self):
+        return lib.parasail_b200_seqdb_size(self.ptr)
+
+    @property
+    def device_bytes(self):
+        return lib.parasail_b200_seqdb_device_bytes(self.ptr)
+
+    def offsets_lengths(self):
+        n = self.count
+        return (lib.parasail_b200_seqdb_offsets(self.ptr)[:n], lib.parasail_b200_seqdb_lengths(self.ptr)[:n])
+
+    def unpack(self):
+        """The one-byte codes of the text (numpy uint8), via a torch buffer."""
+        import torch
+        d = torch.zeros(self.size + 16, dtype=torch.uint8, device="cuda")
+        if lib.parasail_b200_seqdb_unpack(self.ptr, d.data_ptr()) != 0:
+            raise RuntimeError("parasail_b200_seqdb_unpack failed")
+        return d[:self.size].cpu().numpy()
+
+    def align_pairs(self, funcname, first, second, open_, gap, budget=0):
+        np = _np()
+        f = np.ascontiguousarray(first, dtype=np.int32)
+        s = np.ascontiguousarray(second, dtype=np.int32)
+        recs = np.zeros(len(f), dtype=record_dtype())
+        rc = lib.parasail_b200_batch_pairs_seqdb(funcname.encode(), self.matrix, self.ptr, f.ctypes.data,
+                                                 s.ctypes.data, len(f), open_, gap, budget, recs.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("parasail_b200_batch_pairs_seqdb failed")
+        return recs
+
+    def close(self):
+        if self.ptr:
+            lib.parasail_b200_seqdb_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
