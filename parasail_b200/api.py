@@ -144,9 +144,10 @@ class ProfileHandle:
             raise RuntimeError("%s returned NULL" % creator)
 
     def close(self):
-        if self.ptr:
+        # at interpreter exit the module globals may already be gone
+        if self.ptr and lib is not None:
             lib.parasail_profile_free(self.ptr)
-            self.ptr = None
+        self.ptr = None
 
     def __del__(self):
         self.close()
@@ -737,9 +738,9 @@ class SeqDB:
         return recs
 
     def close(self):
-        if self.ptr:
+        if self.ptr and lib is not None:
             lib.parasail_b200_seqdb_free(self.ptr)
-            self.ptr = None
+        self.ptr = None
 
     def __del__(self):
         try:
