@@ -175,6 +175,21 @@ extern int parasail_b200_batch_all_device(
         const uint8_t *d_codes, const int64_t *d_offsets, const int *d_lengths, int n,
         int open, int gap, parasail_b200_record_t *d_records);
 
+/** Trace results of n independent pairs (host memory) with a trace
+ * function of parasail.h (the names parasail_b200_batch_pairs_cigar takes,
+ * and their _profile_32 forms) in one GPU pipeline: results[i] is what the
+ * trace function returns for pair i -- usable with
+ * parasail_result_get_cigar[_extra], parasail_result_get_traceback[_extra]
+ * and parasail_traceback_generic*, freed with parasail_result_free -- or
+ * NULL (with a message) when the pair's scores leave the int16 range of the
+ * traceback kernel. Replaces n calls of the trace function (the reference
+ * aligner's trace outputs, apps/parasail_aligner.cpp:2210-2550). */
+extern int parasail_b200_batch_pairs_trace(
+        const char *funcname, const parasail_matrix_t *matrix,
+        const char *queries, const int64_t *qoffsets, const int *qlengths,
+        const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+        int open, int gap, parasail_result_t **results);
+
 /** CIGARs of n independent pairs (host memory) with a trace function of
  * parasail.h: "sw_trace", "nw_trace_scan", "sg_qx_trace_striped_32",
  * "sg_de_trace_scan_32", ... (serial and 32-bit forms; with or without the

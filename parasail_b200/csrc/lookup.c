@@ -25,6 +25,13 @@
 #define FAM(base, algname, st) SER(base, algname, st) DIR(base, algname, st)
 #define BOTH(base, algname)                                                           \
     FAM(base, algname, 0) FAM(base##_stats, algname "_stats", 1)
+/* the trace forms this library provides: serial, and 32-bit striped/scan
+ * (is_trace set, as parasail/function_lookup.h:8184-8277 records them) */
+#define TRACE(base, algname)                                                          \
+    {base##_trace, #base "_trace", algname, "orig", "NA", "32", "32", 1, 0, 0, 1, 0, 1}, \
+    {base##_trace_scan, #base "_trace_scan", algname, "scan", "NA", "32", "32", 1, 0, 0, 1, 0, 0}, \
+    {base##_trace_scan_32, #base "_trace_scan_32", algname, "scan", "disp", "NA", "32", -1, 0, 0, 1, 0, 0}, \
+    {base##_trace_striped_32, #base "_trace_striped_32", algname, "striped", "disp", "NA", "32", -1, 0, 0, 1, 0, 0},
 
 static const parasail_function_info_t functions[] = {
     BOTH(parasail_sw, "sw")
@@ -40,6 +47,11 @@ static const parasail_function_info_t functions[] = {
     BOTH(parasail_sg_qe_db, "sg_qe_db")
     BOTH(parasail_sg_qb_db, "sg_qb_db")
     BOTH(parasail_sg_qe_de, "sg_qe_de")
+    TRACE(parasail_sw, "sw") TRACE(parasail_nw, "nw") TRACE(parasail_sg, "sg")
+    TRACE(parasail_sg_qb, "sg_qb") TRACE(parasail_sg_qe, "sg_qe") TRACE(parasail_sg_qx, "sg_qx")
+    TRACE(parasail_sg_db, "sg_db") TRACE(parasail_sg_de, "sg_de") TRACE(parasail_sg_dx, "sg_dx")
+    TRACE(parasail_sg_qb_de, "sg_qb_de") TRACE(parasail_sg_qe_db, "sg_qe_db")
+    TRACE(parasail_sg_qb_db, "sg_qb_db") TRACE(parasail_sg_qe_de, "sg_qe_de")
     {NULL, "NULL", "NULL", "NULL", "NULL", "NULL", "NULL", 0, 0, 0, 0, 0, 0},
 };
 
@@ -55,6 +67,12 @@ static const parasail_function_info_t functions[] = {
     PFS(base##_stats, algname "_stats", 1, striped, parasail_profile_create_stats)      \
     PFS(base##_stats, algname "_stats", 1, scan, parasail_profile_create_stats)
 
+#define PTRACE(base, algname)                                                           \
+    {base##_trace_scan_profile_32, parasail_profile_create_32, #base "_trace_scan_profile_32", algname, \
+     "scan_profile", "disp", "NA", "32", -1, 0, 0, 1, 0, 0},                            \
+    {base##_trace_striped_profile_32, parasail_profile_create_32, #base "_trace_striped_profile_32", algname, \
+     "striped_profile", "disp", "NA", "32", -1, 0, 0, 1, 0, 0},
+
 static const parasail_pfunction_info_t pfunctions[] = {
     PBOTH(parasail_sw, "sw")
     PBOTH(parasail_nw, "nw")
@@ -69,6 +87,11 @@ static const parasail_pfunction_info_t pfunctions[] = {
     PBOTH(parasail_sg_qe_db, "sg_qe_db")
     PBOTH(parasail_sg_qb_db, "sg_qb_db")
     PBOTH(parasail_sg_qe_de, "sg_qe_de")
+    PTRACE(parasail_sw, "sw") PTRACE(parasail_nw, "nw") PTRACE(parasail_sg, "sg")
+    PTRACE(parasail_sg_qb, "sg_qb") PTRACE(parasail_sg_qe, "sg_qe") PTRACE(parasail_sg_qx, "sg_qx")
+    PTRACE(parasail_sg_db, "sg_db") PTRACE(parasail_sg_de, "sg_de") PTRACE(parasail_sg_dx, "sg_dx")
+    PTRACE(parasail_sg_qb_de, "sg_qb_de") PTRACE(parasail_sg_qe_db, "sg_qe_db")
+    PTRACE(parasail_sg_qb_db, "sg_qb_db") PTRACE(parasail_sg_qe_de, "sg_qe_de")
     {NULL, NULL, "NULL", "NULL", "NULL", "NULL", "NULL", "NULL", 0, 0, 0, 0, 0, 0},
 };
 

@@ -701,11 +701,9 @@ TRACE_FAMILY(sg_qe_de, PB_SG, PB_S1_END | PB_S2_END)
 
 /* ---- batch CIGARs (include/parasail_b200.h) ------------------------------- */
 
-int parasail_b200_batch_pairs_cigar(const char *funcname, const parasail_matrix_t *matrix,
-                                    const char *queries, const int64_t *qoffsets, const int *qlengths,
-                                    const char *targets, const int64_t *toffsets, const int *tlengths, int n,
-                                    int open, int gap, parasail_b200_record_t *records, uint32_t *cigars,
-                                    int *cigar_lengths, int *beg_query, int *beg_ref)
+/* the algorithm and result flags of a trace function's name
+ * ("sw_trace", "nw_trace_scan_32", ...); -1 when it names none */
+static int parse_trace_name(const char *funcname, int *alg_out, int *sgf_out, int *flags_out)
 {
     static const struct { const char *name; int alg, sgf; } algs[] = {
         {"sw", PB_SW, 0}, {"nw", PB_NW, 0},
@@ -716,18 +714,9 @@ int parasail_b200_batch_pairs_cigar(const char *funcname, const parasail_matrix_
         {"sg", PB_SG, PB_S1_BEG | PB_S1_END | PB_S2_BEG | PB_S2_END},
     };
     const char *s = funcname;
-    int alg = -1, sgf = 0, flags = 0, k, rc;
-    int64_t off = 0;
-    int *ends;
-    pb_trace_path **paths;
+    int alg = -1, sgf = 0, flags = 0;
     size_t a;
-    if (!matrix || !queries || !qoffsets || !qlengths || !targets || !toffsets || !tlengths || !records || !cigars ||
-        !cigar_lengths || !beg_query || !beg_ref || !funcname) {
-        fprintf(stderr, "%s: missing arguments\n", __func__);
-        return -1;
-    }
-    if (n < 0 || open < 0 || gap < 0) { fprintf(stderr, "%s: invalid n/open/gap\n", __func__); return -1; }
-    if (n == 0) return 0;
+    if (!s) return -1;
     if (0 == strncmp(s, "parasail_", 9)) s += 9;
     for (a = 0; a < sizeof algs / sizeof algs[0]; ++a) {
         const size_t l = strlen(algs[a].name);
@@ -735,13 +724,92 @@ int parasail_b200_batch_pairs_cigar(const char *funcname, const parasail_matrix_
             alg = algs[a].alg; sgf = algs[a].sgf; s += l + 6; break;
         }
     }
-    if (alg >= 0) {
-        if (!*s) flags = PARASAIL_FLAG_NOVEC | PARASAIL_FLAG_LANES_1;
-        else if (!strcmp(s, "_scan")) flags = PARASAIL_FLAG_NOVEC_SCAN | PARASAIL_FLAG_LANES_1;
-        else if (!strcmp(s, "_striped_32")) flags = PARASAIL_FLAG_STRIPED | PARASAIL_FLAG_LANES_8;
-        else if (!strcmp(s, "_scan_32")) flags = PARASAIL_FLAG_SCAN | PARASAIL_FLAG_LANES_8;
-        else alg = -1;
+    if (alg < 0) return -1;
+    /* the profile forms give the records of the direct forms */
+    if (!*s) flags = PARASAIL_FLAG_NOVEC | PARASAIL_FLAG_LANES_1;
+    else if (!strcmp(s, "_scan")) flags = PARASAIL_FLAG_NOVEC_SCAN | PARASAIL_FLAG_LANES_1;
+    else if (!strcmp(s, "_striped_32") || !strcmp(s, "_striped_profile_32")) flags = PARASAIL_FLAG_STRIPED | PARASAIL_FLAG_LANES_8;
+    else if (!strcmp(s, "_scan_32") || !strcmp(s, "_scan_profile_32")) flags = PARASAIL_FLAG_SCAN | PARASAIL_FLAG_LANES_8;
+    else return -1;
+    *alg_out = alg;
+    *sgf_out = sgf;
+    *flags_out = alg_flags(alg, sgf) | flags | PARASAIL_FLAG_TRACE | PARASAIL_FLAG_BITS_32;
+    return 0;
+}
+
+/* Trace results of n independent pairs (host characters) in one GPU
+ * pipeline; results[k] NULL for a pair outside the traceback kernels'
+ * 16-bit bounds (a message names it). */
+int parasail_b200_batch_pairs_trace(const char *funcname, const parasail_matrix_t *matrix,
+                                    const char *queries, const int64_t *qoffsets, const int *qlengths,
+                                    const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+                                    int open, int gap, parasail_result_t **results)
+{
+    int alg, sgf, flags, k, rc;
+    int *ends;
+    pb_trace_path **paths;
+    if (!matrix || !queries || !qoffsets || !qlengths || !targets || !toffsets || !tlengths || !results) {
+        fprintf(stderr, "%s: missing arguments\n", __func__);
+        return -1;
     }
+    if (n < 0 || open < 0 || gap < 0) { fprintf(stderr, "%s: invalid n/open/gap\n", __func__); return -1; }
+    if (parse_trace_name(funcname, &alg, &sgf, &flags) != 0) {
+        fprintf(stderr, "%s: unknown trace function '%s'\n", __func__, funcname ? funcname : "(null)");
+        return -1;
+    }
+    if (n == 0) return 0;
+    for (k = 0; k < n; ++k) {
+        results[k] = NULL;
+        if (qlengths[k] <= 0 || tlengths[k] <= 0) { fprintf(stderr, "%s: pair %d has an empty sequence\n", __func__, k); return -1; }
+    }
+    if (!pb_gpu_ready(__func__)) return -1;
+    ends = (int *)malloc(sizeof(int) * 3 * (size_t)n);
+    paths = (pb_trace_path **)calloc((size_t)n, sizeof *paths);
+    if (!ends || !paths) { free(ends); free(paths); return -1; }
+    rc = trace_pairs(alg, sgf, matrix, open, gap, queries, qoffsets, qlengths, targets, toffsets, tlengths, n, ends,
+                     paths);
+    if (rc == -2) fprintf(stderr, "%s: traceback needs a square matrix\n", __func__);
+    for (k = 0; rc == 0 && k < n; ++k) {
+        parasail_result_t *r;
+        if (!paths[k]) {
+            fprintf(stderr, "%s: pair %d leaves the range of the traceback kernel (int16)\n", __func__, k);
+            continue;
+        }
+        if (!(r = pb_result_new(0))) { rc = -1; break; }
+        r->score = ends[3 * k]; r->end_query = ends[3 * k + 1]; r->end_ref = ends[3 * k + 2];
+        r->flag = flags;
+        r->extra = paths[k];
+        paths[k] = NULL;
+        results[k] = r;
+    }
+    for (k = 0; k < n; ++k) if (paths[k]) { free(paths[k]->ops); free(paths[k]); }
+    if (rc != 0) {
+        for (k = 0; k < n; ++k) if (results[k]) { parasail_result_free(results[k]); results[k] = NULL; }
+        fprintf(stderr, "%s: GPU alignment failed\n", __func__);
+    }
+    free(paths);
+    free(ends);
+    return rc;
+}
+
+int parasail_b200_batch_pairs_cigar(const char *funcname, const parasail_matrix_t *matrix,
+                                    const char *queries, const int64_t *qoffsets, const int *qlengths,
+                                    const char *targets, const int64_t *toffsets, const int *tlengths, int n,
+                                    int open, int gap, parasail_b200_record_t *records, uint32_t *cigars,
+                                    int *cigar_lengths, int *beg_query, int *beg_ref)
+{
+    int alg = -1, sgf = 0, flags = 0, k, rc;
+    int64_t off = 0;
+    int *ends;
+    pb_trace_path **paths;
+    if (!matrix || !queries || !qoffsets || !qlengths || !targets || !toffsets || !tlengths || !records || !cigars ||
+        !cigar_lengths || !beg_query || !beg_ref || !funcname) {
+        fprintf(stderr, "%s: missing arguments\n", __func__);
+        return -1;
+    }
+    if (n < 0 || open < 0 || gap < 0) { fprintf(stderr, "%s: invalid n/open/gap\n", __func__); return -1; }
+    if (n == 0) return 0;
+    if (parse_trace_name(funcname, &alg, &sgf, &flags) != 0) alg = -1;
     if (alg < 0) { fprintf(stderr, "%s: unknown trace function '%s'\n", __func__, funcname); return -1; }
     for (k = 0; k < n; ++k)
         if (qlengths[k] <= 0 || tlengths[k] <= 0) { fprintf(stderr, "%s: pair %d has an empty sequence\n", __func__, k); return -1; }
@@ -760,7 +828,7 @@ int parasail_b200_batch_pairs_cigar(const char *funcname, const parasail_matrix_
         cigar_lengths[k] = -1;
         beg_query[k] = beg_ref[k] = 0;
         rec->score = ends[3 * k]; rec->end_query = ends[3 * k + 1]; rec->end_ref = ends[3 * k + 2];
-        rec->flag = alg_flags(alg, sgf) | flags | PARASAIL_FLAG_TRACE | PARASAIL_FLAG_BITS_32;
+        rec->flag = flags;
         if (!paths[k]) continue;
         memset(&r, 0, sizeof r);
         r.score = rec->score; r.end_query = rec->end_query; r.end_ref = rec->end_ref; r.flag = rec->flag;
