@@ -130,6 +130,13 @@ extern parasail_b200_db_plan_t *parasail_b200_db_plan_create(
         const uint8_t *d_codes, const int64_t *d_offsets, const int *d_lengths, int n,
         int open, int gap, parasail_b200_record_t *d_records);
 extern int parasail_b200_db_plan_run(parasail_b200_db_plan_t *plan);
+/** A plan run from host memory: `targets` holds the targets' characters in
+ * the layout of the plan's d_offsets (nbytes of them); they are copied into
+ * the plan's d_codes and mapped there through the profiles' matrix, the
+ * graph replays, and the records (nq * n, query-major) are copied into the
+ * host array `records`. */
+extern int parasail_b200_db_plan_run_host(parasail_b200_db_plan_t *plan, const char *targets, size_t nbytes,
+                                          parasail_b200_record_t *records);
 extern void parasail_b200_db_plan_free(parasail_b200_db_plan_t *plan);
 
 /** Independent pairs: query i against target i, both from host memory,

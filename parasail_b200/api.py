@@ -636,6 +636,8 @@ lib.parasail_b200_db_plan_create.argtypes = [ctypes.c_char_p, ctypes.c_void_p, c
 lib.parasail_b200_db_plan_run.restype = ctypes.c_int
 lib.parasail_b200_db_plan_run.argtypes = [ctypes.c_void_p]
 lib.parasail_b200_db_plan_free.argtypes = [ctypes.c_void_p]
+lib.parasail_b200_db_plan_run_host.restype = ctypes.c_int
+lib.parasail_b200_db_plan_run_host.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
 
 lib.parasail_b200_schedule_get.restype = ctypes.c_uint
 lib.parasail_b200_schedule_set.argtypes = [ctypes.c_uint]

@@ -439,6 +439,8 @@ int parasail_b200_batch_all_device(const char *funcname, const parasail_matrix_t
 
 struct parasail_b200_db_plan {
     void *plan;
+    uint8_t *d_codes;       /* the caller's target buffer the plan reads */
+    uint8_t mapper[256];    /* the profiles' matrix mapper, for runs from host memory */
 };
 
 parasail_b200_db_plan_t *parasail_b200_db_plan_create(const char *funcname, const parasail_profile_t *const *profiles,
@@ -464,6 +466,8 @@ parasail_b200_db_plan_t *parasail_b200_db_plan_create(const char *funcname, cons
     b.alg = job.mode.alg; b.sgflags = job.mode.sgflags; b.stats = job.mode.stats;
     b.open = open; b.gap = gap; b.profs = profs; b.nprofs = nq; b.npairs = n;
     b.d_targets = d_codes; b.d_toff = d_offsets; b.d_tlen = d_lengths;
+    pl->d_codes = (uint8_t *)d_codes;
+    mapper_bytes(profiles[0]->matrix, pl->mapper);
     if (pb_cuda_db_plan_create(&job, &b, (pb_record *)d_records, &pl->plan) != 0) {
         fprintf(stderr, "%s: '%s' cannot be planned (plans hold Smith-Waterman score-only searches with "
                 "open > gap and int8 profiles)\n", __func__, funcname ? funcname : "(null)");
@@ -477,6 +481,16 @@ int parasail_b200_db_plan_run(parasail_b200_db_plan_t *plan)
 {
     if (!plan) { fprintf(stderr, "%s: missing %s\n", __func__, "plan"); return -1; }
     return pb_cuda_db_plan_run(plan->plan);
+}
+
+int parasail_b200_db_plan_run_host(parasail_b200_db_plan_t *plan, const char *targets, size_t nbytes,
+                                   parasail_b200_record_t *records)
+{
+    if (!plan || !records || (nbytes && !targets)) {
+        fprintf(stderr, "%s: missing plan, targets or records\n", __func__);
+        return -1;
+    }
+    return pb_cuda_db_plan_run_host(plan->plan, targets, nbytes, plan->d_codes, plan->mapper, (pb_record *)records);
 }
 
 void parasail_b200_db_plan_free(parasail_b200_db_plan_t *plan)

@@ -154,6 +154,8 @@ int pb_cuda_batch_host(const struct pb_job *job, const pb_batch *tmpl, const uin
  * once as a CUDA graph and replayed. */
 int pb_cuda_db_plan_create(const struct pb_job *job, const pb_batch *b, struct pb_record *d_rec, void **plan);
 int pb_cuda_db_plan_run(void *plan);
+int pb_cuda_db_plan_run_host(void *plan, const char *h_chars, size_t nbytes, uint8_t *d_codes,
+                             const uint8_t *mapper256, struct pb_record *h_rec);
 void pb_cuda_db_plan_free(void *plan);
 
 /* All-vs-all: the upper triangle of n device-resident sequences (codes),

@@ -61,6 +61,8 @@
 
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
 #include <dlfcn.h>
 #include <mutex>
 #include <string>
@@ -175,7 +177,7 @@ k_p16(P16Params p, const int *__restrict__ tlist, int ntl, int *counter)
         if (k >= ntl) break;
         const int task = tlist[k];
         const int s = task * 32 + lane;
-        const bool valid = s < p.nitems;
+        const bool valid = s < p.nitems && p.order[s] >= 0;
         const int item = valid ? p.order[s] : 0;
         const int rows = valid ? p.rows[item] : 0;
         const int cols = valid ? p.cols[item] : 0;
@@ -492,6 +494,7 @@ __global__ void k_p16_walk(P16Params p, const int *__restrict__ tlist, int ntl, 
     const int s = task * 32 + lane;
     if (s >= p.nitems) return;
     const int item = p.order[s];
+    if (item < 0) return;
     const int wmax = p.task_wmax[task];
     const uint4 *tb = p.bits + p.task_bits[task];
     const pb_pair_out e = ends[item];
@@ -577,6 +580,7 @@ __global__ void k_p16_path(P16Params p, const int *__restrict__ tlist, int ntl, 
     const int s = task * 32 + lane;
     if (s >= p.nitems) return;
     const int item = p.order[s];
+    if (item < 0) return;
     const int wmax = p.task_wmax[task];
     const uint4 *tb = p.bits + p.task_bits[task];
     const pb_pair_out e = ends[item];
@@ -674,7 +678,7 @@ __global__ void k_p16_tasks(P16Params p, int ntasks, const int *__restrict__ gro
     const int lane = threadIdx.x & 31;
     if (task >= ntasks) return;
     const int s = task * 32 + lane;
-    const bool valid = s < p.nitems;
+    const bool valid = s < p.nitems && p.order[s] >= 0;
     const int item = valid ? p.order[s] : -1;
     int c = valid ? p.cols[item] : 0, r = valid ? p.rows[item] : 0;
     long long src = -1;
@@ -744,7 +748,35 @@ __global__ void k_p16_check(pb_job job, P16Params p, int *__restrict__ rest, int
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= p.nitems) return;
     const int item = p.order[s];
+    if (item < 0) return;
     if (!p16_definite(job, p.out[item], p.rows[item], p.cols[item])) rest[atomicAdd(nrest, 1)] = item;
+}
+
+/* Task alignment to query groups: the eligible items sorted by (group,
+ * passes, columns) are laid out so that every group starts a task (each
+ * group padded with -1 entries to a multiple of 32). No task then mixes two
+ * queries, and every task of a grouped batch takes the shared-query
+ * variant. */
+__global__ void k_pad_heads(const unsigned long long *__restrict__ keys, int n, int *__restrict__ head)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) head[s] = s == 0 || ((keys[s] >> 43) & 0xfffffull) != ((keys[s - 1] >> 43) & 0xfffffull);
+}
+
+__global__ void k_pad_counts(const int *__restrict__ gstart, int ng, int n, int *__restrict__ pcount)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < ng) pcount[g] = ((g + 1 < ng ? gstart[g + 1] : n) - gstart[g] + 31) & ~31;
+}
+
+__global__ void k_pad_scatter(const int *__restrict__ order, int n, const int *__restrict__ gid,
+                              const int *__restrict__ gstart, const int *__restrict__ pstart, int *__restrict__ out)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) {
+        const int g = gid[s] - 1;
+        out[pstart[g] + (s - gstart[g])] = order[s];
+    }
 }
 
 __global__ void k_mat_to_int8(const int32_t *__restrict__ m, int n, int8_t *__restrict__ m8)
@@ -915,12 +947,53 @@ int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out
         pb_diag_count_launch(1);
     }
     int nrest = N - nelig;
+    /* grouped batches: every group starts a task */
+    int nslots = nelig;
+    int *porder = order;
+    if (nelig > 0 && (dbmode || group)) {
+        int *head = nullptr, *gid = nullptr, *gstart = nullptr, *pcount = nullptr, *pstart = nullptr, *iota = nullptr;
+        int ng = 0, last_start = 0, last_count = 0;
+        P16_CK(cudaMallocAsync((void **)&head, sizeof(int) * nelig, st)); frees.add(head);
+        P16_CK(cudaMallocAsync((void **)&gid, sizeof(int) * nelig, st)); frees.add(gid);
+        P16_CK(cudaMallocAsync((void **)&gstart, sizeof(int) * nelig, st)); frees.add(gstart);
+        P16_CK(cudaMallocAsync((void **)&pcount, sizeof(int) * nelig, st)); frees.add(pcount);
+        P16_CK(cudaMallocAsync((void **)&pstart, sizeof(int) * nelig, st)); frees.add(pstart);
+        P16_CK(cudaMallocAsync((void **)&iota, sizeof(int) * nelig, st)); frees.add(iota);
+        k_pad_heads<<<(nelig + 255) / 256, 256, 0, st>>>(keys_sorted, nelig, head);
+        k_iota_int<<<(nelig + 255) / 256, 256, 0, st>>>(iota, nelig);
+        pb_diag_count_launch(2);
+        size_t b1 = 0, b2 = 0, b3 = 0;
+        void *tmp = nullptr;
+        P16_CK(cub::DeviceScan::InclusiveSum(nullptr, b1, head, gid, nelig, st));
+        P16_CK(cub::DeviceSelect::Flagged(nullptr, b2, iota, head, gstart, counts + 2, nelig, st));
+        P16_CK(cub::DeviceScan::ExclusiveSum(nullptr, b3, pcount, pstart, nelig, st));
+        const size_t tb = std::max(b1, std::max(b2, b3));
+        P16_CK(cudaMallocAsync(&tmp, tb, st)); frees.add(tmp);
+        size_t b = tb;
+        P16_CK(cub::DeviceScan::InclusiveSum(tmp, b, head, gid, nelig, st));
+        b = tb;
+        P16_CK(cub::DeviceSelect::Flagged(tmp, b, iota, head, gstart, counts + 2, nelig, st));
+        P16_CK(cudaMemcpyAsync(&ng, counts + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+        P16_CK(cudaStreamSynchronize(st));
+        k_pad_counts<<<(ng + 255) / 256, 256, 0, st>>>(gstart, ng, nelig, pcount);
+        pb_diag_count_launch(1);
+        b = tb;
+        P16_CK(cub::DeviceScan::ExclusiveSum(tmp, b, pcount, pstart, ng, st));
+        P16_CK(cudaMemcpyAsync(&last_start, pstart + ng - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        P16_CK(cudaMemcpyAsync(&last_count, pcount + ng - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        P16_CK(cudaStreamSynchronize(st));
+        nslots = last_start + last_count;
+        P16_CK(cudaMallocAsync((void **)&porder, sizeof(int) * (size_t)nslots, st)); frees.add(porder);
+        P16_CK(cudaMemsetAsync(porder, 0xff, sizeof(int) * (size_t)nslots, st));
+        k_pad_scatter<<<(nelig + 255) / 256, 256, 0, st>>>(order, nelig, gid, gstart, pstart, porder);
+        pb_diag_count_launch(1);
+    }
     if (nelig > 0) {
-        const int ntasks = (nelig + 31) / 32;
+        const int ntasks = (nslots + 31) / 32;
         P16Params p;
         memset(&p, 0, sizeof p);
         p.alg = m->alg; p.sgflags = m->sgflags; p.open = m->open; p.gap = m->gap; p.mmax = mmax; p.mmin = mmin;
-        p.nletters = L; p.nitems = nelig; p.order = order; p.rows = rows; p.cols = cols;
+        p.nletters = L; p.nitems = nslots; p.order = porder; p.rows = rows; p.cols = cols;
         p.mat8 = d_mat8; p.mat32 = dbmode ? nullptr : b->d_mat;
         p.qall = b->d_qall; p.qoff = b->d_qoff; p.profs = d_profs; p.nt = dbmode ? b->npairs : 0;
         p.targets = b->d_targets; p.toff = b->d_toff;
@@ -1044,7 +1117,7 @@ int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out
         /* items whose width verdicts need exact extremes */
         if (!prefix) {
             P16_CK(cudaMemsetAsync(counts + 1, 0, sizeof(int), st));
-            k_p16_check<<<(nelig + 255) / 256, 256, 0, st>>>(job, p, d_rest + nrest, counts + 1);
+            k_p16_check<<<(nslots + 255) / 256, 256, 0, st>>>(job, p, d_rest + nrest, counts + 1);
             pb_diag_count_launch(1);
             int nx = 0;
             P16_CK(cudaMemcpyAsync(&nx, counts + 1, sizeof(int), cudaMemcpyDeviceToHost, st));

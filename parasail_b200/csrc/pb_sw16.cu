@@ -634,6 +634,7 @@ struct DbPlan {
     pb_batch b;
     std::vector<const pb_device_profile *> profs;
     pb_record *rec = nullptr;
+    uint8_t *map = nullptr;                   /* device mapper of plan runs from host memory */
 };
 
 void plan_destroy(DbPlan *pl)
@@ -645,6 +646,7 @@ void plan_destroy(DbPlan *pl)
         if (pl->o1) cudaFreeAsync(pl->o1, pl->st);
         if (pl->need) cudaFreeAsync(pl->need, pl->st);
         if (pl->counts) cudaFreeAsync(pl->counts, pl->st);
+        if (pl->map) cudaFreeAsync(pl->map, pl->st);
         cudaStreamSynchronize(pl->st);
         cudaStreamDestroy(pl->st);
     }
@@ -739,6 +741,49 @@ extern "C" int pb_cuda_db_plan_run(void *plan)
     }
     if (h[4] > 0) return pb_cuda_batch_run(&pl->job, &pl->b, pl->rec);
     return 0;
+}
+
+namespace {
+
+__global__ void k_map_inplace(uint8_t *__restrict__ buf, int64_t n, const uint8_t *__restrict__ map)
+{
+    __shared__ uint8_t smap[256];
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) smap[k] = map[k];
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        buf[i] = smap[buf[i]];
+}
+
+}  // namespace
+
+/* A plan run from host memory: the targets' characters (the layout the
+ * plan was created with) are copied into d_codes and mapped there, the
+ * graph replays, and the records come back into h_rec, all on the plan's
+ * stream. */
+extern "C" int pb_cuda_db_plan_run_host(void *plan, const char *h_chars, size_t nbytes, uint8_t *d_codes,
+                                        const uint8_t *mapper256, pb_record *h_rec)
+{
+    DbPlan *pl = (DbPlan *)plan;
+    if (!pl) return -1;
+    if (!pl->map) {
+        if (cudaMallocAsync((void **)&pl->map, 256, pl->st) != cudaSuccess) return -1;
+        if (cudaMemcpyAsync(pl->map, mapper256, 256, cudaMemcpyHostToDevice, pl->st) != cudaSuccess) return -1;
+    }
+    if (nbytes && cudaMemcpyAsync(d_codes, h_chars, nbytes, cudaMemcpyHostToDevice, pl->st) != cudaSuccess)
+        return -1;
+    if (nbytes) {
+        int dev = 0, nsm = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        const int64_t want = ((int64_t)nbytes + 255) / 256;
+        k_map_inplace<<<(int)(want < 2 * nsm ? want : 2 * nsm), 256, 0, pl->st>>>(d_codes, (int64_t)nbytes, pl->map);
+        pb_diag_count_launch(1);
+    }
+    if (pb_cuda_db_plan_run(plan) != 0) return -1;
+    const size_t nrec = (size_t)pl->b.npairs * pl->profs.size();
+    if (cudaMemcpyAsync(h_rec, pl->rec, sizeof(pb_record) * nrec, cudaMemcpyDeviceToHost, pl->st) != cudaSuccess)
+        return -1;
+    return cudaStreamSynchronize(pl->st) == cudaSuccess ? 0 : -1;
 }
 
 extern "C" void pb_cuda_db_plan_free(void *plan)

@@ -69,8 +69,11 @@ def _compare(tmp_path, args, out="out.txt", files=()):
 
 def test_aligner_csv_outputs_match_reference(tmp_path):
     rng = random.Random(21)
-    _fasta(str(tmp_path / "prot.fa"), _families(rng, 120, AA, 40, 400))
-    _fasta(str(tmp_path / "q.fa"), _families(rng, 15, AA, 40, 300))
+    db = _families(rng, 120, AA, 40, 400)
+    _fasta(str(tmp_path / "prot.fa"), db)
+    # queries: relatives of some database sequences and unrelated ones
+    _fasta(str(tmp_path / "q.fa"), [mutate(rng, rng.choice(db), AA, 0.25, 0.03) for _ in range(10)] +
+           _families(rng, 5, AA, 40, 300))
     for args in (["-f", "prot.fa"],                                          # sw_stats_striped_16, filter
                  ["-f", "prot.fa", "-x", "-a", "sw_striped_profile_sat"],    # all pairs, score only
                  ["-f", "prot.fa", "-c", "5", "-a", "nw_stats_scan_16"],

@@ -138,6 +138,33 @@ def test_db_batch_matches_single_query_batches():
         p.close()
 
 
+def test_db_batch_non_score_modes_match_single_query_batches():
+    """Database searches through the pair kernel (every function but the SW
+    score search): queries whose target counts are not multiples of a warp
+    task, so task boundaries fall inside a query's items unless the batch
+    aligns them."""
+    rng = random.Random(19)
+    b62 = pb.matrix_lookup("blosum62")
+    queries = [rand_seq(rng, L, AA) for L in (7, 33, 100, 250, 500)]
+    targets = [rand_seq(rng, rng.randint(1, 700), AA) for _ in range(505)]
+    targets += [mutate(rng, q, AA, 0.3, 0.02) for q in queries]
+    for name, creator, alg, st in (("nw_stats_scan_profile_16", "parasail_profile_create_stats_16", O.NW, 1),
+                                   ("sw_stats_striped_profile_32", "parasail_profile_create_stats_32", O.SW, 1),
+                                   ("sg_qx_striped_profile_sat", "parasail_profile_create_sat", O.SG, 0)):
+        profs = [pb.ProfileHandle(creator, q, b62) for q in queries]
+        db = pb.batch_db(name, profs, targets, 11, 1)
+        for k, p in enumerate(profs):
+            one = pb.batch_profile(name, p, targets, 11, 1)
+            assert (db[k] == one).all(), (name, k)
+        sgf = O.S1_BEG | O.S1_END if alg == O.SG else 0
+        exp = _oracle_batch(alg, sgf, st, queries[2], targets, 11, 1, _b62())
+        got = [(int(r["score"]), int(r["end_query"]), int(r["end_ref"])) + ((int(r["matches"]), int(r["similar"]),
+               int(r["length"])) if st else ()) for r in db[2]]
+        assert got == [tuple(e) if st else tuple(e[:3]) for e in exp], name
+        for p in profs:
+            p.close()
+
+
 def test_records_reserved_field_is_zero_and_host_equals_single_calls():
     """The host batch calls copy the device's records straight into the
     caller's array: the reserved field is 0, and every other field equals

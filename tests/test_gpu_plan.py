@@ -45,6 +45,11 @@ def test_plan_replays_equal_batch_db_device():
                                                             d_ref_rec.data_ptr()) == 0
                 torch.cuda.synchronize()
                 assert torch.equal(d_plan_rec, d_ref_rec), name
+            # the same search from host memory: characters in, records out
+            h_rec = np.zeros((nq, n, 8), np.int32)
+            assert pb.lib.parasail_b200_db_plan_run_host(plan, codes.ctypes.data, len(codes), h_rec.ctypes.data) == 0
+            assert (h_rec == d_ref_rec.cpu().numpy()).all(), name
+            assert (d_codes.cpu().numpy() == mapper[codes]).all()
         pb.lib.parasail_b200_db_plan_free(plan)
     # jobs a plan does not hold
     for name, op, gp in (("sw_stats_striped_profile_16", 11, 1), ("nw_scan_profile_16", 11, 1),
