@@ -1023,11 +1023,14 @@ int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out
         std::stable_sort(torder.begin(), torder.end(), [&](int x, int y) {
             return (long long)hn[x] * (hw[x] + 1) > (long long)hn[y] * (hw[y] + 1);
         });
-        /* chunks of tasks whose direction bits fit the budget */
+        /* chunks of tasks whose direction bits fit the budget: half of the
+         * free device memory (at most 96 GiB), so that a chunk of the largest
+         * tasks (about 36 MB of bits each at 1500 x 1500) still fills the
+         * SMs; a budget of a few GiB left chunks of ~200 warps */
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
-        size_t budget = (size_t)8 << 30;
-        if (free_b / 3 < budget) budget = free_b / 3;
+        size_t budget = (size_t)96 << 30;
+        if (free_b / 2 < budget) budget = free_b / 2;
         const size_t budget_u4 = budget / sizeof(uint4);
         /* launch shapes and the pass-boundary buffers, sized for the larger grid */
         int dev = 0, nsm = 0;
