@@ -65,6 +65,7 @@ struct Sw16Task {
 struct Sw16Params {
     int open, gap, npairs, nq, ntasks, maxlen;
     int nteam;               /* tasks [0, nteam) are run by a whole block */
+    int nletters;            /* profile alphabet size */
     const Sw16Query *queries;
     const int8_t *prof_all;  /* concatenated [size][lp] int8 profiles */
     int prof_bytes;

@@ -335,6 +335,151 @@ k_sw16(Sw16Params p, int *task_counter)
     }
 }
 
+/*
+ * Small searches (few warp tasks, e.g. one query against 1,000 targets):
+ * the intra-task wavefront. One warp aligns one (query, target) pair in
+ * exact int32: a pass covers 256 query rows, 8 per lane, and lane k
+ * computes column t - k at iteration t, so the warp's 32 lanes work on 32
+ * columns of one pair at once and the row-to-row dependency chain is 8
+ * rows long instead of the inter-task kernel's per-target 16-row strips on
+ * a handful of SMs. Row above a lane's first row: the previous lane's last
+ * row by __shfl_up_sync, or, for lane 0, the previous pass's bottom row
+ * from the warp's buffer (passes of one pair run one after the other on
+ * the warp). The recurrence and end rule are src/sw.c:102-158's: H =
+ * max(0, H_diag + s, E, F), the first maximum in column-major order, score
+ * 0 at (0, 0) when no cell is positive; with open >= gap, F of the next
+ * row is max(F - gap, max(a, 0) - open) with a = max(H_diag + s, E), one
+ * dependent operation per row.
+ */
+static constexpr int SWW_RL = 8;          /* query rows per lane */
+
+template <bool GE>
+__global__ void __launch_bounds__(SW16_WARPS * 32, 2)
+k_sw_wave(Sw16Params p, int *counter)
+{
+    extern __shared__ __align__(16) int8_t s_prof[];
+    {
+        const int4 *src = reinterpret_cast<const int4 *>(p.prof_all);
+        int4 *dst = reinterpret_cast<int4 *>(s_prof);
+        const int n16 = p.prof_bytes / 16;
+        for (int k = threadIdx.x; k < n16; k += blockDim.x) dst[k] = src[k];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    int2 *buf = reinterpret_cast<int2 *>(p.scratch) + (size_t)(blockIdx.x * SW16_WARPS + wid) * p.maxlen;
+    const int open = p.open, gap = p.gap;
+    const int NEG = INT_MIN / 4;
+    const long long nitems = (long long)p.nq * p.npairs;
+    for (;;) {
+        long long w = 0;
+        if (lane == 0) w = atomicAdd(counter, 1);
+        w = __shfl_sync(0xffffffffu, w, 0);
+        if (w >= nitems) break;
+        const int q = (int)(w / p.npairs);
+        const int pid = p.order[w % p.npairs];
+        const Sw16Query Q = p.queries[q];
+        const int n = Q.qlen, m = p.tlen[pid];
+        const uint8_t *ts = p.targets + p.toff[pid];
+        const int8_t *prof = s_prof + Q.prof_off;
+        const int npass = (n + 32 * SWW_RL - 1) / (32 * SWW_RL);
+        Sw16Best best = {0, -1, -1};
+        int status = 0;
+        for (int pass = 0; pass < npass; ++pass) {
+            const int R0 = pass * 32 * SWW_RL + lane * SWW_RL;
+            const bool rows_in = R0 < Q.lp;           /* profile rows past lp score 0 (dummy rows) */
+            int Hl[SWW_RL], E[SWW_RL];
+#pragma unroll
+            for (int r = 0; r < SWW_RL; ++r) { Hl[r] = 0; E[r] = NEG; }
+            int dg = 0;                               /* H(R0 - 1, j - 1); H(i, -1) = 0 */
+            int sh_h = 0, sh_f = NEG;
+            int2 cur = make_int2(0, NEG);
+            const int nreal = min(SWW_RL, max(0, n - R0));
+            auto res_at = [&](int c) -> int { return (c >= 0 && c < m) ? (int)ts[c] : 0; };
+            int tc_n1 = res_at(-lane), tc_n2 = res_at(1 - lane);
+            for (int it = 0; it <= m - 1 + 31; ++it) {
+                const int j = it - lane;
+                if (((it & 31) == 0) && pass > 0) {
+                    const int c = it + lane;
+                    cur = c < m ? __ldcg(&buf[c]) : make_int2(0, NEG);
+                }
+                const int vh = __shfl_sync(0xffffffffu, cur.x, it & 31);
+                const int vf = __shfl_sync(0xffffffffu, cur.y, it & 31);
+                int up_h = __shfl_up_sync(0xffffffffu, sh_h, 1);
+                int up_f = __shfl_up_sync(0xffffffffu, sh_f, 1);
+                const int tc_raw = tc_n1;
+                tc_n1 = tc_n2;
+                tc_n2 = res_at(j + 2);
+                if (lane == 0) {
+                    /* row above the pass: row -1 (H = 0, F = -inf) or the
+                     * previous pass's bottom row */
+                    up_h = pass > 0 ? vh : 0;
+                    up_f = pass > 0 ? vf : NEG;
+                }
+                if (j >= 0 && j < m) {
+                    int tc = tc_raw;
+                    if (tc >= p.nletters) { status |= PB_ST_BADCODE; tc = 0; }
+                    uint2 sc8 = make_uint2(0u, 0u);
+                    if (rows_in) sc8 = *reinterpret_cast<const uint2 *>(prof + (size_t)tc * Q.lp + R0);
+                    int hd = dg;
+                    int f = max(up_f - gap, up_h - open);
+                    int cmax = 0, last_h = 0, last_f = 0;
+#pragma unroll
+                    for (int r = 0; r < SWW_RL; ++r) {
+                        const uint32_t word = r < 4 ? sc8.x : sc8.y;
+                        const int sc = (int)(int8_t)((word >> (8 * (r & 3))) & 0xffu);
+                        const int e = max(E[r] - gap, Hl[r] - open);
+                        const int a = __viaddmax_s32(hd, sc, e);
+                        const int h = __vimax_s32_relu(a, f);
+                        if (r < nreal) cmax = max(cmax, h);
+                        last_h = h;
+                        last_f = f;
+                        if (GE) f = __viaddmax_s32(f, -gap, max(a, 0) - open);
+                        else f = __viaddmax_s32(f, -gap, h - open);
+                        E[r] = e;
+                        hd = Hl[r];
+                        Hl[r] = h;
+                    }
+                    /* a strictly higher maximum than the lane's best: the
+                     * first row reaching it in this column */
+                    if (cmax > best.score) {
+                        int rr = 0;
+#pragma unroll
+                        for (int r = SWW_RL - 1; r >= 0; --r) if (r < nreal && Hl[r] == cmax) rr = r;
+                        best.score = cmax; best.j = j; best.i = R0 + rr;
+                    }
+                    dg = up_h;
+                    sh_h = last_h;
+                    sh_f = last_f;
+                    if (lane == 31 && pass + 1 < npass) buf[j] = make_int2(last_h, last_f);
+                }
+            }
+            __syncwarp();
+        }
+        /* the lanes' bests in the reference's order: higher score, then
+         * smaller column, then smaller row */
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const int os = __shfl_xor_sync(0xffffffffu, best.score, o);
+            const int oj = __shfl_xor_sync(0xffffffffu, best.j, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, best.i, o);
+            const bool take = oj >= 0 && (best.j < 0 || os > best.score ||
+                                          (os == best.score && (oj < best.j || (oj == best.j && oi < best.i))));
+            if (take) { best.score = os; best.j = oj; best.i = oi; }
+        }
+        status = __reduce_or_sync(0xffffffffu, status);
+        if (lane == 0) {
+            pb_pair_out o = {};
+            o.score = best.j >= 0 ? best.score : 0;
+            o.end_query = best.j >= 0 ? best.i : 0;
+            o.end_ref = best.j >= 0 ? best.j : 0;
+            o.max_h = o.score;
+            o.status = status;
+            p.out[(size_t)q * p.npairs + pid] = o;
+        }
+    }
+}
+
 }  // namespace pb
 
 namespace {
@@ -374,6 +519,7 @@ __global__ void k_scatter(const pb_pair_out *src, const int *list, int n, pb_pai
 struct Sw16Prep {
     pb::Sw16Params p;
     int blocks;
+    bool wave;                    /* few tasks: the intra-task wavefront k_sw_wave */
     size_t prof_bytes;
     int *counter;                 /* [warp tasks, team tasks, error, spare] */
     void *bufs[9];
@@ -465,8 +611,24 @@ static int sw16_prepare(const pb_batch *b, pb_pair_out *d_out_all, size_t prof_b
     if (few) blocks = (int)sorted_tasks.size();
     else if (blocks > need) blocks = need;
     const int maxlen = hlen[0] + 1;
+    /* few tasks: the intra-task wavefront, a warp per pair, as many warps
+     * as pairs (up to the resident warps) */
+    pr->wave = few;
+    if (few) {
+        int wper = 0;
+        auto kw = pb::k_sw_wave<true>;
+        cudaFuncSetAttribute(pb::k_sw_wave<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prof_bytes);
+        cudaFuncSetAttribute(pb::k_sw_wave<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prof_bytes);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, kw, pb::SW16_WARPS * 32, prof_bytes);
+        if (wper < 1) wper = 1;
+        const long long items = (long long)n * nq;
+        const long long want = (items + pb::SW16_WARPS - 1) / pb::SW16_WARPS;
+        blocks = (int)std::min<long long>(want, (long long)wper * nsm);
+    }
     uint32_t *scratch = nullptr;
-    if (cudaMallocAsync((void **)&scratch, sizeof(uint2) * (size_t)maxlen * 32 * blocks * pb::SW16_WARPS, st) != cudaSuccess)
+    const size_t scratch_bytes = few ? sizeof(int2) * (size_t)maxlen * blocks * pb::SW16_WARPS
+                                     : sizeof(uint2) * (size_t)maxlen * 32 * blocks * pb::SW16_WARPS;
+    if (cudaMallocAsync((void **)&scratch, scratch_bytes, st) != cudaSuccess)
         scratch = nullptr;
     /* team tasks: those above a fair share of the work per warp, which one
      * warp alone would finish last */
@@ -480,7 +642,7 @@ static int sw16_prepare(const pb_batch *b, pb_pair_out *d_out_all, size_t prof_b
             ++nteam;
     }
     pb::Sw16Params &p = pr->p;
-    p.open = b->open; p.gap = b->gap; p.npairs = n; p.nq = nq;
+    p.open = b->open; p.gap = b->gap; p.npairs = n; p.nq = nq; p.nletters = b->profs[0]->size;
     p.ntasks = (int)sorted_tasks.size(); p.maxlen = maxlen; p.nteam = nteam;
     p.queries = d_q; p.prof_all = prof_all; p.prof_bytes = (int)prof_bytes;
     p.order = order; p.tasks = d_tasks;
@@ -502,7 +664,14 @@ static int sw16_prepare(const pb_batch *b, pb_pair_out *d_out_all, size_t prof_b
 static void sw16_launch(const Sw16Prep &pr, cudaStream_t st)
 {
     cudaMemsetAsync(pr.counter, 0, sizeof(int) * 4, st);
-    pb::k_sw16<<<pr.blocks, pb::SW16_WARPS * 32, pr.prof_bytes, st>>>(pr.p, pr.counter);
+    if (pr.wave) {
+        if (pr.p.open >= pr.p.gap)
+            pb::k_sw_wave<true><<<pr.blocks, pb::SW16_WARPS * 32, pr.prof_bytes, st>>>(pr.p, pr.counter);
+        else
+            pb::k_sw_wave<false><<<pr.blocks, pb::SW16_WARPS * 32, pr.prof_bytes, st>>>(pr.p, pr.counter);
+    } else {
+        pb::k_sw16<<<pr.blocks, pb::SW16_WARPS * 32, pr.prof_bytes, st>>>(pr.p, pr.counter);
+    }
 }
 
 /* nq profiles against the same targets; out[q * npairs + i]. */
