@@ -192,7 +192,11 @@ k_p16(P16Params p, const int *__restrict__ tlist, int ntl, int *counter)
         if (p.mat8) {
             qseq = p.qall + (valid ? p.qoff[item] : 0);
         } else {
-            const ProfDesc pd = p.profs[p.nt ? item / p.nt : 0];
+            /* an invalid lane (a task's padding) takes the task's query:
+             * in the shared variant every lane writes part of the slice
+             * from its own profile pointer */
+            const int qitem = valid ? item : p.order[task * 32];
+            const ProfDesc pd = p.profs[p.nt ? qitem / p.nt : 0];
             prof8 = pd.prof8;
             lp = pd.lp;
         }
