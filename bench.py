@@ -380,7 +380,7 @@ def leg_config3(pb, timer, args, td):
         ms = timer.run(dev, steps, warm)
         ms_e = timer.run(host, steps, warm)
         r = ref_run(fam, 16, "ACGT:2:-3", 5, 2, "pairs", qf, tf)
-        med, med_e, med_h = statistics.median(ms), statistics.median(ms_e), statistics.median(ms_h)
+        med, med_e = statistics.median(ms), statistics.median(ms_e)
         out["functions"][fam + "_16"] = {
             "value": cells / (med * 1e-3) / 1e9, "unit": "GCUPS", "ms_per_step": med,
             "pairs_per_s": n / (med * 1e-3),
