@@ -7,12 +7,11 @@ and the same function names and signatures for the in-scope entry points
 (score-only and stats SW / NW / 11 semi-global variants, striped and scan,
 8/16/32-bit and the `_sat` 8->16->32 chains, profile and non-profile forms,
 profile creators, parasail_nw_banded, result accessors, matrix functions and
-the name lookups), plus the traceback entry points of the exact widths (the
-serial trace forms and the 32-bit striped/scan trace forms, profile and
+the name lookups), plus the traceback entry points (the serial trace forms
+and the striped/scan trace forms at 8, 16, 32 bits and _sat, profile and
 direct), the CIGAR and traceback-string functions and matrices read from
-files. Out-of-scope families (diag, blocked, table,
-rowcol, 8/16-bit and _sat trace, 64-bit lanes, ISA-specific names) are not
-declared.
+files. Out-of-scope families (diag, blocked, table, rowcol, 64-bit lanes,
+ISA-specific names) are not declared.
 
 Run:  python include/gen_parasail_h.py > include/parasail.h
 """
@@ -401,13 +400,17 @@ def main():
                        "        const char * const restrict s2, const int s2Len,\n"
                        "        const int open, const int gap,\n"
                        "        const parasail_matrix_t* matrix);\n" % name)
-    out.append("\n/* traceback entry points (the exact widths): serial forms, reference\n"
-               " * src/{sw,nw,sg}_trace{,_scan}.c; 32-bit striped/scan forms, reference\n"
-               " * src/{sw,nw,sg}_trace_{striped,scan}_*_32.c. Paths from the GPU. */\n")
+    out.append("\n/* traceback entry points: serial forms, reference\n"
+               " * src/{sw,nw,sg}_trace{,_scan}.c; striped/scan forms at 8, 16, 32 bits\n"
+               " * and the _sat chain, reference src/{sw,nw,sg}_trace_{striped,scan}_*.c\n"
+               " * and src/satcheck.c. Paths from the GPU. */\n")
+    forms = [("trace", False), ("trace_scan", False)]
+    for scheme in ("striped", "scan"):
+        for w in ("8", "16", "32", "sat"):
+            forms.append(("trace_%s_%s" % (scheme, w), False))
+            forms.append(("trace_%s_profile_%s" % (scheme, w), True))
     for alg in ALGS:
-        for suffix, is_prof in (("trace", False), ("trace_scan", False), ("trace_striped_32", False),
-                                ("trace_scan_32", False), ("trace_striped_profile_32", True),
-                                ("trace_scan_profile_32", True)):
+        for suffix, is_prof in forms:
             name = "parasail_%s_%s" % (alg, suffix)
             if is_prof:
                 out.append("extern parasail_result_t* %s(\n"

@@ -2486,9 +2486,10 @@ extern parasail_result_t* parasail_sg_qe_de_stats_scan_profile_sat(
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
 
-/* traceback entry points (the exact widths): serial forms, reference
- * src/{sw,nw,sg}_trace{,_scan}.c; 32-bit striped/scan forms, reference
- * src/{sw,nw,sg}_trace_{striped,scan}_*_32.c. Paths from the GPU. */
+/* traceback entry points: serial forms, reference
+ * src/{sw,nw,sg}_trace{,_scan}.c; striped/scan forms at 8, 16, 32 bits
+ * and the _sat chain, reference src/{sw,nw,sg}_trace_{striped,scan}_*.c
+ * and src/satcheck.c. Paths from the GPU. */
 extern parasail_result_t* parasail_sw_trace(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
@@ -2499,12 +2500,25 @@ extern parasail_result_t* parasail_sw_trace_scan(
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sw_trace_striped_32(
+extern parasail_result_t* parasail_sw_trace_striped_8(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sw_trace_scan_32(
+extern parasail_result_t* parasail_sw_trace_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_trace_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_trace_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_trace_striped_32(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
@@ -2513,7 +2527,48 @@ extern parasail_result_t* parasail_sw_trace_striped_profile_32(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
+extern parasail_result_t* parasail_sw_trace_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_trace_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_trace_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_trace_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_trace_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_trace_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
 extern parasail_result_t* parasail_sw_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sw_trace_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sw_trace_scan_profile_sat(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
@@ -2527,12 +2582,25 @@ extern parasail_result_t* parasail_nw_trace_scan(
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_nw_trace_striped_32(
+extern parasail_result_t* parasail_nw_trace_striped_8(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_nw_trace_scan_32(
+extern parasail_result_t* parasail_nw_trace_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_trace_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_trace_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_trace_striped_32(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
@@ -2541,7 +2609,48 @@ extern parasail_result_t* parasail_nw_trace_striped_profile_32(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
+extern parasail_result_t* parasail_nw_trace_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_trace_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_trace_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_trace_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_trace_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_trace_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
 extern parasail_result_t* parasail_nw_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_nw_trace_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_nw_trace_scan_profile_sat(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
@@ -2555,12 +2664,25 @@ extern parasail_result_t* parasail_sg_trace_scan(
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_trace_striped_32(
+extern parasail_result_t* parasail_sg_trace_striped_8(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_trace_scan_32(
+extern parasail_result_t* parasail_sg_trace_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_trace_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_trace_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_trace_striped_32(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
@@ -2569,7 +2691,48 @@ extern parasail_result_t* parasail_sg_trace_striped_profile_32(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
+extern parasail_result_t* parasail_sg_trace_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_trace_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_trace_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_trace_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_trace_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_trace_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
 extern parasail_result_t* parasail_sg_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_trace_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_trace_scan_profile_sat(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
@@ -2583,12 +2746,25 @@ extern parasail_result_t* parasail_sg_qb_trace_scan(
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_qb_trace_striped_32(
+extern parasail_result_t* parasail_sg_qb_trace_striped_8(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_qb_trace_scan_32(
+extern parasail_result_t* parasail_sg_qb_trace_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_trace_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_trace_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_trace_striped_32(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
@@ -2597,7 +2773,48 @@ extern parasail_result_t* parasail_sg_qb_trace_striped_profile_32(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_trace_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_trace_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_trace_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_trace_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_trace_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_trace_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
 extern parasail_result_t* parasail_sg_qb_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_trace_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_trace_scan_profile_sat(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
@@ -2611,12 +2828,25 @@ extern parasail_result_t* parasail_sg_qe_trace_scan(
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_qe_trace_striped_32(
+extern parasail_result_t* parasail_sg_qe_trace_striped_8(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_qe_trace_scan_32(
+extern parasail_result_t* parasail_sg_qe_trace_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_trace_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_trace_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_trace_striped_32(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
@@ -2625,7 +2855,48 @@ extern parasail_result_t* parasail_sg_qe_trace_striped_profile_32(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_trace_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_trace_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_trace_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_trace_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_trace_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_trace_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
 extern parasail_result_t* parasail_sg_qe_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_trace_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_trace_scan_profile_sat(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
@@ -2639,12 +2910,25 @@ extern parasail_result_t* parasail_sg_qx_trace_scan(
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_qx_trace_striped_32(
+extern parasail_result_t* parasail_sg_qx_trace_striped_8(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_qx_trace_scan_32(
+extern parasail_result_t* parasail_sg_qx_trace_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_trace_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_trace_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_trace_striped_32(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
@@ -2653,7 +2937,48 @@ extern parasail_result_t* parasail_sg_qx_trace_striped_profile_32(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_trace_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_trace_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_trace_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_trace_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_trace_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_trace_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
 extern parasail_result_t* parasail_sg_qx_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qx_trace_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qx_trace_scan_profile_sat(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
@@ -2667,12 +2992,25 @@ extern parasail_result_t* parasail_sg_db_trace_scan(
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_db_trace_striped_32(
+extern parasail_result_t* parasail_sg_db_trace_striped_8(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_db_trace_scan_32(
+extern parasail_result_t* parasail_sg_db_trace_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_trace_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_trace_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_trace_striped_32(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
@@ -2681,7 +3019,48 @@ extern parasail_result_t* parasail_sg_db_trace_striped_profile_32(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_trace_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_trace_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_trace_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_trace_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_trace_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_trace_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
 extern parasail_result_t* parasail_sg_db_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_db_trace_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_db_trace_scan_profile_sat(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
@@ -2695,12 +3074,25 @@ extern parasail_result_t* parasail_sg_de_trace_scan(
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_de_trace_striped_32(
+extern parasail_result_t* parasail_sg_de_trace_striped_8(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_de_trace_scan_32(
+extern parasail_result_t* parasail_sg_de_trace_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_trace_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_trace_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_trace_striped_32(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
@@ -2709,7 +3101,48 @@ extern parasail_result_t* parasail_sg_de_trace_striped_profile_32(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_trace_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_trace_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_trace_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_trace_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_trace_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_trace_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
 extern parasail_result_t* parasail_sg_de_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_de_trace_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_de_trace_scan_profile_sat(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
@@ -2723,12 +3156,25 @@ extern parasail_result_t* parasail_sg_dx_trace_scan(
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_dx_trace_striped_32(
+extern parasail_result_t* parasail_sg_dx_trace_striped_8(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_dx_trace_scan_32(
+extern parasail_result_t* parasail_sg_dx_trace_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_trace_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_trace_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_trace_striped_32(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
@@ -2737,7 +3183,48 @@ extern parasail_result_t* parasail_sg_dx_trace_striped_profile_32(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_trace_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_trace_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_trace_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_trace_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_trace_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_trace_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
 extern parasail_result_t* parasail_sg_dx_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_dx_trace_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_dx_trace_scan_profile_sat(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
@@ -2751,12 +3238,25 @@ extern parasail_result_t* parasail_sg_qb_de_trace_scan(
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_qb_de_trace_striped_32(
+extern parasail_result_t* parasail_sg_qb_de_trace_striped_8(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_qb_de_trace_scan_32(
+extern parasail_result_t* parasail_sg_qb_de_trace_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_trace_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_trace_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_trace_striped_32(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
@@ -2765,7 +3265,48 @@ extern parasail_result_t* parasail_sg_qb_de_trace_striped_profile_32(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_trace_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_trace_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_trace_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_trace_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_trace_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_trace_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
 extern parasail_result_t* parasail_sg_qb_de_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_de_trace_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_de_trace_scan_profile_sat(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
@@ -2779,12 +3320,25 @@ extern parasail_result_t* parasail_sg_qe_db_trace_scan(
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_qe_db_trace_striped_32(
+extern parasail_result_t* parasail_sg_qe_db_trace_striped_8(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_qe_db_trace_scan_32(
+extern parasail_result_t* parasail_sg_qe_db_trace_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_trace_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_trace_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_trace_striped_32(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
@@ -2793,7 +3347,48 @@ extern parasail_result_t* parasail_sg_qe_db_trace_striped_profile_32(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_trace_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_trace_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_trace_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_trace_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_trace_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_trace_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
 extern parasail_result_t* parasail_sg_qe_db_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_db_trace_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_db_trace_scan_profile_sat(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
@@ -2807,12 +3402,25 @@ extern parasail_result_t* parasail_sg_qb_db_trace_scan(
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_qb_db_trace_striped_32(
+extern parasail_result_t* parasail_sg_qb_db_trace_striped_8(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_qb_db_trace_scan_32(
+extern parasail_result_t* parasail_sg_qb_db_trace_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_trace_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_trace_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_trace_striped_32(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
@@ -2821,7 +3429,48 @@ extern parasail_result_t* parasail_sg_qb_db_trace_striped_profile_32(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_trace_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_trace_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_trace_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_trace_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_trace_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_trace_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
 extern parasail_result_t* parasail_sg_qb_db_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qb_db_trace_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qb_db_trace_scan_profile_sat(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
@@ -2835,12 +3484,25 @@ extern parasail_result_t* parasail_sg_qe_de_trace_scan(
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_qe_de_trace_striped_32(
+extern parasail_result_t* parasail_sg_qe_de_trace_striped_8(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
         const parasail_matrix_t* matrix);
-extern parasail_result_t* parasail_sg_qe_de_trace_scan_32(
+extern parasail_result_t* parasail_sg_qe_de_trace_striped_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_trace_striped_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_trace_striped_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_trace_striped_32(
         const char * const restrict s1, const int s1Len,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap,
@@ -2849,7 +3511,48 @@ extern parasail_result_t* parasail_sg_qe_de_trace_striped_profile_32(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_trace_striped_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_trace_striped_profile_sat(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_trace_scan_8(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_trace_scan_profile_8(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_trace_scan_16(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_trace_scan_profile_16(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_trace_scan_32(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
 extern parasail_result_t* parasail_sg_qe_de_trace_scan_profile_32(
+        const parasail_profile_t * const restrict profile,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap);
+extern parasail_result_t* parasail_sg_qe_de_trace_scan_sat(
+        const char * const restrict s1, const int s1Len,
+        const char * const restrict s2, const int s2Len,
+        const int open, const int gap,
+        const parasail_matrix_t* matrix);
+extern parasail_result_t* parasail_sg_qe_de_trace_scan_profile_sat(
         const parasail_profile_t * const restrict profile,
         const char * const restrict s2, const int s2Len,
         const int open, const int gap);

@@ -184,12 +184,13 @@ extern int parasail_b200_batch_all_device(
 
 /** Trace results of n independent pairs (host memory) with a trace
  * function of parasail.h (the names parasail_b200_batch_pairs_cigar takes,
- * and their _profile_32 forms) in one GPU pipeline: results[i] is what the
+ * and their _profile forms) in one GPU pipeline: results[i] is what the
  * trace function returns for pair i -- usable with
  * parasail_result_get_cigar[_extra], parasail_result_get_traceback[_extra]
- * and parasail_traceback_generic*, freed with parasail_result_free -- or
- * NULL (with a message) when the pair's scores leave the int16 range of the
- * traceback kernel. Replaces n calls of the trace function (the reference
+ * and parasail_traceback_generic*, freed with parasail_result_free; a
+ * saturated 8/16-bit result carries no alignment -- or NULL (with a
+ * message) when the pair's scores leave the int16 range of the traceback
+ * kernel. Replaces n calls of the trace function (the reference
  * aligner's trace outputs, apps/parasail_aligner.cpp:2210-2550). */
 extern int parasail_b200_batch_pairs_trace(
         const char *funcname, const parasail_matrix_t *matrix,
@@ -199,14 +200,16 @@ extern int parasail_b200_batch_pairs_trace(
 
 /** CIGARs of n independent pairs (host memory) with a trace function of
  * parasail.h: "sw_trace", "nw_trace_scan", "sg_qx_trace_striped_32",
- * "sg_de_trace_scan_32", ... (serial and 32-bit forms; with or without the
+ * "sg_de_trace_scan_16", "nw_trace_striped_sat", ... (serial forms and the
+ * striped/scan forms at 8, 16, 32 bits and _sat; with or without the
  * "parasail_" prefix). For pair i: records[i] holds the score, ends and
  * flags the trace function returns; its CIGAR -- the one
  * parasail_result_get_cigar gives for that result (src/cigar.c), BAM
  * encoding -- goes to cigars[o_i ..] with o_i = sum over k < i of
  * qlengths[k] + tlengths[k] (the buffer holds sum over all pairs), its
- * element count to cigar_lengths[i] (-1 when the pair's scores leave the
- * int16 range of the traceback kernel), and the first aligned positions
+ * element count to cigar_lengths[i] (-1 when the result is saturated or
+ * the pair's scores leave the int16 range of the traceback kernel), and
+ * the first aligned positions
  * to beg_query[i], beg_ref[i]. Replaces n calls of a trace function
  * followed by parasail_result_get_cigar. */
 extern int parasail_b200_batch_pairs_cigar(

@@ -17,6 +17,7 @@ legs import this package, and only as the checker / CPU baseline. The product
 """
 import ctypes
 import os
+import re
 
 import numpy as np
 
@@ -391,19 +392,35 @@ def ref_traceback_text(r, rp, q, t, mp, aliases=None, case_sensitive=0):
 
 def ref_trace(alg_name, form, q, t, open_, gap, matrix_key, strings=False):
     """The reference's trace function `parasail_{alg}_trace{form}` on one pair
-    (form "", "_scan", "_striped_32" or "_scan_32"; the vector forms call
-    the AVX2 kernels), followed by its parasail_result_get_cigar
-    (src/cigar.c). Returns {score, end_query, end_ref, flag, cigar,
-    beg_query, beg_ref} (cigar None when the reference returns none)."""
+    (form "", "_scan", or "_striped_W" / "_scan_W" with W 8, 16, 32 or sat;
+    the vector forms call the AVX2 kernels and their _sat dispatcher),
+    followed by its parasail_result_get_cigar (src/cigar.c) unless the
+    result is saturated. Returns {score, end_query, end_ref, flag, cigar,
+    beg_query, beg_ref} (cigar None when there is none)."""
     r = ref()
     if r is None:
         return None
     mp = ref_matrix_ptr(matrix_key)
-    fname = "parasail_%s_trace%s" % (alg_name, form.replace("_32", "_avx2_256_32"))
-    fn = getattr(r, fname)
-    fn.restype = ctypes.POINTER(PResult)
-    fn.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
-                   ctypes.c_int, ctypes.POINTER(PMatrix)]
+    def kernel(f):
+        fn = getattr(r, "parasail_%s_trace%s" % (alg_name, re.sub(r"_(8|16|32)$", r"_avx2_256_\1", f)))
+        fn.restype = ctypes.POINTER(PResult)
+        fn.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                       ctypes.c_int, ctypes.POINTER(PMatrix)]
+        return fn
+
+    if form.endswith("_sat"):
+        # the _sat dispatcher (src/satcheck.c:8505-8524): 8 bits, then 16,
+        # then 32 while the result is saturated
+        widths = [form[:-3] + w for w in ("8", "16", "32")]
+
+        def fn(*args):
+            for k, f in enumerate(widths):
+                res = kernel(f)(*args)
+                if k == 2 or not res.contents.flag & 64:
+                    return res
+                r.parasail_result_free(res)
+    else:
+        fn = kernel(form)
     r.parasail_result_get_cigar.restype = ctypes.POINTER(PCigar)
     r.parasail_result_get_cigar.argtypes = [ctypes.POINTER(PResult), ctypes.c_char_p, ctypes.c_int,
                                             ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(PMatrix)]
@@ -415,12 +432,12 @@ def ref_trace(alg_name, form, q, t, open_, gap, matrix_key, strings=False):
     c = rp.contents
     out = {"score": c.score, "end_query": c.end_query, "end_ref": c.end_ref, "flag": c.flag,
            "cigar": None, "beg_query": None, "beg_ref": None}
-    cg = r.parasail_result_get_cigar(rp, qb, len(qb), tb, len(tb), mp)
+    cg = None if c.flag & 64 else r.parasail_result_get_cigar(rp, qb, len(qb), tb, len(tb), mp)
     if cg:
         s = ctypes.cast(r.parasail_cigar_decode(cg), ctypes.c_char_p).value.decode()
         out.update(cigar=s, beg_query=cg.contents.beg_query, beg_ref=cg.contents.beg_ref)
         r.parasail_cigar_free(cg)
-    if strings:
+    if strings and not c.flag & 64:
         out["traceback"] = ref_traceback_text(r, rp, q, t, mp, **(strings if isinstance(strings, dict) else {}))
     r.parasail_result_free(rp)
     return out

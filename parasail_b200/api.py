@@ -593,10 +593,10 @@ def trace(name, s1, s2, open_, gap, matrix, profile=None, strings=False):
     c = r.contents
     out = {"score": c.score, "end_query": c.end_query, "end_ref": c.end_ref, "flag": c.flag,
            "cigar": None, "beg_query": None, "beg_ref": None}
-    cg = lib.parasail_result_get_cigar(r, b1, len(b1), b2, len(b2), matrix)
+    cg = None if c.flag & 64 else lib.parasail_result_get_cigar(r, b1, len(b1), b2, len(b2), matrix)
     if cg:
         out["cigar"], out["beg_query"], out["beg_ref"] = cigar_string(cg)
-    if strings:
+    if strings and not c.flag & 64:
         out["traceback"] = traceback_text(lib, r, s1, s2, matrix, **(strings if isinstance(strings, dict) else {}))
     lib.parasail_result_free(r)
     return out

@@ -25,13 +25,17 @@
 #define FAM(base, algname, st) SER(base, algname, st) DIR(base, algname, st)
 #define BOTH(base, algname)                                                           \
     FAM(base, algname, 0) FAM(base##_stats, algname "_stats", 1)
-/* the trace forms this library provides: serial, and 32-bit striped/scan
+/* the trace forms: serial, and striped/scan at 8/16/32 bits and _sat
  * (is_trace set, as parasail/function_lookup.h:8184-8277 records them) */
+#define TDIR1(base, algname, scheme, w)                                               \
+    {base##_trace_##scheme##_##w, #base "_trace_" #scheme "_" #w, algname, #scheme, "disp", "NA", #w, -1, 0, 0, 1, 0, 0},
 #define TRACE(base, algname)                                                          \
     {base##_trace, #base "_trace", algname, "orig", "NA", "32", "32", 1, 0, 0, 1, 0, 1}, \
     {base##_trace_scan, #base "_trace_scan", algname, "scan", "NA", "32", "32", 1, 0, 0, 1, 0, 0}, \
-    {base##_trace_scan_32, #base "_trace_scan_32", algname, "scan", "disp", "NA", "32", -1, 0, 0, 1, 0, 0}, \
-    {base##_trace_striped_32, #base "_trace_striped_32", algname, "striped", "disp", "NA", "32", -1, 0, 0, 1, 0, 0},
+    TDIR1(base, algname, striped, 8) TDIR1(base, algname, striped, 16)                \
+    TDIR1(base, algname, striped, 32) TDIR1(base, algname, striped, sat)              \
+    TDIR1(base, algname, scan, 8) TDIR1(base, algname, scan, 16)                      \
+    TDIR1(base, algname, scan, 32) TDIR1(base, algname, scan, sat)
 
 static const parasail_function_info_t functions[] = {
     BOTH(parasail_sw, "sw")
@@ -67,11 +71,13 @@ static const parasail_function_info_t functions[] = {
     PFS(base##_stats, algname "_stats", 1, striped, parasail_profile_create_stats)      \
     PFS(base##_stats, algname "_stats", 1, scan, parasail_profile_create_stats)
 
+#define PT1(base, algname, scheme, w)                                                   \
+    {base##_trace_##scheme##_profile_##w, parasail_profile_create_##w, #base "_trace_" #scheme "_profile_" #w, \
+     algname, #scheme "_profile", "disp", "NA", #w, -1, 0, 0, 1, 0, 0},
 #define PTRACE(base, algname)                                                           \
-    {base##_trace_scan_profile_32, parasail_profile_create_32, #base "_trace_scan_profile_32", algname, \
-     "scan_profile", "disp", "NA", "32", -1, 0, 0, 1, 0, 0},                            \
-    {base##_trace_striped_profile_32, parasail_profile_create_32, #base "_trace_striped_profile_32", algname, \
-     "striped_profile", "disp", "NA", "32", -1, 0, 0, 1, 0, 0},
+    PT1(base, algname, scan, 8) PT1(base, algname, scan, 16) PT1(base, algname, scan, 32) \
+    PT1(base, algname, scan, sat) PT1(base, algname, striped, 8)                        \
+    PT1(base, algname, striped, 16) PT1(base, algname, striped, 32) PT1(base, algname, striped, sat)
 
 static const parasail_pfunction_info_t pfunctions[] = {
     PBOTH(parasail_sw, "sw")

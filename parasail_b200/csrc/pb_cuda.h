@@ -209,6 +209,15 @@ struct pb_mode;
 int pb_cuda_lane_pair(int bits, const pb_device_profile *dp, const struct pb_mode *m, const uint8_t *h_codes,
                       int tlen, const pb_pair_out *h_o1, pb_lane_res *h_res);
 
+/* The saturation flag of the reference's 8/16-bit nw/sg trace kernels
+ * (kind 4 striped, 5 scan) for the listed pairs of a host batch (host
+ * characters, mapped on the device; square matrix h_mat[msize*msize]):
+ * sat[k] for pair list[k]. Synchronous. */
+int pb_cuda_trace_sat_host(int bits, int kind, int sgflags, int open, int gap, int mmax, int mmin,
+                           const int32_t *h_mat, int msize, const uint8_t *map, const char *q, const int64_t *qoff,
+                           const int *qlen, const char *t, const int64_t *toff, const int *tlen, const int *list,
+                           int nlist, int *sat);
+
 /* One profile against device-resident targets with no device allocation
  * (pb_noalloc.cu): the exact kernel and the width resolution with their
  * scratch in a fixed-size file-scope device array. Jobs that need the

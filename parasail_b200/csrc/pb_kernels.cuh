@@ -66,6 +66,7 @@ struct Sw16Params {
     int open, gap, npairs, nq, ntasks, maxlen;
     int nteam;               /* tasks [0, nteam) are run by a whole block */
     int nletters;            /* profile alphabet size */
+    int bias;                /* k_sw16<true>: H - open in the registers, scores + open */
     const Sw16Query *queries;
     const int8_t *prof_all;  /* concatenated [size][lp] int8 profiles */
     int prof_bytes;
@@ -74,7 +75,7 @@ struct Sw16Params {
     const uint8_t *targets;
     const int64_t *toff;
     const int *tlen;
-    uint32_t *scratch;       /* per resident warp: [maxlen][32] uint2 */
+    uint32_t *scratch;       /* per resident warp: [maxlen][32] pass boundaries (H, F int16) */
     pb_pair_out *out;        /* [nq][npairs] */
 };
 
@@ -98,7 +99,7 @@ struct P16Params {
     int nt;                       /* db mode: targets per query; 0 in pairs mode */
     const uint8_t *targets;
     const int64_t *toff;
-    uint2 *scratch;               /* per resident warp [maxlen + 1][32] pass boundaries */
+    uint32_t *scratch;            /* per resident warp [maxlen + 1][32] pass boundaries (H, F int16) */
     int maxlen;
     pb_pair_out *out;
     /* traceback paths (optional): per item, steps written backwards into

@@ -14,6 +14,7 @@
 #include <cstdint>
 #include <climits>
 #include <cstring>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "pb_cuda.h"
@@ -97,7 +98,8 @@ template <int W> struct WarpVec {
 };
 
 struct LaneJob {
-    int kind;                                  /* 0 nw/sg, 1 nw/sg stats, 2 sw stats prefix, 3 sw */
+    int kind;                                  /* 0 nw/sg, 1 nw/sg stats, 2 sw stats prefix, 3 sw,
+                                                  4 nw/sg striped trace, 5 nw/sg scan trace */
     int open, gap, mmax, mmin;
     int s1_beg, s1_end, s2_beg, s2_end;
     /* profile mode */
@@ -111,7 +113,7 @@ struct LaneJob {
     void *scratch; int seg_max; int narr;
 };
 
-PB_LHD int lane_narr(int kind) { return kind == 0 ? 3 : kind == 1 ? 12 : kind == 2 ? 16 : 4; }
+PB_LHD int lane_narr(int kind) { return kind == 0 || kind >= 4 ? 3 : kind == 1 ? 12 : kind == 2 ? 16 : 4; }
 
 constexpr int LANE_THREADS = 256;
 
@@ -146,6 +148,8 @@ __global__ void __launch_bounds__(LANE_THREADS) k_lane(LaneJob J)
         if (J.kind == 0) striped_nwsg<WarpVec<W>, W>(v, pr, o);
         else if (J.kind == 1) striped_nwsg_stats<WarpVec<W>, W>(v, pr, o);
         else if (J.kind == 3) striped_sw<WarpVec<W>, W>(v, pr, o);
+        else if (J.kind == 4) striped_nwsg<WarpVec<W>, W, true>(v, pr, o);
+        else if (J.kind == 5) { if (W != 32) scan_nwsg_trace<WarpVec<W>, W>(v, pr, o); }
         else if (W != 32) striped_sw_stats_bias<WarpVec<W>, W>(v, pr, o);
         if (lane == 0) {
             pb_lane_res r;
@@ -156,6 +160,13 @@ __global__ void __launch_bounds__(LANE_THREADS) k_lane(LaneJob J)
         }
         __syncwarp();
     }
+}
+
+/* characters to matrix codes in place */
+__global__ void k_lane_map(uint8_t *__restrict__ buf, int64_t n, const uint8_t *__restrict__ map)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        buf[i] = map[buf[i]];
 }
 
 }  // namespace lane
@@ -176,7 +187,7 @@ int pb_cuda_lane_run(int bits, const pb_lane_args *a, const int *d_list, int nli
     cudaStream_t st = (cudaStream_t)stream;
     using namespace pb::lane;
     if (nlist <= 0) return 0;
-    if ((bits != 8 && bits != 16 && bits != 32) || (bits == 32 && a->kind == 2)) return -1;
+    if ((bits != 8 && bits != 16 && bits != 32) || (bits == 32 && (a->kind == 2 || a->kind == 5))) return -1;
     LaneJob J;
     J.kind = a->kind; J.open = a->open; J.gap = a->gap; J.mmax = a->mmax; J.mmin = a->mmin;
     J.s1_beg = (a->sgflags & PB_S1_BEG) != 0; J.s1_end = (a->sgflags & PB_S1_END) != 0;
@@ -264,6 +275,89 @@ int pb_cuda_lane_pair(int bits, const pb_device_profile *dp, const struct pb_mod
     cudaFreeAsync(d_list, st); cudaFreeAsync(d_o1, st); cudaFreeAsync(d_res, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
     cudaStreamDestroy(st);
+    return rc;
+}
+
+int pb_cuda_trace_sat_host(int bits, int kind, int sgflags, int open, int gap, int mmax, int mmin,
+                           const int32_t *h_mat, int msize, const uint8_t *map, const char *q, const int64_t *qoff,
+                           const int *qlen, const char *t, const int64_t *toff, const int *tlen, const int *list,
+                           int nlist, int *sat)
+{
+    using namespace pb::lane;
+    if (nlist <= 0) return 0;
+    if ((bits != 8 && bits != 16) || (kind != 4 && kind != 5) || msize <= 0) return -1;
+    if (pb_cuda_init() != 0) return -1;
+    /* the listed pairs, packed: queries then targets, in list order */
+    std::vector<int64_t> hqo(nlist), hto(nlist);
+    std::vector<int> hql(nlist), htl(nlist), hid(nlist);
+    int64_t nq = 0, nt = 0;
+    int maxq = 1;
+    for (int k = 0; k < nlist; ++k) {
+        const int p = list[k];
+        hqo[k] = nq; hql[k] = qlen[p]; nq += qlen[p];
+        hto[k] = nt; htl[k] = tlen[p]; nt += tlen[p];
+        hid[k] = k;
+        if (qlen[p] > maxq) maxq = qlen[p];
+    }
+    std::vector<uint8_t> chars((size_t)(nq + nt));
+    for (int k = 0; k < nlist; ++k) {
+        const int p = list[k];
+        memcpy(chars.data() + hqo[k], q + qoff[p], (size_t)qlen[p]);
+        memcpy(chars.data() + nq + hto[k], t + toff[p], (size_t)tlen[p]);
+    }
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    uint8_t *d_chars = nullptr, *d_map = nullptr;
+    int32_t *d_mat = nullptr;
+    int64_t *d_qo = nullptr, *d_to = nullptr;
+    int *d_ql = nullptr, *d_tl = nullptr, *d_list = nullptr;
+    pb_lane_res *d_res = nullptr;
+    int rc = 0;
+    if (cudaMallocAsync((void **)&d_chars, (size_t)(nq + nt) + 16, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_map, 256, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_mat, sizeof(int32_t) * (size_t)msize * msize, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_qo, sizeof(int64_t) * nlist, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_to, sizeof(int64_t) * nlist, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_ql, sizeof(int) * nlist, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_tl, sizeof(int) * nlist, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_list, sizeof(int) * nlist, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_res, sizeof(pb_lane_res) * nlist, st) != cudaSuccess)
+        rc = -1;
+    std::vector<pb_lane_res> hres;
+    if (rc == 0) {
+        cudaMemcpyAsync(d_chars, chars.data(), (size_t)(nq + nt), cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_map, map, 256, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_mat, h_mat, sizeof(int32_t) * (size_t)msize * msize, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_qo, hqo.data(), sizeof(int64_t) * nlist, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_to, hto.data(), sizeof(int64_t) * nlist, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_ql, hql.data(), sizeof(int) * nlist, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_tl, htl.data(), sizeof(int) * nlist, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_list, hid.data(), sizeof(int) * nlist, cudaMemcpyHostToDevice, st);
+        const int64_t n = nq + nt;
+        const int blocks = (int)((n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024);
+        k_lane_map<<<blocks, 256, 0, st>>>(d_chars, n, d_map);
+        pb_diag_count_launch(1);
+        pb_lane_args a;
+        memset(&a, 0, sizeof a);
+        a.kind = kind; a.sgflags = sgflags; a.open = open; a.gap = gap; a.mmax = mmax; a.mmin = mmin;
+        a.max_qlen = maxq;
+        a.mat = d_mat; a.msize = msize; a.qall = d_chars; a.qoff = d_qo; a.qlens = d_ql;
+        a.targets = d_chars + nq; a.toff = d_to; a.tlen = d_tl;
+        rc = pb_cuda_lane_run(bits, &a, d_list, nlist, d_res, nullptr, 0, st);
+        if (rc == 0) {
+            hres.resize(nlist);
+            cudaMemcpyAsync(hres.data(), d_res, sizeof(pb_lane_res) * nlist, cudaMemcpyDeviceToHost, st);
+        }
+    }
+    cudaFreeAsync(d_chars, st); cudaFreeAsync(d_map, st); cudaFreeAsync(d_mat, st);
+    cudaFreeAsync(d_qo, st); cudaFreeAsync(d_to, st); cudaFreeAsync(d_ql, st); cudaFreeAsync(d_tl, st);
+    cudaFreeAsync(d_list, st); cudaFreeAsync(d_res, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
+    cudaStreamDestroy(st);
+    for (int k = 0; rc == 0 && k < nlist; ++k) {
+        if (hres[k].valid != bits) { rc = -1; break; }
+        sat[k] = hres[k].saturated;
+    }
     return rc;
 }
 

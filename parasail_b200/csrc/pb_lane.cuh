@@ -17,6 +17,9 @@
  *   sw statistics:     util/templates/sw_stats_striped_bias.c:226-637 (the
  *                      biased kernel the FASTSTATS wrapper :644-730 runs on
  *                      the prefix [0, end_query] x [0, end_ref])
+ *   nw/sg trace:       util/templates/{nw,sg}_trace_striped.c (the
+ *                      score-only passes, lazy-F loop on >=) and
+ *                      {nw,sg}_trace_scan.c (saturation flag only)
  *
  * with the profile of src/memory_avx2.c:28-253 / :255-528 (values truncated
  * to W bits, padded rows 0; similar = truncated value > 0).
@@ -98,8 +101,13 @@ struct Out {
     int score, end_query, end_ref, matches, similar, length, saturated;
 };
 
-/* ---- nw / sg, score only (NW == SG with no free ends) ---- */
-template <class P, int W>
+/* ---- nw / sg, score only (NW == SG with no free ends) ----
+ * TRACE: the trace kernels (util/templates/nw_trace_striped.c,
+ * sg_trace_striped.c) run the same passes and checks; their lazy-F loop
+ * continues while F - gap >= H - open in some lane
+ * (src/nw_trace_striped_avx2_256_8.c:418-423) where the score kernel's
+ * continues on >. */
+template <class P, int W, bool TRACE = false>
 PB_LHD void striped_nwsg(P &v, const Problem &pr, Out &o)
 {
     typedef typename P::V V;
@@ -166,7 +174,8 @@ PB_LHD void striped_nwsg(P &v, const Problem &pr, Out &o)
                     vSatMax = v.max(vSatMax, vH);
                     vH = v.template subs<W>(vH, vGapO);
                     vF = v.template subs<W>(vF, vGapE);
-                    if (!v.any(v.cmpgt(vF, vH))) { done = true; break; }
+                    const V go = TRACE ? v.or_(v.cmpgt(vF, vH), v.cmpeq(vF, vH)) : v.cmpgt(vF, vH);
+                    if (!v.any(go)) { done = true; break; }
                 }
             }
         }
@@ -651,6 +660,92 @@ PB_LHD void striped_sw(P &v, const Problem &pr, Out &o)
     o.score = (int)((long long)score - bias);
     o.end_query = end_query;
     o.end_ref = end_ref;
+    o.matches = o.similar = o.length = 0;
+}
+
+/* ---- nw / sg trace, scan: the saturation flag of util/templates/
+ * nw_trace_scan.c and sg_trace_scan.c (src/nw_trace_scan_avx2_256_8.c:
+ * 238-350, src/sg_trace_scan_avx2_256_8.c:255-262). The checks cover E as
+ * the first loop updates it, H and F of the final loop, and for SG the
+ * gap ramp of pvGapper; the prefix scan adds set1(-segLen*gap), which the
+ * lane width truncates. A non-saturated trace result is the exact DP's, so
+ * only the flag is produced. ---- */
+template <int W> PB_LHD int gapper_at(int open, int gap, int segLen, int i)
+{
+    /* pvGapper[i]: subs(0, open) then segLen-1-i saturating subtractions of
+     * gap; a constant saturating step stays clamped once it clamps */
+    const long long x0 = clampw<W>(-(long long)wrap<W>(open));
+    return clampw<W>(x0 - (long long)(segLen - 1 - i) * wrap<W>(gap));
+}
+
+template <class P, int W>
+PB_LHD void scan_nwsg_trace(P &v, const Problem &pr, Out &o)
+{
+    typedef typename P::V V;
+    constexpr int L = Lim<W>::LANES;
+    const int s1Len = pr.qlen, s2Len = pr.tlen;
+    const int segLen = (s1Len + L - 1) / L;
+    const int open = pr.open, gap = pr.gap;
+    const bool sg = pr.s1_beg || pr.s1_end || pr.s2_beg || pr.s2_end;
+    const int NEG_LIMIT = wrap<W>((-open < pr.mmin ? (long long)Lim<W>::MIN + open : (long long)Lim<W>::MIN - pr.mmin) + 1);
+    const int POS_LIMIT = wrap<W>((long long)Lim<W>::MAX - pr.mmax - 1);
+    const V vGapO = v.set1(wrap<W>(open)), vGapE = v.set1(wrap<W>(gap));
+    const V vNegLimit = v.set1(NEG_LIMIT), vPosLimit = v.set1(POS_LIMIT);
+    const V vNegInfFront = v.insert0(v.set1(0), NEG_LIMIT);
+    const V vSegLenXgap = v.template adds<W>(vNegInfFront, v.shift1(v.set1(wrap<W>(-(long long)segLen * gap))));
+    const V vGapper0 = v.set1(gapper_at<W>(open, gap, segLen, 0));
+    V vSatMin = vPosLimit, vSatMax = vNegLimit;
+    if (sg) {
+        /* the ramp's values after each step, monotone: its two ends */
+        const long long x0 = clampw<W>(-(long long)wrap<W>(open));
+        const int a = clampw<W>(x0 - wrap<W>(gap)), b = clampw<W>(x0 - (long long)segLen * wrap<W>(gap));
+        vSatMin = v.min(vSatMin, v.set1(a < b ? a : b));
+    }
+
+    typename P::Arr pe = v.arr(0, segLen), pht = v.arr(1, segLen), ph = v.arr(2, segLen);
+    for (int i = 0; i < segLen; ++i) {
+        V h, e;
+        v.template init_he<W>(h, e, i, segLen, pr.s1_beg, open, gap);
+        v.store(ph, i, h);
+        v.store(pe, i, e);
+    }
+    for (int j = 0; j < s2Len; ++j) {
+        const int bj = v.template boundary<W>(pr, j), bj1 = v.template boundary<W>(pr, j + 1);
+        const int k_t = pr.t[j];
+        V vHp = v.insert0(v.shift1(v.load(ph, segLen - 1)), bj);
+        V vHt = v.template subs<W>(vNegLimit, vGapper0);
+        V vF = vNegLimit;
+        for (int i = 0; i < segLen; ++i) {
+            const V vH = v.load(ph, i);
+            V vE = v.load(pe, i);
+            vE = v.max(v.template subs<W>(vH, vGapO), v.template subs<W>(vE, vGapE));
+            vSatMin = v.min(vSatMin, vE);
+            vF = v.max(vF, v.template adds<W>(vHt, v.set1(gapper_at<W>(open, gap, segLen, i))));
+            vHp = v.template adds<W>(vHp, v.template prof<W>(pr, k_t, i, segLen));
+            vHt = v.max(vE, vHp);
+            v.store(pe, i, vE);
+            v.store(pht, i, vHt);
+            v.store(ph, i, vHp);
+            vHp = vH;
+        }
+        /* pseudo prefix scan on F */
+        vHt = v.insert0(v.shift1(vHt), bj1);
+        vF = v.max(vF, v.template adds<W>(vHt, vGapper0));
+        for (int k = 0; k < L - 2; ++k) vF = v.max(vF, v.template adds<W>(v.shift1(vF), vSegLenXgap));
+        vF = v.template adds<W>(v.shift1(vF), vNegInfFront);
+        V vH = v.max(vF, vHt);
+        for (int i = 0; i < segLen; ++i) {
+            vF = v.max(v.template subs<W>(vH, vGapO), v.template subs<W>(vF, vGapE));
+            vH = v.max(v.load(pht, i), vF);
+            v.store(ph, i, vH);
+            vSatMin = v.min(vSatMin, vH);
+            vSatMin = v.min(vSatMin, vF);
+            vSatMax = v.max(vSatMax, vH);
+        }
+        if (v.any(v.or_(v.cmpgt(vNegLimit, vSatMin), v.cmpgt(vSatMax, vPosLimit)))) break;
+    }
+    o.saturated = v.any(v.or_(v.cmpgt(vNegLimit, vSatMin), v.cmpgt(vSatMax, vPosLimit))) ? 1 : 0;
+    o.score = o.end_query = o.end_ref = 0;
     o.matches = o.similar = o.length = 0;
 }
 

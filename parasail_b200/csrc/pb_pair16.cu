@@ -160,7 +160,8 @@ k_p16(P16Params p, const int *__restrict__ tlist, int ntl, int *counter)
         for (int k = threadIdx.x; k < L * L; k += blockDim.x) s_mat[k] = p.mat8[k];
     __syncthreads();
 
-    uint2 *buf = p.scratch + (size_t)(blockIdx.x * WARPS + wid) * (size_t)(p.maxlen + 1) * 32;
+    /* pass boundary: strip B's bottom row per column, H low and F high */
+    uint32_t *buf = p.scratch + (size_t)(blockIdx.x * WARPS + wid) * (size_t)(p.maxlen + 1) * 32;
     const int open = p.open, gap = p.gap, sgf = p.sgflags;
     const uint32_t gO = p16_splat(-open), gE = p16_splat(-gap);
     const int nwarps_total = gridDim.x * WARPS;
@@ -299,7 +300,7 @@ k_p16(P16Params p, const int *__restrict__ tlist, int ntl, int *counter)
             int cb = 0;
             const bool more = pass + 1 < npass;
             const bool lastpass = ENDS && ALG != PB_SW && pass == p_last;
-            const uint2 vnone = make_uint2(0u, NEG);
+            const uint32_t vnone = p16_prmt(0u, NEG, 0x5410u);
             auto code_at = [&](int j) -> int {
                 int c = j < cols ? tseq[j] : 0;
                 if (c >= L) { c = 0; status |= PB_ST_BADCODE; }
@@ -307,11 +308,14 @@ k_p16(P16Params p, const int *__restrict__ tlist, int ntl, int *counter)
             };
             int c_n1 = code_at(0);
             int c_n2 = code_at(1);
-            uint2 v_n1 = vnone, v_n2 = vnone;
+            uint32_t v_n1 = vnone, v_n2 = vnone;
             if (pass != 0) {
                 if (0 <= wmax) v_n1 = __ldcg(&buf[lane]);
                 if (1 <= wmax) v_n2 = __ldcg(&buf[32 + lane]);
             }
+            /* unrolled by two: the prefetch registers then rotate by renaming
+             * instead of by moves, which would wait for the loads */
+#pragma unroll 2
             for (int j = 0; j <= wmax; ++j) {
                 const int ca = c_n1;
                 c_n1 = c_n2;
@@ -322,11 +326,11 @@ k_p16(P16Params p, const int *__restrict__ tlist, int ntl, int *counter)
                     fu = p16_prmt(NEG, prev_f, 0x5410u);
                     top -= top_step;
                 } else {
-                    const uint2 v = v_n1;
+                    const uint32_t v = v_n1;
                     v_n1 = v_n2;
                     v_n2 = j + 2 <= wmax ? __ldcg(&buf[(size_t)(j + 2) * 32 + lane]) : vnone;
-                    hu = p16_prmt(v.x, prev_h, 0x5432u);     /* lo <- previous pass's strip B bottom */
-                    fu = p16_prmt(v.y, prev_f, 0x5432u);
+                    hu = p16_prmt(v, prev_h, 0x5410u);       /* lo <- previous pass's strip B bottom */
+                    fu = p16_prmt(v, prev_f, 0x5432u);
                 }
                 const uint4 pa4 = *reinterpret_cast<const uint4 *>(sl + ca * P16_PASS);
                 const uint4 pb4 = *reinterpret_cast<const uint4 *>(sl + cb * P16_PASS + P16_R);
@@ -374,7 +378,7 @@ k_p16(P16Params p, const int *__restrict__ tlist, int ntl, int *counter)
                     if (lastpass && (sgf & PB_S2_END) && r == r_last) lastv = h;
                 }
                 if (BITS) tbits[((size_t)pass * (wmax + 1) + j) * 32 + lane] = make_uint4(aD, aF, aE, aV);
-                if (j >= 1 && more) buf[(size_t)(j - 1) * 32 + lane] = make_uint2(hu, fu);
+                if (j >= 1 && more) buf[(size_t)(j - 1) * 32 + lane] = p16_prmt(hu, fu, 0x7632u);
                 prev_h = hu;
                 prev_f = fu;
                 cb = ca;
@@ -1053,8 +1057,8 @@ int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out
             grid[sh] = (per_sm < 1 ? 1 : per_sm) * nsm;
         }
         const size_t rwarps = (size_t)std::max(grid[0] * warps[0], grid[1] * warps[1]);
-        uint2 *scratch = nullptr;
-        P16_CK(cudaMallocAsync((void **)&scratch, sizeof(uint2) * (size_t)(maxlen + 1) * 32 * rwarps, st));
+        uint32_t *scratch = nullptr;
+        P16_CK(cudaMallocAsync((void **)&scratch, sizeof(uint32_t) * (size_t)(maxlen + 1) * 32 * rwarps, st));
         frees.add(scratch);
         p.scratch = scratch;
         p.maxlen = maxlen;

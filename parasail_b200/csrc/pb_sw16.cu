@@ -9,14 +9,17 @@
  * target column j, the high half strip B (rows r0+16..r0+31) at column j-1,
  * so strip B reads strip A's bottom row from the previous iteration and both
  * halves of one DPX instruction always do useful, independent work. A pass
- * hands its bottom row (H and the vertical-gap value F) to the next pass
- * through a per-warp buffer laid out [column][lane]: one contiguous
- * 256-byte transaction per warp access. The int8 query profiles of all the
- * batch's queries live in shared memory; a column's 16 + 16 scores are two
- * 16-byte loads expanded to int16x2 words by sign-extending byte permutes.
- * The recurrence is written so that only two DPX operations per row sit on
- * the column's dependency chain (F = viaddmax(H_up, -open, F_up - gap) and
- * H = max(A, F), with A = max(H_diag + s, E, 0) computed off the chain).
+ * hands its bottom row (H and the vertical-gap value F, 16 bits each) to the
+ * next pass through a per-warp buffer laid out [column][lane]: one
+ * contiguous 128-byte transaction per warp access. The int8 query profiles
+ * of all the batch's queries live in shared memory; a column's 16 + 16
+ * scores are two 16-byte loads expanded to int16x2 words by sign-extending
+ * byte permutes. The recurrence is written so that two DPX operations per
+ * row sit on the column's dependency chain (F = viaddmax(H_up, -open,
+ * F_up - gap) and H = max(A, F), with A = max(H_diag + s, E, 0) computed off
+ * the chain), and one in the biased form (k_sw16<true>, open >= gap): the
+ * registers hold H - open and the profile s + open, and
+ * F(i+1) = max(F(i) - gap, A(i) - open) since F(i) - open <= F(i) - gap.
  *
  * Semantics: the Smith-Waterman recurrence of the reference's striped/scan
  * kernels and of src/sw.c:131-158, with its end-position rule (first column
@@ -82,6 +85,7 @@ __device__ __forceinline__ void fold_best(Sw16Best &best, bool &have, const Sw16
     }
 }
 
+template <bool BIAS>
 __global__ void __launch_bounds__(SW16_WARPS * 32, 2)
 k_sw16(Sw16Params p, int *task_counter)
 {
@@ -90,16 +94,31 @@ k_sw16(Sw16Params p, int *task_counter)
         const int4 *src = reinterpret_cast<const int4 *>(p.prof_all);
         int4 *dst = reinterpret_cast<int4 *>(s_prof);
         const int n16 = p.prof_bytes / 16;
-        for (int k = threadIdx.x; k < n16; k += blockDim.x) dst[k] = src[k];
+        /* BIAS: every score + open (the host checked that it stays in int8) */
+        const uint32_t b4 = BIAS ? 0x01010101u * (uint32_t)(uint8_t)p.open : 0u;
+        for (int k = threadIdx.x; k < n16; k += blockDim.x) {
+            int4 v = src[k];
+            if (BIAS) {
+                v.x = (int)__vadd4((uint32_t)v.x, b4); v.y = (int)__vadd4((uint32_t)v.y, b4);
+                v.z = (int)__vadd4((uint32_t)v.z, b4); v.w = (int)__vadd4((uint32_t)v.w, b4);
+            }
+            dst[k] = v;
+        }
     }
     __syncthreads();
 
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
-    /* the block's SW16_WARPS buffers: warp w's is team_buf + w * maxlen * 32 */
-    uint2 *team_buf = reinterpret_cast<uint2 *>(p.scratch) + (size_t)blockIdx.x * SW16_WARPS * p.maxlen * 32;
+    /* the block's SW16_WARPS buffers: warp w's is team_buf + w * maxlen * 32;
+     * an entry is strip B's bottom row at one column, H in the low and F in
+     * the high 16 bits */
+    uint32_t *team_buf = p.scratch + (size_t)blockIdx.x * SW16_WARPS * p.maxlen * 32;
     const uint32_t gapO = splat16(-p.open);
     const uint32_t gapE = splat16(-p.gap);
+    /* BIAS: the H registers, the pass buffer, the column maxima and the
+     * best-so-far hold H - open, so "H = 0" reads as -open */
+    const uint32_t zeroH = BIAS ? gapO : 0u;
+    const int bias = BIAS ? p.open : 0;
     /* team tasks: the tasks at the front of the list (the most expensive,
      * each more than a fair share of the work per warp) are run by all
      * warps of a block together, pass k of the task on warp k % SW16_WARPS;
@@ -140,8 +159,8 @@ k_sw16(Sw16Params p, int *task_counter)
             }
             if (task >= p.ntasks) break;
         }
-        uint2 *out_buf = team_buf + (size_t)(team ? trank : wid) * p.maxlen * 32;
-        const uint2 *in_buf = team ? team_buf + (size_t)((trank + tsize - 1) % tsize) * p.maxlen * 32 : out_buf;
+        uint32_t *out_buf = team_buf + (size_t)(team ? trank : wid) * p.maxlen * 32;
+        const uint32_t *in_buf = team ? team_buf + (size_t)((trank + tsize - 1) % tsize) * p.maxlen * 32 : out_buf;
         const Sw16Task T = p.tasks[task];
         const Sw16Query Q = p.queries[T.q];
         const int s = T.first + lane;
@@ -185,28 +204,32 @@ k_sw16(Sw16Params p, int *task_counter)
             if (!wait_for(33)) break;
             uint32_t H[SW16_R], E[SW16_R];
 #pragma unroll
-            for (int r = 0; r < SW16_R; ++r) { H[r] = 0u; E[r] = gapO; }
-            uint32_t dg = 0u;               /* lo: H(r0-1, j-1); hi: H(r0+15, j-2) */
-            uint32_t prev_h = 0u, prev_f = gapO;   /* lo halves: strip A bottom at j-1 */
+            for (int r = 0; r < SW16_R; ++r) { H[r] = zeroH; E[r] = gapO; }
+            uint32_t dg = zeroH;            /* lo: H(r0-1, j-1); hi: H(r0+15, j-2) */
+            uint32_t prev_h = zeroH, prev_f = gapO;   /* lo halves: strip A bottom at j-1 */
             Sw16Best sa = {0, -1, -1}, sb = {0, -1, -1};
-            uint32_t sbest = 0u;
+            uint32_t sbest = zeroH;
             int cb = 0;                     /* residue of column j-1 (strip B) */
             const int8_t *pa_base = prof + r0;
             const int8_t *pb_base = prof + r0 + SW16_R;
             const bool more = r0 + 2 * SW16_R < ql;
             /* the residue and the previous pass's boundary of a column are
-             * loaded two columns ahead: both come from L2 or DRAM, and the
-             * two-op chain of one column is too short to cover that latency
-             * (this pass overwrites buf[j-1] at column j, never buf[j+2]) */
-            const uint2 vnone = make_uint2(0u, gapO);
+             * loaded two and three columns ahead: both come from L2 or DRAM,
+             * and the chain of one column is too short to cover that latency
+             * (this pass overwrites buf[j-1] at column j, never buf[j+3]) */
+            const uint32_t vnone = prmt(zeroH, gapO, 0x5410u);
             int c_n1 = 0 < len ? tseq[0] : 0;
             int c_n2 = 1 < len ? tseq[1] : 0;
-            uint2 v_n1 = vnone, v_n2 = vnone;
+            uint32_t v_n1 = vnone, v_n2 = vnone, v_n3 = vnone;
             if (r0 != 0) {
                 if (0 < wmax) v_n1 = __ldcg(&in_buf[lane]);
                 if (1 < wmax) v_n2 = __ldcg(&in_buf[32 + lane]);
+                if (2 < wmax) v_n3 = __ldcg(&in_buf[64 + lane]);
             }
             bool aborted = false;
+            /* unrolled by two: the prefetch registers then rotate by renaming
+             * instead of by moves, which would wait for the loads */
+#pragma unroll 2
             for (int j = 0; j <= wmax; ++j) {
                 if (team && j > 0 && (j & 31) == 0 && !wait_for(j + 33)) { aborted = true; break; }
                 const int ca = c_n1;
@@ -214,20 +237,22 @@ k_sw16(Sw16Params p, int *task_counter)
                 c_n2 = j + 2 < len ? tseq[j + 2] : 0;
                 uint32_t hu, fu;
                 if (r0 == 0) {
-                    hu = prev_h << 16;                      /* top row H = 0 */
+                    hu = prmt(zeroH, prev_h, 0x5410u);      /* top row H = 0 */
                     fu = prmt(gapO, prev_f, 0x5410u);       /* top row F = -inf */
                 } else {
-                    const uint2 v = v_n1;
+                    const uint32_t v = v_n1;
                     v_n1 = v_n2;
-                    v_n2 = j + 2 < wmax ? __ldcg(&in_buf[(size_t)(j + 2) * 32 + lane]) : vnone;
-                    hu = prmt(v.x, prev_h, 0x5432u);        /* lo <- previous pass's strip B bottom */
-                    fu = prmt(v.y, prev_f, 0x5432u);
+                    v_n2 = v_n3;
+                    v_n3 = j + 3 < wmax ? __ldcg(&in_buf[(size_t)(j + 3) * 32 + lane]) : vnone;
+                    hu = prmt(v, prev_h, 0x5410u);          /* lo <- previous pass's strip B bottom */
+                    fu = prmt(v, prev_f, 0x5432u);
                 }
                 const uint4 pa4 = *reinterpret_cast<const uint4 *>(pa_base + (size_t)ca * lp);
                 const uint4 pb4 = *reinterpret_cast<const uint4 *>(pb_base + (size_t)cb * lp);
                 uint32_t hd = dg;
                 dg = hu;
-                uint32_t cmax = 0u;
+                uint32_t cmax = zeroH;
+                uint32_t aop = 0u;          /* BIAS: the previous row's max(H_diag + s, E, 0) - open */
 #pragma unroll
                 for (int r = 0; r < SW16_R; ++r) {
                     const uint32_t wa = r < 4 ? pa4.x : r < 8 ? pa4.y : r < 12 ? pa4.z : pa4.w;
@@ -239,21 +264,43 @@ k_sw16(Sw16Params p, int *task_counter)
                         case 2: sc = pack_pair<2>(wa, wb); break;
                         default: sc = pack_pair<3>(wa, wb); break;
                     }
-                    /* E(i,j) = max(E(i,j-1) - gap, H(i,j-1) - open): off the chain */
-                    const uint32_t e = __viaddmax_s16x2(E[r], gapE, __vadd2(H[r], gapO));
-                    const uint32_t a = __viaddmax_s16x2_relu(hd, sc, e);
-                    /* F(i,j) = max(H(i-1,j) - open, F(i-1,j) - gap): on the chain */
-                    const uint32_t f = __viaddmax_s16x2(hu, gapO, __vadd2(fu, gapE));
-                    const uint32_t h = __vmaxs2(a, f);
-                    E[r] = e;
-                    hd = H[r];
-                    H[r] = h;
-                    hu = h;
-                    fu = f;
-                    if (r & 1) cmax = __vimax3_s16x2(cmax, H[r - 1], h);
+                    if (BIAS) {
+                        /* registers hold HO = H - open and the profile s + open:
+                         *   E(i,j) = max(E(i,j-1) - gap, HO(i,j-1))
+                         *   a      = max(HO(i-1,j-1) + (s + open), E, 0)
+                         *   F(i,j) = max(F(i-1,j) - gap, HO(i-1,j))
+                         *          = max(F(i-1,j) - gap, a(i-1) - open)  (open >= gap)
+                         *   HO     = max(a - open, F - open)
+                         * so one DPX operation per row sits on the chain */
+                        const uint32_t e = __viaddmax_s16x2(E[r], gapE, H[r]);
+                        const uint32_t a = __viaddmax_s16x2_relu(hd, sc, e);
+                        const uint32_t ao = __vadd2(a, gapO);
+                        const uint32_t f = __viaddmax_s16x2(fu, gapE, r == 0 ? hu : aop);
+                        const uint32_t ho = __viaddmax_s16x2(f, gapO, ao);
+                        E[r] = e;
+                        hd = H[r];
+                        H[r] = ho;
+                        hu = ho;
+                        fu = f;
+                        aop = ao;
+                        if (r & 1) cmax = __vimax3_s16x2(cmax, H[r - 1], ho);
+                    } else {
+                        /* E(i,j) = max(E(i,j-1) - gap, H(i,j-1) - open): off the chain */
+                        const uint32_t e = __viaddmax_s16x2(E[r], gapE, __vadd2(H[r], gapO));
+                        const uint32_t a = __viaddmax_s16x2_relu(hd, sc, e);
+                        /* F(i,j) = max(H(i-1,j) - open, F(i-1,j) - gap): on the chain */
+                        const uint32_t f = __viaddmax_s16x2(hu, gapO, __vadd2(fu, gapE));
+                        const uint32_t h = __vmaxs2(a, f);
+                        E[r] = e;
+                        hd = H[r];
+                        H[r] = h;
+                        hu = h;
+                        fu = f;
+                        if (r & 1) cmax = __vimax3_s16x2(cmax, H[r - 1], h);
+                    }
                 }
                 if (j >= 1 && more) {
-                    out_buf[(size_t)(j - 1) * 32 + lane] = make_uint2(hu, fu);
+                    out_buf[(size_t)(j - 1) * 32 + lane] = prmt(hu, fu, 0x7632u);
                     /* team: publish every 32 columns and the last one */
                     if (team && (((j - 1) & 31) == 31 || j - 1 == wmax - 1)) {
                         __threadfence_block();
@@ -269,7 +316,7 @@ k_sw16(Sw16Params p, int *task_counter)
                      * left boundary (H = 0, E = -inf) */
 #pragma unroll
                     for (int r = 0; r < SW16_R; ++r) {
-                        H[r] &= 0xffffu;
+                        H[r] = (H[r] & 0xffffu) | (zeroH & 0xffff0000u);
                         E[r] = (E[r] & 0xffffu) | (gapO & 0xffff0000u);
                     }
                 }
@@ -283,18 +330,18 @@ k_sw16(Sw16Params p, int *task_counter)
                         int rr = 0;
 #pragma unroll
                         for (int r = SW16_R - 1; r >= 0; --r) if (s16lo(H[r]) == c) rr = r;
-                        sa.score = c; sa.j = j; sa.i = r0 + rr;
-                        if (c >= Q.posmax) status |= PB_ST_OVERFLOW16;
+                        sa.score = c + bias; sa.j = j; sa.i = r0 + rr;
+                        if (c + bias >= Q.posmax) status |= PB_ST_OVERFLOW16;
                     }
                     if (up_b) {
                         const int c = s16hi(cmax);
                         int rr = 0;
 #pragma unroll
                         for (int r = SW16_R - 1; r >= 0; --r) if (s16hi(H[r]) == c) rr = r;
-                        sb.score = c; sb.j = j - 1; sb.i = r0 + SW16_R + rr;
-                        if (c >= Q.posmax) status |= PB_ST_OVERFLOW16;
+                        sb.score = c + bias; sb.j = j - 1; sb.i = r0 + SW16_R + rr;
+                        if (c + bias >= Q.posmax) status |= PB_ST_OVERFLOW16;
                     }
-                    sbest = (uint32_t)(uint16_t)sa.score | ((uint32_t)(uint16_t)sb.score << 16);
+                    sbest = (uint32_t)(uint16_t)(sa.score - bias) | ((uint32_t)(uint16_t)(sb.score - bias) << 16);
                 }
             }
             if (aborted) break;
@@ -440,9 +487,10 @@ k_sw_wave(Sw16Params p, int *counter)
                         hd = Hl[r];
                         Hl[r] = h;
                     }
-                    /* a strictly higher maximum than the lane's best: the
-                     * first row reaching it in this column */
-                    if (cmax > best.score) {
+                    /* a higher maximum than the lane's best, or the same one
+                     * in an earlier column (a later pass revisits the
+                     * columns): the first row reaching it in this column */
+                    if (cmax > best.score || (cmax == best.score && j < best.j)) {
                         int rr = 0;
 #pragma unroll
                         for (int r = SWW_RL - 1; r >= 0; --r) if (r < nreal && Hl[r] == cmax) rr = r;
@@ -598,8 +646,17 @@ static int sw16_prepare(const pb_batch *b, pb_pair_out *d_out_all, size_t prof_b
     int per_sm = 0, nsm = 0, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaFuncSetAttribute(pb::k_sw16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prof_bytes);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pb::k_sw16, pb::SW16_WARPS * 32, prof_bytes);
+    /* the biased kernel (one DPX operation per row on the dependency
+     * chain) needs open >= gap and every score + open inside int8 */
+    bool bias = b->open >= b->gap;
+    for (int q = 0; q < nq; ++q)
+        if (b->profs[q]->mmax + b->open > 127 || b->profs[q]->mmin + b->open < -128) bias = false;
+    cudaFuncSetAttribute(pb::k_sw16<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prof_bytes);
+    cudaFuncSetAttribute(pb::k_sw16<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prof_bytes);
+    if (bias)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pb::k_sw16<true>, pb::SW16_WARPS * 32, prof_bytes);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pb::k_sw16<false>, pb::SW16_WARPS * 32, prof_bytes);
     if (per_sm < 1) per_sm = 1;
     int blocks = per_sm * nsm;
     const int need = (int)((sorted_tasks.size() + pb::SW16_WARPS - 1) / pb::SW16_WARPS);
@@ -627,7 +684,7 @@ static int sw16_prepare(const pb_batch *b, pb_pair_out *d_out_all, size_t prof_b
     }
     uint32_t *scratch = nullptr;
     const size_t scratch_bytes = few ? sizeof(int2) * (size_t)maxlen * blocks * pb::SW16_WARPS
-                                     : sizeof(uint2) * (size_t)maxlen * 32 * blocks * pb::SW16_WARPS;
+                                     : sizeof(uint32_t) * (size_t)maxlen * 32 * blocks * pb::SW16_WARPS;
     if (cudaMallocAsync((void **)&scratch, scratch_bytes, st) != cudaSuccess)
         scratch = nullptr;
     /* team tasks: those above a fair share of the work per warp, which one
@@ -643,6 +700,7 @@ static int sw16_prepare(const pb_batch *b, pb_pair_out *d_out_all, size_t prof_b
     }
     pb::Sw16Params &p = pr->p;
     p.open = b->open; p.gap = b->gap; p.npairs = n; p.nq = nq; p.nletters = b->profs[0]->size;
+    p.bias = bias ? 1 : 0;
     p.ntasks = (int)sorted_tasks.size(); p.maxlen = maxlen; p.nteam = nteam;
     p.queries = d_q; p.prof_all = prof_all; p.prof_bytes = (int)prof_bytes;
     p.order = order; p.tasks = d_tasks;
@@ -670,7 +728,10 @@ static void sw16_launch(const Sw16Prep &pr, cudaStream_t st)
         else
             pb::k_sw_wave<false><<<pr.blocks, pb::SW16_WARPS * 32, pr.prof_bytes, st>>>(pr.p, pr.counter);
     } else {
-        pb::k_sw16<<<pr.blocks, pb::SW16_WARPS * 32, pr.prof_bytes, st>>>(pr.p, pr.counter);
+        if (pr.p.bias)
+            pb::k_sw16<true><<<pr.blocks, pb::SW16_WARPS * 32, pr.prof_bytes, st>>>(pr.p, pr.counter);
+        else
+            pb::k_sw16<false><<<pr.blocks, pb::SW16_WARPS * 32, pr.prof_bytes, st>>>(pr.p, pr.counter);
     }
 }
 

@@ -9,6 +9,10 @@
  *   parasail_{alg}_trace_{striped,scan}[_profile]_32       (the 32-bit
  *       trace kernels, e.g. src/sw_trace_striped_avx2_256_32.c: flags
  *       STRIPED / SCAN, 32 bits, 8 lanes)
+ *   parasail_{alg}_trace_{striped,scan}[_profile]_{8,16,sat} (the 8- and
+ *       16-bit trace kernels and the _sat chain 8 -> 16 -> 32: a result
+ *       equal to the 32-bit one unless the kernel of that width saturates,
+ *       which returns score and ends 0 with PARASAIL_FLAG_SATURATED)
  * -- return the score and ends of the alignment with PARASAIL_FLAG_TRACE,
  * and parasail_result_get_cigar builds the CIGAR from the path with the
  * rules of src/cigar_template.c: steps walked back from the end cell
@@ -182,7 +186,10 @@ parasail_cigar_t *parasail_result_get_cigar_extra(parasail_result_t *result, con
     PB_CHECK_NULL(seqA);
     PB_CHECK_NULL(seqB);
     if (!(result->flag & PARASAIL_FLAG_TRACE) || !result->extra) {
-        fprintf(stderr, "%s: assert(%s) failed\n", __func__, "parasail_result_is_trace(result)");
+        if (result->flag & PARASAIL_FLAG_SATURATED)
+            fprintf(stderr, "%s: the result is saturated and holds no alignment\n", __func__);
+        else
+            fprintf(stderr, "%s: assert(%s) failed\n", __func__, "parasail_result_is_trace(result)");
         return NULL;
     }
     if (alphabet_aliases && strlen(alphabet_aliases) % 2 != 0) {
@@ -569,38 +576,6 @@ static int trace_pairs(int alg, int sgflags, const parasail_matrix_t *matrix, in
     return rc;
 }
 
-static parasail_result_t *trace_one(const char *func, int alg, int sgflags, int flags, const char *s1, int s1Len,
-                                    const char *s2, int s2Len, int open, int gap, const parasail_matrix_t *matrix)
-{
-    int ends[3];
-    pb_trace_path *path = NULL;
-    const int64_t zero = 0;
-    parasail_result_t *r;
-    int rc;
-    if (!pb_gpu_ready(func)) return NULL;
-    rc = trace_pairs(alg, sgflags, matrix, open, gap, s1, &zero, &s1Len, s2, &zero, &s2Len, 1, ends, &path);
-    if (rc == -2) {
-        fprintf(stderr, "%s: traceback needs a square matrix\n", func);
-        return NULL;
-    }
-    if (rc != 0) {
-        fprintf(stderr, "%s: GPU alignment failed: %s\n", func, pb_cuda_last_error());
-        return NULL;
-    }
-    if (!path) {
-        fprintf(stderr, "%s: the pair's scores leave the range of the traceback kernel (int16)\n", func);
-        return NULL;
-    }
-    r = pb_result_new(0);
-    if (!r) { free(path->ops); free(path); return NULL; }
-    r->score = ends[0];
-    r->end_query = ends[1];
-    r->end_ref = ends[2];
-    r->flag = flags | PARASAIL_FLAG_TRACE | PARASAIL_FLAG_BITS_32;
-    r->extra = path;
-    return r;
-}
-
 static int alg_flags(int alg, int sgflags)
 {
     int f = alg == PB_SW ? PARASAIL_FLAG_SW : alg == PB_NW ? PARASAIL_FLAG_NW : PARASAIL_FLAG_SG;
@@ -611,6 +586,174 @@ static int alg_flags(int alg, int sgflags)
         if (sgflags & PB_S2_END) f |= PARASAIL_FLAG_SG_S2_END;
     }
     return f;
+}
+
+/* ---- widths of the vector trace forms ------------------------------------ */
+
+/* A trace form: serial (kind 0) or serial scan (1), or a vector form,
+ * striped (2) or scan (3), at 8, 16 or 32 bits or the _sat chain (bits 0). */
+typedef struct trace_form {
+    int alg, sgf, kind, bits;
+} trace_form;
+
+/* the reference's BITS / LANES flags of its AVX2 trace kernels */
+static int width_flags(int w)
+{
+    return w == 8 ? PARASAIL_FLAG_BITS_8 | PARASAIL_FLAG_LANES_32
+         : w == 16 ? PARASAIL_FLAG_BITS_16 | PARASAIL_FLAG_LANES_16
+         : PARASAIL_FLAG_BITS_32 | PARASAIL_FLAG_LANES_8;
+}
+
+static int form_flags(const trace_form *f, int width)
+{
+    const int fl = alg_flags(f->alg, f->sgf) | PARASAIL_FLAG_TRACE;
+    if (f->kind == 0) return fl | PARASAIL_FLAG_NOVEC | PARASAIL_FLAG_BITS_32 | PARASAIL_FLAG_LANES_1;
+    if (f->kind == 1) return fl | PARASAIL_FLAG_NOVEC_SCAN | PARASAIL_FLAG_BITS_32 | PARASAIL_FLAG_LANES_1;
+    return fl | (f->kind == 2 ? PARASAIL_FLAG_STRIPED : PARASAIL_FLAG_SCAN) | width_flags(width);
+}
+
+/* A sound verdict that the w-bit nw/sg trace kernel (striped or scan) does
+ * not saturate: every value it checks stays inside [NEG_LIMIT, POS_LIMIT]
+ * (constants of e.g. src/nw_trace_striped_avx2_256_8.c:170-171). Every H
+ * is at least the least boundary value (-open - gap * (rows or columns))
+ * plus min(matrix, 0) per diagonal step, every checked E and F at least
+ * that minus open, every H at most max(matrix, 0) per aligned pair; the SG
+ * scan kernels also check the gap ramp -open - segLen * gap. Penalties
+ * that wrap in the lane are never clean. */
+static int nwsg_clean(int w, int qlen, int tlen, int open, int gap, int mmax, int mmin)
+{
+    const int64_t imin = w == 8 ? INT8_MIN : INT16_MIN, imax = w == 8 ? INT8_MAX : INT16_MAX;
+    const int64_t neg = ((-(int64_t)open < mmin) ? imin + open : imin - mmin) + 1;
+    const int64_t pos = imax - mmax - 1;
+    const int64_t lanes = 256 / w, seg = (qlen + lanes - 1) / lanes, pad = seg * lanes;
+    const int64_t far = (pad > tlen ? pad : tlen) - 1, diag = (pad < tlen ? pad : tlen) + 1;
+    const int64_t lb = -(int64_t)open - (int64_t)gap * far + (mmin < 0 ? (int64_t)mmin * diag : 0);
+    if (open > imax || gap > imax) return 0;
+    if (lb - open - gap < neg) return 0;
+    if (-(int64_t)open - (int64_t)gap * seg < neg) return 0;
+    return (int64_t)(mmax > 0 ? mmax : 0) * (qlen < tlen ? qlen : tlen) <= pos;
+}
+
+/* Per pair, the width whose trace kernel gives a vector form's result and
+ * whether that kernel saturated (the _sat dispatchers of src/satcheck.c
+ * run 8, then 16, then 32 bits while the result saturates). A kernel of any
+ * width that does not saturate returns the exact result the path
+ * describes. SW: the 8/16-bit trace kernels (unbiased lanes; src/
+ * sw_trace_striped_avx2_256_8.c:398-418, sw_trace_scan_avx2_256_8.c:
+ * 352-359) saturate exactly when the alignment score exceeds
+ * INT_MAX_w - max(matrix) - 1 (penalties that wrap in the lane are taken
+ * as saturating). NW/SG: clean by nwsg_clean, else the lane-exact
+ * emulation of the kernel on the GPU decides (pb_lane.cuh). sat[k] is -1
+ * for a SW pair with no path: its score, and so its width, is unknown. */
+static int trace_widths(const trace_form *f, const parasail_matrix_t *matrix, int open, int gap, const char *q,
+                        const int64_t *qoff, const int *qlen, const char *t, const int64_t *toff, const int *tlen,
+                        int n, const int *ends, pb_trace_path *const *paths, int *width, int *sat)
+{
+    static const int chain[3] = {8, 16, 32};
+    const int first = f->bits == 16 ? 1 : f->bits == 32 ? 2 : 0;
+    const int last = f->bits == 0 ? 2 : first;
+    int *pending = (int *)malloc(sizeof(int) * (size_t)n);
+    int *list = (int *)malloc(sizeof(int) * (size_t)n);
+    int *lsat = (int *)malloc(sizeof(int) * (size_t)n);
+    uint8_t map[256];
+    int np = 0, c, i, k, rc = 0;
+    if (!pending || !list || !lsat) { free(pending); free(list); free(lsat); return -1; }
+    for (k = 0; k < n; ++k) pending[np++] = k;
+    mapper_of(matrix, map);
+    for (c = first; c <= last && np > 0 && rc == 0; ++c) {
+        const int w = chain[c];
+        const int64_t imax = w == 8 ? INT8_MAX : INT16_MAX;
+        int nl = 0, nn = 0;
+        for (i = 0; i < np; ++i) {
+            k = pending[i];
+            width[k] = w;
+            sat[k] = 0;
+            if (w == 32) continue;
+            if (f->alg == PB_SW) {
+                if (open > imax || gap > imax) sat[k] = 1;
+                else if (!paths[k]) sat[k] = -1;
+                else sat[k] = ends[3 * k] > imax - matrix->max - 1;
+            } else if (!nwsg_clean(w, qlen[k], tlen[k], open, gap, matrix->max, matrix->min)) {
+                list[nl++] = k;
+            }
+        }
+        if (nl > 0) {
+            rc = pb_cuda_trace_sat_host(w, f->kind == 2 ? 4 : 5, f->sgf, open, gap, matrix->max, matrix->min,
+                                        matrix->matrix, matrix->size, map, q, qoff, qlen, t, toff, tlen, list, nl,
+                                        lsat);
+            for (i = 0; rc == 0 && i < nl; ++i) sat[list[i]] = lsat[i];
+        }
+        for (i = 0; i < np; ++i) if (sat[pending[i]] == 1) pending[nn++] = pending[i];
+        if (c < last) np = nn;
+    }
+    free(pending);
+    free(list);
+    free(lsat);
+    return rc;
+}
+
+/* Trace results of n pairs (host characters): results[k] NULL, with a
+ * message, for a pair whose result needs a path that the 16-bit pair
+ * kernels cannot give. Returns 0, or -1 (message printed, no results). */
+static int trace_results(const char *who, const trace_form *f, const parasail_matrix_t *matrix, int open, int gap,
+                         const char *q, const int64_t *qoff, const int *qlen, const char *t, const int64_t *toff,
+                         const int *tlen, int n, parasail_result_t **results)
+{
+    int *ends = (int *)malloc(sizeof(int) * 3 * (size_t)n);
+    int *width = (int *)malloc(sizeof(int) * (size_t)n);
+    int *sat = (int *)malloc(sizeof(int) * (size_t)n);
+    pb_trace_path **paths = (pb_trace_path **)calloc((size_t)n, sizeof *paths);
+    int k, rc;
+    for (k = 0; k < n; ++k) results[k] = NULL;
+    if (!ends || !width || !sat || !paths) { free(ends); free(width); free(sat); free(paths); return -1; }
+    rc = trace_pairs(f->alg, f->sgf, matrix, open, gap, q, qoff, qlen, t, toff, tlen, n, ends, paths);
+    if (rc == -2) fprintf(stderr, "%s: traceback needs a square matrix\n", who);
+    else if (rc != 0) fprintf(stderr, "%s: GPU alignment failed: %s\n", who, pb_cuda_last_error());
+    for (k = 0; k < n; ++k) { width[k] = 32; sat[k] = 0; }
+    if (rc == 0 && f->kind >= 2 && f->bits != 32) {
+        rc = trace_widths(f, matrix, open, gap, q, qoff, qlen, t, toff, tlen, n, ends, paths, width, sat);
+        if (rc != 0) fprintf(stderr, "%s: GPU alignment failed: %s\n", who, pb_cuda_last_error());
+    }
+    for (k = 0; rc == 0 && k < n; ++k) {
+        parasail_result_t *r;
+        if (sat[k] != 1 && !paths[k]) {
+            fprintf(stderr, "%s: pair %d leaves the range of the traceback kernel (int16)\n", who, k);
+            continue;
+        }
+        if (!(r = pb_result_new(0))) { rc = -1; break; }
+        r->flag = form_flags(f, width[k]);
+        if (sat[k] == 1) {
+            /* the saturated kernel's result (e.g. src/nw_trace_striped_avx2_256_8.c:431-437) */
+            r->flag |= PARASAIL_FLAG_SATURATED;
+        } else {
+            r->score = ends[3 * k];
+            r->end_query = ends[3 * k + 1];
+            r->end_ref = ends[3 * k + 2];
+            r->extra = paths[k];
+            paths[k] = NULL;
+        }
+        results[k] = r;
+    }
+    for (k = 0; k < n; ++k) if (paths[k]) { free(paths[k]->ops); free(paths[k]); }
+    if (rc != 0)
+        for (k = 0; k < n; ++k) if (results[k]) { parasail_result_free(results[k]); results[k] = NULL; }
+    free(ends);
+    free(width);
+    free(sat);
+    free(paths);
+    return rc;
+}
+
+static parasail_result_t *trace_one(const char *func, int alg, int sgflags, int kind, int bits, const char *s1,
+                                    int s1Len, const char *s2, int s2Len, int open, int gap,
+                                    const parasail_matrix_t *matrix)
+{
+    const trace_form f = {alg, sgflags, kind, bits};
+    const int64_t zero = 0;
+    parasail_result_t *r = NULL;
+    if (!pb_gpu_ready(func)) return NULL;
+    if (trace_results(func, &f, matrix, open, gap, s1, &zero, &s1Len, s2, &zero, &s2Len, 1, &r) != 0) return NULL;
+    return r;
 }
 
 /* the reference's checks and messages (parasail/memory.h:46-80) */
@@ -631,14 +774,33 @@ static int alg_flags(int alg, int sgflags)
     PB_CHECK_GE0(open);                                                   \
     PB_CHECK_GE0(gap)
 
+/* one vector trace form at one width (W = 8, 16, 32 or sat; BITS 0 = sat),
+ * direct and profile */
+#define TRACE_VEC(name, ALG, SGF, SCHEME, KIND, W, BITS)                                                       \
+    parasail_result_t *parasail_##name##_trace_##SCHEME##_##W(const char *const restrict s1, const int s1Len,   \
+                                                              const char *const restrict s2, const int s2Len,    \
+                                                              const int open, const int gap,                    \
+                                                              const parasail_matrix_t *matrix)                  \
+    {                                                                                                           \
+        TRACE_CHECKS();                                                                                         \
+        return trace_one(__func__, ALG, SGF, KIND, BITS, s1, s1Len, s2, s2Len, open, gap, matrix);             \
+    }                                                                                                           \
+    parasail_result_t *parasail_##name##_trace_##SCHEME##_profile_##W(                                          \
+        const parasail_profile_t *const restrict profile, const char *const restrict s2, const int s2Len,       \
+        const int open, const int gap)                                                                          \
+    {                                                                                                           \
+        PCHECKS();                                                                                              \
+        return trace_one(__func__, ALG, SGF, KIND, BITS, profile->s1, profile->s1Len, s2, s2Len, open, gap,    \
+                         profile->matrix);                                                                      \
+    }
+
 #define TRACE_FAMILY(name, ALG, SGF)                                                                           \
     parasail_result_t *parasail_##name##_trace(const char *const restrict s1, const int s1Len,                  \
                                                const char *const restrict s2, const int s2Len, const int open,   \
                                                const int gap, const parasail_matrix_t *matrix)                  \
     {                                                                                                           \
         TRACE_CHECKS();                                                                                         \
-        return trace_one(__func__, ALG, SGF, alg_flags(ALG, SGF) | PARASAIL_FLAG_NOVEC | PARASAIL_FLAG_LANES_1,  \
-                         s1, s1Len, s2, s2Len, open, gap, matrix);                                              \
+        return trace_one(__func__, ALG, SGF, 0, 32, s1, s1Len, s2, s2Len, open, gap, matrix);                  \
     }                                                                                                           \
     parasail_result_t *parasail_##name##_trace_scan(const char *const restrict s1, const int s1Len,             \
                                                     const char *const restrict s2, const int s2Len,              \
@@ -646,44 +808,16 @@ static int alg_flags(int alg, int sgflags)
                                                     const parasail_matrix_t *matrix)                            \
     {                                                                                                           \
         TRACE_CHECKS();                                                                                         \
-        return trace_one(__func__, ALG, SGF,                                                                    \
-                         alg_flags(ALG, SGF) | PARASAIL_FLAG_NOVEC_SCAN | PARASAIL_FLAG_LANES_1, s1, s1Len, s2,  \
-                         s2Len, open, gap, matrix);                                                             \
+        return trace_one(__func__, ALG, SGF, 1, 32, s1, s1Len, s2, s2Len, open, gap, matrix);                  \
     }                                                                                                           \
-    parasail_result_t *parasail_##name##_trace_striped_32(const char *const restrict s1, const int s1Len,       \
-                                                          const char *const restrict s2, const int s2Len,        \
-                                                          const int open, const int gap,                        \
-                                                          const parasail_matrix_t *matrix)                      \
-    {                                                                                                           \
-        TRACE_CHECKS();                                                                                         \
-        return trace_one(__func__, ALG, SGF, alg_flags(ALG, SGF) | PARASAIL_FLAG_STRIPED | PARASAIL_FLAG_LANES_8, \
-                         s1, s1Len, s2, s2Len, open, gap, matrix);                                              \
-    }                                                                                                           \
-    parasail_result_t *parasail_##name##_trace_scan_32(const char *const restrict s1, const int s1Len,          \
-                                                       const char *const restrict s2, const int s2Len,           \
-                                                       const int open, const int gap,                           \
-                                                       const parasail_matrix_t *matrix)                         \
-    {                                                                                                           \
-        TRACE_CHECKS();                                                                                         \
-        return trace_one(__func__, ALG, SGF, alg_flags(ALG, SGF) | PARASAIL_FLAG_SCAN | PARASAIL_FLAG_LANES_8,   \
-                         s1, s1Len, s2, s2Len, open, gap, matrix);                                              \
-    }                                                                                                           \
-    parasail_result_t *parasail_##name##_trace_striped_profile_32(const parasail_profile_t *const restrict profile, \
-                                                                  const char *const restrict s2, const int s2Len, \
-                                                                  const int open, const int gap)                \
-    {                                                                                                           \
-        PCHECKS();                                                                                              \
-        return trace_one(__func__, ALG, SGF, alg_flags(ALG, SGF) | PARASAIL_FLAG_STRIPED | PARASAIL_FLAG_LANES_8, \
-                         profile->s1, profile->s1Len, s2, s2Len, open, gap, profile->matrix);                   \
-    }                                                                                                           \
-    parasail_result_t *parasail_##name##_trace_scan_profile_32(const parasail_profile_t *const restrict profile,   \
-                                                               const char *const restrict s2, const int s2Len,    \
-                                                               const int open, const int gap)                   \
-    {                                                                                                           \
-        PCHECKS();                                                                                              \
-        return trace_one(__func__, ALG, SGF, alg_flags(ALG, SGF) | PARASAIL_FLAG_SCAN | PARASAIL_FLAG_LANES_8,   \
-                         profile->s1, profile->s1Len, s2, s2Len, open, gap, profile->matrix);                   \
-    }
+    TRACE_VEC(name, ALG, SGF, striped, 2, 8, 8)                                                                 \
+    TRACE_VEC(name, ALG, SGF, striped, 2, 16, 16)                                                               \
+    TRACE_VEC(name, ALG, SGF, striped, 2, 32, 32)                                                               \
+    TRACE_VEC(name, ALG, SGF, striped, 2, sat, 0)                                                               \
+    TRACE_VEC(name, ALG, SGF, scan, 3, 8, 8)                                                                    \
+    TRACE_VEC(name, ALG, SGF, scan, 3, 16, 16)                                                                  \
+    TRACE_VEC(name, ALG, SGF, scan, 3, 32, 32)                                                                  \
+    TRACE_VEC(name, ALG, SGF, scan, 3, sat, 0)
 
 TRACE_FAMILY(sw, PB_SW, 0)
 TRACE_FAMILY(nw, PB_NW, 0)
@@ -701,9 +835,10 @@ TRACE_FAMILY(sg_qe_de, PB_SG, PB_S1_END | PB_S2_END)
 
 /* ---- batch CIGARs (include/parasail_b200.h) ------------------------------- */
 
-/* the algorithm and result flags of a trace function's name
- * ("sw_trace", "nw_trace_scan_32", ...); -1 when it names none */
-static int parse_trace_name(const char *funcname, int *alg_out, int *sgf_out, int *flags_out)
+/* the trace form a function name gives ("sw_trace", "nw_trace_scan_16",
+ * "sg_qx_trace_striped_profile_sat", ...; the profile forms give the
+ * results of the direct forms); -1 when it names none */
+static int parse_trace_name(const char *funcname, trace_form *f)
 {
     static const struct { const char *name; int alg, sgf; } algs[] = {
         {"sw", PB_SW, 0}, {"nw", PB_NW, 0},
@@ -713,47 +848,48 @@ static int parse_trace_name(const char *funcname, int *alg_out, int *sgf_out, in
         {"sg_db", PB_SG, PB_S2_BEG}, {"sg_de", PB_SG, PB_S2_END}, {"sg_dx", PB_SG, PB_S2_BEG | PB_S2_END},
         {"sg", PB_SG, PB_S1_BEG | PB_S1_END | PB_S2_BEG | PB_S2_END},
     };
+    static const struct { const char *w; int bits; } widths[] = {{"8", 8}, {"16", 16}, {"32", 32}, {"sat", 0}};
     const char *s = funcname;
-    int alg = -1, sgf = 0, flags = 0;
     size_t a;
     if (!s) return -1;
+    memset(f, 0, sizeof *f);
+    f->alg = -1;
     if (0 == strncmp(s, "parasail_", 9)) s += 9;
     for (a = 0; a < sizeof algs / sizeof algs[0]; ++a) {
         const size_t l = strlen(algs[a].name);
         if (0 == strncmp(s, algs[a].name, l) && 0 == strncmp(s + l, "_trace", 6)) {
-            alg = algs[a].alg; sgf = algs[a].sgf; s += l + 6; break;
+            f->alg = algs[a].alg; f->sgf = algs[a].sgf; s += l + 6; break;
         }
     }
-    if (alg < 0) return -1;
-    /* the profile forms give the records of the direct forms */
-    if (!*s) flags = PARASAIL_FLAG_NOVEC | PARASAIL_FLAG_LANES_1;
-    else if (!strcmp(s, "_scan")) flags = PARASAIL_FLAG_NOVEC_SCAN | PARASAIL_FLAG_LANES_1;
-    else if (!strcmp(s, "_striped_32") || !strcmp(s, "_striped_profile_32")) flags = PARASAIL_FLAG_STRIPED | PARASAIL_FLAG_LANES_8;
-    else if (!strcmp(s, "_scan_32") || !strcmp(s, "_scan_profile_32")) flags = PARASAIL_FLAG_SCAN | PARASAIL_FLAG_LANES_8;
+    if (f->alg < 0) return -1;
+    f->bits = 32;
+    if (!*s) { f->kind = 0; return 0; }
+    if (!strcmp(s, "_scan")) { f->kind = 1; return 0; }
+    if (0 == strncmp(s, "_striped_", 9)) { f->kind = 2; s += 9; }
+    else if (0 == strncmp(s, "_scan_", 6)) { f->kind = 3; s += 6; }
     else return -1;
-    *alg_out = alg;
-    *sgf_out = sgf;
-    *flags_out = alg_flags(alg, sgf) | flags | PARASAIL_FLAG_TRACE | PARASAIL_FLAG_BITS_32;
-    return 0;
+    if (0 == strncmp(s, "profile_", 8)) s += 8;
+    for (a = 0; a < sizeof widths / sizeof widths[0]; ++a)
+        if (!strcmp(s, widths[a].w)) { f->bits = widths[a].bits; return 0; }
+    return -1;
 }
 
 /* Trace results of n independent pairs (host characters) in one GPU
- * pipeline; results[k] NULL for a pair outside the traceback kernels'
- * 16-bit bounds (a message names it). */
+ * pipeline; results[k] NULL for a pair whose result needs a path outside
+ * the traceback kernels' 16-bit bounds (a message names it). */
 int parasail_b200_batch_pairs_trace(const char *funcname, const parasail_matrix_t *matrix,
                                     const char *queries, const int64_t *qoffsets, const int *qlengths,
                                     const char *targets, const int64_t *toffsets, const int *tlengths, int n,
                                     int open, int gap, parasail_result_t **results)
 {
-    int alg, sgf, flags, k, rc;
-    int *ends;
-    pb_trace_path **paths;
+    trace_form f;
+    int k;
     if (!matrix || !queries || !qoffsets || !qlengths || !targets || !toffsets || !tlengths || !results) {
         fprintf(stderr, "%s: missing arguments\n", __func__);
         return -1;
     }
     if (n < 0 || open < 0 || gap < 0) { fprintf(stderr, "%s: invalid n/open/gap\n", __func__); return -1; }
-    if (parse_trace_name(funcname, &alg, &sgf, &flags) != 0) {
+    if (parse_trace_name(funcname, &f) != 0) {
         fprintf(stderr, "%s: unknown trace function '%s'\n", __func__, funcname ? funcname : "(null)");
         return -1;
     }
@@ -763,33 +899,8 @@ int parasail_b200_batch_pairs_trace(const char *funcname, const parasail_matrix_
         if (qlengths[k] <= 0 || tlengths[k] <= 0) { fprintf(stderr, "%s: pair %d has an empty sequence\n", __func__, k); return -1; }
     }
     if (!pb_gpu_ready(__func__)) return -1;
-    ends = (int *)malloc(sizeof(int) * 3 * (size_t)n);
-    paths = (pb_trace_path **)calloc((size_t)n, sizeof *paths);
-    if (!ends || !paths) { free(ends); free(paths); return -1; }
-    rc = trace_pairs(alg, sgf, matrix, open, gap, queries, qoffsets, qlengths, targets, toffsets, tlengths, n, ends,
-                     paths);
-    if (rc == -2) fprintf(stderr, "%s: traceback needs a square matrix\n", __func__);
-    for (k = 0; rc == 0 && k < n; ++k) {
-        parasail_result_t *r;
-        if (!paths[k]) {
-            fprintf(stderr, "%s: pair %d leaves the range of the traceback kernel (int16)\n", __func__, k);
-            continue;
-        }
-        if (!(r = pb_result_new(0))) { rc = -1; break; }
-        r->score = ends[3 * k]; r->end_query = ends[3 * k + 1]; r->end_ref = ends[3 * k + 2];
-        r->flag = flags;
-        r->extra = paths[k];
-        paths[k] = NULL;
-        results[k] = r;
-    }
-    for (k = 0; k < n; ++k) if (paths[k]) { free(paths[k]->ops); free(paths[k]); }
-    if (rc != 0) {
-        for (k = 0; k < n; ++k) if (results[k]) { parasail_result_free(results[k]); results[k] = NULL; }
-        fprintf(stderr, "%s: GPU alignment failed\n", __func__);
-    }
-    free(paths);
-    free(ends);
-    return rc;
+    return trace_results(__func__, &f, matrix, open, gap, queries, qoffsets, qlengths, targets, toffsets, tlengths,
+                         n, results);
 }
 
 int parasail_b200_batch_pairs_cigar(const char *funcname, const parasail_matrix_t *matrix,
@@ -798,10 +909,10 @@ int parasail_b200_batch_pairs_cigar(const char *funcname, const parasail_matrix_
                                     int open, int gap, parasail_b200_record_t *records, uint32_t *cigars,
                                     int *cigar_lengths, int *beg_query, int *beg_ref)
 {
-    int alg = -1, sgf = 0, flags = 0, k, rc;
+    trace_form f;
+    parasail_result_t **res;
     int64_t off = 0;
-    int *ends;
-    pb_trace_path **paths;
+    int k, rc;
     if (!matrix || !queries || !qoffsets || !qlengths || !targets || !toffsets || !tlengths || !records || !cigars ||
         !cigar_lengths || !beg_query || !beg_ref || !funcname) {
         fprintf(stderr, "%s: missing arguments\n", __func__);
@@ -809,31 +920,28 @@ int parasail_b200_batch_pairs_cigar(const char *funcname, const parasail_matrix_
     }
     if (n < 0 || open < 0 || gap < 0) { fprintf(stderr, "%s: invalid n/open/gap\n", __func__); return -1; }
     if (n == 0) return 0;
-    if (parse_trace_name(funcname, &alg, &sgf, &flags) != 0) alg = -1;
-    if (alg < 0) { fprintf(stderr, "%s: unknown trace function '%s'\n", __func__, funcname); return -1; }
+    if (parse_trace_name(funcname, &f) != 0) {
+        fprintf(stderr, "%s: unknown trace function '%s'\n", __func__, funcname);
+        return -1;
+    }
     for (k = 0; k < n; ++k)
         if (qlengths[k] <= 0 || tlengths[k] <= 0) { fprintf(stderr, "%s: pair %d has an empty sequence\n", __func__, k); return -1; }
     if (!pb_gpu_ready(__func__)) return -1;
-    ends = (int *)malloc(sizeof(int) * 3 * (size_t)n);
-    paths = (pb_trace_path **)calloc((size_t)n, sizeof *paths);
-    if (!ends || !paths) { free(ends); free(paths); return -1; }
-    rc = trace_pairs(alg, sgf, matrix, open, gap, queries, qoffsets, qlengths, targets, toffsets, tlengths, n, ends,
-                     paths);
-    if (rc == -2) fprintf(stderr, "%s: traceback needs a square matrix\n", __func__);
+    res = (parasail_result_t **)calloc((size_t)n, sizeof *res);
+    if (!res) return -1;
+    rc = trace_results(__func__, &f, matrix, open, gap, queries, qoffsets, qlengths, targets, toffsets, tlengths, n,
+                       res);
     for (k = 0; rc == 0 && k < n; off += (int64_t)qlengths[k] + tlengths[k], ++k) {
-        parasail_result_t r;
-        parasail_cigar_t *c;
         parasail_b200_record_t *rec = &records[k];
+        parasail_cigar_t *c;
         memset(rec, 0, sizeof *rec);
         cigar_lengths[k] = -1;
         beg_query[k] = beg_ref[k] = 0;
-        rec->score = ends[3 * k]; rec->end_query = ends[3 * k + 1]; rec->end_ref = ends[3 * k + 2];
-        rec->flag = flags;
-        if (!paths[k]) continue;
-        memset(&r, 0, sizeof r);
-        r.score = rec->score; r.end_query = rec->end_query; r.end_ref = rec->end_ref; r.flag = rec->flag;
-        r.extra = paths[k];
-        c = parasail_result_get_cigar(&r, queries + qoffsets[k], qlengths[k], targets + toffsets[k], tlengths[k],
+        if (!res[k]) continue;
+        rec->score = res[k]->score; rec->end_query = res[k]->end_query; rec->end_ref = res[k]->end_ref;
+        rec->flag = res[k]->flag;
+        if (!res[k]->extra) continue;    /* saturated: no alignment */
+        c = parasail_result_get_cigar(res[k], queries + qoffsets[k], qlengths[k], targets + toffsets[k], tlengths[k],
                                       matrix);
         if (c) {
             memcpy(cigars + off, c->seq, sizeof(uint32_t) * (size_t)c->len);
@@ -843,9 +951,7 @@ int parasail_b200_batch_pairs_cigar(const char *funcname, const parasail_matrix_
             parasail_cigar_free(c);
         }
     }
-    for (k = 0; k < n; ++k) if (paths[k]) { free(paths[k]->ops); free(paths[k]); }
-    free(paths);
-    free(ends);
-    if (rc != 0) fprintf(stderr, "%s: GPU alignment failed\n", __func__);
+    for (k = 0; k < n; ++k) if (res[k]) parasail_result_free(res[k]);
+    free(res);
     return rc;
 }

@@ -87,13 +87,15 @@ template <int W> void run(int kind, const Problem &pr, Out &o)
     if (kind == 0) striped_nwsg<HostVec<W>, W>(v, pr, o);
     else if (kind == 1) striped_nwsg_stats<HostVec<W>, W>(v, pr, o);
     else if (kind == 2) striped_sw_stats_bias<HostVec<W>, W>(v, pr, o);
-    else striped_sw<HostVec<W>, W>(v, pr, o);
+    else if (kind == 3) striped_sw<HostVec<W>, W>(v, pr, o);
+    else if (kind == 4) striped_nwsg<HostVec<W>, W, true>(v, pr, o);
+    else scan_nwsg_trace<HostVec<W>, W>(v, pr, o);
 }
 
 }  // namespace
 
 /* kind: 0 nw/sg score-only, 1 nw/sg statistics, 2 sw statistics (biased),
- * 3 sw score-only;
+ * 3 sw score-only, 4 nw/sg striped trace, 5 nw/sg scan trace (flag only);
  * sg = {s1_beg, s1_end, s2_beg, s2_end}; out = {score, end_query, end_ref,
  * matches, similar, length, saturated} */
 extern "C" int lane_host_run(int kind, int bits, const int32_t *prof, int size, int lp, const uint8_t *qcodes, int qlen,
@@ -108,7 +110,7 @@ extern "C" int lane_host_run(int kind, int bits, const int32_t *prof, int size, 
     Out o;
     if (bits == 8) run<8>(kind, pr, o);
     else if (bits == 16) run<16>(kind, pr, o);
-    else if (bits == 32 && kind != 2) run<32>(kind, pr, o);
+    else if (bits == 32 && kind != 2 && kind != 5) run<32>(kind, pr, o);
     else return -1;
     out[0] = o.score; out[1] = o.end_query; out[2] = o.end_ref;
     out[3] = o.matches; out[4] = o.similar; out[5] = o.length; out[6] = o.saturated;

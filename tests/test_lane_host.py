@@ -158,3 +158,59 @@ def test_lane_emulation_linear_and_wrapped_penalties(lanelib, seed):
                     bad.append((name, kind, bits, key, op, gp, q, t, exp, got))
     assert total == 6 * 3 * len(cases)
     assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])
+
+
+def _ref_trace_flag(name, scheme, bits, q, t, op, gp, key):
+    """Saturation flag and score of the reference's AVX2 trace kernel
+    parasail_{name}_trace_{scheme}_avx2_256_{bits}."""
+    import ctypes
+    r = O.ref()
+    fn = getattr(r, "parasail_%s_trace_%s_avx2_256_%d" % (name, scheme, bits))
+    fn.restype = ctypes.POINTER(O.PResult)
+    fn.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                   ctypes.POINTER(O.PMatrix)]
+    rp = fn(q.encode(), len(q), t.encode(), len(t), op, gp, O.ref_matrix_ptr(key))
+    out = (int(bool(rp.contents.flag & 64)), rp.contents.score)
+    r.parasail_result_free(rp)
+    return out
+
+
+@pytest.mark.parametrize("seed", [5, 6])
+def test_trace_kernel_saturation_emulation(lanelib, seed):
+    """The 8/16-bit nw/sg trace kernels (util/templates/{nw,sg}_trace_striped.c:
+    the score-only passes with the lazy-F loop continuing on ties;
+    {nw,sg}_trace_scan.c: E, H, F and the SG gap ramp checked): the
+    emulation's saturation flag equals the reference kernel's, and the
+    striped emulation's score equals the reference's when not saturated,
+    over penalties with open > gap, open == gap, open < gap and wrapped
+    values, and lengths around the 8- and 16-bit limits."""
+    rng = random.Random(seed)
+    bad, total, nsat = [], 0, 0
+    for it in range(6):
+        for bits in (8, 16):
+            for scheme, kind in (("striped", 4), ("scan", 5)):
+                for name in ALGS:
+                    if it % 2:
+                        key, a = "blosum62", AA
+                        op, gp = rng.choice([(11, 1), (10, 2), (3, 1), (40, 2), (127, 5), (200, 1), (1, 1), (0, 1),
+                                             (1, 3), (5, 5)])
+                    else:
+                        key, a = ("ACGT", 2, -3), DNA
+                        op, gp = rng.choice([(5, 2), (4, 1), (2, 1), (60, 3), (130, 0), (1, 1), (0, 2), (3, 3)])
+                    hi = rng.randint(300, 1500) if (bits == 16 and rng.random() < 0.6) else rng.randint(1, 300)
+                    q = rand_seq(rng, rng.randint(1, hi), a)
+                    t = mutate(rng, q, a, 0.2, 0.04) if it % 3 == 0 else rand_seq(rng, rng.randint(1, hi), a)
+                    m = _matrix(key)
+                    sg = [0, 0, 0, 0]
+                    if name.startswith("sg"):
+                        f = O.SG_CASES[name]
+                        sg = [int(bool(f & O.S1_BEG)), int(bool(f & O.S1_END)), int(bool(f & O.S2_BEG)),
+                              int(bool(f & O.S2_END))]
+                    esat, escore = _ref_trace_flag(name, scheme, bits, q, t, op, gp, key)
+                    o = _emulate(lanelib, kind, bits, m, q, t, op, gp, sg)
+                    total += 1
+                    nsat += esat
+                    if int(o[6]) != esat or (kind == 4 and not esat and int(o[0]) != escore):
+                        bad.append((name, scheme, bits, key, op, gp, q, t, esat, escore, list(o)))
+    assert total == 6 * 2 * 2 * len(ALGS) and 60 < nsat < total - 60
+    assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])

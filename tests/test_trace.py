@@ -1,5 +1,6 @@
-"""Traceback and CIGAR: the trace entry points of parasail.h (serial and
-32-bit striped/scan forms, direct and profile) and the batch CIGAR call,
+"""Traceback and CIGAR: the trace entry points of parasail.h (serial forms
+and striped/scan forms at 8, 16, 32 bits and _sat, direct and profile) and
+the batch CIGAR call,
 against the reference's own trace functions and parasail_result_get_cigar
 (src/cigar.c) compiled into oracle/_ref; and the CIGAR string helpers on
 CPU."""
@@ -15,6 +16,7 @@ pb = pytest.importorskip("parasail_b200")
 ALGS = ["sw", "nw", "sg", "sg_qb", "sg_qe", "sg_qx", "sg_db", "sg_de", "sg_dx", "sg_qb_de", "sg_qe_db",
         "sg_qb_db", "sg_qe_de"]
 FORMS = ["", "_scan", "_striped_32", "_scan_32"]
+NARROW = ["_striped_8", "_striped_16", "_striped_sat", "_scan_8", "_scan_16", "_scan_sat"]
 
 
 def test_cigar_string_round_trip():
@@ -115,3 +117,67 @@ def test_traceback_strings_and_printout_vs_reference():
                             bad.append((alg, form, kw, q, t, got, exp))
     assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:1])
     assert total > 400
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(O.ref() is None, reason="reference library not built")
+def test_trace_narrow_widths_vs_reference():
+    """8/16-bit and _sat trace forms on pairs around the 8-bit limits: the
+    saturation flag, score, ends, width flags and CIGAR equal the
+    reference's AVX2 trace kernels and its _sat dispatcher (src/satcheck.c),
+    at open > gap, open == gap and (nw/sg) penalties that wrap in 8 bits."""
+    rng = random.Random(321)
+    b62 = pb.matrix_lookup("blosum62")
+    dna = pb.matrix_create("ACGT", 2, -3)
+    bad, total, nsat = [], 0, 0
+    for key, m, alpha, pens in (("blosum62", b62, AA, ((11, 1), (3, 3), (5, 2))),
+                                (("ACGT", 2, -3), dna, DNA, ((5, 2), (2, 2), (130, 1)))):
+        for _ in range(8):
+            q = rand_seq(rng, rng.randint(1, 90), alpha)
+            t = mutate(rng, q, alpha, 0.1, 0.03) if rng.random() < 0.6 else rand_seq(rng, rng.randint(1, 90), alpha)
+            for op, gp in pens:
+                for alg in ALGS:
+                    if alg == "sw" and op > 127:
+                        continue     # wrapped SW penalties are taken as saturating
+                    for form in NARROW:
+                        exp = O.ref_trace(alg, form, q, t, op, gp, key)
+                        if alg == "sw" and exp["score"] < 0:
+                            continue
+                        got = pb.trace("parasail_%s_trace%s" % (alg, form), q, t, op, gp, m)
+                        total += 1
+                        nsat += bool(exp["flag"] & 64)
+                        if got != exp:
+                            bad.append((alg, form, op, gp, q, t, got, exp))
+    assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])
+    assert total > 3000 and 300 < nsat < total - 300
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(O.ref() is None, reason="reference library not built")
+def test_trace_narrow_profile_and_batch_forms():
+    """The profile forms (parasail_profile_create_8/16/sat) and the batch
+    CIGAR and trace calls with 8/16/_sat names give the direct forms'
+    results, saturated pairs included (no CIGAR, flag set)."""
+    rng = random.Random(17)
+    b62 = pb.matrix_lookup("blosum62")
+    pairs = _pairs(rng, 24, AA)
+    qs, ts = [p[0] for p in pairs], [p[1] for p in pairs]
+    for alg in ("sw", "nw", "sg_qx", "sg_de"):
+        for form in ("_striped", "_scan"):
+            for w in ("8", "16", "sat"):
+                for q, t in pairs[:4]:
+                    prof = pb.ProfileHandle("parasail_profile_create_%s" % w, q, b62)
+                    a = pb.trace("parasail_%s_trace%s_profile_%s" % (alg, form, w), q, t, 11, 1, b62, profile=prof)
+                    prof.close()
+                    b = pb.trace("parasail_%s_trace%s_%s" % (alg, form, w), q, t, 11, 1, b62)
+                    assert a == b, (alg, form, w)
+        for name in ("%s_trace_striped_8" % alg, "%s_trace_scan_sat" % alg):
+            got = pb.batch_pairs_cigar(name, b62, qs, ts, 11, 1)
+            nsat = 0
+            for q, t, g in zip(qs, ts, got):
+                one = pb.trace("parasail_" + name, q, t, 11, 1, b62)
+                assert g == one, (name, q, t)
+                assert g == O.ref_trace(alg, name.split("_trace")[1], q, t, 11, 1, "blosum62"), (name, q, t)
+                nsat += bool(g["flag"] & 64)
+            if name.endswith("_8") and alg != "sw":
+                assert nsat > 0
