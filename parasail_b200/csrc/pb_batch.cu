@@ -6,6 +6,8 @@
 #include <cstdio>
 #include <cstdint>
 #include <cstring>
+#include <algorithm>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "pb_cuda.h"
@@ -304,9 +306,30 @@ __global__ void k_map_codes(uint8_t *__restrict__ buf, int64_t n, const uint8_t 
 
 }  // namespace
 
+namespace {
+
+/* characters [lo, hi) of raw to codes at the same offsets */
+__global__ void k_map_into(const uint8_t *__restrict__ raw, uint8_t *__restrict__ codes, int64_t lo, int64_t hi,
+                           const uint8_t *__restrict__ map)
+{
+    __shared__ uint8_t smap[256];
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) smap[k] = map[k];
+    __syncthreads();
+    for (int64_t i = lo + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < hi; i += (int64_t)gridDim.x * blockDim.x)
+        codes[i] = smap[raw[i]];
+}
+
+}  // namespace
+
 /* Host-memory batch: copies the characters of targets (and, in pairs mode,
  * queries) to the device, maps them to codes there, runs the pipeline and
- * copies the records back. */
+ * copies the records back. With one query set (pairs mode or a single
+ * profile) and enough pairs, the items run in chunks whose copies overlap
+ * the previous chunk's alignment: chunk k + 1's characters go up and chunk
+ * k - 1's records come back on a copy stream while chunk k runs. Every
+ * chunk's characters land at their own offsets in one device buffer (a
+ * separate raw buffer is mapped into it, so chunks whose byte ranges
+ * overlap map the same bytes to the same codes). */
 extern "C" int pb_cuda_batch_host(const pb_job *job, const pb_batch *tmpl, const uint8_t *mapper256,
                                   const char *h_targets, const int64_t *h_toff, const int *h_tlen,
                                   const char *h_queries, const int64_t *h_qoff, const int *h_qlen,
@@ -314,69 +337,97 @@ extern "C" int pb_cuda_batch_host(const pb_job *job, const pb_batch *tmpl, const
 {
     if (pb_cuda_init() != 0) return -1;
     if (n <= 0) return 0;
-    cudaStream_t st = nullptr;
-    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    const int nq = tmpl->nprofs > 0 ? tmpl->nprofs : 1;
+    /* chunks: at least 65,536 items each, at most 4 */
+    constexpr int CH_MIN = 1 << 16;
+    const int nch = nq == 1 ? std::max(1, std::min(4, n / CH_MIN)) : 1;
+    std::vector<int> cut(nch + 1);
+    for (int k = 0; k <= nch; ++k) cut[k] = (int)((int64_t)n * k / nch);
+    /* each chunk's byte ranges [lo, hi) of targets and queries */
+    std::vector<int64_t> tlo(nch, INT64_MAX), thi(nch, 0), qlo(nch, INT64_MAX), qhi(nch, 0);
     int64_t tbytes = 0, qbytes = 0;
-    for (int i = 0; i < n; ++i) {
-        const int64_t e = h_toff[i] + h_tlen[i];
-        tbytes = e > tbytes ? e : tbytes;
-        if (h_queries) {
-            const int64_t q = h_qoff[i] + h_qlen[i];
-            qbytes = q > qbytes ? q : qbytes;
+    for (int k = 0; k < nch; ++k)
+        for (int i = cut[k]; i < cut[k + 1]; ++i) {
+            tlo[k] = std::min(tlo[k], h_toff[i]);
+            thi[k] = std::max(thi[k], h_toff[i] + h_tlen[i]);
+            if (h_queries) {
+                qlo[k] = std::min(qlo[k], h_qoff[i]);
+                qhi[k] = std::max(qhi[k], h_qoff[i] + h_qlen[i]);
+            }
         }
-    }
-    uint8_t *d_t = nullptr, *d_q = nullptr, *d_map = nullptr;
+    for (int k = 0; k < nch; ++k) { tbytes = std::max(tbytes, thi[k]); if (h_queries) qbytes = std::max(qbytes, qhi[k]); }
+    cudaStream_t cs = nullptr;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    std::vector<cudaEvent_t> ready(nch, nullptr);
+    uint8_t *d_t = nullptr, *d_traw = nullptr, *d_q = nullptr, *d_qraw = nullptr, *d_map = nullptr;
     int64_t *d_toff = nullptr, *d_qoff = nullptr;
     int *d_tlen = nullptr, *d_qlen = nullptr;
     pb_record *d_rec = nullptr;
     int rc = 0;
-    const int nq = tmpl->nprofs > 0 ? tmpl->nprofs : 1;
-    if (cudaMallocAsync((void **)&d_t, tbytes + 16, st) != cudaSuccess ||
-        cudaMallocAsync((void **)&d_toff, sizeof(int64_t) * n, st) != cudaSuccess ||
-        cudaMallocAsync((void **)&d_tlen, sizeof(int) * n, st) != cudaSuccess ||
-        cudaMallocAsync((void **)&d_map, 256, st) != cudaSuccess ||
-        cudaMallocAsync((void **)&d_rec, sizeof(pb_record) * n * (size_t)nq, st) != cudaSuccess)
+    for (int k = 0; k < nch && rc == 0; ++k)
+        if (cudaEventCreateWithFlags(&ready[k], cudaEventDisableTiming) != cudaSuccess) rc = -1;
+    if (rc == 0 &&
+        (cudaMallocAsync((void **)&d_t, tbytes + 16, cs) != cudaSuccess ||
+         cudaMallocAsync((void **)&d_traw, tbytes + 16, cs) != cudaSuccess ||
+         cudaMallocAsync((void **)&d_toff, sizeof(int64_t) * n, cs) != cudaSuccess ||
+         cudaMallocAsync((void **)&d_tlen, sizeof(int) * n, cs) != cudaSuccess ||
+         cudaMallocAsync((void **)&d_map, 256, cs) != cudaSuccess ||
+         cudaMallocAsync((void **)&d_rec, sizeof(pb_record) * n * (size_t)nq, cs) != cudaSuccess))
         rc = -1;
     if (rc == 0 && h_queries &&
-        (cudaMallocAsync((void **)&d_q, qbytes + 16, st) != cudaSuccess ||
-         cudaMallocAsync((void **)&d_qoff, sizeof(int64_t) * n, st) != cudaSuccess ||
-         cudaMallocAsync((void **)&d_qlen, sizeof(int) * n, st) != cudaSuccess))
+        (cudaMallocAsync((void **)&d_q, qbytes + 16, cs) != cudaSuccess ||
+         cudaMallocAsync((void **)&d_qraw, qbytes + 16, cs) != cudaSuccess ||
+         cudaMallocAsync((void **)&d_qoff, sizeof(int64_t) * n, cs) != cudaSuccess ||
+         cudaMallocAsync((void **)&d_qlen, sizeof(int) * n, cs) != cudaSuccess))
         rc = -1;
-    if (rc == 0) {
-        cudaMemcpyAsync(d_t, h_targets, tbytes, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(d_toff, h_toff, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(d_tlen, h_tlen, sizeof(int) * n, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(d_map, mapper256, 256, cudaMemcpyHostToDevice, st);
-        k_map_codes<<<296, 256, 0, st>>>(d_t, tbytes, d_map);
+    auto stage = [&](int k) {
+        /* chunk k's offsets, lengths and characters, mapped to codes */
+        const size_t i0 = (size_t)cut[k], ni = (size_t)(cut[k + 1] - cut[k]);
+        cudaMemcpyAsync(d_toff + i0, h_toff + i0, sizeof(int64_t) * ni, cudaMemcpyHostToDevice, cs);
+        cudaMemcpyAsync(d_tlen + i0, h_tlen + i0, sizeof(int) * ni, cudaMemcpyHostToDevice, cs);
+        cudaMemcpyAsync(d_traw + tlo[k], h_targets + tlo[k], thi[k] - tlo[k], cudaMemcpyHostToDevice, cs);
+        k_map_into<<<296, 256, 0, cs>>>(d_traw, d_t, tlo[k], thi[k], d_map);
         pb_diag_count_launch(1);
         if (h_queries) {
-            cudaMemcpyAsync(d_q, h_queries, qbytes, cudaMemcpyHostToDevice, st);
-            cudaMemcpyAsync(d_qoff, h_qoff, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
-            cudaMemcpyAsync(d_qlen, h_qlen, sizeof(int) * n, cudaMemcpyHostToDevice, st);
-            k_map_codes<<<296, 256, 0, st>>>(d_q, qbytes, d_map);
+            cudaMemcpyAsync(d_qoff + i0, h_qoff + i0, sizeof(int64_t) * ni, cudaMemcpyHostToDevice, cs);
+            cudaMemcpyAsync(d_qlen + i0, h_qlen + i0, sizeof(int) * ni, cudaMemcpyHostToDevice, cs);
+            cudaMemcpyAsync(d_qraw + qlo[k], h_queries + qlo[k], qhi[k] - qlo[k], cudaMemcpyHostToDevice, cs);
+            k_map_into<<<296, 256, 0, cs>>>(d_qraw, d_q, qlo[k], qhi[k], d_map);
             pb_diag_count_launch(1);
         }
-        if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
-    }
+        cudaEventRecord(ready[k], cs);
+    };
     if (rc == 0) {
-        pb_batch b = *tmpl;
-        b.npairs = n;
-        b.d_targets = d_t; b.d_toff = d_toff; b.d_tlen = d_tlen;
-        if (h_queries) { b.d_qall = d_q; b.d_qoff = d_qoff; b.d_qlen = d_qlen; }
-        rc = pb_cuda_batch_run(job, &b, d_rec);
+        cudaMemcpyAsync(d_map, mapper256, 256, cudaMemcpyHostToDevice, cs);
+        stage(0);
     }
-    if (rc == 0 && cudaMemcpyAsync(h_rec, d_rec, sizeof(pb_record) * n * (size_t)nq, cudaMemcpyDeviceToHost, st) != cudaSuccess)
-        rc = -1;
-    if (d_t) cudaFreeAsync(d_t, st);
-    if (d_toff) cudaFreeAsync(d_toff, st);
-    if (d_tlen) cudaFreeAsync(d_tlen, st);
-    if (d_map) cudaFreeAsync(d_map, st);
-    if (d_rec) cudaFreeAsync(d_rec, st);
-    if (d_q) cudaFreeAsync(d_q, st);
-    if (d_qoff) cudaFreeAsync(d_qoff, st);
-    if (d_qlen) cudaFreeAsync(d_qlen, st);
-    if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
-    cudaStreamDestroy(st);
+    for (int k = 0; k < nch && rc == 0; ++k) {
+        if (k + 1 < nch) stage(k + 1);
+        if (cudaEventSynchronize(ready[k]) != cudaSuccess) { rc = -1; break; }
+        const int i0 = cut[k];
+        pb_batch b = *tmpl;
+        b.npairs = cut[k + 1] - i0;
+        b.d_targets = d_t; b.d_toff = d_toff + i0; b.d_tlen = d_tlen + i0;
+        if (h_queries) { b.d_qall = d_q; b.d_qoff = d_qoff + i0; b.d_qlen = d_qlen + i0; }
+        rc = pb_cuda_batch_run(job, &b, d_rec + (size_t)i0 * nq);
+        if (rc == 0 && cudaMemcpyAsync(h_rec + (size_t)i0 * nq, d_rec + (size_t)i0 * nq,
+                                       sizeof(pb_record) * (size_t)b.npairs * nq, cudaMemcpyDeviceToHost,
+                                       cs) != cudaSuccess)
+            rc = -1;
+    }
+    if (d_t) cudaFreeAsync(d_t, cs);
+    if (d_traw) cudaFreeAsync(d_traw, cs);
+    if (d_toff) cudaFreeAsync(d_toff, cs);
+    if (d_tlen) cudaFreeAsync(d_tlen, cs);
+    if (d_map) cudaFreeAsync(d_map, cs);
+    if (d_rec) cudaFreeAsync(d_rec, cs);
+    if (d_q) cudaFreeAsync(d_q, cs);
+    if (d_qraw) cudaFreeAsync(d_qraw, cs);
+    if (d_qoff) cudaFreeAsync(d_qoff, cs);
+    if (d_qlen) cudaFreeAsync(d_qlen, cs);
+    if (cudaStreamSynchronize(cs) != cudaSuccess) rc = -1;
+    for (int k = 0; k < nch; ++k) if (ready[k]) cudaEventDestroy(ready[k]);
+    cudaStreamDestroy(cs);
     return rc;
 }
 

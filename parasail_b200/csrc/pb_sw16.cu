@@ -398,9 +398,9 @@ k_sw16(Sw16Params p, int *task_counter)
  * row is max(F - gap, max(a, 0) - open) with a = max(H_diag + s, E), one
  * dependent operation per row.
  */
-static constexpr int SWW_RL = 8;          /* query rows per lane */
-
-template <bool GE>
+/* RL query rows per lane (4, 8, 12 or 16; a pass covers 32 * RL rows),
+ * chosen per launch from the query lengths (wave_rows) */
+template <bool GE, int RL>
 __global__ void __launch_bounds__(SW16_WARPS * 32, 2)
 k_sw_wave(Sw16Params p, int *counter)
 {
@@ -429,19 +429,21 @@ k_sw_wave(Sw16Params p, int *counter)
         const int n = Q.qlen, m = p.tlen[pid];
         const uint8_t *ts = p.targets + p.toff[pid];
         const int8_t *prof = s_prof + Q.prof_off;
-        const int npass = (n + 32 * SWW_RL - 1) / (32 * SWW_RL);
+        const int npass = (n + 32 * RL - 1) / (32 * RL);
         Sw16Best best = {0, -1, -1};
         int status = 0;
         for (int pass = 0; pass < npass; ++pass) {
-            const int R0 = pass * 32 * SWW_RL + lane * SWW_RL;
-            const bool rows_in = R0 < Q.lp;           /* profile rows past lp score 0 (dummy rows) */
-            int Hl[SWW_RL], E[SWW_RL];
+            const int R0 = pass * 32 * RL + lane * RL;
+            /* a lane whose rows reach past lp (a multiple of 64, at least
+             * qlen + 32) holds only dummy rows: they score 0 */
+            const bool rows_in = R0 + RL <= Q.lp;
+            int Hl[RL], E[RL];
 #pragma unroll
-            for (int r = 0; r < SWW_RL; ++r) { Hl[r] = 0; E[r] = NEG; }
+            for (int r = 0; r < RL; ++r) { Hl[r] = 0; E[r] = NEG; }
             int dg = 0;                               /* H(R0 - 1, j - 1); H(i, -1) = 0 */
             int sh_h = 0, sh_f = NEG;
             int2 cur = make_int2(0, NEG);
-            const int nreal = min(SWW_RL, max(0, n - R0));
+            const int nreal = min(RL, max(0, n - R0));
             auto res_at = [&](int c) -> int { return (c >= 0 && c < m) ? (int)ts[c] : 0; };
             int tc_n1 = res_at(-lane), tc_n2 = res_at(1 - lane);
             for (int it = 0; it <= m - 1 + 31; ++it) {
@@ -466,15 +468,17 @@ k_sw_wave(Sw16Params p, int *counter)
                 if (j >= 0 && j < m) {
                     int tc = tc_raw;
                     if (tc >= p.nletters) { status |= PB_ST_BADCODE; tc = 0; }
-                    uint2 sc8 = make_uint2(0u, 0u);
-                    if (rows_in) sc8 = *reinterpret_cast<const uint2 *>(prof + (size_t)tc * Q.lp + R0);
+                    /* R0 and lp are multiples of 4: word loads */
+                    uint32_t sw[RL / 4];
+#pragma unroll
+                    for (int k = 0; k < RL / 4; ++k)
+                        sw[k] = rows_in ? reinterpret_cast<const uint32_t *>(prof + (size_t)tc * Q.lp + R0)[k] : 0u;
                     int hd = dg;
                     int f = max(up_f - gap, up_h - open);
                     int cmax = 0, last_h = 0, last_f = 0;
 #pragma unroll
-                    for (int r = 0; r < SWW_RL; ++r) {
-                        const uint32_t word = r < 4 ? sc8.x : sc8.y;
-                        const int sc = (int)(int8_t)((word >> (8 * (r & 3))) & 0xffu);
+                    for (int r = 0; r < RL; ++r) {
+                        const int sc = (int)(int8_t)((sw[r >> 2] >> (8 * (r & 3))) & 0xffu);
                         const int e = max(E[r] - gap, Hl[r] - open);
                         const int a = __viaddmax_s32(hd, sc, e);
                         const int h = __vimax_s32_relu(a, f);
@@ -493,7 +497,7 @@ k_sw_wave(Sw16Params p, int *counter)
                     if (cmax > best.score || (cmax == best.score && j < best.j)) {
                         int rr = 0;
 #pragma unroll
-                        for (int r = SWW_RL - 1; r >= 0; --r) if (r < nreal && Hl[r] == cmax) rr = r;
+                        for (int r = RL - 1; r >= 0; --r) if (r < nreal && Hl[r] == cmax) rr = r;
                         best.score = cmax; best.j = j; best.i = R0 + rr;
                     }
                     dg = up_h;
@@ -568,6 +572,7 @@ struct Sw16Prep {
     pb::Sw16Params p;
     int blocks;
     bool wave;                    /* few tasks: the intra-task wavefront k_sw_wave */
+    int wave_rl;                  /* its rows per lane */
     size_t prof_bytes;
     int *counter;                 /* [warp tasks, team tasks, error, spare] */
     void *bufs[9];
@@ -577,6 +582,34 @@ static void sw16_release(Sw16Prep *pr, cudaStream_t st)
 {
     for (void *x : pr->bufs) if (x) cudaFreeAsync(x, st);
     memset(pr->bufs, 0, sizeof pr->bufs);
+}
+
+typedef void (*WaveKernel)(pb::Sw16Params, int *);
+
+/* k_sw_wave for (open >= gap, rows per lane) */
+static WaveKernel wave_kernel(bool ge, int rl)
+{
+    if (ge) {
+        switch (rl) {
+            case 4: return pb::k_sw_wave<true, 4>;
+            case 12: return pb::k_sw_wave<true, 12>;
+            case 16: return pb::k_sw_wave<true, 16>;
+            default: return pb::k_sw_wave<true, 8>;
+        }
+    }
+    switch (rl) {
+        case 4: return pb::k_sw_wave<false, 4>;
+        case 12: return pb::k_sw_wave<false, 12>;
+        case 16: return pb::k_sw_wave<false, 16>;
+        default: return pb::k_sw_wave<false, 8>;
+    }
+}
+
+static void wave_set_smem(int bytes)
+{
+    for (int ge = 0; ge < 2; ++ge)
+        for (int rl = 4; rl <= 16; rl += 4)
+            cudaFuncSetAttribute(wave_kernel(ge != 0, rl), cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 static int sw16_prepare(const pb_batch *b, pb_pair_out *d_out_all, size_t prof_bytes, cudaStream_t st,
@@ -672,11 +705,22 @@ static int sw16_prepare(const pb_batch *b, pb_pair_out *d_out_all, size_t prof_b
      * as pairs (up to the resident warps) */
     pr->wave = few;
     if (few) {
+        /* rows per lane: the fewest row-steps over the batch's queries,
+         * npass * (RL + 4) per column, the 4 standing for the per-column
+         * shuffles and loads (one query of 300 rows: one pass of 12 rows
+         * per lane instead of two of 8) */
+        int best_rl = 8;
+        double best_cost = -1.0;
+        for (int rl = 4; rl <= 16; rl += 4) {
+            double cost = 0.0;
+            for (int q = 0; q < nq; ++q) cost += (double)((hq[q].qlen + 32 * rl - 1) / (32 * rl)) * (rl + 4);
+            if (best_cost < 0.0 || cost < best_cost) { best_cost = cost; best_rl = rl; }
+        }
+        pr->wave_rl = best_rl;
         int wper = 0;
-        auto kw = pb::k_sw_wave<true>;
-        cudaFuncSetAttribute(pb::k_sw_wave<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prof_bytes);
-        cudaFuncSetAttribute(pb::k_sw_wave<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prof_bytes);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, kw, pb::SW16_WARPS * 32, prof_bytes);
+        wave_set_smem((int)prof_bytes);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, wave_kernel(b->open >= b->gap, best_rl),
+                                                      pb::SW16_WARPS * 32, prof_bytes);
         if (wper < 1) wper = 1;
         const long long items = (long long)n * nq;
         const long long want = (items + pb::SW16_WARPS - 1) / pb::SW16_WARPS;
@@ -723,10 +767,8 @@ static void sw16_launch(const Sw16Prep &pr, cudaStream_t st)
 {
     cudaMemsetAsync(pr.counter, 0, sizeof(int) * 4, st);
     if (pr.wave) {
-        if (pr.p.open >= pr.p.gap)
-            pb::k_sw_wave<true><<<pr.blocks, pb::SW16_WARPS * 32, pr.prof_bytes, st>>>(pr.p, pr.counter);
-        else
-            pb::k_sw_wave<false><<<pr.blocks, pb::SW16_WARPS * 32, pr.prof_bytes, st>>>(pr.p, pr.counter);
+        wave_kernel(pr.p.open >= pr.p.gap, pr.wave_rl)<<<pr.blocks, pb::SW16_WARPS * 32, pr.prof_bytes, st>>>(
+            pr.p, pr.counter);
     } else {
         if (pr.p.bias)
             pb::k_sw16<true><<<pr.blocks, pb::SW16_WARPS * 32, pr.prof_bytes, st>>>(pr.p, pr.counter);

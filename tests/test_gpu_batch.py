@@ -26,7 +26,7 @@ def _oracle_batch(alg, sgf, stats, q, targets, op, gp, m):
     return [(r.score, r.end_query, r.end_ref, r.matches, r.similar, r.length) for r in res]
 
 
-@pytest.mark.parametrize("qlen", [1, 15, 16, 17, 100, 333, 1200])
+@pytest.mark.parametrize("qlen", [1, 15, 16, 17, 100, 333, 480, 1200])
 def test_sw16_batch_vs_oracle(qlen):
     rng = random.Random(qlen)
     q = rand_seq(rng, qlen, AA)

@@ -156,3 +156,45 @@ def test_schedule_table_routes_global_pairs_and_keeps_results():
     finally:
         pb.lib.parasail_b200_schedule_set(saved)
     pb.lib.parasail_matrix_free(dna)
+
+
+def test_chunked_host_batch_equals_device_and_one_profile():
+    """A host batch of 140,000 pairs runs in overlapped chunks (copies of
+    chunk k + 1 during the alignment of chunk k): its records equal the
+    device call's; a single-profile host batch over as many targets equals
+    the device-resident profile call."""
+    rng = np.random.default_rng(5)
+    n = 140_000
+    ql = rng.integers(20, 60, n)
+    tl = ql + rng.integers(0, 20, n)
+    letters = np.frombuffer(b"ACGT", np.uint8)
+    qb = letters[rng.integers(0, 4, int(ql.sum()))]
+    tb = letters[rng.integers(0, 4, int(tl.sum()))]
+    qo = np.concatenate([[0], np.cumsum(ql)[:-1]]).astype(np.int64)
+    to = np.concatenate([[0], np.cumsum(tl)[:-1]]).astype(np.int64)
+    ql, tl = ql.astype(np.int32), tl.astype(np.int32)
+    dna = pb.matrix_create("ACGT", 2, -3)
+    mapper = np.ctypeslib.as_array(dna.contents.mapper, shape=(256,)).astype(np.uint8)
+    for name in ("sg_qx_stats_striped_16", "sw_striped_sat"):
+        h_rec = np.zeros((n, 8), np.int32)
+        assert pb.lib.parasail_b200_batch_pairs(name.encode(), dna, qb.ctypes.data, qo.ctypes.data, ql.ctypes.data,
+                                                tb.ctypes.data, to.ctypes.data, tl.ctypes.data, n, 5, 2,
+                                                h_rec.ctypes.data) == 0
+        d = [torch.from_numpy(x).cuda() for x in (mapper[qb], qo, ql, mapper[tb], to, tl)]
+        d_rec = torch.zeros((n, 8), dtype=torch.int32, device="cuda")
+        assert pb.lib.parasail_b200_batch_pairs_device(name.encode(), dna, *[x.data_ptr() for x in d], n, 5, 2,
+                                                       d_rec.data_ptr()) == 0
+        assert np.array_equal(h_rec[:, :7], d_rec.cpu().numpy()[:, :7]), name
+    q = "ACGTTGCAAGGCTTACGATCGATCGGATCCA" * 3
+    targets = [bytes(tb[to[k]:to[k] + tl[k]]).decode() for k in range(n)]
+    prof = pb.ProfileHandle("parasail_profile_create_16", q, dna)
+    host = pb.batch_profile("nw_scan_profile_16", prof, targets, 5, 2, packed=(tb, to, tl))
+    prof.close()
+    # the first and the last chunk against the oracle
+    pick = list(range(150)) + list(range(n - 150, n))
+    exp = O.align_batch(O.NW, 0, 0, [q] * len(pick), [targets[k] for k in pick], 5, 2,
+                        O.Matrix.simple("ACGT", 2, -3))
+    for k, e in zip(pick, exp):
+        a = host[k]
+        assert (int(a["score"]), int(a["end_query"]), int(a["end_ref"])) == (e.score, e.end_query, e.end_ref), k
+    pb.lib.parasail_matrix_free(dna)
