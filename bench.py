@@ -53,8 +53,8 @@ QUERY_LENGTHS = (100, 250, 500, 1000, 2000)
 N_TARGETS = 200_000
 OPS_PER_CELL = 6   # SW score-only algorithmic lane-operations per cell
 # DRAM bytes (read + write) per cell of k_sw16 on this workload, from one ncu
-# capture of a full-size launch (136.2 GB for 2.7213e11 cells)
-SW16_DRAM_BYTES_PER_CELL = 136.18e9 / 2.7213e11
+# capture of a full-size launch (60.1 GB for 2.7213e11 cells)
+SW16_DRAM_BYTES_PER_CELL = 60.08e9 / 2.7213e11
 REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
 FIELDS = ("score", "end_query", "end_ref", "flag", "matches", "similar", "length")
 

@@ -129,6 +129,22 @@ __global__ void k_scratch_sizes(const int *__restrict__ tlen, const int *__restr
     if (p < n) sizes[p] = (int64_t)(tlim ? tlim[p] : tlen[p]) * nv;
 }
 
+/* pairs mode: each pair's work (query length x target length), with the
+ * warp-per-pair items (the rule of k_exact_db_items) flagged in bit 62 */
+__global__ void k_exact_pair_items(const int *__restrict__ qlen, const int *__restrict__ tlen,
+                                   const int *__restrict__ qlim, const int *__restrict__ tlim, int n,
+                                   unsigned long long *__restrict__ keys, int *__restrict__ idx, int *nwarp)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int ql = qlim ? qlim[k] : qlen[k], tl = tlim ? tlim[k] : tlen[k];
+    const long long cells = (long long)ql * tl;
+    const bool w = ql >= 32 || (ql >= 8 && cells >= (1LL << 14));
+    keys[k] = (unsigned long long)cells | (w ? 1ull << 62 : 0ull);
+    idx[k] = k;
+    if (w) atomicAdd(nwarp, 1);
+}
+
 /* every query against every target: scratch per (query, target) item,
  * query-major, and the item's work (query length x target length) */
 __global__ void k_exact_db_items(const int *__restrict__ tlen, const int *__restrict__ qlens,
@@ -353,8 +369,60 @@ int pb_cuda_align_exact(const pb_batch *b)
     p.qlim = b->d_qlim; p.tlim = b->d_tlim;
     p.scratch = scratch; p.soff = soff; p.out = b->d_out;
     p.mat = b->d_mat; p.msize = b->msize; p.qall = b->d_qall; p.qoff = b->d_qoff; p.qlen = b->d_qlen;
-    pb::launch_exact(p, b->alg, b->stats != 0, st);
-    pb_diag_count_launch(2);   /* k_scratch_sizes, k_exact */
+    if (b->nprofs == 0 && b->d_mat) {
+        /* pairs with their own queries: long pairs one per warp on a side
+         * stream (most cells first), the rest one per thread beside them */
+        const int n = b->npairs;
+        unsigned long long *keys = nullptr, *keys_sorted = nullptr;
+        int *idx = nullptr, *order = nullptr, *d_nwarp = nullptr;
+        void *stmp = nullptr;
+        size_t stmp_bytes = 0;
+        CK(cudaMallocAsync((void **)&keys, sizeof(unsigned long long) * n, st));
+        frees.add(keys);
+        CK(cudaMallocAsync((void **)&keys_sorted, sizeof(unsigned long long) * n, st));
+        frees.add(keys_sorted);
+        CK(cudaMallocAsync((void **)&idx, sizeof(int) * n, st));
+        frees.add(idx);
+        CK(cudaMallocAsync((void **)&order, sizeof(int) * n, st));
+        frees.add(order);
+        CK(cudaMallocAsync((void **)&d_nwarp, sizeof(int), st));
+        frees.add(d_nwarp);
+        CK(cudaMemsetAsync(d_nwarp, 0, sizeof(int), st));
+        k_exact_pair_items<<<(n + 255) / 256, 256, 0, st>>>(b->d_qlen, b->d_tlen, b->d_qlim, b->d_tlim, n, keys, idx,
+                                                           d_nwarp);
+        cub::DeviceRadixSort::SortPairsDescending(nullptr, stmp_bytes, keys, keys_sorted, idx, order, n, 0, 64, st);
+        CK(cudaMallocAsync(&stmp, stmp_bytes, st));
+        frees.add(stmp);
+        cub::DeviceRadixSort::SortPairsDescending(stmp, stmp_bytes, keys, keys_sorted, idx, order, n, 0, 64, st);
+        int nwarp = 0;
+        CK(cudaMemcpyAsync(&nwarp, d_nwarp, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        p.order = order;
+        cudaStream_t st2 = nullptr;
+        cudaEvent_t ev = nullptr;
+        if (nwarp > 0) {
+            if (side_stream(&st2, &ev) != 0) { snprintf(g_err, sizeof g_err, "side stream creation failed"); return -1; }
+            CK(cudaEventRecord(ev, st));
+            CK(cudaStreamWaitEvent(st2, ev, 0));
+            pb::launch_exact_warp(p, b->alg, b->stats != 0, nwarp, st2);
+            pb_diag_count_launch(1);
+        }
+        if (n - nwarp > 0) {
+            pb::ExactParams pt = p;
+            pt.order = order + nwarp;
+            pt.npairs = n - nwarp;
+            pb::launch_exact(pt, b->alg, b->stats != 0, st);
+            pb_diag_count_launch(1);
+        }
+        if (st2) {
+            CK(cudaEventRecord(ev, st2));
+            CK(cudaStreamWaitEvent(st, ev, 0));
+        }
+        pb_diag_count_launch(2);   /* k_scratch_sizes, k_exact_pair_items (plus the library sort) */
+    } else {
+        pb::launch_exact(p, b->alg, b->stats != 0, st);
+        pb_diag_count_launch(2);   /* k_scratch_sizes, k_exact */
+    }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
     return 0;

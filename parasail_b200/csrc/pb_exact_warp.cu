@@ -50,7 +50,10 @@ __device__ __forceinline__ EwCell ew_shfl(const EwCell &c, int src)
                   __shfl_sync(0xffffffffu, c.s, src), __shfl_sync(0xffffffffu, c.l, src)};
 }
 
-template <int ALG, bool STATS>
+/* PAIRS: pair k has its own query codes (qall + qoff[k], qlen[k]) scored
+ * through the square matrix mat[target letter * msize + query letter];
+ * else every query of profs against the same nt targets */
+template <int ALG, bool STATS, bool PAIRS>
 __global__ void __launch_bounds__(EW_WARPS * 32)
 k_exact_warp(ExactParams p, int nitems)
 {
@@ -59,8 +62,15 @@ k_exact_warp(ExactParams p, int nitems)
     const int item = blockIdx.x * EW_WARPS + (threadIdx.x >> 5);
     if (item >= nitems) return;
     const int pid = p.order[item];
-    const int ti = pid % p.nt;
-    const ProfDesc pd = p.profs[pid / p.nt];
+    const int ti = PAIRS ? pid : pid % p.nt;
+    ProfDesc pd;
+    const uint8_t *qseq = nullptr;
+    if (PAIRS) {
+        qseq = p.qall + p.qoff[pid];
+        pd.prof = nullptr; pd.qcodes = nullptr; pd.lp = 0; pd.qlen = p.qlen[pid]; pd.size = p.msize;
+    } else {
+        pd = p.profs[pid / p.nt];
+    }
     const uint8_t *tseq = p.targets + p.toff[ti];
     const int ql = p.qlim ? p.qlim[pid] : pd.qlen;       /* a prefix of the pair when limited */
     const int tl = p.tlim ? p.tlim[pid] : p.tlen[ti];
@@ -88,6 +98,15 @@ k_exact_warp(ExactParams p, int nitems)
     const int pass_rows = 32 * EW_R;
     for (int r0 = 0; r0 < nrows; r0 += pass_rows) {
         const int R0 = r0 + lane * EW_R;
+        int qc[PAIRS ? EW_R : 1];
+        if (PAIRS) {
+#pragma unroll
+            for (int r = 0; r < EW_R; ++r) {
+                int c = R0 + r < ql ? qseq[R0 + r] : 0;
+                if (c >= p.msize) { status |= PB_ST_BADCODE; c = 0; }
+                qc[r] = c;
+            }
+        }
         int Hl[EW_R], E[EW_R];
         int HlM[EW_R], HlS[EW_R], HlL[EW_R], EM[EW_R], ES[EW_R], EL[EW_R];
 #pragma unroll
@@ -130,7 +149,7 @@ k_exact_warp(ExactParams p, int nitems)
             const int code = tseq[j];
             if (code >= pd.size) status |= PB_ST_BADCODE;
             const int csafe = code < pd.size ? code : 0;
-            const int32_t *prow = pd.prof + (size_t)csafe * pd.lp;
+            const int32_t *prow = PAIRS ? p.mat + (size_t)csafe * p.msize : pd.prof + (size_t)csafe * pd.lp;
             int hu = up_h, fu = up_f;
             int hd = dg, hdM = dgM, hdS = dgS, hdL = dgL;
             dg = up_h;
@@ -139,7 +158,7 @@ k_exact_warp(ExactParams p, int nitems)
             for (int r = 0; r < EW_R; ++r) {
                 const int i = R0 + r;
                 const bool real = i < ql;
-                const int sc = real ? prow[i] : 0;
+                const int sc = real ? (PAIRS ? __ldg(&prow[qc[r]]) : prow[i]) : 0;
                 const int f_opn = hu - open, f_ext = fu - gap;
                 const int fn = max(f_opn, f_ext);
                 const int e_opn = Hl[r] - open, e_ext = E[r] - gap;
@@ -161,7 +180,7 @@ k_exact_warp(ExactParams p, int nitems)
                     const int eL = (eo ? HlL[r] : EL[r]) + 1;
                     EM[r] = eM; ES[r] = eS; EL[r] = eL;
                     const bool isd = hn == hdag, isf = hn == fn;
-                    const int mt = real ? (pd.qcodes[i] == code) : 0;
+                    const int mt = real ? ((PAIRS ? qc[r] : (int)pd.qcodes[i]) == code) : 0;
                     hM = isd ? hdM + mt : (isf ? fM : eM);
                     hS = isd ? hdS + (sc > 0) : (isf ? fS : eS);
                     hL = isd ? hdL + 1 : (isf ? fL : eL);
@@ -294,19 +313,24 @@ k_exact_warp(ExactParams p, int nitems)
     p.out[pid] = o;
 }
 
-template <bool STATS>
+template <bool STATS, bool PAIRS>
 static void launch_ew(const ExactParams &p, int alg, int nitems, cudaStream_t st)
 {
     const int blocks = (nitems + EW_WARPS - 1) / EW_WARPS;
-    if (alg == PB_SW) k_exact_warp<PB_SW, STATS><<<blocks, EW_WARPS * 32, 0, st>>>(p, nitems);
-    else if (alg == PB_NW) k_exact_warp<PB_NW, STATS><<<blocks, EW_WARPS * 32, 0, st>>>(p, nitems);
-    else k_exact_warp<PB_SG, STATS><<<blocks, EW_WARPS * 32, 0, st>>>(p, nitems);
+    if (alg == PB_SW) k_exact_warp<PB_SW, STATS, PAIRS><<<blocks, EW_WARPS * 32, 0, st>>>(p, nitems);
+    else if (alg == PB_NW) k_exact_warp<PB_NW, STATS, PAIRS><<<blocks, EW_WARPS * 32, 0, st>>>(p, nitems);
+    else k_exact_warp<PB_SG, STATS, PAIRS><<<blocks, EW_WARPS * 32, 0, st>>>(p, nitems);
 }
 
 void launch_exact_warp(const ExactParams &p, int alg, bool stats, int nitems, cudaStream_t st)
 {
     if (nitems <= 0) return;
-    if (stats) launch_ew<true>(p, alg, nitems, st); else launch_ew<false>(p, alg, nitems, st);
+    const bool pairs = p.mat != nullptr;
+    if (stats) {
+        if (pairs) launch_ew<true, true>(p, alg, nitems, st); else launch_ew<true, false>(p, alg, nitems, st);
+    } else {
+        if (pairs) launch_ew<false, true>(p, alg, nitems, st); else launch_ew<false, false>(p, alg, nitems, st);
+    }
 }
 
 int exact_warp_pass_rows(bool stats) { return 32 * (stats ? EwRows<true>::value : EwRows<false>::value); }

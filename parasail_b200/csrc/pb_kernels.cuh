@@ -76,6 +76,7 @@ struct Sw16Params {
     const int64_t *toff;
     const int *tlen;
     uint32_t *scratch;       /* per resident warp: [maxlen][32] pass boundaries (H, F int16) */
+    uint4 *colsave;          /* k_sw16, per resident thread: its strips' best columns (8 x 16 bytes) */
     pb_pair_out *out;        /* [nq][npairs] */
 };
 
@@ -100,6 +101,7 @@ struct P16Params {
     const uint8_t *targets;
     const int64_t *toff;
     uint32_t *scratch;            /* per resident warp [maxlen + 1][32] pass boundaries (H, F int16) */
+    uint4 *colsave;               /* SW ends, per resident thread: its strips' best columns (8 x 16 bytes) */
     int maxlen;
     pb_pair_out *out;
     /* traceback paths (optional): per item, steps written backwards into

@@ -162,6 +162,9 @@ k_p16(P16Params p, const int *__restrict__ tlist, int ntl, int *counter)
 
     /* pass boundary: strip B's bottom row per column, H low and F high */
     uint32_t *buf = p.scratch + (size_t)(blockIdx.x * WARPS + wid) * (size_t)(p.maxlen + 1) * 32;
+    /* SW ends: this thread's copies of its strips' best columns */
+    uint4 *save = ENDS && ALG == PB_SW ? p.colsave + ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * (P16_R / 2)
+                                       : nullptr;
     const int open = p.open, gap = p.gap, sgf = p.sgflags;
     const uint32_t gO = p16_splat(-open), gE = p16_splat(-gap);
     const int nwarps_total = gridDim.x * WARPS;
@@ -394,19 +397,21 @@ k_p16(P16Params p, const int *__restrict__ tlist, int ntl, int *counter)
                 }
                 if (ENDS && ALG == PB_SW) {
                     /* a strictly higher column maximum than the strip's best
-                     * so far: the first column reaching it, smallest row */
+                     * so far: the first column reaching it, kept whole (the
+                     * warp takes this branch whenever any lane improves; the
+                     * smallest row is looked up once per pass) */
                     const int c_lo = p16_lo(cmax), c_hi = p16_hi(cmax);
                     if (c_lo > sa.score && j < cols) {
-                        int rr = 0;
 #pragma unroll
-                        for (int r = P16_R - 1; r >= 0; --r) if (p16_lo(H[r]) == c_lo) rr = r;
-                        sa.score = c_lo; sa.j = j; sa.i = r0 + rr;
+                        for (int k = 0; k < P16_R / 4; ++k)
+                            save[k] = make_uint4(H[4 * k], H[4 * k + 1], H[4 * k + 2], H[4 * k + 3]);
+                        sa.score = c_lo; sa.j = j;
                     }
                     if (c_hi > sb.score && j >= 1 && j <= cols) {
-                        int rr = 0;
 #pragma unroll
-                        for (int r = P16_R - 1; r >= 0; --r) if (p16_hi(H[r]) == c_hi) rr = r;
-                        sb.score = c_hi; sb.j = j - 1; sb.i = r0 + P16_R + rr;
+                        for (int k = 0; k < P16_R / 4; ++k)
+                            save[P16_R / 4 + k] = make_uint4(H[4 * k], H[4 * k + 1], H[4 * k + 2], H[4 * k + 3]);
+                        sb.score = c_hi; sb.j = j - 1;
                     }
                 }
                 if (ENDS && ALG != PB_SW) {
@@ -432,6 +437,28 @@ k_p16(P16Params p, const int *__restrict__ tlist, int ntl, int *counter)
                 }
             }
             if (ENDS && ALG == PB_SW) {
+                if (sa.j >= 0) {
+                    int rr = P16_R - 1;
+#pragma unroll
+                    for (int k = P16_R / 4 - 1; k >= 0; --k) {
+                        const uint4 w = save[k];
+                        const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+                        for (int x = 3; x >= 0; --x) if (p16_lo(ws[x]) == sa.score) rr = 4 * k + x;
+                    }
+                    sa.i = r0 + rr;
+                }
+                if (sb.j >= 0) {
+                    int rr = P16_R - 1;
+#pragma unroll
+                    for (int k = P16_R / 4 - 1; k >= 0; --k) {
+                        const uint4 w = save[P16_R / 4 + k];
+                        const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+                        for (int x = 3; x >= 0; --x) if (p16_hi(ws[x]) == sb.score) rr = 4 * k + x;
+                    }
+                    sb.i = r0 + P16_R + rr;
+                }
                 const P16Best cand[2] = {sa, sb};
 #pragma unroll
                 for (int x = 0; x < 2; ++x) {
@@ -1061,6 +1088,11 @@ int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out
         P16_CK(cudaMallocAsync((void **)&scratch, sizeof(uint32_t) * (size_t)(maxlen + 1) * 32 * rwarps, st));
         frees.add(scratch);
         p.scratch = scratch;
+        p.colsave = nullptr;
+        if (ends_on && m->alg == PB_SW) {
+            P16_CK(cudaMallocAsync((void **)&p.colsave, sizeof(uint4) * (P16_R / 2) * 32 * rwarps, st));
+            frees.add(p.colsave);
+        }
         p.maxlen = maxlen;
         p.task_wmax = twmax; p.task_npass = tnpass; p.task_bits = tbits;
         int *d_tlist = nullptr, *d_counter = nullptr;

@@ -131,6 +131,8 @@ k_sw16(Sw16Params p, int *task_counter)
     __shared__ int s_have[SW16_WARPS][32];
     __shared__ int s_status[SW16_WARPS][32];
     volatile int *verr = task_counter + 2;
+    /* this thread's copies of its strips' best columns: A's 16 words, then B's */
+    uint4 *save = p.colsave + ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * (SW16_R / 2);
     bool team = p.nteam > 0;
 
     /* warp tasks: the first of each warp block-strided, so that the largest
@@ -325,26 +327,52 @@ k_sw16(Sw16Params p, int *task_counter)
                 const bool up_a = !ge_lo && j < len;
                 const bool up_b = !ge_hi && j >= 1 && j <= len;
                 if (up_a || up_b) {
+                    /* a new strip maximum: keep the column (the warp takes
+                     * this branch whenever any lane improves, so the row is
+                     * looked up once per pass, from the saved column) */
                     if (up_a) {
                         const int c = s16lo(cmax);
-                        int rr = 0;
 #pragma unroll
-                        for (int r = SW16_R - 1; r >= 0; --r) if (s16lo(H[r]) == c) rr = r;
-                        sa.score = c + bias; sa.j = j; sa.i = r0 + rr;
+                        for (int k = 0; k < SW16_R / 4; ++k)
+                            save[k] = make_uint4(H[4 * k], H[4 * k + 1], H[4 * k + 2], H[4 * k + 3]);
+                        sa.score = c + bias; sa.j = j;
                         if (c + bias >= Q.posmax) status |= PB_ST_OVERFLOW16;
                     }
                     if (up_b) {
                         const int c = s16hi(cmax);
-                        int rr = 0;
 #pragma unroll
-                        for (int r = SW16_R - 1; r >= 0; --r) if (s16hi(H[r]) == c) rr = r;
-                        sb.score = c + bias; sb.j = j - 1; sb.i = r0 + SW16_R + rr;
+                        for (int k = 0; k < SW16_R / 4; ++k)
+                            save[SW16_R / 4 + k] = make_uint4(H[4 * k], H[4 * k + 1], H[4 * k + 2], H[4 * k + 3]);
+                        sb.score = c + bias; sb.j = j - 1;
                         if (c + bias >= Q.posmax) status |= PB_ST_OVERFLOW16;
                     }
                     sbest = (uint32_t)(uint16_t)(sa.score - bias) | ((uint32_t)(uint16_t)(sb.score - bias) << 16);
                 }
             }
             if (aborted) break;
+            /* the first row of each strip's best column reaching its maximum */
+            if (sa.j >= 0) {
+                int rr = SW16_R - 1;
+#pragma unroll
+                for (int k = SW16_R / 4 - 1; k >= 0; --k) {
+                    const uint4 w = save[k];
+                    const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+                    for (int x = 3; x >= 0; --x) if (s16lo(ws[x]) == sa.score - bias) rr = 4 * k + x;
+                }
+                sa.i = r0 + rr;
+            }
+            if (sb.j >= 0) {
+                int rr = SW16_R - 1;
+#pragma unroll
+                for (int k = SW16_R / 4 - 1; k >= 0; --k) {
+                    const uint4 w = save[SW16_R / 4 + k];
+                    const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+                    for (int x = 3; x >= 0; --x) if (s16hi(ws[x]) == sb.score - bias) rr = 4 * k + x;
+                }
+                sb.i = r0 + SW16_R + rr;
+            }
             fold_best(best, have, sa);
             fold_best(best, have, sb);
         }
@@ -575,7 +603,7 @@ struct Sw16Prep {
     int wave_rl;                  /* its rows per lane */
     size_t prof_bytes;
     int *counter;                 /* [warp tasks, team tasks, error, spare] */
-    void *bufs[9];
+    void *bufs[10];
 };
 
 static void sw16_release(Sw16Prep *pr, cudaStream_t st)
@@ -731,6 +759,11 @@ static int sw16_prepare(const pb_batch *b, pb_pair_out *d_out_all, size_t prof_b
                                      : sizeof(uint32_t) * (size_t)maxlen * 32 * blocks * pb::SW16_WARPS;
     if (cudaMallocAsync((void **)&scratch, scratch_bytes, st) != cudaSuccess)
         scratch = nullptr;
+    /* k_sw16: per thread, the two strips' best columns (2 x 16 words) */
+    uint4 *colsave = nullptr;
+    if (!few && cudaMallocAsync((void **)&colsave, sizeof(uint4) * (pb::SW16_R / 2) * (size_t)blocks * pb::SW16_WARPS * 32,
+                                st) != cudaSuccess)
+        colsave = nullptr;
     /* team tasks: those above a fair share of the work per warp, which one
      * warp alone would finish last */
     int nteam = few ? (int)sorted_tasks.size() : 0;
@@ -749,12 +782,13 @@ static int sw16_prepare(const pb_batch *b, pb_pair_out *d_out_all, size_t prof_b
     p.queries = d_q; p.prof_all = prof_all; p.prof_bytes = (int)prof_bytes;
     p.order = order; p.tasks = d_tasks;
     p.targets = b->d_targets; p.toff = b->d_toff; p.tlen = b->d_tlen;
-    p.scratch = scratch; p.out = d_out_all;
+    p.scratch = scratch; p.out = d_out_all; p.colsave = colsave;
     pr->blocks = blocks;
     pr->counter = counter;
-    void *owned[9] = {keys_sorted, idx, order, counter, tmp, prof_all, d_tasks, d_q, scratch};
+    void *owned[10] = {keys_sorted, idx, order, counter, tmp, prof_all, d_tasks, d_q, scratch, colsave};
     memcpy(pr->bufs, owned, sizeof owned);
     if (!keys_sorted || !idx || !order || !counter || !tmp || !prof_all || !d_tasks || !d_q || !scratch ||
+        (!few && !colsave) ||
         cudaGetLastError() != cudaSuccess) {
         sw16_release(pr, st);
         return -1;

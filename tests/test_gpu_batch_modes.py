@@ -198,3 +198,34 @@ def test_chunked_host_batch_equals_device_and_one_profile():
         a = host[k]
         assert (int(a["score"]), int(a["end_query"]), int(a["end_ref"])) == (e.score, e.end_query, e.end_ref), k
     pb.lib.parasail_matrix_free(dna)
+
+
+def test_long_pairs_past_16_bits_run_one_warp_per_pair():
+    """Pairs outside the 16-bit bounds of the pair kernels (6,000-residue DNA
+    pairs at +5/-4) in pairs mode go to the exact kernels: the long ones one
+    warp per pair, short ones (mixed in) one thread per pair; scores, ends
+    and statistics equal the oracle's."""
+    rng = random.Random(61)
+    qs, ts = [], []
+    for k in range(6):
+        q = rand_seq(rng, rng.randint(5800, 6400), DNA)
+        qs.append(q)
+        ts.append(mutate(rng, q, DNA, 0.05, 0.01) if k % 2 == 0 else rand_seq(rng, rng.randint(5800, 6400), DNA))
+    for _ in range(40):
+        q = rand_seq(rng, rng.randint(3, 40), DNA)
+        qs.append(q)
+        ts.append(mutate(rng, q, DNA, 0.1, 0.02))
+    m = pb.matrix_create("ACGT", 5, -4)
+    om = O.Matrix.simple("ACGT", 5, -4)
+    for name, alg, sgf, stats in (("sg_qx_stats_scan_32", O.SG, O.SG_CASES["sg_qx"], 1),
+                                  ("nw_stats_striped_32", O.NW, 0, 1),
+                                  ("sw_stats_scan_32", O.SW, 0, 1),
+                                  ("sg_de_scan_32", O.SG, O.SG_CASES["sg_de"], 0)):
+        got = pb.batch_pairs(name, m, qs, ts, 10, 1)
+        exp = O.align_batch(alg, sgf, stats, qs, ts, 10, 1, om)
+        for k, (g, e) in enumerate(zip(got, exp)):
+            want = (e.score, e.end_query, e.end_ref) + ((e.matches, e.similar, e.length) if stats else ())
+            have = tuple(int(g[f]) for f in ("score", "end_query", "end_ref")) + \
+                (tuple(int(g[f]) for f in ("matches", "similar", "length")) if stats else ())
+            assert have == want, (name, k, len(qs[k]), len(ts[k]))
+    pb.lib.parasail_matrix_free(m)
