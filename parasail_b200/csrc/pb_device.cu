@@ -129,15 +129,19 @@ __global__ void k_scratch_sizes(const int *__restrict__ tlen, const int *__restr
     if (p < n) sizes[p] = (int64_t)(tlim ? tlim[p] : tlen[p]) * nv;
 }
 
-/* pairs mode: each pair's work (query length x target length), with the
- * warp-per-pair items (the rule of k_exact_db_items) flagged in bit 62 */
-__global__ void k_exact_pair_items(const int *__restrict__ qlen, const int *__restrict__ tlen,
+/* one query per pair (its own codes, qlen[k], or a profile per pair,
+ * profs[prof_index[k]]): each pair's work (query length x target length),
+ * with the warp-per-pair items (the rule of k_exact_db_items) flagged in
+ * bit 62 */
+__global__ void k_exact_pair_items(const int *__restrict__ qlen, const pb::ProfDesc *__restrict__ profs,
+                                   const int *__restrict__ prof_index, const int *__restrict__ tlen,
                                    const int *__restrict__ qlim, const int *__restrict__ tlim, int n,
                                    unsigned long long *__restrict__ keys, int *__restrict__ idx, int *nwarp)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const int ql = qlim ? qlim[k] : qlen[k], tl = tlim ? tlim[k] : tlen[k];
+    const int q = qlen ? qlen[k] : profs[prof_index[k]].qlen;
+    const int ql = qlim ? qlim[k] : q, tl = tlim ? tlim[k] : tlen[k];
     const long long cells = (long long)ql * tl;
     const bool w = ql >= 32 || (ql >= 8 && cells >= (1LL << 14));
     keys[k] = (unsigned long long)cells | (w ? 1ull << 62 : 0ull);
@@ -369,9 +373,12 @@ int pb_cuda_align_exact(const pb_batch *b)
     p.qlim = b->d_qlim; p.tlim = b->d_tlim;
     p.scratch = scratch; p.soff = soff; p.out = b->d_out;
     p.mat = b->d_mat; p.msize = b->msize; p.qall = b->d_qall; p.qoff = b->d_qoff; p.qlen = b->d_qlen;
-    if (b->nprofs == 0 && b->d_mat) {
-        /* pairs with their own queries: long pairs one per warp on a side
-         * stream (most cells first), the rest one per thread beside them */
+    /* the exact kernels score through the matrix whenever one is given */
+    const bool per_pair = (b->d_mat && b->d_qlen) || (!b->d_mat && b->nprofs > 0 && b->d_prof_index);
+    if (per_pair) {
+        /* one query per pair (its own codes, or a profile per pair): long
+         * pairs one per warp on a side stream (most cells first), the rest
+         * one per thread beside them */
         const int n = b->npairs;
         unsigned long long *keys = nullptr, *keys_sorted = nullptr;
         int *idx = nullptr, *order = nullptr, *d_nwarp = nullptr;
@@ -388,8 +395,10 @@ int pb_cuda_align_exact(const pb_batch *b)
         CK(cudaMallocAsync((void **)&d_nwarp, sizeof(int), st));
         frees.add(d_nwarp);
         CK(cudaMemsetAsync(d_nwarp, 0, sizeof(int), st));
-        k_exact_pair_items<<<(n + 255) / 256, 256, 0, st>>>(b->d_qlen, b->d_tlen, b->d_qlim, b->d_tlim, n, keys, idx,
-                                                           d_nwarp);
+        const bool matmode = b->d_mat != nullptr;
+        k_exact_pair_items<<<(n + 255) / 256, 256, 0, st>>>(matmode ? b->d_qlen : nullptr, d_profs,
+                                                           matmode ? nullptr : b->d_prof_index, b->d_tlen,
+                                                           b->d_qlim, b->d_tlim, n, keys, idx, d_nwarp);
         cub::DeviceRadixSort::SortPairsDescending(nullptr, stmp_bytes, keys, keys_sorted, idx, order, n, 0, 64, st);
         CK(cudaMallocAsync(&stmp, stmp_bytes, st));
         frees.add(stmp);

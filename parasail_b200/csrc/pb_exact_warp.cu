@@ -52,7 +52,8 @@ __device__ __forceinline__ EwCell ew_shfl(const EwCell &c, int src)
 
 /* PAIRS: pair k has its own query codes (qall + qoff[k], qlen[k]) scored
  * through the square matrix mat[target letter * msize + query letter];
- * else every query of profs against the same nt targets */
+ * else profiles: every query of profs against the same nt targets, or
+ * (nt = 0) pair k's profile profs[prof_index[k]] against target k */
 template <int ALG, bool STATS, bool PAIRS>
 __global__ void __launch_bounds__(EW_WARPS * 32)
 k_exact_warp(ExactParams p, int nitems)
@@ -62,14 +63,15 @@ k_exact_warp(ExactParams p, int nitems)
     const int item = blockIdx.x * EW_WARPS + (threadIdx.x >> 5);
     if (item >= nitems) return;
     const int pid = p.order[item];
-    const int ti = PAIRS ? pid : pid % p.nt;
+    const int ti = PAIRS || !p.nt ? pid : pid % p.nt;
     ProfDesc pd;
     const uint8_t *qseq = nullptr;
     if (PAIRS) {
         qseq = p.qall + p.qoff[pid];
         pd.prof = nullptr; pd.qcodes = nullptr; pd.lp = 0; pd.qlen = p.qlen[pid]; pd.size = p.msize;
     } else {
-        pd = p.profs[pid / p.nt];
+        /* every query against nt targets, or one profile per pair */
+        pd = p.profs[p.nt ? pid / p.nt : (p.prof_index ? p.prof_index[pid] : 0)];
     }
     const uint8_t *tseq = p.targets + p.toff[ti];
     const int ql = p.qlim ? p.qlim[pid] : pd.qlen;       /* a prefix of the pair when limited */
