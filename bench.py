@@ -363,7 +363,7 @@ def leg_config3(pb, timer, args, td):
     qf, tf = os.path.join(td, "c3q.txt"), os.path.join(td, "c3t.txt")
     write_lines(qf, rb, ro, rl)
     write_lines(tf, wb, wo, wl)
-    steps, warm = max(1, min(args.steps, 3)), 1
+    steps, warm = max(1, min(args.steps, 5)), 2
     out = {"workload": "%d DNA read/window pairs (reads U[100,300], windows read+32; 5%% subs, 0.5%% ins, "
                        "0.5%% del), +2/-3, open 5, extend 2" % n,
            "cells_per_step": cells, "steps": steps, "warmup": warm, "functions": {}}
