@@ -130,7 +130,8 @@ __global__ void k_scratch_sizes(const int *__restrict__ tlen, const int *__restr
 }
 
 /* one query per pair (its own codes, qlen[k], or a profile per pair,
- * profs[prof_index[k]]): each pair's work (query length x target length),
+ * profs[prof_index[k]], or one profile for all, profs[0]): each pair's work
+ * (query length x target length),
  * with the warp-per-pair items (the rule of k_exact_db_items) flagged in
  * bit 62 */
 __global__ void k_exact_pair_items(const int *__restrict__ qlen, const pb::ProfDesc *__restrict__ profs,
@@ -140,7 +141,7 @@ __global__ void k_exact_pair_items(const int *__restrict__ qlen, const pb::ProfD
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const int q = qlen ? qlen[k] : profs[prof_index[k]].qlen;
+    const int q = qlen ? qlen[k] : profs[prof_index ? prof_index[k] : 0].qlen;
     const int ql = qlim ? qlim[k] : q, tl = tlim ? tlim[k] : tlen[k];
     const long long cells = (long long)ql * tl;
     const bool w = ql >= 32 || (ql >= 8 && cells >= (1LL << 14));
@@ -373,8 +374,10 @@ int pb_cuda_align_exact(const pb_batch *b)
     p.qlim = b->d_qlim; p.tlim = b->d_tlim;
     p.scratch = scratch; p.soff = soff; p.out = b->d_out;
     p.mat = b->d_mat; p.msize = b->msize; p.qall = b->d_qall; p.qoff = b->d_qoff; p.qlen = b->d_qlen;
-    /* the exact kernels score through the matrix whenever one is given */
-    const bool per_pair = (b->d_mat && b->d_qlen) || (!b->d_mat && b->nprofs > 0 && b->d_prof_index);
+    /* the exact kernels score through the matrix whenever one is given;
+     * profile mode without an index is one profile against every target
+     * (the single calls of parasail.h among them) */
+    const bool per_pair = (b->d_mat && b->d_qlen) || (!b->d_mat && b->nprofs > 0);
     if (per_pair) {
         /* one query per pair (its own codes, or a profile per pair): long
          * pairs one per warp on a side stream (most cells first), the rest
@@ -399,10 +402,15 @@ int pb_cuda_align_exact(const pb_batch *b)
         k_exact_pair_items<<<(n + 255) / 256, 256, 0, st>>>(matmode ? b->d_qlen : nullptr, d_profs,
                                                            matmode ? nullptr : b->d_prof_index, b->d_tlen,
                                                            b->d_qlim, b->d_tlim, n, keys, idx, d_nwarp);
-        cub::DeviceRadixSort::SortPairsDescending(nullptr, stmp_bytes, keys, keys_sorted, idx, order, n, 0, 64, st);
-        CK(cudaMallocAsync(&stmp, stmp_bytes, st));
-        frees.add(stmp);
-        cub::DeviceRadixSort::SortPairsDescending(stmp, stmp_bytes, keys, keys_sorted, idx, order, n, 0, 64, st);
+        if (n > 1) {
+            cub::DeviceRadixSort::SortPairsDescending(nullptr, stmp_bytes, keys, keys_sorted, idx, order, n, 0, 64,
+                                                      st);
+            CK(cudaMallocAsync(&stmp, stmp_bytes, st));
+            frees.add(stmp);
+            cub::DeviceRadixSort::SortPairsDescending(stmp, stmp_bytes, keys, keys_sorted, idx, order, n, 0, 64, st);
+        } else {
+            order = idx;     /* one pair: nothing to order */
+        }
         int nwarp = 0;
         CK(cudaMemcpyAsync(&nwarp, d_nwarp, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));

@@ -92,7 +92,11 @@ __device__ __forceinline__ int sext_byte(uint32_t lo, uint32_t hi, int k)
  */
 static constexpr long long NWL_SPIN_CYCLES = 1ll << 32;
 
-template <bool BANDED, bool GE>
+/* BIAS (with GE): the H registers, the pass ring and the lane hand-off hold
+ * H - open, and the score table s + open (the host checked that it stays in
+ * int8); E = max(E - gap, HO), A = max(HO_diag + s', E), F = max(F - gap,
+ * A - open), HO = max(A - open, F - open) */
+template <bool BANDED, bool GE, bool BIAS>
 __global__ void __launch_bounds__(NWL_WARPS * 32, 3)
 k_nw_wave(NwWaveParams p, int *counter, int *error)
 {
@@ -206,13 +210,14 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
             for (int r = 0; r < NWL_RL; ++r) {
                 const int i = R0 + r;
                 int v = NWL_NEG;
-                if (jlo == 0 && (!BANDED || (i + 1 >= lo && i + 1 <= hi))) v = -open - i * gap;
+                if (jlo == 0 && (!BANDED || (i + 1 >= lo && i + 1 <= hi))) v = -open - i * gap - (BIAS ? open : 0);
                 Hl[r] = v;
                 E[r] = NWL_NEG;
             }
             int dg;
             if (jlo == 0) {
                 dg = (R0 == 0) ? 0 : ((!BANDED || (R0 >= lo && R0 <= hi)) ? -open - (R0 - 1) * gap : NWL_NEG);
+                if (BIAS && dg != NWL_NEG) dg -= open;
             } else {
                 dg = NWL_NEG;
                 bool ok = true;
@@ -263,7 +268,7 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
                 if (lane == 0 && active) {
                     if (r0 == 0) {
                         const bool inb = !BANDED || (-1 - j >= lo && -1 - j <= hi);
-                        up_h = inb ? -open - j * gap : NWL_NEG;
+                        up_h = inb ? -open - j * gap - (BIAS ? open : 0) : NWL_NEG;
                         up_f = NWL_NEG;
                     } else {
                         up_h = vh;
@@ -286,7 +291,7 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
                         row_hi = *reinterpret_cast<const uint32_t *>(s_mat + tc * 32 + 4);
                     }
                     /* F of row R0 from the row above (previous lane or pass) */
-                    int f = max(up_f - gap, up_h - open);
+                    int f = BIAS ? __viaddmax_s32(up_f, -gap, up_h) : max(up_f - gap, up_h - open);
                     /* row R0 + r lies in the band iff 0 <= R0 + r - j - lo <= hi - lo */
                     const int dlo = R0 - j - lo;
                     const unsigned bw = (unsigned)(hi - lo);
@@ -299,7 +304,7 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
                         for (int r = 0; r < NWL_RL; ++r) {
                             const int sc = p.small_alpha ? sext_byte(row_lo, row_hi, qc[r]) : (int)s_mat[tc * 32 + qc[r]];
                             /* E and the diagonal/E part a are off the row-to-row chain */
-                            int e = max(E[r] - gap, Hl[r] - open);
+                            int e = BIAS ? __viaddmax_s32(E[r], -gap, Hl[r]) : max(E[r] - gap, Hl[r] - open);
                             int a = __viaddmax_s32(hd, sc, e);
                             if (MASK) {
                                 const bool in = (unsigned)(dlo + r) <= bw;
@@ -307,15 +312,24 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
                                 a = in ? a : NWL_NEG;
                                 f = in ? f : NWL_NEG;
                             }
-                            const int h = max(a, f);
-                            last_h = h;
-                            last_f = f;
-                            /* F of the next row: max(F - gap, H - open). With
-                             * open >= gap, H - open = max(a, F) - open and
-                             * F - open <= F - gap, so only a - open is needed:
-                             * one dependent operation per row */
-                            if (GE) f = __viaddmax_s32(f, -gap, a - open);
-                            else f = max(f - gap, h - open);
+                            int h;
+                            if (BIAS) {
+                                const int ao = a - open;
+                                h = __viaddmax_s32(f, -open, ao);     /* H - open */
+                                last_h = h;
+                                last_f = f;
+                                f = __viaddmax_s32(f, -gap, ao);
+                            } else {
+                                h = max(a, f);
+                                last_h = h;
+                                last_f = f;
+                                /* F of the next row: max(F - gap, H - open). With
+                                 * open >= gap, H - open = max(a, F) - open and
+                                 * F - open <= F - gap, so only a - open is needed:
+                                 * one dependent operation per row */
+                                if (GE) f = __viaddmax_s32(f, -gap, a - open);
+                                else f = max(f - gap, h - open);
+                            }
                             E[r] = e;
                             hd = Hl[r];
                             Hl[r] = h;
@@ -331,7 +345,7 @@ k_nw_wave(NwWaveParams p, int *counter, int *error)
                     if (j == m - 1 && R0 <= n - 1 && n - 1 < R0 + NWL_RL) {
 #pragma unroll
                         for (int r = 0; r < NWL_RL; ++r)
-                            if (R0 + r == n - 1) { result = Hl[r]; have_result = true; }
+                            if (R0 + r == n - 1) { result = Hl[r] + (BIAS ? open : 0); have_result = true; }
                     }
                     dg = up_h;
                     sh_h = last_h;
@@ -468,11 +482,19 @@ static int nw_long_impl(int npairs, int open, int gap, const int32_t *h_mat, int
     int nsm = 0, dev = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    /* the one-operation F chain needs open >= gap */
+    /* the one-operation F chain needs open >= gap; the biased form also every
+     * score + open inside int8 */
     const bool ge = open >= gap;
+    bool bias = ge;
+    for (int k = 0; k < msize * msize; ++k)
+        if (h_mat[k] + open > 127 || h_mat[k] + open < -128) bias = false;
+    if (bias)
+        for (int k = 0; k < msize * msize; ++k) hm[k] = (int8_t)(h_mat[k] + open);
     void (*kern)(pb::NwWaveParams, int *, int *) =
-        d_lo ? (ge ? pb::k_nw_wave<true, true> : pb::k_nw_wave<true, false>)
-             : (ge ? pb::k_nw_wave<false, true> : pb::k_nw_wave<false, false>);
+        d_lo ? (bias ? pb::k_nw_wave<true, true, true> : ge ? pb::k_nw_wave<true, true, false>
+                                                            : pb::k_nw_wave<true, false, false>)
+             : (bias ? pb::k_nw_wave<false, true, true> : ge ? pb::k_nw_wave<false, true, false>
+                                                             : pb::k_nw_wave<false, false, false>);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, pb::NWL_WARPS * 32, 0);
     if (per_sm < 1) per_sm = 1;
     const int plain_max = per_sm * nsm;

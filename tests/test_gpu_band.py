@@ -59,6 +59,9 @@ def test_nw_long_vs_oracle_dna_and_protein():
     # open < gap takes the kernel's general F recurrence
     got = pb.nw_long(dna, *_pack(qs[:40]), *_pack(ts[:40]), 1, 3)
     assert got.tolist() == [O.align(O.NW, 0, 0, q, t, 1, 3, om)["score"] for q, t in zip(qs[:40], ts[:40])]
+    # open >= gap with scores + open past int8: the unbiased one-operation chain
+    got = pb.nw_long(b62, *_pack(ps), *_pack(pt), 120, 2)
+    assert got.tolist() == [O.align(O.NW, 0, 0, q, t, 120, 2, ob)["score"] for q, t in zip(ps, pt)]
 
 
 def test_banded_vs_oracle_and_certificate_soundness():
