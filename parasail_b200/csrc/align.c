@@ -60,6 +60,14 @@ static int run_pair(int kernel, const pb_device_profile *dp, const pb_mode *m, i
     b.alg = m->alg; b.sgflags = m->sgflags; b.stats = stats;
     b.open = m->open; b.gap = m->gap; b.pad_rows = pad_rows;
     b.profs = profs; b.nprofs = 1;
+    /* one pair: the single-pair paths (one upload, one launch, one
+     * download); the batch pipeline for what they do not take */
+    if (kernel == 1 && qlim <= 0 && tlim <= 0) {
+        const int rc = pb_cuda_sw_single(dp, m->open, m->gap, codes, tlen, out);
+        if (rc != -2) return rc;
+    } else if (kernel == 0) {
+        return pb_cuda_exact_single(&b, codes, tlen, qlim, tlim, out);
+    }
     return pb_cuda_align_host(kernel, &b, codes, &off, &tlen, qlim > 0 ? &qlim : NULL,
                               tlim > 0 ? &tlim : NULL, NULL, 1, out);
 }

@@ -251,6 +251,16 @@ void pb_diag_count_launch(long n);
 void pb_diag_sw16_time(double ms);
 
 /* Host convenience: copy targets to the device, run, copy results back. */
+/* Single pairs (the one-pair calls of parasail.h) through a per-thread
+ * device arena: one upload, one launch, one download. pb_cuda_exact_single:
+ * the exact kernel (qlim/tlim > 0: a prefix). pb_cuda_sw_single: the SW
+ * score wavefront kernel (int8 profile required; -2 when dp has none). */
+void *pb_cuda_stream(void);   /* the calling thread's stream (a cudaStream_t) */
+char *pb_single_arena(size_t bytes, size_t host_bytes, char **host);
+int pb_cuda_exact_single(const pb_batch *tmpl, const uint8_t *h_codes, int tlen, int qlim, int tlim,
+                         pb_pair_out *h_out);
+int pb_cuda_sw_single(const pb_device_profile *dp, int open, int gap, const uint8_t *h_codes, int tlen,
+                      pb_pair_out *h_out);
 int pb_cuda_align_host(int kernel /* 0 exact, 1 sw16 */, const pb_batch *tmpl,
                        const uint8_t *h_targets, const int64_t *h_toff,
                        const int *h_tlen, const int *h_qlim, const int *h_tlim,

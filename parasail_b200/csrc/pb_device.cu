@@ -548,6 +548,100 @@ int pb_cuda_align_exact_db(const pb_batch *b)
     return 0;
 }
 
+/* ---- single pairs (the one-pair calls of parasail.h) ----------------------
+ * A per-thread device arena holds one pair's descriptors, target codes,
+ * scratch and output: one upload, one launch, one download and one
+ * synchronisation per call, instead of the batch pipeline's set-up. */
+
+namespace {
+
+struct SingleArena {
+    char *d = nullptr;
+    size_t cap = 0;
+    std::vector<char> h;     /* host staging of the upload */
+};
+thread_local SingleArena g_single;
+
+size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+}  // namespace
+
+/* the calling thread's stream of the library */
+void *pb_cuda_stream(void) { return (void *)stream(); }
+
+/* the calling thread's arena of at least `bytes` device bytes, and (host)
+ * a zeroed host staging buffer of host_bytes */
+char *pb_single_arena(size_t bytes, size_t host_bytes, char **host)
+{
+    if (bytes > g_single.cap) {
+        if (g_single.d) cudaFree(g_single.d);
+        size_t cap = bytes < ((size_t)1 << 20) ? ((size_t)1 << 20) : bytes;
+        cap = (cap + 4095) & ~(size_t)4095;
+        if (cudaMalloc((void **)&g_single.d, cap) != cudaSuccess) {
+            g_single.d = nullptr;
+            g_single.cap = 0;
+            return nullptr;
+        }
+        g_single.cap = cap;
+    }
+    g_single.h.assign(host_bytes, 0);
+    if (host) *host = g_single.h.data();
+    return g_single.d;
+}
+
+/* One pair on the exact kernel from host target codes: the warp kernel for a
+ * pair of 32 rows or more (or of 8 rows and 2^14 cells), else one thread.
+ * qlim/tlim > 0 limit the pair to a prefix (the FASTSTATS pass). */
+int pb_cuda_exact_single(const pb_batch *tmpl, const uint8_t *h_codes, int tlen, int qlim, int tlim,
+                         pb_pair_out *h_out)
+{
+    if (pb_cuda_init() != 0) return -1;
+    if (tmpl->nprofs != 1 || tlen <= 0) return -1;
+    const pb_device_profile *dp = tmpl->profs[0];
+    const int nv = tmpl->stats ? 8 : 2;
+    const int ql = qlim > 0 ? qlim : dp->qlen, tl = tlim > 0 ? tlim : tlen;
+    /* [ProfDesc][soff, toff: int64][order, tlen, qlim, tlim: int][out][codes] then scratch */
+    const size_t o_pd = 0, o_soff = align16(sizeof(pb::ProfDesc)), o_toff = o_soff + 8, o_ints = o_toff + 8;
+    const size_t o_out = align16(o_ints + 16), o_codes = align16(o_out + sizeof(pb_pair_out));
+    const size_t up = align16(o_codes + (size_t)tlen + 16);
+    const size_t total = up + sizeof(int) * ((size_t)tl * nv + 16);
+    char *h = nullptr;
+    char *d = pb_single_arena(total, up, &h);
+    if (!d) { snprintf(g_err, sizeof g_err, "single-pair arena allocation failed"); return -1; }
+    pb::ProfDesc pd;
+    pd.prof = dp->d_prof32; pd.prof8 = dp->d_prof8; pd.qcodes = dp->d_qcodes;
+    pd.qlen = dp->qlen; pd.lp = dp->lp; pd.size = dp->size; pd.pad_ = 0;
+    memcpy(h + o_pd, &pd, sizeof pd);
+    const int ints[4] = {0, tlen, qlim, tlim};
+    memcpy(h + o_ints, ints, sizeof ints);
+    memcpy(h + o_codes, h_codes, (size_t)tlen);
+    cudaStream_t st = stream();
+    CK(cudaMemcpyAsync(d, h, up, cudaMemcpyHostToDevice, st));
+    pb::ExactParams p;
+    p.alg = tmpl->alg; p.sgflags = tmpl->sgflags; p.open = tmpl->open; p.gap = tmpl->gap;
+    p.pad_rows = tmpl->pad_rows; p.npairs = 1;
+    p.profs = reinterpret_cast<const pb::ProfDesc *>(d + o_pd); p.prof_index = nullptr;
+    p.targets = reinterpret_cast<const uint8_t *>(d + o_codes);
+    p.toff = reinterpret_cast<const int64_t *>(d + o_toff);
+    p.tlen = reinterpret_cast<const int *>(d + o_ints) + 1;
+    p.qlim = qlim > 0 ? reinterpret_cast<const int *>(d + o_ints) + 2 : nullptr;
+    p.tlim = tlim > 0 ? reinterpret_cast<const int *>(d + o_ints) + 3 : nullptr;
+    p.scratch = reinterpret_cast<int *>(d + up);
+    p.soff = reinterpret_cast<const int64_t *>(d + o_soff);
+    p.out = reinterpret_cast<pb_pair_out *>(d + o_out);
+    p.mat = nullptr; p.msize = 0; p.qall = nullptr; p.qoff = nullptr; p.qlen = nullptr;
+    p.order = reinterpret_cast<const int *>(d + o_ints);
+    p.nt = 0;
+    const long long cells = (long long)ql * tl;
+    if (ql >= 32 || (ql >= 8 && cells >= (1LL << 14))) pb::launch_exact_warp(p, tmpl->alg, tmpl->stats != 0, 1, st);
+    else pb::launch_exact(p, tmpl->alg, tmpl->stats != 0, st);
+    pb_diag_count_launch(1);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h_out, d + o_out, sizeof(pb_pair_out), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return 0;
+}
+
 int pb_cuda_align_host(int kernel, const pb_batch *tmpl,
                        const uint8_t *h_targets, const int64_t *h_toff,
                        const int *h_tlen, const int *h_qlim, const int *h_tlim,

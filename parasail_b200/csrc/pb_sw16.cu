@@ -43,6 +43,7 @@
 
 #include <algorithm>
 #include <vector>
+#include <mutex>
 
 namespace pb {
 
@@ -907,6 +908,68 @@ extern "C" int pb_cuda_align_sw16_multi(const pb_batch *b, pb_pair_out *d_out_al
     if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
     cudaStreamDestroy(st);
     return rc;
+}
+
+/* One SW score pair from host target codes: the wavefront kernel on one
+ * warp (exact int32, no overflow rerun), its descriptors and the codes in
+ * one upload to the thread's arena, the output in one download. */
+extern "C" int pb_cuda_sw_single(const pb_device_profile *dp, int open, int gap, const uint8_t *h_codes, int tlen,
+                                 pb_pair_out *h_out)
+{
+    if (pb_cuda_init() != 0) return -1;
+    if (!dp->fits8 || !dp->d_prof8 || tlen <= 0 || open + gap > 30000) return -2;
+    const size_t prof_bytes = (size_t)dp->size * dp->lp;
+    static int smem_max = -1;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        int dev = 0, optin = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        wave_set_smem(optin);
+        smem_max = optin;
+    });
+    if ((long long)prof_bytes > smem_max) return -2;
+    /* [Sw16Query][toff int64][order, tlen, counter x4: int][out][codes] then the scratch of 8 warps */
+    const size_t o_q = 0, o_toff = 16, o_ints = 24, o_out = 48;
+    const size_t o_codes = (o_out + sizeof(pb_pair_out) + 15) & ~(size_t)15;
+    const size_t up = (o_codes + (size_t)tlen + 16 + 15) & ~(size_t)15;
+    const size_t total = up + sizeof(int2) * (size_t)(tlen + 1) * pb::SW16_WARPS;
+    char *h = nullptr;
+    char *d = pb_single_arena(total, up, &h);
+    if (!d) return -1;
+    pb::Sw16Query q;
+    q.prof_off = 0; q.qlen = dp->qlen; q.lp = dp->lp; q.posmax = 32767 - dp->mmax - 1;
+    memcpy(h + o_q, &q, sizeof q);
+    const int ints[6] = {0, tlen, 0, 0, 0, 0};
+    memcpy(h + o_ints, ints, sizeof ints);
+    memcpy(h + o_codes, h_codes, (size_t)tlen);
+    cudaStream_t st = (cudaStream_t)pb_cuda_stream();
+    if (cudaMemcpyAsync(d, h, up, cudaMemcpyHostToDevice, st) != cudaSuccess) return -1;
+    pb::Sw16Params p;
+    memset(&p, 0, sizeof p);
+    p.open = open; p.gap = gap; p.npairs = 1; p.nq = 1; p.ntasks = 1; p.maxlen = tlen + 1;
+    p.nletters = dp->size;
+    p.queries = reinterpret_cast<const pb::Sw16Query *>(d + o_q);
+    p.prof_all = dp->d_prof8; p.prof_bytes = (int)prof_bytes;
+    p.order = reinterpret_cast<const int *>(d + o_ints);
+    p.targets = reinterpret_cast<const uint8_t *>(d + o_codes);
+    p.toff = reinterpret_cast<const int64_t *>(d + o_toff);
+    p.tlen = reinterpret_cast<const int *>(d + o_ints) + 1;
+    p.scratch = reinterpret_cast<uint32_t *>(d + up);
+    p.out = reinterpret_cast<pb_pair_out *>(d + o_out);
+    int rl = 8;
+    double best = -1.0;
+    for (int r = 4; r <= 16; r += 4) {
+        const double c = (double)((dp->qlen + 32 * r - 1) / (32 * r)) * (r + 4);
+        if (best < 0.0 || c < best) { best = c; rl = r; }
+    }
+    int *counter = reinterpret_cast<int *>(d + o_ints) + 2;
+    wave_kernel(open >= gap, rl)<<<1, pb::SW16_WARPS * 32, prof_bytes, st>>>(p, counter);
+    pb_diag_count_launch(1);
+    if (cudaGetLastError() != cudaSuccess) return -1;
+    if (cudaMemcpyAsync(h_out, d + o_out, sizeof(pb_pair_out), cudaMemcpyDeviceToHost, st) != cudaSuccess) return -1;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return -1;
+    return 0;
 }
 
 extern "C" int pb_cuda_align_sw16(const pb_batch *b)
