@@ -94,6 +94,7 @@ typedef struct pb_batch {
 /* --- device management ------------------------------------------------- */
 int pb_cuda_init(void);                     /* 0 ok, <0 no usable GPU */
 const char *pb_cuda_last_error(void);
+void pb_cuda_set_error(const char *what, const char *detail);
 int pb_cuda_device_count(void);
 
 /* --- profiles ------------------------------------------------------------ */
@@ -256,6 +257,8 @@ void pb_diag_sw16_time(double ms);
  * the exact kernel (qlim/tlim > 0: a prefix). pb_cuda_sw_single: the SW
  * score wavefront kernel (int8 profile required; -2 when dp has none). */
 void *pb_cuda_stream(void);   /* the calling thread's stream (a cudaStream_t) */
+/* raise (never lower) a kernel's dynamic shared-memory limit; 0 or -1 */
+int pb_raise_smem(const void *func, int bytes);
 char *pb_single_arena(size_t bytes, size_t host_bytes, char **host);
 int pb_cuda_exact_single(const pb_batch *tmpl, const uint8_t *h_codes, int tlen, int qlim, int tlim,
                          pb_pair_out *h_out);

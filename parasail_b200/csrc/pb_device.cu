@@ -209,6 +209,10 @@ int pb_cuda_init(void)
 }
 
 const char *pb_cuda_last_error(void) { return g_err; }
+void pb_cuda_set_error(const char *what, const char *detail)
+{
+    snprintf(g_err, sizeof g_err, "%s: %s", what, detail ? detail : "");
+}
 
 int pb_cuda_device_count(void)
 {
@@ -569,6 +573,28 @@ size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 /* the calling thread's stream of the library */
 void *pb_cuda_stream(void) { return (void *)stream(); }
 
+/* Raises a kernel's dynamic shared-memory limit to at least `bytes`, never
+ * lowering it: a limit set for a small launch must not fail a larger one of
+ * another call, another host thread or a recorded graph. */
+int pb_raise_smem(const void *func, int bytes)
+{
+    static std::mutex mu;
+    static std::vector<std::pair<const void *, int>> seen;
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto &x : seen)
+        if (x.first == func) {
+            if (bytes <= x.second) return 0;
+            if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
+                return -1;
+            x.second = bytes;
+            return 0;
+        }
+    const int want = bytes > 48 * 1024 ? bytes : 48 * 1024;
+    if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, want) != cudaSuccess) return -1;
+    seen.emplace_back(func, want);
+    return 0;
+}
+
 /* the calling thread's arena of at least `bytes` device bytes, and (host)
  * a zeroed host staging buffer of host_bytes */
 char *pb_single_arena(size_t bytes, size_t host_bytes, char **host)
@@ -597,6 +623,7 @@ int pb_cuda_exact_single(const pb_batch *tmpl, const uint8_t *h_codes, int tlen,
 {
     if (pb_cuda_init() != 0) return -1;
     if (tmpl->nprofs != 1 || tlen <= 0) return -1;
+    cudaGetLastError();   /* a launch error below is this call's own */
     const pb_device_profile *dp = tmpl->profs[0];
     const int nv = tmpl->stats ? 8 : 2;
     const int ql = qlim > 0 ? qlim : dp->qlen, tl = tlim > 0 ? tlim : tlen;

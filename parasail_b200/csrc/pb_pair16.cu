@@ -1079,7 +1079,7 @@ int p16_pass(const pb_job &job, const pb_batch *b, int prefix, const pb_pair_out
             smem[sh] = p16_smem(sh == 1, L, d_mat8 != nullptr);
             kern[sh] = pick(m->alg, bits, ends_on, sh == 1, warps[sh]);
             int per_sm = 0;
-            cudaFuncSetAttribute(kern[sh], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem[sh]);
+            pb_raise_smem((const void *)kern[sh], (int)smem[sh]);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern[sh], warps[sh] * 32, smem[sh]);
             grid[sh] = (per_sm < 1 ? 1 : per_sm) * nsm;
         }

@@ -638,7 +638,7 @@ static void wave_set_smem(int bytes)
 {
     for (int ge = 0; ge < 2; ++ge)
         for (int rl = 4; rl <= 16; rl += 4)
-            cudaFuncSetAttribute(wave_kernel(ge != 0, rl), cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            pb_raise_smem((const void *)wave_kernel(ge != 0, rl), bytes);
 }
 
 static int sw16_prepare(const pb_batch *b, pb_pair_out *d_out_all, size_t prof_bytes, cudaStream_t st,
@@ -713,8 +713,8 @@ static int sw16_prepare(const pb_batch *b, pb_pair_out *d_out_all, size_t prof_b
     bool bias = b->open >= b->gap;
     for (int q = 0; q < nq; ++q)
         if (b->profs[q]->mmax + b->open > 127 || b->profs[q]->mmin + b->open < -128) bias = false;
-    cudaFuncSetAttribute(pb::k_sw16<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prof_bytes);
-    cudaFuncSetAttribute(pb::k_sw16<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prof_bytes);
+    pb_raise_smem((const void *)pb::k_sw16<true>, (int)prof_bytes);
+    pb_raise_smem((const void *)pb::k_sw16<false>, (int)prof_bytes);
     if (bias)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pb::k_sw16<true>, pb::SW16_WARPS * 32, prof_bytes);
     else
@@ -918,17 +918,21 @@ extern "C" int pb_cuda_sw_single(const pb_device_profile *dp, int open, int gap,
 {
     if (pb_cuda_init() != 0) return -1;
     if (!dp->fits8 || !dp->d_prof8 || tlen <= 0 || open + gap > 30000) return -2;
+    cudaGetLastError();   /* a launch error below is this call's own */
     const size_t prof_bytes = (size_t)dp->size * dp->lp;
-    static int smem_max = -1;
-    static std::once_flag once;
-    std::call_once(once, [] {
+    /* the kernels' shared-memory limit raised to this profile (never lowered) */
+    {
         int dev = 0, optin = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        wave_set_smem(optin);
-        smem_max = optin;
-    });
-    if ((long long)prof_bytes > smem_max) return -2;
+        if ((long long)prof_bytes > optin) return -2;
+        wave_set_smem((int)prof_bytes);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            pb_cuda_set_error("single-pair SW shared memory", cudaGetErrorString(e));
+            return -1;
+        }
+    }
     /* [Sw16Query][toff int64][order, tlen, counter x4: int][out][codes] then the scratch of 8 warps */
     const size_t o_q = 0, o_toff = 16, o_ints = 24, o_out = 48;
     const size_t o_codes = (o_out + sizeof(pb_pair_out) + 15) & ~(size_t)15;
@@ -936,7 +940,7 @@ extern "C" int pb_cuda_sw_single(const pb_device_profile *dp, int open, int gap,
     const size_t total = up + sizeof(int2) * (size_t)(tlen + 1) * pb::SW16_WARPS;
     char *h = nullptr;
     char *d = pb_single_arena(total, up, &h);
-    if (!d) return -1;
+    if (!d) { pb_cuda_set_error("single-pair arena", "allocation failed"); return -1; }
     pb::Sw16Query q;
     q.prof_off = 0; q.qlen = dp->qlen; q.lp = dp->lp; q.posmax = 32767 - dp->mmax - 1;
     memcpy(h + o_q, &q, sizeof q);
@@ -944,7 +948,10 @@ extern "C" int pb_cuda_sw_single(const pb_device_profile *dp, int open, int gap,
     memcpy(h + o_ints, ints, sizeof ints);
     memcpy(h + o_codes, h_codes, (size_t)tlen);
     cudaStream_t st = (cudaStream_t)pb_cuda_stream();
-    if (cudaMemcpyAsync(d, h, up, cudaMemcpyHostToDevice, st) != cudaSuccess) return -1;
+    if (cudaMemcpyAsync(d, h, up, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        pb_cuda_set_error("single-pair upload", cudaGetErrorString(cudaGetLastError()));
+        return -1;
+    }
     pb::Sw16Params p;
     memset(&p, 0, sizeof p);
     p.open = open; p.gap = gap; p.npairs = 1; p.nq = 1; p.ntasks = 1; p.maxlen = tlen + 1;
@@ -966,9 +973,18 @@ extern "C" int pb_cuda_sw_single(const pb_device_profile *dp, int open, int gap,
     int *counter = reinterpret_cast<int *>(d + o_ints) + 2;
     wave_kernel(open >= gap, rl)<<<1, pb::SW16_WARPS * 32, prof_bytes, st>>>(p, counter);
     pb_diag_count_launch(1);
-    if (cudaGetLastError() != cudaSuccess) return -1;
-    if (cudaMemcpyAsync(h_out, d + o_out, sizeof(pb_pair_out), cudaMemcpyDeviceToHost, st) != cudaSuccess) return -1;
-    if (cudaStreamSynchronize(st) != cudaSuccess) return -1;
+    {
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            pb_cuda_set_error("single-pair SW launch", cudaGetErrorString(e));
+            return -1;
+        }
+    }
+    if (cudaMemcpyAsync(h_out, d + o_out, sizeof(pb_pair_out), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        pb_cuda_set_error("single-pair SW", cudaGetErrorString(cudaGetLastError()));
+        return -1;
+    }
     return 0;
 }
 
