@@ -239,42 +239,38 @@ int pb_cuda_lane_pair(int bits, const pb_device_profile *dp, const struct pb_mod
                       int tlen, const pb_pair_out *h_o1, pb_lane_res *h_res)
 {
     if (pb_cuda_init() != 0) return -1;
-    cudaStream_t st = nullptr;
-    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return -1;
-    uint8_t *d_t = nullptr;
-    int64_t *d_off = nullptr;
-    int *d_len = nullptr, *d_list = nullptr;
-    pb_pair_out *d_o1 = nullptr;
-    pb_lane_res *d_res = nullptr;
-    const int64_t zero = 0;
-    const int list0 = 0;
-    int rc = 0;
-    if (cudaMallocAsync((void **)&d_t, (size_t)tlen + 16, st) != cudaSuccess ||
-        cudaMallocAsync((void **)&d_off, sizeof(int64_t), st) != cudaSuccess ||
-        cudaMallocAsync((void **)&d_len, sizeof(int), st) != cudaSuccess ||
-        cudaMallocAsync((void **)&d_list, sizeof(int), st) != cudaSuccess ||
-        cudaMallocAsync((void **)&d_o1, sizeof(pb_pair_out), st) != cudaSuccess ||
-        cudaMallocAsync((void **)&d_res, sizeof(pb_lane_res), st) != cudaSuccess)
+    cudaGetLastError();   /* a launch error below is this call's own */
+    /* the thread's single-pair arena: [toff int64][tlen, list: int][o1][res][codes] then one warp's scratch */
+    const int kind = pb_lane_kind(m);
+    const size_t o_toff = 0, o_ints = 8, o_o1 = 16;
+    const size_t o_res = (o_o1 + sizeof(pb_pair_out) + 15) & ~(size_t)15;
+    const size_t o_codes = (o_res + sizeof(pb_lane_res) + 15) & ~(size_t)15;
+    const size_t up = (o_codes + (size_t)tlen + 16 + 255) & ~(size_t)255;
+    const size_t per_warp = pb_cuda_lane_scratch_per_warp(bits, kind, dp->qlen);
+    char *h = nullptr;
+    char *d = pb_single_arena(up + per_warp, up, &h);
+    if (!d) { pb_cuda_set_error("single-pair arena", "allocation failed"); return -1; }
+    const int ints[2] = {tlen, 0};
+    memcpy(h + o_ints, ints, sizeof ints);
+    memcpy(h + o_o1, h_o1, sizeof(pb_pair_out));
+    memcpy(h + o_codes, h_codes, (size_t)tlen);
+    cudaStream_t st = (cudaStream_t)pb_cuda_stream();
+    if (cudaMemcpyAsync(d, h, up, cudaMemcpyHostToDevice, st) != cudaSuccess) return -1;
+    pb_lane_args a;
+    memset(&a, 0, sizeof a);
+    a.kind = kind; a.sgflags = m->sgflags; a.open = m->open; a.gap = m->gap;
+    a.mmax = dp->mmax; a.mmin = dp->mmin; a.max_qlen = dp->qlen;
+    a.prof = dp->d_prof32; a.qcodes = dp->d_qcodes; a.lp = dp->lp; a.qlen = dp->qlen; a.size = dp->size;
+    a.targets = reinterpret_cast<const uint8_t *>(d + o_codes);
+    a.toff = reinterpret_cast<const int64_t *>(d + o_toff);
+    a.tlen = reinterpret_cast<const int *>(d + o_ints);
+    a.o1 = reinterpret_cast<const pb_pair_out *>(d + o_o1);
+    pb_lane_res *d_res = reinterpret_cast<pb_lane_res *>(d + o_res);
+    int rc = pb_cuda_lane_run(bits, &a, reinterpret_cast<const int *>(d + o_ints) + 1, 1, d_res, d + up, per_warp, st);
+    if (rc == 0 && cudaMemcpyAsync(h_res, d_res, sizeof(pb_lane_res), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         rc = -1;
-    if (rc == 0) {
-        cudaMemcpyAsync(d_t, h_codes, tlen, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(d_off, &zero, sizeof zero, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(d_len, &tlen, sizeof tlen, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(d_list, &list0, sizeof list0, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(d_o1, h_o1, sizeof(pb_pair_out), cudaMemcpyHostToDevice, st);
-        pb_lane_args a;
-        memset(&a, 0, sizeof a);
-        a.kind = pb_lane_kind(m); a.sgflags = m->sgflags; a.open = m->open; a.gap = m->gap;
-        a.mmax = dp->mmax; a.mmin = dp->mmin; a.max_qlen = dp->qlen;
-        a.prof = dp->d_prof32; a.qcodes = dp->d_qcodes; a.lp = dp->lp; a.qlen = dp->qlen; a.size = dp->size;
-        a.targets = d_t; a.toff = d_off; a.tlen = d_len; a.o1 = d_o1;
-        rc = pb_cuda_lane_run(bits, &a, d_list, 1, d_res, nullptr, 0, st);
-        if (rc == 0) cudaMemcpyAsync(h_res, d_res, sizeof(pb_lane_res), cudaMemcpyDeviceToHost, st);
-    }
-    cudaFreeAsync(d_t, st); cudaFreeAsync(d_off, st); cudaFreeAsync(d_len, st);
-    cudaFreeAsync(d_list, st); cudaFreeAsync(d_o1, st); cudaFreeAsync(d_res, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
-    cudaStreamDestroy(st);
+    if (rc != 0) pb_cuda_set_error("single-pair lane-exact kernel", cudaGetErrorString(cudaGetLastError()));
     return rc;
 }
 
