@@ -95,6 +95,9 @@ def lib():
         _lib.oracle_align.argtypes = [ctypes.c_int] * 3 + [
             ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
             ctypes.c_int, ctypes.c_int, ctypes.POINTER(OMatrix), ctypes.POINTER(OResult)]
+        _lib.oracle_align_scan.argtypes = [ctypes.c_int] * 2 + [
+            ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+            ctypes.c_int, ctypes.c_int, ctypes.POINTER(OMatrix), ctypes.POINTER(OResult)]
         _lib.oracle_padstats.argtypes = [ctypes.c_int] * 3 + [
             ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
             ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -185,6 +188,18 @@ def align(alg, sgflags, stats, q, t, open_, gap, m):
     if stats:
         out.update(matches=r.matches, similar=r.similar, length=r.length)
     return out
+
+
+def align_scan(alg, sgflags, q, t, open_, gap, m):
+    """The reference's serial scan forms (score only): src/nw_scan.c,
+    src/sg_scan.c, src/sw_scan.c, which depart from align() at open < gap."""
+    qc, tc = m.codes(q), m.codes(t)
+    r = OResult()
+    rc = lib().oracle_align_scan(alg, sgflags, _ip(qc), len(qc), _ip(tc), len(tc), open_, gap,
+                                 ctypes.byref(m._om), ctypes.byref(r))
+    if rc != 0:
+        raise ValueError("oracle_align_scan rejected its input")
+    return {"score": r.score, "end_query": r.end_query, "end_ref": r.end_ref}
 
 
 def padstats(alg, sgflags, stats, q, t, open_, gap, m, padlen):

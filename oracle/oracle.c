@@ -402,3 +402,81 @@ int oracle_nw_band(const int *s1, int s1Len, const int *s2, int s2Len,
     free(F);
     return 0;
 }
+
+/* The reference's serial scan forms, score only (src/nw_scan.c:116-168,
+ * src/sg_scan.c:142-238, src/sw_scan.c:123-172): per target column, E from
+ * the previous column's H, Ht = max(H(i-1, j-1) + s, E), then a running
+ * Ft(i) = max(Ht(i-1), Ft(i-1) - gap) with Ht(-1) the column's top boundary,
+ * and H = max(Ht, Ft - open) (SW also 0). Ft extends from Ht, not from H, so
+ * at open < gap these forms do not reopen a vertical gap from a vertical gap
+ * and differ from the serial DP; at open >= gap they equal it. End rules:
+ * SW the first maximum in column-major order; SG the last row's maximum over
+ * columns < s2Len - 1 (s2_end), then the last column over all rows
+ * (s1_end), then the corner (s2_end), each by a strict >. */
+int oracle_align_scan(int alg, int sgflags,
+                      const int *s1, int s1Len, const int *s2, int s2Len,
+                      int open, int gap, const oracle_matrix_t *m,
+                      oracle_result_t *r)
+{
+    const int s1_beg = (alg == ORACLE_SG) && (sgflags & ORACLE_S1_BEG);
+    const int s1_end = (alg == ORACLE_SG) && (sgflags & ORACLE_S1_END);
+    const int s2_beg = (alg == ORACLE_SG) && (sgflags & ORACLE_S2_BEG);
+    const int s2_end = (alg == ORACLE_SG) && (sgflags & ORACLE_S2_END);
+    int64_t *HB, *H, *E, *HtB, *Ht;
+    int64_t score = NEG_INF;
+    int end_query = s1Len, end_ref = s2Len, i, j;
+    if (!s2 || s2Len <= 0 || !s1 || s1Len <= 0 || open < 0 || gap < 0 || !m || !r)
+        return -1;
+    HB = malloc((size_t)(s1Len + 1) * sizeof(int64_t));
+    HtB = malloc((size_t)(s1Len + 1) * sizeof(int64_t));
+    E = malloc((size_t)s1Len * sizeof(int64_t));
+    if (!HB || !HtB || !E) { free(HB); free(HtB); free(E); return -1; }
+    H = HB + 1;
+    Ht = HtB + 1;
+    H[-1] = 0;
+    for (i = 0; i < s1Len; ++i) {
+        H[i] = (alg == ORACLE_SW || s1_beg) ? 0 : -(int64_t)open - (int64_t)i * gap;
+        E[i] = NEG_INF;
+    }
+    for (j = 0; j < s2Len; ++j) {
+        int64_t Ft = NEG_INF;
+        const int64_t top = (alg == ORACLE_SW || s2_beg) ? 0 : -(int64_t)open - (int64_t)j * gap;
+        for (i = 0; i < s1Len; ++i) {
+            const int64_t eo = H[i] - open, ee = E[i] - gap;
+            E[i] = eo > ee ? eo : ee;
+        }
+        for (i = 0; i < s1Len; ++i) {
+            const int64_t hd = H[i - 1] + subst(m, s1, i, s2[j]);
+            Ht[i] = hd > E[i] ? hd : E[i];
+        }
+        Ht[-1] = top;
+        for (i = 0; i < s1Len; ++i) {
+            const int64_t fe = Ft - gap;
+            int64_t h;
+            Ft = Ht[i - 1] >= fe ? Ht[i - 1] : fe;
+            h = Ht[i] > Ft - open ? Ht[i] : Ft - open;
+            if (alg == ORACLE_SW) {
+                if (h < 0) h = 0;
+                if (h > score) { score = h; end_query = i; end_ref = j; }
+            }
+            H[i] = h;
+            if (s1_end && j == s2Len - 1 && h > score) { score = h; end_query = i; end_ref = j; }
+        }
+        H[-1] = top;
+        if (s2_end && j < s2Len - 1 && H[s1Len - 1] > score) {
+            score = H[s1Len - 1]; end_query = s1Len - 1; end_ref = j;
+        }
+    }
+    if (alg == ORACLE_SG && s2_end && H[s1Len - 1] > score) {
+        score = H[s1Len - 1]; end_query = s1Len - 1; end_ref = s2Len - 1;
+    }
+    if (alg == ORACLE_NW || (alg == ORACLE_SG && !s1_end && !s2_end)) {
+        score = H[s1Len - 1]; end_query = s1Len - 1; end_ref = s2Len - 1;
+    }
+    memset(r, 0, sizeof *r);
+    r->score = (int)score;
+    r->end_query = end_query;
+    r->end_ref = end_ref;
+    free(HB); free(HtB); free(E);
+    return 0;
+}

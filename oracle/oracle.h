@@ -58,6 +58,14 @@ int oracle_align(int alg, int sgflags, int stats,
                  int open, int gap, const oracle_matrix_t *m,
                  oracle_result_t *r);
 
+/* The reference's serial scan forms, score only (src/nw_scan.c,
+ * src/sg_scan.c, src/sw_scan.c): F extends from Ht = max(diagonal, E), so
+ * they differ from oracle_align at open < gap. Returns 0 on success. */
+int oracle_align_scan(int alg, int sgflags,
+                      const int *s1, int s1Len, const int *s2, int s2Len,
+                      int open, int gap, const oracle_matrix_t *m,
+                      oracle_result_t *r);
+
 /* Same recurrence over padLen >= s1Len query rows; fills *ps. */
 int oracle_padstats(int alg, int sgflags, int stats,
                     const int *s1, int s1Len, int padLen,

@@ -50,7 +50,7 @@ static int sg_bits(int alg, int sgflags)
  * reruns out-of-range pairs on the exact kernel itself; 0 = exact kernel. */
 static int run_pair(int kernel, const pb_device_profile *dp, const pb_mode *m, int stats,
                     int pad_rows, const uint8_t *codes, int tlen, int qlim, int tlim,
-                    pb_pair_out *out)
+                    int scan_vgap, pb_pair_out *out)
 {
     pb_batch b;
     const pb_device_profile *profs[1];
@@ -60,6 +60,7 @@ static int run_pair(int kernel, const pb_device_profile *dp, const pb_mode *m, i
     b.alg = m->alg; b.sgflags = m->sgflags; b.stats = stats;
     b.open = m->open; b.gap = m->gap; b.pad_rows = pad_rows;
     b.profs = profs; b.nprofs = 1;
+    b.scan_vgap = scan_vgap;
     /* one pair: the single-pair paths (one upload, one launch, one
      * download); the batch pipeline for what they do not take */
     if (kernel == 1 && qlim <= 0 && tlim <= 0) {
@@ -100,15 +101,19 @@ int pb_run_job_pair(const pb_device_profile *dp, const pb_job *job, const uint8_
     const int score_only_sw = m->alg == PB_SW && (!m->stats || pb_job_is_faststats(job));
     const int pad = (job->bits < 0 || (m->alg == PB_SW && !m->stats)) ? 0
                   : (job->bits == 0 || job->bits == 8) ? 32 : job->bits == 16 ? 16 : 8;
+    /* the serial scan forms at open < gap, where their vertical gap departs
+     * from the serial DP's (score only) */
+    const int scan_vgap = job->bits < 0 && (job->base_flags & PARASAIL_FLAG_NOVEC_SCAN) && !m->stats
+                        && m->open < m->gap;
     int rc;
     memset(&o2, 0, sizeof o2);
     if (score_only_sw && job->bits >= 0)
-        rc = run_pair(1, dp, m, 0, 0, codes, tlen, 0, 0, &o1);
+        rc = run_pair(1, dp, m, 0, 0, codes, tlen, 0, 0, 0, &o1);
     else
-        rc = run_pair(0, dp, m, m->stats, pad, codes, tlen, 0, 0, &o1);
+        rc = run_pair(0, dp, m, m->stats, pad, codes, tlen, 0, 0, scan_vgap, &o1);
     if (rc != 0) return rc;
     if (pb_needs_pass2(job, &o1)) {
-        rc = run_pair(0, dp, m, 1, 32, codes, tlen, o1.end_query + 1, o1.end_ref + 1, &o2);
+        rc = run_pair(0, dp, m, 1, 32, codes, tlen, o1.end_query + 1, o1.end_ref + 1, 0, &o2);
         if (rc != 0) return rc;
     }
     {

@@ -89,6 +89,10 @@ typedef struct pb_batch {
     /* pairs mode, optional: per-pair query id; pairs with one id share the
      * query (e.g. the rows of an all-vs-all batch) */
     const int *d_qgroup;
+    /* 1: the vertical gap of the reference's serial scan forms (src/nw_scan.c
+     * etc.: F extends from max(diagonal, E), not from H), score only, on the
+     * single-pair exact path */
+    int scan_vgap;
 } pb_batch;
 
 /* --- device management ------------------------------------------------- */

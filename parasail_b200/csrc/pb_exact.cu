@@ -19,16 +19,16 @@
 
 namespace pb {
 
-template <int ALG, bool STATS, int R>
+template <int ALG, bool STATS, int R, bool SCANF>
 __global__ void __launch_bounds__(128)
 k_exact(ExactParams p)
 {
     const int pid = blockIdx.x * blockDim.x + threadIdx.x;
     if (pid >= p.npairs) return;
-    exact_pair<ALG, STATS, R>(p, pid);
+    exact_pair<ALG, STATS, R, SCANF>(p, pid);
 }
 
-template <int ALG, bool STATS>
+template <int ALG, bool STATS, bool SCANF = false>
 static void launch_alg(const ExactParams &p, cudaStream_t st)
 {
     /* score-only: 32-row strips (34 vs 29 GCUPS for NW against 16 rows,
@@ -36,12 +36,19 @@ static void launch_alg(const ExactParams &p, cudaStream_t st)
     constexpr int R = STATS ? 8 : 32;
     const int threads = 128;
     const int blocks = (p.npairs + threads - 1) / threads;
-    k_exact<ALG, STATS, R><<<blocks, threads, 0, st>>>(p);
+    k_exact<ALG, STATS, R, SCANF><<<blocks, threads, 0, st>>>(p);
 }
 
 void launch_exact(const ExactParams &p, int alg, bool stats, cudaStream_t st)
 {
     if (p.npairs <= 0) return;
+    if (p.scan_vgap && !stats) {
+        /* the serial scan forms' vertical gap */
+        if (alg == PB_SW) launch_alg<PB_SW, false, true>(p, st);
+        else if (alg == PB_NW) launch_alg<PB_NW, false, true>(p, st);
+        else launch_alg<PB_SG, false, true>(p, st);
+        return;
+    }
     if (alg == PB_SW) { if (stats) launch_alg<PB_SW, true>(p, st); else launch_alg<PB_SW, false>(p, st); }
     else if (alg == PB_NW) { if (stats) launch_alg<PB_NW, true>(p, st); else launch_alg<PB_NW, false>(p, st); }
     else { if (stats) launch_alg<PB_SG, true>(p, st); else launch_alg<PB_SG, false>(p, st); }

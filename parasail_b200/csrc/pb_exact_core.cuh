@@ -48,9 +48,16 @@ __host__ __device__ __forceinline__ int left_h(int i, int open, int gap, int sgf
     return -open - i * gap;
 }
 
-template <int ALG, bool STATS, int R>
+/* SCANF (score only): the vertical gap of the reference's serial scan forms
+ * (src/nw_scan.c:128-146, src/sg_scan.c:155-173, src/sw_scan.c:146-152),
+ * F(i) = max(Ht(i-1) - open, F(i-1) - gap) with Ht = max(diagonal, E): a
+ * vertical gap is not reopened from a vertical gap, which differs from the
+ * serial DP at open < gap. The kernel then carries in fu the F of the next
+ * row instead of the F of the row above. */
+template <int ALG, bool STATS, int R, bool SCANF = false>
 __host__ __device__ __forceinline__ void exact_pair(const ExactParams &p, const int k)
 {
+    static_assert(!(SCANF && STATS), "the scan vertical gap is score-only");
     const int pid = p.order ? p.order[k] : k;          /* output slot */
     const int ti = p.nt ? pid % p.nt : pid;            /* target (and per-pair query) index */
 
@@ -113,7 +120,7 @@ __host__ __device__ __forceinline__ void exact_pair(const ExactParams &p, const 
             int *bj = buf + (size_t)j * NV;
             if (r0 == 0) {
                 hu = top_h<ALG>(j, open, gap, sgf);
-                fu = NEG_INF;
+                fu = SCANF ? hu - open : NEG_INF;
             } else {
                 hu = bj[0];
                 fu = bj[1];
@@ -142,11 +149,12 @@ __host__ __device__ __forceinline__ void exact_pair(const ExactParams &p, const 
                 const int sc = real ? (matmode ? prow[pd.qcodes[i]] : prow[i]) : 0;
                 /* F: vertical gap (along the query), E: horizontal gap */
                 const int f_opn = hu - open, f_ext = fu - gap;
-                const int fn = max(f_opn, f_ext);
+                const int fn = SCANF ? fu : max(f_opn, f_ext);
                 const int e_opn = Hl[r] - open, e_ext = E[r] - gap;
                 const int en = max(e_opn, e_ext);
                 const int hdag = Dg[r] + sc;
-                int hn = max(max(hdag, en), fn);
+                const int ht = max(hdag, en);
+                int hn = max(ht, fn);
                 if (ALG == PB_SW) hn = max(hn, 0);
                 int hM = 0, hS = 0, hL = 0, fM = 0, fS = 0, fL = 0;
                 if (STATS) {
@@ -214,7 +222,7 @@ __host__ __device__ __forceinline__ void exact_pair(const ExactParams &p, const 
                 }
                 Hl[r] = hn;
                 if (STATS) { HlM[r] = hM; HlS[r] = hS; HlL[r] = hL; }
-                hu = hn; fu = fn;
+                hu = hn; fu = SCANF ? max(ht - open, fn - gap) : fn;
                 if (STATS) { huM = hM; huS = hS; huL = hL; fuM = fM; fuS = fS; fuL = fL; }
             }
             if (r0 + R < nrows) {

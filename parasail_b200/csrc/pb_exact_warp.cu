@@ -54,10 +54,11 @@ __device__ __forceinline__ EwCell ew_shfl(const EwCell &c, int src)
  * through the square matrix mat[target letter * msize + query letter];
  * else profiles: every query of profs against the same nt targets, or
  * (nt = 0) pair k's profile profs[prof_index[k]] against target k */
-template <int ALG, bool STATS, bool PAIRS>
+template <int ALG, bool STATS, bool PAIRS, bool SCANF>
 __global__ void __launch_bounds__(EW_WARPS * 32)
 k_exact_warp(ExactParams p, int nitems)
 {
+    static_assert(!(SCANF && STATS), "the scan vertical gap is score-only");
     constexpr int EW_R = EwRows<STATS>::value;
     const int lane = threadIdx.x & 31;
     const int item = blockIdx.x * EW_WARPS + (threadIdx.x >> 5);
@@ -139,7 +140,7 @@ k_exact_warp(ExactParams p, int nitems)
             if (j < 0 || j >= tl) continue;
             if (lane == 0) {
                 if (r0 == 0) {
-                    up_h = top_h<ALG>(j, open, gap, sgf); up_f = NEG_INF;
+                    up_h = top_h<ALG>(j, open, gap, sgf); up_f = SCANF ? up_h - open : NEG_INF;
                     huM = huS = huL = fuM = fuS = fuL = 0;
                 } else if (STATS) {
                     const int4 a = buf4[2 * j], b = buf4[2 * j + 1];
@@ -162,11 +163,12 @@ k_exact_warp(ExactParams p, int nitems)
                 const bool real = i < ql;
                 const int sc = real ? (PAIRS ? __ldg(&prow[qc[r]]) : prow[i]) : 0;
                 const int f_opn = hu - open, f_ext = fu - gap;
-                const int fn = max(f_opn, f_ext);
+                const int fn = SCANF ? fu : max(f_opn, f_ext);
                 const int e_opn = Hl[r] - open, e_ext = E[r] - gap;
                 const int en = max(e_opn, e_ext);
                 const int hdag = hd + sc;
-                int hn = max(max(hdag, en), fn);
+                const int ht = max(hdag, en);
+                int hn = max(ht, fn);
                 if (ALG == PB_SW) hn = max(hn, 0);
                 int hM = 0, hS = 0, hL = 0, fM = 0, fS = 0, fL = 0;
                 if (STATS) {
@@ -229,7 +231,7 @@ k_exact_warp(ExactParams p, int nitems)
                 hd = Hl[r];
                 Hl[r] = hn;
                 hu = hn;
-                fu = fn;
+                fu = SCANF ? max(ht - open, fn - gap) : fn;
                 if (STATS) {
                     hdM = HlM[r]; hdS = HlS[r]; hdL = HlL[r];
                     HlM[r] = hM; HlS[r] = hS; HlL[r] = hL;
@@ -315,13 +317,13 @@ k_exact_warp(ExactParams p, int nitems)
     p.out[pid] = o;
 }
 
-template <bool STATS, bool PAIRS>
+template <bool STATS, bool PAIRS, bool SCANF = false>
 static void launch_ew(const ExactParams &p, int alg, int nitems, cudaStream_t st)
 {
     const int blocks = (nitems + EW_WARPS - 1) / EW_WARPS;
-    if (alg == PB_SW) k_exact_warp<PB_SW, STATS, PAIRS><<<blocks, EW_WARPS * 32, 0, st>>>(p, nitems);
-    else if (alg == PB_NW) k_exact_warp<PB_NW, STATS, PAIRS><<<blocks, EW_WARPS * 32, 0, st>>>(p, nitems);
-    else k_exact_warp<PB_SG, STATS, PAIRS><<<blocks, EW_WARPS * 32, 0, st>>>(p, nitems);
+    if (alg == PB_SW) k_exact_warp<PB_SW, STATS, PAIRS, SCANF><<<blocks, EW_WARPS * 32, 0, st>>>(p, nitems);
+    else if (alg == PB_NW) k_exact_warp<PB_NW, STATS, PAIRS, SCANF><<<blocks, EW_WARPS * 32, 0, st>>>(p, nitems);
+    else k_exact_warp<PB_SG, STATS, PAIRS, SCANF><<<blocks, EW_WARPS * 32, 0, st>>>(p, nitems);
 }
 
 void launch_exact_warp(const ExactParams &p, int alg, bool stats, int nitems, cudaStream_t st)
@@ -330,6 +332,9 @@ void launch_exact_warp(const ExactParams &p, int alg, bool stats, int nitems, cu
     const bool pairs = p.mat != nullptr;
     if (stats) {
         if (pairs) launch_ew<true, true>(p, alg, nitems, st); else launch_ew<true, false>(p, alg, nitems, st);
+    } else if (p.scan_vgap) {
+        /* the serial scan forms' vertical gap, one query per call */
+        launch_ew<false, false, true>(p, alg, nitems, st);
     } else {
         if (pairs) launch_ew<false, true>(p, alg, nitems, st); else launch_ew<false, false>(p, alg, nitems, st);
     }

@@ -672,10 +672,11 @@ PB_LHD void striped_sw(P &v, const Problem &pr, Out &o)
  * only the flag is produced. ---- */
 template <int W> PB_LHD int gapper_at(int open, int gap, int segLen, int i)
 {
-    /* pvGapper[i]: subs(0, open) then segLen-1-i saturating subtractions of
-     * gap; a constant saturating step stays clamped once it clamps */
-    const long long x0 = clampw<W>(-(long long)wrap<W>(open));
-    return clampw<W>(x0 - (long long)(segLen - 1 - i) * wrap<W>(gap));
+    /* pvGapper[i]: 0 - open, then segLen-1-i subtractions of gap in the
+     * lane's arithmetic (saturating at 8/16 bits: a constant saturating step
+     * stays clamped once it clamps; wrapping at 32) */
+    const long long x0 = lane_arith<W>(-(long long)wrap<W>(open));
+    return lane_arith<W>(x0 - (long long)(segLen - 1 - i) * wrap<W>(gap));
 }
 
 template <class P, int W>
@@ -746,6 +747,193 @@ PB_LHD void scan_nwsg_trace(P &v, const Problem &pr, Out &o)
     }
     o.saturated = v.any(v.or_(v.cmpgt(vNegLimit, vSatMin), v.cmpgt(vSatMax, vPosLimit))) ? 1 : 0;
     o.score = o.end_query = o.end_ref = 0;
+    o.matches = o.similar = o.length = 0;
+}
+
+/* ---- nw / sg scan, score only: util/templates/nw_scan.c and sg_scan.c
+ * (src/nw_scan_avx2_256_16.c:255-394, src/sg_scan_avx2_256_16.c:270-444):
+ * E and the H of the diagonal in a first loop over the segments, F by a
+ * pseudo prefix scan across the lanes, final H and F in a second loop.
+ * Checked: H (and for SG F and the gap ramp of pvGapper). Ends as in the
+ * striped kernels (column maxima of the last row, the last column in memory
+ * order). ---- */
+template <class P, int W>
+PB_LHD void scan_nwsg(P &v, const Problem &pr, Out &o)
+{
+    typedef typename P::V V;
+    constexpr int L = Lim<W>::LANES;
+    const int s1Len = pr.qlen, s2Len = pr.tlen;
+    const int segLen = (s1Len + L - 1) / L;
+    const int offset = (s1Len - 1) % segLen;
+    const int lastLane = (s1Len - 1) / segLen;
+    const int open = pr.open, gap = pr.gap;
+    const bool sg = pr.s1_beg || pr.s1_end || pr.s2_beg || pr.s2_end;
+    const int NEG_LIMIT = wrap<W>((-open < pr.mmin ? (long long)Lim<W>::MIN + open : (long long)Lim<W>::MIN - pr.mmin) + 1);
+    const int POS_LIMIT = wrap<W>((long long)Lim<W>::MAX - pr.mmax - 1);
+    const V vGapO = v.set1(wrap<W>(open)), vGapE = v.set1(wrap<W>(gap));
+    const V vNegLimit = v.set1(NEG_LIMIT), vPosLimit = v.set1(POS_LIMIT);
+    const V vNegInfFront = v.insert0(v.set1(0), NEG_LIMIT);
+    const V vSegLenXgap = v.template adds<W>(vNegInfFront, v.shift1(v.set1(wrap<W>(-(long long)segLen * gap))));
+    const V vGapper0 = v.set1(gapper_at<W>(open, gap, segLen, 0));
+    const V vPosMask = v.lane_eq(lastLane);
+    V vSatMin = vPosLimit, vSatMax = vNegLimit, vMaxH = vNegLimit;
+    if (sg) {
+        const long long x0 = lane_arith<W>(-(long long)wrap<W>(open));
+        const int a = lane_arith<W>(x0 - wrap<W>(gap)), b = lane_arith<W>(x0 - (long long)segLen * wrap<W>(gap));
+        vSatMin = v.min(vSatMin, v.set1(a < b ? a : b));
+    }
+    int end_query = s1Len - 1, end_ref = s2Len - 1;
+    int score = NEG_LIMIT;
+
+    typename P::Arr pe = v.arr(0, segLen), pht = v.arr(1, segLen), ph = v.arr(2, segLen);
+    for (int i = 0; i < segLen; ++i) {
+        V h, e;
+        v.template init_he<W>(h, e, i, segLen, pr.s1_beg, open, gap);
+        v.store(ph, i, h);
+        v.store(pe, i, e);
+    }
+    for (int j = 0; j < s2Len; ++j) {
+        const int bj = v.template boundary<W>(pr, j), bj1 = v.template boundary<W>(pr, j + 1);
+        const int k_t = pr.t[j];
+        V vHp = v.insert0(v.shift1(v.load(ph, segLen - 1)), bj);
+        V vHt = v.template subs<W>(vNegLimit, vGapper0);
+        V vF = vNegLimit;
+        for (int i = 0; i < segLen; ++i) {
+            const V vH = v.load(ph, i);
+            V vE = v.load(pe, i);
+            vE = v.max(v.template subs<W>(vE, vGapE), v.template subs<W>(vH, vGapO));
+            vHp = v.template adds<W>(vHp, v.template prof<W>(pr, k_t, i, segLen));
+            vF = v.max(vF, v.template adds<W>(vHt, v.set1(gapper_at<W>(open, gap, segLen, i))));
+            vHt = v.max(vE, vHp);
+            v.store(pe, i, vE);
+            v.store(pht, i, vHt);
+            vHp = vH;
+        }
+        vHt = v.insert0(v.shift1(vHt), bj1);
+        vF = v.max(vF, v.template adds<W>(vHt, vGapper0));
+        for (int k = 0; k < L - 2; ++k) vF = v.max(vF, v.template adds<W>(v.shift1(vF), vSegLenXgap));
+        vF = v.template adds<W>(v.shift1(vF), vNegInfFront);
+        V vH = v.max(vHt, vF);
+        for (int i = 0; i < segLen; ++i) {
+            vF = v.max(v.template subs<W>(vF, vGapE), v.template subs<W>(vH, vGapO));
+            vH = v.max(v.load(pht, i), vF);
+            v.store(ph, i, vH);
+            vSatMin = v.min(vSatMin, vH);
+            if (sg) vSatMin = v.min(vSatMin, vF);
+            vSatMax = v.max(vSatMax, vH);
+        }
+        {
+            vH = v.load(ph, offset);
+            const V vCompare = v.and_(vPosMask, v.cmpgt(vH, vMaxH));
+            vMaxH = v.max(vH, vMaxH);
+            if (v.any(vCompare)) end_ref = j;
+        }
+        if (v.any(v.or_(v.cmpgt(vNegLimit, vSatMin), v.cmpgt(vSatMax, vPosLimit)))) break;
+    }
+    if (pr.s2_end) {
+        score = v.extract(vMaxH, lastLane);
+        end_query = s1Len - 1;
+    }
+    if (pr.s1_end) {
+        for (int i = 0; i < segLen; ++i) {
+            for (int l = 0; l < L; ++l) {
+                const int temp = i + l * segLen;
+                if (temp >= s1Len) continue;
+                const int t = v.extract(v.load(ph, i), l);
+                if (t > score) {
+                    score = t; end_query = temp; end_ref = s2Len - 1;
+                } else if (t == score && end_ref == s2Len - 1 && temp < end_query) {
+                    end_query = temp;
+                }
+            }
+        }
+    }
+    if (!pr.s1_end && !pr.s2_end) {
+        score = v.extract(v.load(ph, offset), lastLane);
+        end_ref = s2Len - 1;
+        end_query = s1Len - 1;
+    }
+    o.saturated = v.any(v.or_(v.cmpgt(vNegLimit, vSatMin), v.cmpgt(vSatMax, vPosLimit))) ? 1 : 0;
+    if (o.saturated) { score = 0; end_query = 0; end_ref = 0; }
+    o.score = score; o.end_query = end_query; o.end_ref = end_ref;
+    o.matches = o.similar = o.length = 0;
+}
+
+/* ---- sw scan, score only: util/templates/sw_scan.c
+ * (src/sw_scan_avx2_256_16.c:226-380): the scan passes with H clamped at 0,
+ * the column maxima folded into vMaxH, the column of a new maximum copied,
+ * and the smallest row of the best score found in that copy (padded rows
+ * included). Checked: H. ---- */
+template <class P, int W>
+PB_LHD void scan_sw(P &v, const Problem &pr, Out &o)
+{
+    typedef typename P::V V;
+    constexpr int L = Lim<W>::LANES;
+    const int s1Len = pr.qlen, s2Len = pr.tlen;
+    const int segLen = (s1Len + L - 1) / L;
+    const int open = pr.open, gap = pr.gap;
+    const int NEG_LIMIT = wrap<W>((-open < pr.mmin ? (long long)Lim<W>::MIN + open : (long long)Lim<W>::MIN - pr.mmin) + 1);
+    const int POS_LIMIT = wrap<W>((long long)Lim<W>::MAX - pr.mmax - 1);
+    const V vGapO = v.set1(wrap<W>(open)), vGapE = v.set1(wrap<W>(gap));
+    const V vZero = v.set1(0);
+    const V vNegLimit = v.set1(NEG_LIMIT), vPosLimit = v.set1(POS_LIMIT);
+    const V vNegInfFront = v.insert0(vZero, NEG_LIMIT);
+    const V vSegLenXgap = v.template adds<W>(vNegInfFront, v.shift1(v.set1(wrap<W>(-(long long)segLen * gap))));
+    const V vGapper0 = v.set1(gapper_at<W>(open, gap, segLen, 0));
+    V vSatMin = vPosLimit, vSatMax = vNegLimit, vMaxH = vNegLimit, vMaxHUnit = vNegLimit;
+    int score = NEG_LIMIT, end_ref = 0, end_query = 0;
+
+    typename P::Arr pe = v.arr(0, segLen), pht = v.arr(1, segLen), ph = v.arr(2, segLen), pmax = v.arr(3, segLen);
+    for (int i = 0; i < segLen; ++i) {
+        v.store(ph, i, vZero);
+        v.store(pe, i, vNegLimit);
+    }
+    for (int j = 0; j < s2Len; ++j) {
+        const int k_t = pr.t[j];
+        V vHp = v.shift1(v.load(ph, segLen - 1));
+        V vHt = vZero;
+        V vF = vNegLimit;
+        for (int i = 0; i < segLen; ++i) {
+            const V vH = v.load(ph, i);
+            V vE = v.load(pe, i);
+            vE = v.max(v.template subs<W>(vE, vGapE), v.template subs<W>(vH, vGapO));
+            vHp = v.template adds<W>(vHp, v.template prof<W>(pr, k_t, i, segLen));
+            vF = v.max(vF, v.template adds<W>(vHt, v.set1(gapper_at<W>(open, gap, segLen, i))));
+            vHt = v.max(vE, vHp);
+            v.store(pe, i, vE);
+            v.store(pht, i, vHt);
+            vHp = vH;
+        }
+        vHt = v.shift1(vHt);
+        vF = v.max(vF, v.template adds<W>(vHt, vGapper0));
+        for (int k = 0; k < L - 2; ++k) vF = v.max(vF, v.template adds<W>(v.shift1(vF), vSegLenXgap));
+        vF = v.template adds<W>(v.shift1(vF), vNegInfFront);
+        V vH = v.max(v.max(vHt, vF), vZero);
+        for (int i = 0; i < segLen; ++i) {
+            vF = v.max(v.template subs<W>(vF, vGapE), v.template subs<W>(vH, vGapO));
+            vH = v.max(v.max(v.load(pht, i), vF), vZero);
+            v.store(ph, i, vH);
+            vSatMin = v.min(vSatMin, vH);
+            vSatMax = v.max(vSatMax, vH);
+            vMaxH = v.max(vH, vMaxH);
+        }
+        if (v.any(v.cmpgt(vMaxH, vMaxHUnit))) {
+            score = v.hmax(vMaxH);
+            vMaxHUnit = v.set1(score);
+            end_ref = j;
+            for (int i = 0; i < segLen; ++i) v.store(pmax, i, v.load(ph, i));
+        }
+        if (v.any(v.or_(v.cmpgt(vNegLimit, vSatMin), v.cmpgt(vSatMax, vPosLimit)))) break;
+    }
+    /* the smallest row holding the score in the copied column (memory order,
+     * padded rows included: src/sw_scan_avx2_256_16.c:356-368) */
+    end_query = s1Len;
+    for (int i = 0; i < segLen; ++i)
+        for (int l = 0; l < L; ++l)
+            if (v.extract(v.load(pmax, i), l) == score && i + l * segLen < end_query) end_query = i + l * segLen;
+    o.saturated = v.any(v.or_(v.cmpgt(vNegLimit, vSatMin), v.cmpgt(vSatMax, vPosLimit))) ? 1 : 0;
+    if (o.saturated) { score = 0; end_query = 0; end_ref = 0; }
+    o.score = score; o.end_query = end_query; o.end_ref = end_ref;
     o.matches = o.similar = o.length = 0;
 }
 

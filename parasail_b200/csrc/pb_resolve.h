@@ -173,21 +173,26 @@ enum { PB_REC_FALLBACK = 1 };
  * loop stops on a tie between F - gap and H - open, which open <= gap makes
  * common), and in the statistics kernels open < gap (they continue on ties,
  * and agree with the exact DP at open == gap). The SW statistics kernels of
- * the FASTSTATS wrapper are not emulated in these regimes. */
+ * the FASTSTATS wrapper are not emulated in these regimes. The score-only
+ * scan kernels depart from the exact DP at open < gap (their prefix scan of
+ * F assumes F - gap >= F - open) and with a wrapped penalty; their
+ * statistics forms are not emulated. */
 PB_HD static inline int pb_lane_forced(const pb_mode *m, int bits)
 {
-    if (!m->striped || (m->alg == PB_SW && m->stats)) return 0;
-    if (bits < 32 && (m->open > int_max_w(bits) || m->gap > int_max_w(bits))) return 1;
+    const int wrapped = bits < 32 && (m->open > int_max_w(bits) || m->gap > int_max_w(bits));
+    if (!m->striped) return !m->stats && (m->open < m->gap || wrapped);
+    if (m->alg == PB_SW && m->stats) return 0;
+    if (wrapped) return 1;
     return m->stats ? m->open < m->gap : m->open <= m->gap;
 }
 
 /* Widths whose verdict the lane-exact kernels (pb_lane.cuh) give: the
  * 8/16-bit striped nw/sg kernels and the 8/16-bit SW statistics kernel of
  * the FASTSTATS wrapper whenever the exact values do not show a CLEAN run,
- * and every striped width pb_lane_forced names. */
+ * and every width pb_lane_forced names (striped or scan). */
 PB_HD static inline int pb_lane_applies(const pb_mode *m, int bits)
 {
-    if (!m->striped) return 0;
+    if (!m->striped) return pb_lane_forced(m, bits);
     if (m->alg == PB_SW) return m->stats ? (bits == 8 || bits == 16) : pb_lane_forced(m, bits);
     return bits == 8 || bits == 16 || pb_lane_forced(m, bits);
 }
@@ -195,6 +200,7 @@ PB_HD static inline int pb_lane_applies(const pb_mode *m, int bits)
 /* lane kernel kind for a mode (pb_lane_args.kind) */
 PB_HD static inline int pb_lane_kind(const pb_mode *m)
 {
+    if (!m->striped) return m->alg == PB_SW ? 7 : 6;     /* scan, score only */
     return m->alg == PB_SW ? (m->stats ? 2 : 3) : (m->stats ? 1 : 0);
 }
 

@@ -76,6 +76,36 @@ def test_serial_forms_vs_oracle(alg_name):
                 assert got["flag"] & (pb.FLAG_NOVEC_SCAN if scan else pb.FLAG_NOVEC)
 
 
+@pytest.mark.parametrize("alg_name", ["sw", "nw", "sg", "sg_qx", "sg_qe_db", "sg_qb_de", "sg_dx"])
+def test_serial_scan_open_below_gap_vs_oracle(alg_name):
+    """parasail_*_scan at open < gap, where the reference's serial scan forms
+    extend a vertical gap only from max(diagonal, E) and so differ from the
+    serial DP: against the oracle's restatement of those forms (and the live
+    reference when it was built), for queries on the thread kernel (< 32
+    rows), the warp kernel and several warp passes (> 512 rows)."""
+    rng = random.Random(len(alg_name) * 104729)
+    alg, sgf = O.alg_of(alg_name)
+    differs = 0
+    for it in range(12):
+        key, a = ("blosum62", AA) if it % 2 else (("ACGT", 2, -3), DNA)
+        op, gp = rng.choice([(0, 1), (1, 2), (2, 5), (1, 3)])
+        ql = rng.choice([rng.randint(1, 31), rng.randint(32, 300), rng.randint(513, 1300)])
+        q = rand_seq(rng, ql, a)
+        t = mutate(rng, q, a) if it % 3 == 0 else rand_seq(rng, rng.randint(1, 900), a)
+        got = pb.align("parasail_%s_scan" % alg_name, q, t, op, gp, _pb_matrix(key))
+        exp = O.align_scan(alg, sgf, q, t, op, gp, _o_matrix(key))
+        assert {k: got[k] for k in exp} == exp, (alg_name, op, gp, len(q), len(t), got, exp)
+        assert got["flag"] & pb.FLAG_NOVEC_SCAN
+        if O.ref() is not None:
+            r = O.ref_serial(alg_name, 0, q, t, op, gp, key, scan=True)
+            assert {k: r[k] for k in exp} == exp
+        differs += exp != O.align(alg, sgf, 0, q, t, op, gp, _o_matrix(key))
+        # the plain serial form keeps the serial DP
+        assert {k: v for k, v in pb.align("parasail_%s" % alg_name, q, t, op, gp, _pb_matrix(key)).items()
+                if k in exp} == O.align(alg, sgf, 0, q, t, op, gp, _o_matrix(key))
+    assert differs >= 1
+
+
 def _vector_cases():
     return json.load(open(os.path.join(GOLDEN, "vector_golden.json")))["cases"]
 
@@ -276,4 +306,47 @@ def test_batch_striped_narrow_vs_live_reference(width):
                     if any(r.get(k) != v for k, v in exp.items()):
                         bad.append((name, key, q, t, r, exp))
     assert total >= 500
+    assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])
+
+
+@pytest.mark.skipif(O.ref() is None, reason="reference library not built")
+@pytest.mark.parametrize("width", ["8", "16", "32", "sat"])
+def test_scan_open_below_gap_and_wrapped_vs_live_reference(width):
+    """Score-only scan kernels where the reference departs from the exact DP
+    (open < gap: their prefix scan of F takes F - gap >= F - open; a penalty
+    above the lane maximum wraps in set1): the direct and profile forms and
+    batches of both kinds, run on the lane-exact scan kernels, against the
+    reference's AVX2 kernels."""
+    rng = random.Random({"8": 28, "16": 216, "32": 232, "sat": 87}[width])
+    bad, total = [], 0
+    for alg_name in ("sw", "nw", "sg", "sg_qx", "sg_de", "sg_qb_db", "sg_qe_db"):
+        for it in range(5):
+            protein = it % 2 == 1
+            key, a = ("blosum62", AA) if protein else (("ACGT", 2, -3), DNA)
+            m = _pb_matrix(key)
+            c = [(0, 1), (1, 2), (2, 5), (1, 3)]
+            if width in ("8", "sat"):
+                c.append((200, 1) if protein else (130, 2))
+            op, gp = rng.choice(c)
+            q = rand_seq(rng, rng.randint(1, 200), a)
+            targets = [mutate(rng, q, a, 0.2, 0.04) if k % 3 == 0 else rand_seq(rng, rng.randint(1, 220), a)
+                       for k in range(10)]
+            exp = [O.ref_vector(alg_name, 0, "scan", width, q, t, op, gp, key) for t in targets]
+            got = {}
+            got["direct"] = [pb.align("parasail_%s_scan_%s" % (alg_name, width), q, t, op, gp, m)
+                             for t in targets]
+            prof = pb.ProfileHandle("parasail_profile_create_%s" % width, q, m)
+            got["profile"] = [pb.align_profile("parasail_%s_scan_profile_%s" % (alg_name, width), prof, t, op, gp)
+                              for t in targets]
+            got["batch"] = pb.records_to_dicts(
+                pb.batch_profile("%s_scan_profile_%s" % (alg_name, width), prof, targets, op, gp), 0)
+            prof.close()
+            got["pairs"] = pb.records_to_dicts(
+                pb.batch_pairs("%s_scan_%s" % (alg_name, width), m, [q] * len(targets), targets, op, gp), 0)
+            for form, rs in got.items():
+                for t, r, e in zip(targets, rs, exp):
+                    total += 1
+                    if any(r.get(k) != v for k, v in e.items()):
+                        bad.append((form, alg_name, width, op, gp, q, t, r, e))
+    assert total == 7 * 5 * 10 * 4
     assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])

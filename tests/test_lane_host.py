@@ -214,3 +214,46 @@ def test_trace_kernel_saturation_emulation(lanelib, seed):
                         bad.append((name, scheme, bits, key, op, gp, q, t, esat, escore, list(o)))
     assert total == 6 * 2 * 2 * len(ALGS) and 60 < nsat < total - 60
     assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])
+
+
+@pytest.mark.parametrize("seed", [7, 8])
+def test_scan_kernel_emulation(lanelib, seed):
+    """The score-only scan kernels (util/templates/nw_scan.c, sg_scan.c,
+    sw_scan.c) restated lane by lane: score, ends and the saturation flag
+    equal the reference's AVX2 kernels at 8, 16 and 32 bits, including open
+    < gap (where their prefix scan of F departs from the exact DP) and
+    penalties that wrap in the lane."""
+    rng = random.Random(seed)
+    bad, total, differs = [], 0, 0
+    for it in range(5):
+        for bits in (8, 16, 32):
+            for name in ALGS + ["sw"]:
+                if it % 2:
+                    key, a = "blosum62", AA
+                    op, gp = rng.choice([(11, 1), (10, 2), (1, 3), (0, 2), (2, 5), (200, 1), (1, 1), (3, 4)])
+                else:
+                    key, a = ("ACGT", 2, -3), DNA
+                    op, gp = rng.choice([(5, 2), (0, 1), (1, 3), (2, 4), (130, 2), (1, 1)])
+                hi = rng.randint(1, 260)
+                q = rand_seq(rng, rng.randint(1, hi), a)
+                t = mutate(rng, q, a, 0.2, 0.04) if it % 3 == 0 else rand_seq(rng, rng.randint(1, hi), a)
+                m = _matrix(key)
+                sg = [0, 0, 0, 0]
+                if name.startswith("sg"):
+                    f = O.SG_CASES[name]
+                    sg = [int(bool(f & O.S1_BEG)), int(bool(f & O.S1_END)), int(bool(f & O.S2_BEG)),
+                          int(bool(f & O.S2_END))]
+                exp = O.ref_vector(name, 0, "scan", str(bits), q, t, op, gp, key)
+                o = _emulate(lanelib, 7 if name == "sw" else 6, bits, m, q, t, op, gp, sg)
+                got = {"score": int(o[0]), "end_query": int(o[1]), "end_ref": int(o[2])}
+                total += 1
+                e = dict(exp)
+                esat = int(bool(e.pop("flag") & 64))
+                if not esat and op < gp:
+                    ex = O.align(O.alg_of(name)[0], O.alg_of(name)[1], 0, q, t, op, gp, m)
+                    differs += (ex["score"], ex["end_query"], ex["end_ref"]) != (e["score"], e["end_query"],
+                                                                             e["end_ref"])
+                if esat != int(o[6]) or any(got.get(k) != v for k, v in e.items()):
+                    bad.append((name, bits, key, op, gp, q, t, exp, got))
+    assert total == 5 * 3 * (len(ALGS) + 1) and differs > 5
+    assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])

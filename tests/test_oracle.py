@@ -90,6 +90,34 @@ def test_serial_vs_reference(alg_name, stats):
 
 
 @needs_ref
+def test_serial_scan_vs_reference():
+    """The serial scan forms (src/nw_scan.c, src/sg_scan.c, src/sw_scan.c)
+    restated: equal to the reference at every penalty, and at open < gap
+    different from the serial DP for a good share of pairs."""
+    rng = random.Random(31)
+    b62 = _blosum62()
+    dna = O.Matrix.simple("ACGT", 2, -3)
+    differs = 0
+    for it in range(260):
+        alg_name = ALGS[it % len(ALGS)]
+        alg, sgf = O.alg_of(alg_name)
+        if it % 2:
+            m, mk, a = b62, "blosum62", AA
+        else:
+            m, mk, a = dna, ("ACGT", 2, -3), DNA
+        op, gp = rng.choice([(0, 1), (1, 2), (2, 5), (1, 3), (5, 2), (11, 1), (3, 3)])
+        q = rand_seq(rng, rng.randint(1, 90), a)
+        t = mutate(rng, q, a) if it % 3 == 0 else rand_seq(rng, rng.randint(1, 90), a)
+        got = O.align_scan(alg, sgf, q, t, op, gp, m)
+        exp = O.ref_serial(alg_name, 0, q, t, op, gp, mk, scan=True)
+        assert got == {k: exp[k] for k in got}, (alg_name, op, gp, q, t, got, exp)
+        differs += got != O.align(alg, sgf, 0, q, t, op, gp, m)
+        if op >= gp:
+            assert got == O.align(alg, sgf, 0, q, t, op, gp, m)
+    assert differs > 20
+
+
+@needs_ref
 def test_banded_vs_reference():
     rng = random.Random(7)
     dna = O.Matrix.simple("ACGT", 2, -3)
