@@ -184,7 +184,9 @@ int pb_cuda_trace_pairs_host(const struct pb_job *job, const pb_batch *tmpl, con
 /* Lane-exact emulation of the reference's 8/16-bit striped kernels
  * (pb_lane.cu) for the pairs listed in d_list. kind: 0 nw/sg score-only,
  * 1 nw/sg with statistics, 2 the SW statistics kernel on the FASTSTATS prefix
- * [0, o1.end_query] x [0, o1.end_ref]. Profile mode (prof, qcodes, lp, qlen)
+ * [0, o1.end_query] x [0, o1.end_ref], 3 sw score-only, 4/5 the nw/sg
+ * trace kernels' saturation flag (striped/scan), 6/7 nw/sg and sw scan
+ * score-only, 8/9 nw/sg and sw scan with statistics. Profile mode (prof, qcodes, lp, qlen)
  * or matrix mode (mat, msize, qall, qoff, qlens). */
 /* One lane-exact kernel result; valid = the width of the kernel that
  * wrote it (0: none). */

@@ -17,6 +17,9 @@
  *   sw statistics:     util/templates/sw_stats_striped_bias.c:226-637 (the
  *                      biased kernel the FASTSTATS wrapper :644-730 runs on
  *                      the prefix [0, end_query] x [0, end_ref])
+ *   scan forms:        util/templates/{nw,sg,sw}_scan.c and
+ *                      {nw,sg,sw}_stats_scan.c (open < gap, wrapped
+ *                      penalties: the prefix scan of F is not the DP's)
  *   nw/sg trace:       util/templates/{nw,sg}_trace_striped.c (the
  *                      score-only passes, lazy-F loop on >=) and
  *                      {nw,sg}_trace_scan.c (saturation flag only)
@@ -935,6 +938,242 @@ PB_LHD void scan_sw(P &v, const Problem &pr, Out &o)
     if (o.saturated) { score = 0; end_query = 0; end_ref = 0; }
     o.score = score; o.end_query = end_query; o.end_ref = end_ref;
     o.matches = o.similar = o.length = 0;
+}
+
+/* ---- nw / sg / sw scan with statistics: util/templates/nw_stats_scan.c,
+ * sg_stats_scan.c, sw_stats_scan.c (src/nw_stats_scan_avx2_256_16.c:
+ * 310-600, src/sg_stats_scan_avx2_256_16.c:615-675, src/sw_stats_scan_
+ * avx2_256_16.c:319-612). First loop: E with its counts, the diagonal H
+ * (stored in place of H) and Ht = max(E, diagonal), the running F of the
+ * gap ramp pvGapper with its length ramp pvGapperL. Prefix scan of F over
+ * the lanes, ties to the shifted value. Final loop: F from H, H = max of
+ * diagonal, E and F with counts by diagonal > F > E (SW: clamped at 0 and
+ * counts zeroed there). Checked: H and its three counts, every column, no
+ * early exit. SW keeps a copy of the column where the lane maximum grew;
+ * its end row is the smallest row of that copy holding the score, padded
+ * rows included. The first-loop F blend reads Ht's counts before the loop
+ * has set them; it can only pick them when F is still the gap ramp, whose
+ * counts never reach a result, and they start at zero here. ---- */
+template <class P, int W, bool SW>
+PB_LHD void scan_stats(P &v, const Problem &pr, Out &o)
+{
+    typedef typename P::V V;
+    constexpr int L = Lim<W>::LANES;
+    const int s1Len = pr.qlen, s2Len = pr.tlen;
+    const int segLen = (s1Len + L - 1) / L;
+    const int offset = (s1Len - 1) % segLen;
+    const int lastLane = (s1Len - 1) / segLen;
+    const int open = pr.open, gap = pr.gap;
+    const int NEG_LIMIT = wrap<W>((-open < pr.mmin ? (long long)Lim<W>::MIN + open : (long long)Lim<W>::MIN - pr.mmin) + 1);
+    const int POS_LIMIT = wrap<W>((long long)Lim<W>::MAX - pr.mmax - 1);
+    const V vGapO = v.set1(wrap<W>(open)), vGapE = v.set1(wrap<W>(gap));
+    const V vZero = v.set1(0), vOne = v.set1(1);
+    const V vNegLimit = v.set1(NEG_LIMIT), vPosLimit = v.set1(POS_LIMIT);
+    const V vNegInfFront = v.insert0(vZero, NEG_LIMIT);
+    const V vSegLenXgap = v.template adds<W>(vNegInfFront, v.shift1(v.set1(wrap<W>(-(long long)segLen * gap))));
+    const V vSegLen = v.shift1(v.set1(wrap<W>(segLen)));
+    const V vPosMask = v.lane_eq(lastLane);
+    V vSatMin = vPosLimit, vSatMax = vNegLimit;
+    V vMaxH = vNegLimit, vMaxM = vNegLimit, vMaxS = vNegLimit, vMaxL = vNegLimit, vMaxHUnit = vNegLimit;
+    int end_query = SW ? 0 : s1Len - 1, end_ref = SW ? 0 : s2Len - 1;
+    int score = NEG_LIMIT, matches = 0, similar = 0, length = 0;
+
+    typename P::Arr pe = v.arr(0, segLen), pem = v.arr(1, segLen), pes = v.arr(2, segLen), pel = v.arr(3, segLen);
+    typename P::Arr ph = v.arr(4, segLen), phm = v.arr(5, segLen), phs = v.arr(6, segLen), phl = v.arr(7, segLen);
+    typename P::Arr px = SW ? v.arr(8, segLen) : ph, pxm = SW ? v.arr(9, segLen) : ph;
+    typename P::Arr pxs = SW ? v.arr(10, segLen) : ph, pxl = SW ? v.arr(11, segLen) : ph;
+    for (int i = 0; i < segLen; ++i) {
+        v.store(phm, i, vZero); v.store(phs, i, vZero); v.store(phl, i, vZero);
+        v.store(pe, i, vNegLimit); v.store(pem, i, vZero); v.store(pes, i, vZero); v.store(pel, i, vZero);
+        if (SW) {
+            v.store(ph, i, vZero);
+        } else {
+            V h, e;
+            v.template init_he<W>(h, e, i, segLen, pr.s1_beg, open, gap);
+            v.store(ph, i, h);
+        }
+    }
+    for (int j = 0; j < s2Len; ++j) {
+        const int k_t = pr.t[j];
+        V vHp = v.shift1(v.load(ph, segLen - 1));
+        V vHpM = v.shift1(v.load(phm, segLen - 1));
+        V vHpS = v.shift1(v.load(phs, segLen - 1));
+        V vHpL = v.shift1(v.load(phl, segLen - 1));
+        if (!SW) vHp = v.insert0(vHp, v.template boundary<W>(pr, j));
+        V vHt = SW ? vZero : v.template subs<W>(vNegLimit, v.set1(gapper_at<W>(open, gap, segLen, 0)));
+        V vHtM = vZero, vHtS = vZero, vHtL = vZero;
+        V vF = vNegLimit, vFM = vZero, vFS = vZero, vFL = vZero;
+        for (int i = 0; i < segLen; ++i) {
+            const V vH = v.load(ph, i), vHM = v.load(phm, i), vHS = v.load(phs, i), vHL = v.load(phl, i);
+            V vE = v.load(pe, i), vEM = v.load(pem, i), vES = v.load(pes, i), vEL = v.load(pel, i);
+            /* pvGapperL[i]: 1, then segLen-1-i lane additions of one */
+            const V vGapperL = v.set1(lane_arith<W>((long long)segLen - i));
+            const V vE_opn = v.template subs<W>(vH, vGapO);
+            const V vE_ext = v.template subs<W>(vE, vGapE);
+            V case1 = v.cmpgt(vE_opn, vE_ext);
+            vE = v.max(vE_opn, vE_ext);
+            vEM = v.blend(vEM, vHM, case1);
+            vES = v.blend(vES, vHS, case1);
+            vEL = v.template adds<W>(v.blend(vEL, vHL, case1), vOne);
+            const V vGapper = v.template adds<W>(vHt, v.set1(gapper_at<W>(open, gap, segLen, i)));
+            case1 = v.or_(v.cmpgt(vF, vGapper), v.cmpeq(vF, vGapper));
+            vF = v.max(vF, vGapper);
+            vFM = v.blend(vHtM, vFM, case1);
+            vFS = v.blend(vHtS, vFS, case1);
+            vFL = v.blend(v.template adds<W>(vHtL, vGapperL), vFL, case1);
+            vHp = v.template adds<W>(vHp, v.template prof<W>(pr, k_t, i, segLen));
+            vHpM = v.template adds<W>(vHpM, v.template match<W>(pr, k_t, i, segLen));
+            vHpS = v.template adds<W>(vHpS, v.template similar<W>(pr, k_t, i, segLen));
+            vHpL = v.template adds<W>(vHpL, vOne);
+            case1 = v.cmpgt(vE, vHp);
+            vHt = v.max(vE, vHp);
+            vHtM = v.blend(vHpM, vEM, case1);
+            vHtS = v.blend(vHpS, vES, case1);
+            vHtL = v.blend(vHpL, vEL, case1);
+            v.store(pe, i, vE); v.store(pem, i, vEM); v.store(pes, i, vES); v.store(pel, i, vEL);
+            v.store(ph, i, vHp); v.store(phm, i, vHpM); v.store(phs, i, vHpS); v.store(phl, i, vHpL);
+            vHp = vH; vHpM = vHM; vHpS = vHS; vHpL = vHL;
+        }
+        /* pseudo prefix scan on F and H */
+        vHt = v.shift1(vHt); vHtM = v.shift1(vHtM); vHtS = v.shift1(vHtS); vHtL = v.shift1(vHtL);
+        if (!SW) vHt = v.insert0(vHt, v.template boundary<W>(pr, j + 1));
+        {
+            const V vGapper = v.template adds<W>(vHt, v.set1(gapper_at<W>(open, gap, segLen, 0)));
+            const V vGapperL = v.set1(lane_arith<W>((long long)segLen));
+            const V case1 = v.or_(v.cmpgt(vGapper, vF), v.cmpeq(vGapper, vF));
+            vF = v.max(vF, vGapper);
+            vFM = v.blend(vFM, vHtM, case1);
+            vFS = v.blend(vFS, vHtS, case1);
+            vFL = v.blend(vFL, v.template adds<W>(vHtL, vGapperL), case1);
+        }
+        for (int k = 0; k < L - 2; ++k) {
+            V vFt = v.shift1(vF);
+            const V vFtM = v.shift1(vFM), vFtS = v.shift1(vFS), vFtL = v.shift1(vFL);
+            vFt = v.template adds<W>(vFt, vSegLenXgap);
+            const V case1 = v.or_(v.cmpgt(vFt, vF), v.cmpeq(vFt, vF));
+            vF = v.max(vF, vFt);
+            vFM = v.blend(vFM, vFtM, case1);
+            vFS = v.blend(vFS, vFtS, case1);
+            vFL = v.blend(vFL, v.template adds<W>(vFtL, vSegLen), case1);
+        }
+        /* final H */
+        vF = v.shift1(vF); vFM = v.shift1(vFM); vFS = v.shift1(vFS); vFL = v.shift1(vFL);
+        vF = v.template adds<W>(vF, vNegInfFront);
+        V vH, vHM, vHS, vHL;
+        {
+            const V case1 = v.cmpgt(vF, vHt);
+            vH = v.max(vF, vHt);
+            vHM = v.blend(vHtM, vFM, case1);
+            vHS = v.blend(vHtS, vFS, case1);
+            vHL = v.blend(vHtL, vFL, case1);
+        }
+        for (int i = 0; i < segLen; ++i) {
+            const V vHq = v.load(ph, i), vHqM = v.load(phm, i), vHqS = v.load(phs, i), vHqL = v.load(phl, i);
+            const V vE = v.load(pe, i), vEM = v.load(pem, i), vES = v.load(pes, i), vEL = v.load(pel, i);
+            const V vF_opn = v.template subs<W>(vH, vGapO);
+            const V vF_ext = v.template subs<W>(vF, vGapE);
+            vF = v.max(vF_opn, vF_ext);
+            V case1 = v.cmpgt(vF_opn, vF_ext);
+            vFM = v.blend(vFM, vHM, case1);
+            vFS = v.blend(vFS, vHS, case1);
+            vFL = v.template adds<W>(v.blend(vFL, vHL, case1), vOne);
+            vH = v.max(v.max(vHq, vE), vF);
+            if (SW) vH = v.max(vH, vZero);
+            case1 = v.cmpeq(vH, vHq);
+            const V case2 = v.cmpeq(vH, vF);
+            vHM = v.blend(v.blend(vEM, vFM, case2), vHqM, case1);
+            vHS = v.blend(v.blend(vES, vFS, case2), vHqS, case1);
+            vHL = v.blend(v.blend(vEL, vFL, case2), vHqL, case1);
+            if (SW) {
+                const V case0 = v.cmpeq(vH, vZero);
+                vHM = v.blend(vHM, vZero, case0);
+                vHS = v.blend(vHS, vZero, case0);
+                vHL = v.blend(vHL, vZero, case0);
+            }
+            v.store(ph, i, vH); v.store(phm, i, vHM); v.store(phs, i, vHS); v.store(phl, i, vHL);
+            vSatMin = v.min(vSatMin, vH);
+            vSatMax = v.max(vSatMax, vH);
+            vSatMax = v.max(vSatMax, vHM);
+            vSatMax = v.max(vSatMax, vHS);
+            vSatMax = v.max(vSatMax, vHL);
+            if (SW) {
+                const V cond_max = v.cmpgt(vH, vMaxH);
+                vMaxH = v.max(vH, vMaxH);
+                vMaxM = v.blend(vMaxM, vHM, cond_max);
+                vMaxS = v.blend(vMaxS, vHS, cond_max);
+                vMaxL = v.blend(vMaxL, vHL, cond_max);
+            }
+        }
+        if (SW) {
+            if (v.any(v.cmpgt(vMaxH, vMaxHUnit))) {
+                score = v.hmax(vMaxH);
+                vMaxHUnit = v.set1(score);
+                end_ref = j;
+                for (int i = 0; i < segLen; ++i) {
+                    v.store(px, i, v.load(ph, i)); v.store(pxm, i, v.load(phm, i));
+                    v.store(pxs, i, v.load(phs, i)); v.store(pxl, i, v.load(phl, i));
+                }
+            }
+        } else {
+            const V vHo = v.load(ph, offset);
+            const V cond_max = v.cmpgt(vHo, vMaxH);
+            vMaxH = v.max(vMaxH, vHo);
+            vMaxM = v.blend(vMaxM, v.load(phm, offset), cond_max);
+            vMaxS = v.blend(vMaxS, v.load(phs, offset), cond_max);
+            vMaxL = v.blend(vMaxL, v.load(phl, offset), cond_max);
+            if (v.any(v.and_(vPosMask, cond_max))) end_ref = j;
+        }
+    }
+    if (SW) {
+        end_query = s1Len;
+        for (int i = 0; i < segLen; ++i) {
+            const V th = v.load(px, i), tm = v.load(pxm, i), ts = v.load(pxs, i), tl = v.load(pxl, i);
+            for (int l = 0; l < L; ++l) {
+                const int temp = i + l * segLen;
+                if (v.extract(th, l) == score && temp < end_query) {
+                    end_query = temp;
+                    matches = v.extract(tm, l); similar = v.extract(ts, l); length = v.extract(tl, l);
+                }
+            }
+        }
+    } else {
+        if (pr.s2_end) {
+            end_query = s1Len - 1;
+            score = v.extract(vMaxH, lastLane);
+            matches = v.extract(vMaxM, lastLane);
+            similar = v.extract(vMaxS, lastLane);
+            length = v.extract(vMaxL, lastLane);
+        }
+        if (pr.s1_end) {
+            for (int i = 0; i < segLen; ++i) {
+                const V th = v.load(ph, i), tm = v.load(phm, i), ts = v.load(phs, i), tl = v.load(phl, i);
+                for (int l = 0; l < L; ++l) {
+                    const int temp = i + l * segLen;
+                    if (temp >= s1Len) continue;
+                    const int t = v.extract(th, l);
+                    if (t > score) {
+                        score = t; end_query = temp; end_ref = s2Len - 1;
+                        matches = v.extract(tm, l); similar = v.extract(ts, l); length = v.extract(tl, l);
+                    } else if (t == score && end_ref == s2Len - 1 && temp < end_query) {
+                        end_query = temp;
+                        matches = v.extract(tm, l); similar = v.extract(ts, l); length = v.extract(tl, l);
+                    }
+                }
+            }
+        }
+        if (!pr.s1_end && !pr.s2_end) {
+            score = v.extract(v.load(ph, offset), lastLane);
+            matches = v.extract(v.load(phm, offset), lastLane);
+            similar = v.extract(v.load(phs, offset), lastLane);
+            length = v.extract(v.load(phl, offset), lastLane);
+            end_ref = s2Len - 1;
+            end_query = s1Len - 1;
+        }
+    }
+    o.saturated = v.any(v.or_(v.cmpgt(vNegLimit, vSatMin), v.cmpgt(vSatMax, vPosLimit))) ? 1 : 0;
+    if (o.saturated) { score = matches = similar = length = 0; end_query = end_ref = 0; }
+    o.score = score; o.end_query = end_query; o.end_ref = end_ref;
+    o.matches = matches; o.similar = similar; o.length = length;
 }
 
 }  // namespace lane

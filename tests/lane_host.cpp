@@ -91,14 +91,17 @@ template <int W> void run(int kind, const Problem &pr, Out &o)
     else if (kind == 4) striped_nwsg<HostVec<W>, W, true>(v, pr, o);
     else if (kind == 5) scan_nwsg_trace<HostVec<W>, W>(v, pr, o);
     else if (kind == 6) scan_nwsg<HostVec<W>, W>(v, pr, o);
-    else scan_sw<HostVec<W>, W>(v, pr, o);
+    else if (kind == 7) scan_sw<HostVec<W>, W>(v, pr, o);
+    else if (kind == 8) scan_stats<HostVec<W>, W, false>(v, pr, o);
+    else scan_stats<HostVec<W>, W, true>(v, pr, o);
 }
 
 }  // namespace
 
 /* kind: 0 nw/sg score-only, 1 nw/sg statistics, 2 sw statistics (biased),
  * 3 sw score-only, 4 nw/sg striped trace, 5 nw/sg scan trace (flag only),
- * 6 nw/sg scan score-only, 7 sw scan score-only;
+ * 6 nw/sg scan score-only, 7 sw scan score-only, 8 nw/sg scan statistics,
+ * 9 sw scan statistics;
  * sg = {s1_beg, s1_end, s2_beg, s2_end}; out = {score, end_query, end_ref,
  * matches, similar, length, saturated} */
 extern "C" int lane_host_run(int kind, int bits, const int32_t *prof, int size, int lp, const uint8_t *qcodes, int qlen,

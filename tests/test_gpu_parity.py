@@ -350,3 +350,51 @@ def test_scan_open_below_gap_and_wrapped_vs_live_reference(width):
                         bad.append((form, alg_name, width, op, gp, q, t, r, e))
     assert total == 7 * 5 * 10 * 4
     assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])
+
+
+@pytest.mark.skipif(O.ref() is None, reason="reference library not built")
+@pytest.mark.parametrize("width", ["8", "16", "32", "sat"])
+def test_stats_scan_open_below_gap_and_wrapped_vs_live_reference(width):
+    """Statistics scan kernels where the reference departs from the exact DP
+    (open < gap; a penalty above the lane maximum): the direct and profile
+    forms and batches of both kinds, run on the lane-exact statistics scan
+    kernels, against the reference's AVX2 kernels (score, ends, matches,
+    similar, length, flags)."""
+    rng = random.Random({"8": 38, "16": 316, "32": 332, "sat": 97}[width])
+    bad, total, differs = [], 0, 0
+    for alg_name in ("sw", "nw", "sg", "sg_qx", "sg_de", "sg_qb_db", "sg_qe_db"):
+        for it in range(5):
+            protein = it % 2 == 1
+            key, a = ("blosum62", AA) if protein else (("ACGT", 2, -3), DNA)
+            m = _pb_matrix(key)
+            c = [(0, 1), (1, 2), (2, 5), (1, 3)]
+            if width in ("8", "sat"):
+                c.append((200, 1) if protein else (130, 2))
+            op, gp = rng.choice(c)
+            q = rand_seq(rng, rng.randint(1, 200), a)
+            targets = [mutate(rng, q, a, 0.2, 0.04) if k % 3 == 0 else rand_seq(rng, rng.randint(1, 220), a)
+                       for k in range(10)]
+            exp = [O.ref_vector(alg_name, 1, "scan", width, q, t, op, gp, key) for t in targets]
+            got = {}
+            got["direct"] = [pb.align("parasail_%s_stats_scan_%s" % (alg_name, width), q, t, op, gp, m)
+                             for t in targets]
+            prof = pb.ProfileHandle("parasail_profile_create_stats_%s" % width, q, m)
+            got["profile"] = [pb.align_profile("parasail_%s_stats_scan_profile_%s" % (alg_name, width), prof, t,
+                                               op, gp) for t in targets]
+            got["batch"] = pb.records_to_dicts(
+                pb.batch_profile("%s_stats_scan_profile_%s" % (alg_name, width), prof, targets, op, gp), 1)
+            prof.close()
+            got["pairs"] = pb.records_to_dicts(
+                pb.batch_pairs("%s_stats_scan_%s" % (alg_name, width), m, [q] * len(targets), targets, op, gp), 1)
+            for t, e in zip(targets, exp):
+                if not e["flag"] & pb.FLAG_SATURATED and op < gp:
+                    ex = O.align(O.alg_of(alg_name)[0], O.alg_of(alg_name)[1], 1, q, t, op, gp, _o_matrix(key))
+                    differs += any(ex[k] != e[k] for k in ex if k in e)
+            for form, rs in got.items():
+                for t, r, e in zip(targets, rs, exp):
+                    total += 1
+                    if any(r.get(k) != v for k, v in e.items()):
+                        bad.append((form, alg_name, width, op, gp, q, t, r, e))
+    assert total == 7 * 5 * 10 * 4
+    assert differs >= 1
+    assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])

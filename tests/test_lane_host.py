@@ -257,3 +257,48 @@ def test_scan_kernel_emulation(lanelib, seed):
                     bad.append((name, bits, key, op, gp, q, t, exp, got))
     assert total == 5 * 3 * (len(ALGS) + 1) and differs > 5
     assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])
+
+
+@pytest.mark.parametrize("seed", [9, 10])
+def test_stats_scan_kernel_emulation(lanelib, seed):
+    """The statistics scan kernels (util/templates/nw_stats_scan.c,
+    sg_stats_scan.c, sw_stats_scan.c) restated lane by lane: score, ends,
+    matches, similar, length and the saturation flag equal the reference's
+    AVX2 kernels at 8, 16 and 32 bits, including open < gap (where their
+    prefix scan of F departs from the exact DP) and penalties that wrap in
+    the lane."""
+    rng = random.Random(seed)
+    bad, total, differs, nsat = [], 0, 0, 0
+    for it in range(4):
+        for bits in (8, 16, 32):
+            for name in ALGS + ["sw"]:
+                if it % 2:
+                    key, a = "blosum62", AA
+                    op, gp = rng.choice([(11, 1), (10, 2), (1, 3), (0, 2), (2, 5), (200, 1), (1, 1), (3, 4)])
+                else:
+                    key, a = ("ACGT", 2, -3), DNA
+                    op, gp = rng.choice([(5, 2), (0, 1), (1, 3), (2, 4), (130, 2), (1, 1)])
+                hi = rng.randint(1, 220)
+                q = rand_seq(rng, rng.randint(1, hi), a)
+                t = mutate(rng, q, a, 0.2, 0.04) if it % 3 == 0 else rand_seq(rng, rng.randint(1, hi), a)
+                m = _matrix(key)
+                sg = [0, 0, 0, 0]
+                if name.startswith("sg"):
+                    f = O.SG_CASES[name]
+                    sg = [int(bool(f & O.S1_BEG)), int(bool(f & O.S1_END)), int(bool(f & O.S2_BEG)),
+                          int(bool(f & O.S2_END))]
+                exp = O.ref_vector(name, 1, "scan", str(bits), q, t, op, gp, key)
+                o = _emulate(lanelib, 9 if name == "sw" else 8, bits, m, q, t, op, gp, sg)
+                got = {"score": int(o[0]), "end_query": int(o[1]), "end_ref": int(o[2]),
+                       "matches": int(o[3]), "similar": int(o[4]), "length": int(o[5])}
+                total += 1
+                e = dict(exp)
+                esat = int(bool(e.pop("flag") & 64))
+                nsat += esat
+                if not esat and op < gp:
+                    ex = O.align(O.alg_of(name)[0], O.alg_of(name)[1], 1, q, t, op, gp, m)
+                    differs += any(ex[k] != e[k] for k in got)
+                if esat != int(o[6]) or any(got.get(k) != v for k, v in e.items() if k in got):
+                    bad.append((name, bits, key, op, gp, q, t, exp, got))
+    assert total == 4 * 3 * (len(ALGS) + 1) and differs > 3 and nsat > 3
+    assert not bad, "%d mismatches, first: %r" % (len(bad), bad[:2])
