@@ -98,6 +98,7 @@ def lib():
         _lib.oracle_align_scan.argtypes = [ctypes.c_int] * 2 + [
             ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
             ctypes.c_int, ctypes.c_int, ctypes.POINTER(OMatrix), ctypes.POINTER(OResult)]
+        _lib.oracle_align_scan_stats.argtypes = _lib.oracle_align_scan.argtypes
         _lib.oracle_padstats.argtypes = [ctypes.c_int] * 3 + [
             ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
             ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -200,6 +201,20 @@ def align_scan(alg, sgflags, q, t, open_, gap, m):
     if rc != 0:
         raise ValueError("oracle_align_scan rejected its input")
     return {"score": r.score, "end_query": r.end_query, "end_ref": r.end_ref}
+
+
+def align_scan_stats(alg, sgflags, q, t, open_, gap, m):
+    """The reference's serial scan forms with statistics: src/nw_stats_scan.c,
+    src/sg_stats_scan.c, src/sw_stats_scan.c, which depart from align() at
+    open < gap."""
+    qc, tc = m.codes(q), m.codes(t)
+    r = OResult()
+    rc = lib().oracle_align_scan_stats(alg, sgflags, _ip(qc), len(qc), _ip(tc), len(tc), open_, gap,
+                                       ctypes.byref(m._om), ctypes.byref(r))
+    if rc != 0:
+        raise ValueError("oracle_align_scan_stats rejected its input")
+    return {"score": r.score, "end_query": r.end_query, "end_ref": r.end_ref,
+            "matches": r.matches, "similar": r.similar, "length": r.length}
 
 
 def padstats(alg, sgflags, stats, q, t, open_, gap, m, padlen):

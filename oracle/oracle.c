@@ -480,3 +480,109 @@ int oracle_align_scan(int alg, int sgflags,
     free(HB); free(HtB); free(E);
     return 0;
 }
+
+/* The reference's serial scan forms with statistics (src/nw_stats_scan.c:
+ * 162-279, src/sg_stats_scan.c:186-364, src/sw_stats_scan.c:159-283): the
+ * scan recurrence of oracle_align_scan with the counts of the chosen cell.
+ * E's counts come from H (strict >) or extend; Ht takes the diagonal's
+ * counts when diagonal >= E; the running Ft takes H(i-1)'s counts when
+ * H(i-1) > Ft(i-1) - gap (H(i-1) of this column; row -1 reads the previous
+ * column's top boundary, counts 0), else extends; H takes Ht's counts when
+ * Ht > Ft - open, on a tie F's when E beat the diagonal, else Ft's. SW
+ * clamps H at 0 with counts 0 and keeps the first maximum in column-major
+ * order; SG keeps the last row's maximum over columns (s2_end) and then the
+ * last column's rows (s1_end; with s2_end a tie in a lower row moves the
+ * end there). */
+int oracle_align_scan_stats(int alg, int sgflags,
+                            const int *s1, int s1Len, const int *s2, int s2Len,
+                            int open, int gap, const oracle_matrix_t *m,
+                            oracle_result_t *r)
+{
+    const int s1_beg = (alg == ORACLE_SG) && (sgflags & ORACLE_S1_BEG);
+    const int s1_end = (alg == ORACLE_SG) && (sgflags & ORACLE_S1_END);
+    const int s2_beg = (alg == ORACLE_SG) && (sgflags & ORACLE_S2_BEG);
+    const int s2_end = (alg == ORACLE_SG) && (sgflags & ORACLE_S2_END);
+    const int sw = alg == ORACLE_SW;
+    int64_t *buf, *H, *HM, *HS, *HL, *E, *EM, *ES, *EL, *Ht, *HtM, *HtS, *HtL;
+    char *Ex;
+    int64_t score = NEG_INF, matches = 0, similar = 0, length = 0;
+    int end_query = s1Len, end_ref = s2Len, i, j;
+    if (!s2 || s2Len <= 0 || !s1 || s1Len <= 0 || open < 0 || gap < 0 || !m || !r)
+        return -1;
+    buf = calloc((size_t)(s1Len + 1) * 12, sizeof(int64_t));
+    Ex = calloc((size_t)s1Len, 1);
+    if (!buf || !Ex) { free(buf); free(Ex); return -1; }
+    /* H, HM, HS, HL, Ht, HtM, HtS, HtL with a row -1; E, EM, ES, EL */
+    H = buf + 1; HM = H + (s1Len + 1); HS = HM + (s1Len + 1); HL = HS + (s1Len + 1);
+    Ht = HL + (s1Len + 1); HtM = Ht + (s1Len + 1); HtS = HtM + (s1Len + 1); HtL = HtS + (s1Len + 1);
+    E = HtL + s1Len; EM = E + (s1Len + 1); ES = EM + (s1Len + 1); EL = ES + (s1Len + 1);
+    H[-1] = 0;
+    for (i = 0; i < s1Len; ++i) {
+        H[i] = (sw || s1_beg) ? 0 : -(int64_t)open - (int64_t)i * gap;
+        E[i] = NEG_INF;
+    }
+    for (j = 0; j < s2Len; ++j) {
+        int64_t Ft = NEG_INF, FtM = 0, FtS = 0, FtL = 0;
+        const int64_t top = (sw || s2_beg) ? 0 : -(int64_t)open - (int64_t)j * gap;
+        for (i = 0; i < s1Len; ++i) {
+            const int64_t eo = H[i] - open, ee = E[i] - gap;
+            if (eo > ee) { E[i] = eo; EM[i] = HM[i]; ES[i] = HS[i]; EL[i] = HL[i]; }
+            else E[i] = ee;
+            EL[i] += 1;
+        }
+        Ht[-1] = top;
+        for (i = 0; i < s1Len; ++i) {
+            const int64_t sc = subst(m, s1, i, s2[j]);
+            const int64_t hd = H[i - 1] + sc;
+            Ex[i] = E[i] > hd;
+            if (hd >= E[i]) {
+                Ht[i] = hd; HtM[i] = HM[i - 1] + (s1[i] == s2[j]); HtS[i] = HS[i - 1] + (sc > 0);
+                HtL[i] = HL[i - 1] + 1;
+            } else {
+                Ht[i] = E[i]; HtM[i] = EM[i]; HtS[i] = ES[i]; HtL[i] = EL[i];
+            }
+        }
+        for (i = 0; i < s1Len; ++i) {
+            const int64_t fe = Ft - gap;
+            int64_t fo;
+            Ft = Ht[i - 1] >= fe ? Ht[i - 1] : fe;
+            fo = Ft - open;
+            if (H[i - 1] > fe) { FtM = HM[i - 1]; FtS = HS[i - 1]; FtL = HL[i - 1]; }
+            FtL += 1;
+            if (Ht[i] > fo || (Ht[i] == fo && !Ex[i])) {
+                H[i] = Ht[i] > fo ? Ht[i] : fo; HM[i] = HtM[i]; HS[i] = HtS[i]; HL[i] = HtL[i];
+            } else {
+                H[i] = fo; HM[i] = FtM; HS[i] = FtS; HL[i] = FtL;
+            }
+            if (sw) {
+                if (H[i] <= 0) { H[i] = 0; HM[i] = HS[i] = HL[i] = 0; }
+                if (H[i] > score) {
+                    score = H[i]; matches = HM[i]; similar = HS[i]; length = HL[i];
+                    end_query = i; end_ref = j;
+                }
+            }
+        }
+        H[-1] = top;
+        if (s2_end && H[s1Len - 1] > score) {
+            score = H[s1Len - 1]; matches = HM[s1Len - 1]; similar = HS[s1Len - 1]; length = HL[s1Len - 1];
+            end_query = s1Len - 1; end_ref = j;
+        }
+    }
+    if (s1_end) {
+        for (i = 0; i < s1Len; ++i) {
+            if (H[i] > score || (s2_end && H[i] == score && end_ref == s2Len - 1 && i < end_query)) {
+                score = H[i]; matches = HM[i]; similar = HS[i]; length = HL[i];
+                end_query = i; end_ref = s2Len - 1;
+            }
+        }
+    }
+    if (!sw && !s1_end && !s2_end) {
+        score = H[s1Len - 1]; matches = HM[s1Len - 1]; similar = HS[s1Len - 1]; length = HL[s1Len - 1];
+        end_query = s1Len - 1; end_ref = s2Len - 1;
+    }
+    memset(r, 0, sizeof *r);
+    r->score = (int)score; r->end_query = end_query; r->end_ref = end_ref;
+    r->matches = (int)matches; r->similar = (int)similar; r->length = (int)length;
+    free(buf); free(Ex);
+    return 0;
+}

@@ -66,6 +66,15 @@ int oracle_align_scan(int alg, int sgflags,
                       int open, int gap, const oracle_matrix_t *m,
                       oracle_result_t *r);
 
+/* The reference's serial scan forms with statistics (src/nw_stats_scan.c,
+ * src/sg_stats_scan.c, src/sw_stats_scan.c): the recurrence of
+ * oracle_align_scan with the counts of the chosen cell. Returns 0 on
+ * success. */
+int oracle_align_scan_stats(int alg, int sgflags,
+                            const int *s1, int s1Len, const int *s2, int s2Len,
+                            int open, int gap, const oracle_matrix_t *m,
+                            oracle_result_t *r);
+
 /* Same recurrence over padLen >= s1Len query rows; fills *ps. */
 int oracle_padstats(int alg, int sgflags, int stats,
                     const int *s1, int s1Len, int padLen,

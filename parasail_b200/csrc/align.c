@@ -102,9 +102,8 @@ int pb_run_job_pair(const pb_device_profile *dp, const pb_job *job, const uint8_
     const int pad = (job->bits < 0 || (m->alg == PB_SW && !m->stats)) ? 0
                   : (job->bits == 0 || job->bits == 8) ? 32 : job->bits == 16 ? 16 : 8;
     /* the serial scan forms at open < gap, where their vertical gap departs
-     * from the serial DP's (score only) */
-    const int scan_vgap = job->bits < 0 && (job->base_flags & PARASAIL_FLAG_NOVEC_SCAN) && !m->stats
-                        && m->open < m->gap;
+     * from the serial DP's (with or without statistics) */
+    const int scan_vgap = job->bits < 0 && (job->base_flags & PARASAIL_FLAG_NOVEC_SCAN) && m->open < m->gap;
     int rc;
     memset(&o2, 0, sizeof o2);
     if (score_only_sw && job->bits >= 0)

@@ -659,7 +659,7 @@ int pb_cuda_exact_single(const pb_batch *tmpl, const uint8_t *h_codes, int tlen,
     p.mat = nullptr; p.msize = 0; p.qall = nullptr; p.qoff = nullptr; p.qlen = nullptr;
     p.order = reinterpret_cast<const int *>(d + o_ints);
     p.nt = 0;
-    p.scan_vgap = tmpl->scan_vgap && !tmpl->stats;
+    p.scan_vgap = tmpl->scan_vgap;
     const long long cells = (long long)ql * tl;
     if (ql >= 32 || (ql >= 8 && cells >= (1LL << 14))) pb::launch_exact_warp(p, tmpl->alg, tmpl->stats != 0, 1, st);
     else pb::launch_exact(p, tmpl->alg, tmpl->stats != 0, st);

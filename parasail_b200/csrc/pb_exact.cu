@@ -42,11 +42,17 @@ static void launch_alg(const ExactParams &p, cudaStream_t st)
 void launch_exact(const ExactParams &p, int alg, bool stats, cudaStream_t st)
 {
     if (p.npairs <= 0) return;
-    if (p.scan_vgap && !stats) {
+    if (p.scan_vgap) {
         /* the serial scan forms' vertical gap */
-        if (alg == PB_SW) launch_alg<PB_SW, false, true>(p, st);
-        else if (alg == PB_NW) launch_alg<PB_NW, false, true>(p, st);
-        else launch_alg<PB_SG, false, true>(p, st);
+        if (stats) {
+            if (alg == PB_SW) launch_alg<PB_SW, true, true>(p, st);
+            else if (alg == PB_NW) launch_alg<PB_NW, true, true>(p, st);
+            else launch_alg<PB_SG, true, true>(p, st);
+        } else {
+            if (alg == PB_SW) launch_alg<PB_SW, false, true>(p, st);
+            else if (alg == PB_NW) launch_alg<PB_NW, false, true>(p, st);
+            else launch_alg<PB_SG, false, true>(p, st);
+        }
         return;
     }
     if (alg == PB_SW) { if (stats) launch_alg<PB_SW, true>(p, st); else launch_alg<PB_SW, false>(p, st); }

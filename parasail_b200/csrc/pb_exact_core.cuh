@@ -48,16 +48,21 @@ __host__ __device__ __forceinline__ int left_h(int i, int open, int gap, int sgf
     return -open - i * gap;
 }
 
-/* SCANF (score only): the vertical gap of the reference's serial scan forms
+/* SCANF: the vertical gap of the reference's serial scan forms
  * (src/nw_scan.c:128-146, src/sg_scan.c:155-173, src/sw_scan.c:146-152),
  * F(i) = max(Ht(i-1) - open, F(i-1) - gap) with Ht = max(diagonal, E): a
  * vertical gap is not reopened from a vertical gap, which differs from the
  * serial DP at open < gap. The kernel then carries in fu the F of the next
- * row instead of the F of the row above. */
+ * row instead of the F of the row above.
+ * With statistics (src/nw_stats_scan.c:215-228) F takes H(i-1)'s counts
+ * when H(i-1) - open > F(i-1) - gap. Given fu = F(i), that test is
+ * H(i-1) - open > fu, except on a tie, where it holds exactly when F(i)
+ * came from Ht(i-1) - open strictly; that one bit travels with the carried
+ * F length as its complement (~len < 0), so strip buffers keep their size.
+ * Row 0 reads the bit set (the reference's F starts at -infinity). */
 template <int ALG, bool STATS, int R, bool SCANF = false>
 __host__ __device__ __forceinline__ void exact_pair(const ExactParams &p, const int k)
 {
-    static_assert(!(SCANF && STATS), "the scan vertical gap is score-only");
     const int pid = p.order ? p.order[k] : k;          /* output slot */
     const int ti = p.nt ? pid % p.nt : pid;            /* target (and per-pair query) index */
 
@@ -121,6 +126,7 @@ __host__ __device__ __forceinline__ void exact_pair(const ExactParams &p, const 
             if (r0 == 0) {
                 hu = top_h<ALG>(j, open, gap, sgf);
                 fu = SCANF ? hu - open : NEG_INF;
+                if (SCANF && STATS) fuL = ~0;
             } else {
                 hu = bj[0];
                 fu = bj[1];
@@ -160,10 +166,11 @@ __host__ __device__ __forceinline__ void exact_pair(const ExactParams &p, const 
                 if (STATS) {
                     /* src/sw_stats.c:205-237: gap-source choice by strict >,
                      * then cell choice diagonal > F > E, SW resets at H <= 0 */
-                    const bool fo = f_opn > f_ext;
+                    const bool fb = SCANF && fuL < 0;
+                    const bool fo = SCANF ? (f_opn > fu || (f_opn == fu && fb)) : f_opn > f_ext;
                     fM = fo ? huM : fuM;
                     fS = fo ? huS : fuS;
-                    fL = (fo ? huL : fuL) + 1;
+                    fL = (fo ? huL : (fb ? ~fuL : fuL)) + 1;
                     const bool eo = e_opn > e_ext;
                     const int eM = eo ? HlM[r] : EM[r];
                     const int eS = eo ? HlS[r] : ES[r];
@@ -223,7 +230,10 @@ __host__ __device__ __forceinline__ void exact_pair(const ExactParams &p, const 
                 Hl[r] = hn;
                 if (STATS) { HlM[r] = hM; HlS[r] = hS; HlL[r] = hL; }
                 hu = hn; fu = SCANF ? max(ht - open, fn - gap) : fn;
-                if (STATS) { huM = hM; huS = hS; huL = hL; fuM = fM; fuS = fS; fuL = fL; }
+                if (STATS) {
+                    huM = hM; huS = hS; huL = hL; fuM = fM; fuS = fS;
+                    fuL = (SCANF && ht - open > fn - gap) ? ~fL : fL;
+                }
             }
             if (r0 + R < nrows) {
                 bj[0] = hu; bj[1] = fu;

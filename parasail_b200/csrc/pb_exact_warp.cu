@@ -58,7 +58,6 @@ template <int ALG, bool STATS, bool PAIRS, bool SCANF>
 __global__ void __launch_bounds__(EW_WARPS * 32)
 k_exact_warp(ExactParams p, int nitems)
 {
-    static_assert(!(SCANF && STATS), "the scan vertical gap is score-only");
     constexpr int EW_R = EwRows<STATS>::value;
     const int lane = threadIdx.x & 31;
     const int item = blockIdx.x * EW_WARPS + (threadIdx.x >> 5);
@@ -142,6 +141,7 @@ k_exact_warp(ExactParams p, int nitems)
                 if (r0 == 0) {
                     up_h = top_h<ALG>(j, open, gap, sgf); up_f = SCANF ? up_h - open : NEG_INF;
                     huM = huS = huL = fuM = fuS = fuL = 0;
+                    if (SCANF && STATS) fuL = ~0;   /* F of row 0 from the top (exact_pair's SCANF) */
                 } else if (STATS) {
                     const int4 a = buf4[2 * j], b = buf4[2 * j + 1];
                     up_h = a.x; up_f = a.y; huM = a.z; huS = a.w; huL = b.x; fuM = b.y; fuS = b.z; fuL = b.w;
@@ -174,10 +174,11 @@ k_exact_warp(ExactParams p, int nitems)
                 if (STATS) {
                     /* src/sw_stats.c:205-237: gap-source choice by strict >,
                      * then cell choice diagonal > F > E, SW resets at H <= 0 */
-                    const bool fo = f_opn > f_ext;
+                    const bool fb = SCANF && fuL < 0;
+                    const bool fo = SCANF ? (f_opn > fu || (f_opn == fu && fb)) : f_opn > f_ext;
                     fM = fo ? huM : fuM;
                     fS = fo ? huS : fuS;
-                    fL = (fo ? huL : fuL) + 1;
+                    fL = (fo ? huL : (fb ? ~fuL : fuL)) + 1;
                     const bool eo = e_opn > e_ext;
                     const int eM = eo ? HlM[r] : EM[r];
                     const int eS = eo ? HlS[r] : ES[r];
@@ -235,7 +236,8 @@ k_exact_warp(ExactParams p, int nitems)
                 if (STATS) {
                     hdM = HlM[r]; hdS = HlS[r]; hdL = HlL[r];
                     HlM[r] = hM; HlS[r] = hS; HlL[r] = hL;
-                    huM = hM; huS = hS; huL = hL; fuM = fM; fuS = fS; fuL = fL;
+                    huM = hM; huS = hS; huL = hL; fuM = fM; fuS = fS;
+                    fuL = (SCANF && ht - open > fn - gap) ? ~fL : fL;
                 }
             }
             sh_h = hu;
@@ -330,11 +332,11 @@ void launch_exact_warp(const ExactParams &p, int alg, bool stats, int nitems, cu
 {
     if (nitems <= 0) return;
     const bool pairs = p.mat != nullptr;
-    if (stats) {
-        if (pairs) launch_ew<true, true>(p, alg, nitems, st); else launch_ew<true, false>(p, alg, nitems, st);
-    } else if (p.scan_vgap) {
+    if (p.scan_vgap) {
         /* the serial scan forms' vertical gap, one query per call */
-        launch_ew<false, false, true>(p, alg, nitems, st);
+        if (stats) launch_ew<true, false, true>(p, alg, nitems, st); else launch_ew<false, false, true>(p, alg, nitems, st);
+    } else if (stats) {
+        if (pairs) launch_ew<true, true>(p, alg, nitems, st); else launch_ew<true, false>(p, alg, nitems, st);
     } else {
         if (pairs) launch_ew<false, true>(p, alg, nitems, st); else launch_ew<false, false>(p, alg, nitems, st);
     }

@@ -44,8 +44,8 @@ struct ExactParams {
     /* > 0: pair index = query * nt + target, every query of profs against
      * the same nt targets (outputs query-major); 0: one pair per target */
     int nt = 0;
-    /* 1: the vertical gap of the reference's serial scan forms (score
-     * only; exact_pair's SCANF) */
+    /* 1: the vertical gap of the reference's serial scan forms (with or
+     * without statistics; exact_pair's SCANF) */
     int scan_vgap = 0;
 };
 

@@ -106,6 +106,36 @@ def test_serial_scan_open_below_gap_vs_oracle(alg_name):
     assert differs >= 1
 
 
+@pytest.mark.parametrize("alg_name", ["sw", "nw", "sg", "sg_qx", "sg_qe_db", "sg_qb_de", "sg_dx"])
+def test_serial_stats_scan_open_below_gap_vs_oracle(alg_name):
+    """parasail_*_stats_scan at open < gap (the vertical gap of the
+    reference's serial scan forms, with the counts of the cells it chooses):
+    against the oracle's restatement (and the live reference when it was
+    built), for queries on the thread kernel (< 32 rows), the warp kernel and
+    several warp passes."""
+    rng = random.Random(len(alg_name) * 7919)
+    alg, sgf = O.alg_of(alg_name)
+    differs = 0
+    for it in range(12):
+        key, a = ("blosum62", AA) if it % 2 else (("ACGT", 2, -3), DNA)
+        op, gp = rng.choice([(0, 1), (1, 2), (2, 5), (1, 3)])
+        ql = rng.choice([rng.randint(1, 31), rng.randint(32, 300), rng.randint(300, 1100)])
+        q = rand_seq(rng, ql, a)
+        t = mutate(rng, q, a) if it % 3 == 0 else rand_seq(rng, rng.randint(1, 900), a)
+        got = pb.align("parasail_%s_stats_scan" % alg_name, q, t, op, gp, _pb_matrix(key))
+        exp = O.align_scan_stats(alg, sgf, q, t, op, gp, _o_matrix(key))
+        assert {k: got[k] for k in exp} == exp, (alg_name, op, gp, len(q), len(t), got, exp)
+        assert got["flag"] & pb.FLAG_NOVEC_SCAN
+        if O.ref() is not None:
+            r = O.ref_serial(alg_name, 1, q, t, op, gp, key, scan=True)
+            assert {k: r[k] for k in exp} == exp
+        differs += exp != O.align(alg, sgf, 1, q, t, op, gp, _o_matrix(key))
+        # the plain serial statistics form keeps the serial DP
+        assert {k: v for k, v in pb.align("parasail_%s_stats" % alg_name, q, t, op, gp, _pb_matrix(key)).items()
+                if k in exp} == O.align(alg, sgf, 1, q, t, op, gp, _o_matrix(key))
+    assert differs >= 1
+
+
 def _vector_cases():
     return json.load(open(os.path.join(GOLDEN, "vector_golden.json")))["cases"]
 

@@ -118,6 +118,36 @@ def test_serial_scan_vs_reference():
 
 
 @needs_ref
+def test_serial_stats_scan_vs_reference():
+    """The serial scan forms with statistics (src/nw_stats_scan.c,
+    src/sg_stats_scan.c, src/sw_stats_scan.c) restated: score, ends and
+    counts equal the reference at every penalty; at open >= gap they equal
+    the serial statistics DP, at open < gap they differ for a good share of
+    pairs."""
+    rng = random.Random(37)
+    b62 = _blosum62()
+    dna = O.Matrix.simple("ACGT", 2, -3)
+    differs = 0
+    for it in range(260):
+        alg_name = ALGS[it % len(ALGS)]
+        alg, sgf = O.alg_of(alg_name)
+        if it % 2:
+            m, mk, a = b62, "blosum62", AA
+        else:
+            m, mk, a = dna, ("ACGT", 2, -3), DNA
+        op, gp = rng.choice([(0, 1), (1, 2), (2, 5), (1, 3), (5, 2), (11, 1), (3, 3)])
+        q = rand_seq(rng, rng.randint(1, 90), a)
+        t = mutate(rng, q, a) if it % 3 == 0 else rand_seq(rng, rng.randint(1, 90), a)
+        got = O.align_scan_stats(alg, sgf, q, t, op, gp, m)
+        exp = O.ref_serial(alg_name, 1, q, t, op, gp, mk, scan=True)
+        assert got == {k: exp[k] for k in got}, (alg_name, op, gp, q, t, got, exp)
+        differs += got != O.align(alg, sgf, 1, q, t, op, gp, m)
+        if op >= gp:
+            assert got == O.align(alg, sgf, 1, q, t, op, gp, m)
+    assert differs > 20
+
+
+@needs_ref
 def test_banded_vs_reference():
     rng = random.Random(7)
     dna = O.Matrix.simple("ACGT", 2, -3)
