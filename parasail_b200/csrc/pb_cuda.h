@@ -186,7 +186,7 @@ int pb_cuda_trace_pairs_host(const struct pb_job *job, const pb_batch *tmpl, con
  * 1 nw/sg with statistics, 2 the SW statistics kernel on the FASTSTATS prefix
  * [0, o1.end_query] x [0, o1.end_ref], 3 sw score-only, 4/5 the nw/sg
  * trace kernels' saturation flag (striped/scan), 6/7 nw/sg and sw scan
- * score-only, 8/9 nw/sg and sw scan with statistics. Profile mode (prof, qcodes, lp, qlen)
+ * score-only, 8 nw/sg scan with statistics. Profile mode (prof, qcodes, lp, qlen)
  * or matrix mode (mat, msize, qall, qoff, qlens). */
 /* One lane-exact kernel result; valid = the width of the kernel that
  * wrote it (0: none). */

@@ -100,8 +100,7 @@ template <int W> struct WarpVec {
 struct LaneJob {
     int kind;                                  /* 0 nw/sg, 1 nw/sg stats, 2 sw stats prefix, 3 sw,
                                                   4 nw/sg striped trace, 5 nw/sg scan trace,
-                                                  6 nw/sg scan, 7 sw scan, 8 nw/sg scan stats,
-                                                  9 sw scan stats */
+                                                  6 nw/sg scan, 7 sw scan, 8 nw/sg scan stats */
     int open, gap, mmax, mmin;
     int s1_beg, s1_end, s2_beg, s2_end;
     /* profile mode */
@@ -117,8 +116,7 @@ struct LaneJob {
 
 PB_LHD int lane_narr(int kind)
 {
-    return kind == 0 || (kind >= 4 && kind <= 6) ? 3 : kind == 1 || kind == 9 ? 12 : kind == 2 ? 16
-         : kind == 8 ? 8 : 4;
+    return kind == 0 || (kind >= 4 && kind <= 6) ? 3 : kind == 1 ? 12 : kind == 2 ? 16 : kind == 8 ? 8 : 4;
 }
 
 constexpr int LANE_THREADS = 256;
@@ -159,7 +157,6 @@ __global__ void __launch_bounds__(LANE_THREADS) k_lane(LaneJob J)
         else if (J.kind == 6) scan_nwsg<WarpVec<W>, W>(v, pr, o);
         else if (J.kind == 7) scan_sw<WarpVec<W>, W>(v, pr, o);
         else if (J.kind == 8) scan_stats<WarpVec<W>, W, false>(v, pr, o);
-        else if (J.kind == 9) scan_stats<WarpVec<W>, W, true>(v, pr, o);
         else if (W != 32) striped_sw_stats_bias<WarpVec<W>, W>(v, pr, o);
         if (lane == 0) {
             pb_lane_res r;

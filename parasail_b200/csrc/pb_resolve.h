@@ -176,11 +176,13 @@ enum { PB_REC_FALLBACK = 1 };
  * the FASTSTATS wrapper are not emulated in these regimes. The scan
  * kernels, score-only and statistics alike, depart from the exact DP at
  * open < gap (their prefix scan of F assumes F - gap >= F - open) and with
- * a wrapped penalty, and agree with it at open == gap. */
+ * a wrapped penalty, and agree with it at open == gap. The SW statistics
+ * scan kernel is not emulated in these regimes (its restatement,
+ * pb_lane.cuh scan_stats<SW>, is pinned on the host only). */
 PB_HD static inline int pb_lane_forced(const pb_mode *m, int bits)
 {
     const int wrapped = bits < 32 && (m->open > int_max_w(bits) || m->gap > int_max_w(bits));
-    if (!m->striped) return m->open < m->gap || wrapped;
+    if (!m->striped) return (!m->stats || m->alg != PB_SW) && (m->open < m->gap || wrapped);
     if (m->alg == PB_SW && m->stats) return 0;
     if (wrapped) return 1;
     return m->stats ? m->open < m->gap : m->open <= m->gap;
@@ -200,7 +202,7 @@ PB_HD static inline int pb_lane_applies(const pb_mode *m, int bits)
 /* lane kernel kind for a mode (pb_lane_args.kind) */
 PB_HD static inline int pb_lane_kind(const pb_mode *m)
 {
-    if (!m->striped) return m->alg == PB_SW ? (m->stats ? 9 : 7) : (m->stats ? 8 : 6);   /* scan */
+    if (!m->striped) return m->alg == PB_SW ? 7 : (m->stats ? 8 : 6);   /* scan */
     return m->alg == PB_SW ? (m->stats ? 2 : 3) : (m->stats ? 1 : 0);
 }
 
