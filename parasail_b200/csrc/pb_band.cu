@@ -505,14 +505,18 @@ extern "C" int pb_cuda_band_forward(const pb_band_model *m, int n, const float *
 extern "C" int pb_cuda_band_gradients(const pb_band_model *m, int n, const float *d_x, const float *d_target,
                                       float tau, float *d_gw, float *d_gb, float *loss_out)
 {
-    float *h1, *h2, *y, *dy, *d2, *d1, *loss;
-    cudaMallocAsync((void **)&h1, sizeof(float) * n * pb::MLP_H, 0);
-    cudaMallocAsync((void **)&h2, sizeof(float) * n * pb::MLP_H, 0);
-    cudaMallocAsync((void **)&d1, sizeof(float) * n * pb::MLP_H, 0);
-    cudaMallocAsync((void **)&d2, sizeof(float) * n * pb::MLP_H, 0);
-    cudaMallocAsync((void **)&y, sizeof(float) * n * pb::MLP_OUT, 0);
-    cudaMallocAsync((void **)&dy, sizeof(float) * n * pb::MLP_OUT, 0);
-    cudaMallocAsync((void **)&loss, sizeof(float) * n, 0);
+    if (n <= 0) return -1;
+    float *h1 = nullptr, *h2 = nullptr, *y = nullptr, *dy = nullptr, *d2 = nullptr, *d1 = nullptr, *loss = nullptr;
+    float **const bufs[7] = {&h1, &h2, &d1, &d2, &y, &dy, &loss};
+    const size_t per[7] = {pb::MLP_H, pb::MLP_H, pb::MLP_H, pb::MLP_H, pb::MLP_OUT, pb::MLP_OUT, 1};
+    /* every buffer checked before any kernel writes through it */
+    for (int b = 0; b < 7; ++b) {
+        if (cudaMallocAsync((void **)bufs[b], sizeof(float) * n * per[b], 0) != cudaSuccess) {
+            for (int c = 0; c < b; ++c) cudaFreeAsync(*bufs[c], 0);
+            cudaGetLastError();
+            return -1;
+        }
+    }
     const pb::MlpWeights w = weights_of(m);
     pb::k_mlp_fwd<<<n, pb::MLP_H>>>(n, d_x, w, h1, h2, y);
     pb::k_mlp_delta<<<n, pb::MLP_H>>>(n, y, d_target, tau, w, h1, h2, dy, d2, d1, loss);
@@ -564,7 +568,8 @@ extern "C" int pb_cuda_band_certify(int npairs, int a, int open, int ext, const 
 {
     pb::CostModel c = {a, open, ext};
     int *d_fail = nullptr;
-    cudaMallocAsync((void **)&d_fail, sizeof(int), 0);
+    if (npairs <= 0) { if (h_failures) *h_failures = 0; return 0; }
+    if (cudaMallocAsync((void **)&d_fail, sizeof(int), 0) != cudaSuccess) { cudaGetLastError(); return -1; }
     cudaMemset(d_fail, 0, sizeof(int));
     pb::k_certify<<<(npairs + 255) / 256, 256>>>(npairs, c, d_qlen, d_tlen, d_lo, d_hi, d_score, d_cert, d_fail);
     pb_diag_count_launch(1);
@@ -598,10 +603,17 @@ extern "C" int pb_cuda_band_tune(pb_band_model *m, int n, const float *d_x, cons
     float *y = nullptr;
     int *lo = nullptr, *hi = nullptr;
     unsigned long long *cost = nullptr;
-    cudaMallocAsync((void **)&y, sizeof(float) * n * pb::MLP_OUT, 0);
-    cudaMallocAsync((void **)&lo, sizeof(int) * n, 0);
-    cudaMallocAsync((void **)&hi, sizeof(int) * n, 0);
-    cudaMallocAsync((void **)&cost, sizeof(unsigned long long), 0);
+    if (cudaMallocAsync((void **)&y, sizeof(float) * n * pb::MLP_OUT, 0) != cudaSuccess ||
+        cudaMallocAsync((void **)&lo, sizeof(int) * n, 0) != cudaSuccess ||
+        cudaMallocAsync((void **)&hi, sizeof(int) * n, 0) != cudaSuccess ||
+        cudaMallocAsync((void **)&cost, sizeof(unsigned long long), 0) != cudaSuccess) {
+        /* nothing has been launched: free what was allocated */
+        if (y) cudaFreeAsync(y, 0);
+        if (lo) cudaFreeAsync(lo, 0);
+        if (hi) cudaFreeAsync(hi, 0);
+        cudaGetLastError();
+        return -1;
+    }
     int rc = pb_cuda_band_forward(m, n, d_x, nullptr, nullptr, y);
     unsigned long long best = ~0ull;
     float bw = m->widen;

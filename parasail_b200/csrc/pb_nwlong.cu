@@ -526,13 +526,29 @@ static int nw_long_impl(int npairs, int open, int gap, const int32_t *h_mat, int
             break;
         }
     }
-    cudaMallocAsync((void **)&d_mat, hm.size(), st);
+    /* the work-queue buffers, each checked before any launch writes
+     * through it; a failure frees what was allocated and ends the call */
+    auto give_up = [&]() {
+        if (d_mat) cudaFreeAsync(d_mat, st);
+        if (idx) cudaFreeAsync(idx, st);
+        if (order) cudaFreeAsync(order, st);
+        if (keys) cudaFreeAsync(keys, st);
+        if (keys_sorted) cudaFreeAsync(keys_sorted, st);
+        if (counter) cudaFreeAsync(counter, st);
+        if (tmp) cudaFreeAsync(tmp, st);
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+        cudaGetLastError();
+        return -1;
+    };
+    if (cudaMallocAsync((void **)&d_mat, hm.size(), st) != cudaSuccess ||
+        cudaMallocAsync((void **)&idx, sizeof(int) * npairs, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&order, sizeof(int) * npairs, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&keys, sizeof(unsigned long long) * npairs, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&keys_sorted, sizeof(unsigned long long) * npairs, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&counter, sizeof(int) * 32, st) != cudaSuccess)
+        return give_up();
     cudaMemcpyAsync(d_mat, hm.data(), hm.size(), cudaMemcpyHostToDevice, st);
-    cudaMallocAsync((void **)&idx, sizeof(int) * npairs, st);
-    cudaMallocAsync((void **)&order, sizeof(int) * npairs, st);
-    cudaMallocAsync((void **)&keys, sizeof(unsigned long long) * npairs, st);
-    cudaMallocAsync((void **)&keys_sorted, sizeof(unsigned long long) * npairs, st);
-    cudaMallocAsync((void **)&counter, sizeof(int) * 32, st);
     cudaMemsetAsync(counter, 0, sizeof(int) * 32, st);
     /* counter[0..7]: pair counters of the class launches; [8..9]: total
      * work; [16..23]: pairs per class */
@@ -544,7 +560,7 @@ static int nw_long_impl(int npairs, int open, int gap, const int32_t *h_mat, int
                                                            counter + 16);
     pb_diag_count_launch(3);
     cub::DeviceRadixSort::SortPairsDescending(nullptr, tmpb, keys, keys_sorted, idx, order, npairs, 0, 64, st);
-    cudaMallocAsync(&tmp, tmpb, st);
+    if (cudaMallocAsync(&tmp, tmpb, st) != cudaSuccess) return give_up();
     cub::DeviceRadixSort::SortPairsDescending(tmp, tmpb, keys, keys_sorted, idx, order, npairs, 0, 64, st);
     /* pairs sorted by class, largest first; one launch per class, each on
      * its own stream, the largest teams first; they never wait on each other */
@@ -584,9 +600,9 @@ static int nw_long_impl(int npairs, int open, int gap, const int32_t *h_mat, int
     int rc = 0, herr = 0;
     cudaStream_t sc[pb::NWL_CLASSES] = {};
     cudaEvent_t ev = nullptr, evc[pb::NWL_CLASSES] = {};
-    cudaMallocAsync((void **)&d_err, sizeof(int), st);
-    cudaMemsetAsync(d_err, 0, sizeof(int), st);
-    if (cudaMallocAsync((void **)&scratch, sizeof(int2) * (size_t)(maxlen + 1) * blocks * pb::NWL_WARPS, st) != cudaSuccess ||
+    if (cudaMallocAsync((void **)&d_err, sizeof(int), st) != cudaSuccess) rc = -1;
+    else cudaMemsetAsync(d_err, 0, sizeof(int), st);
+    if (rc != 0 || cudaMallocAsync((void **)&scratch, sizeof(int2) * (size_t)(maxlen + 1) * blocks * pb::NWL_WARPS, st) != cudaSuccess ||
         cudaMallocAsync((void **)&prog, sizeof(long long) * (size_t)blocks * pb::NWL_WARPS, st) != cudaSuccess ||
         cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
         rc = -1;
@@ -637,7 +653,7 @@ static int nw_long_impl(int npairs, int open, int gap, const int32_t *h_mat, int
     cudaFreeAsync(tmp, st);
     if (scratch) cudaFreeAsync(scratch, st);
     if (prog) cudaFreeAsync(prog, st);
-    cudaFreeAsync(d_err, st);
+    if (d_err) cudaFreeAsync(d_err, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
     for (int c = 0; c < pb::NWL_CLASSES; ++c) {
         if (sc[c]) cudaStreamDestroy(sc[c]);

@@ -650,22 +650,34 @@ static int sw16_prepare(const pb_batch *b, pb_pair_out *d_out_all, size_t prof_b
     /* targets sorted by length, descending */
     int *keys_sorted = nullptr, *idx = nullptr, *order = nullptr, *counter = nullptr;
     void *tmp = nullptr;
+    int8_t *prof_all = nullptr;
+    pb::Sw16Task *d_tasks = nullptr;
+    pb::Sw16Query *d_q = nullptr;
     size_t tmp_sort = 0;
-    cudaMallocAsync((void **)&keys_sorted, sizeof(int) * n, st);
-    cudaMallocAsync((void **)&idx, sizeof(int) * n, st);
-    cudaMallocAsync((void **)&order, sizeof(int) * n, st);
-    cudaMallocAsync((void **)&counter, sizeof(int) * 4, st);
+    /* an allocation that fails ends the call before anything writes
+     * through it, releasing what was allocated */
+    auto give_up = [&]() {
+        void *owned[10] = {keys_sorted, idx, order, counter, tmp, prof_all, d_tasks, d_q, nullptr, nullptr};
+        memcpy(pr->bufs, owned, sizeof owned);
+        sw16_release(pr, st);
+        cudaGetLastError();
+        return -1;
+    };
+    if (cudaMallocAsync((void **)&keys_sorted, sizeof(int) * n, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&idx, sizeof(int) * n, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&order, sizeof(int) * n, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&counter, sizeof(int) * 4, st) != cudaSuccess)
+        return give_up();
     k_iota<<<(n + 255) / 256, 256, 0, st>>>(idx, n);
     cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_sort, b->d_tlen, keys_sorted, idx, order, n, 0, 32, st);
-    cudaMallocAsync(&tmp, tmp_sort, st);
+    if (cudaMallocAsync(&tmp, tmp_sort, st) != cudaSuccess) return give_up();
     cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_sort, b->d_tlen, keys_sorted, idx, order, n, 0, 32, st);
     std::vector<int> hlen(n);
     cudaMemcpyAsync(hlen.data(), keys_sorted, sizeof(int) * n, cudaMemcpyDeviceToHost, st);
     cudaMemsetAsync(counter, 0, sizeof(int) * 4, st);   /* warp tasks, team tasks, error */
     /* concatenated int8 profiles */
     std::vector<pb::Sw16Query> hq(nq);
-    int8_t *prof_all = nullptr;
-    cudaMallocAsync((void **)&prof_all, prof_bytes, st);
+    if (cudaMallocAsync((void **)&prof_all, prof_bytes, st) != cudaSuccess) return give_up();
     {
         size_t off = 0;
         for (int q = 0; q < nq; ++q) {
@@ -698,10 +710,9 @@ static int sw16_prepare(const pb_batch *b, pb_pair_out *d_out_all, size_t prof_b
     });
     std::vector<pb::Sw16Task> sorted_tasks(tasks.size());
     for (size_t k = 0; k < perm.size(); ++k) sorted_tasks[k] = tasks[perm[k]];
-    pb::Sw16Task *d_tasks = nullptr;
-    pb::Sw16Query *d_q = nullptr;
-    cudaMallocAsync((void **)&d_tasks, sizeof(pb::Sw16Task) * sorted_tasks.size(), st);
-    cudaMallocAsync((void **)&d_q, sizeof(pb::Sw16Query) * nq, st);
+    if (cudaMallocAsync((void **)&d_tasks, sizeof(pb::Sw16Task) * sorted_tasks.size(), st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_q, sizeof(pb::Sw16Query) * nq, st) != cudaSuccess)
+        return give_up();
     cudaMemcpyAsync(d_tasks, sorted_tasks.data(), sizeof(pb::Sw16Task) * sorted_tasks.size(), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(d_q, hq.data(), sizeof(pb::Sw16Query) * nq, cudaMemcpyHostToDevice, st);
 
@@ -873,9 +884,12 @@ extern "C" int pb_cuda_align_sw16_multi(const pb_batch *b, pb_pair_out *d_out_al
     /* pairs that left the 16-bit range: the exact kernel, per query */
     int *list = nullptr, *otlen = nullptr;
     int64_t *otoff = nullptr;
-    cudaMallocAsync((void **)&list, sizeof(int) * n, st);
-    cudaMallocAsync((void **)&otlen, sizeof(int) * n, st);
-    cudaMallocAsync((void **)&otoff, sizeof(int64_t) * n, st);
+    if (cudaMallocAsync((void **)&list, sizeof(int) * n, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&otlen, sizeof(int) * n, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&otoff, sizeof(int64_t) * n, st) != cudaSuccess) {
+        cudaGetLastError();
+        rc = -1;   /* nothing below runs; the buffers that exist are freed */
+    }
     for (int q = 0; q < nq && rc == 0; ++q) {
         int nover = 0;
         pb_pair_out *oq = d_out_all + (size_t)q * n;
@@ -887,7 +901,11 @@ extern "C" int pb_cuda_align_sw16_multi(const pb_batch *b, pb_pair_out *d_out_al
         cudaStreamSynchronize(st);
         if (nover > 0) {
             pb_pair_out *tmpo = nullptr;
-            cudaMallocAsync((void **)&tmpo, sizeof(pb_pair_out) * nover, st);
+            if (cudaMallocAsync((void **)&tmpo, sizeof(pb_pair_out) * nover, st) != cudaSuccess) {
+                cudaGetLastError();
+                rc = -1;
+                break;
+            }
             cudaStreamSynchronize(st);
             pb_batch sub = *b;
             sub.profs = &b->profs[q];
@@ -903,7 +921,9 @@ extern "C" int pb_cuda_align_sw16_multi(const pb_batch *b, pb_pair_out *d_out_al
             cudaFreeAsync(tmpo, st);
         }
     }
-    cudaFreeAsync(list, st); cudaFreeAsync(otlen, st); cudaFreeAsync(otoff, st);
+    if (list) cudaFreeAsync(list, st);
+    if (otlen) cudaFreeAsync(otlen, st);
+    if (otoff) cudaFreeAsync(otoff, st);
     sw16_release(&prep, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
     cudaStreamDestroy(st);
